@@ -1,0 +1,201 @@
+/*
+ * mpcd_c.h — C-ABI of the B200 SRC/MPCD time step (libmpcd_b200.so).
+ *
+ * Plain C: POD structs, pointers and sizes, integer status codes. No exceptions, STL or
+ * torch types cross this boundary. Every entry point returns MPCD_OK (0) on success or a
+ * status code; mpcd_last_error() returns the message of the calling thread's last failure.
+ *
+ * Conventions (identical to the reference's C++ API and file formats):
+ *   - particle arrays are interleaved [x1, y1, x2, y2, ...] doubles of length 2n, in
+ *     particle-id order (reference include/types.h:74-79);
+ *   - cell index c = iy + Ny*ix (reference src/common_grid.cpp:18);
+ *   - all RNG seeds are the reference's std::mt19937_64 seeds.
+ *
+ * Each function below names the reference interface it replaces (file:line, relative to
+ * the reference project root).
+ */
+#ifndef MPCD_C_H
+#define MPCD_C_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+enum mpcd_status {
+    MPCD_OK = 0,
+    MPCD_ERR_INVALID_ARG = 1,   /* bad size, mode or flag (reference: std::runtime_error) */
+    MPCD_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    MPCD_ERR_UNSUPPORTED_BC = 3,/* a particle crossed a wall whose mode is not supported */
+    MPCD_ERR_DEVICE = 4,        /* a kernel raised its device-side error flag */
+    MPCD_ERR_NO_DEVICE = 5,     /* no CUDA device / extension not usable */
+    MPCD_ERR_CAPACITY = 6,      /* a bounded device buffer would overflow */
+    MPCD_ERR_STATE = 7          /* call order: e.g. closure without a saved reference */
+};
+
+/* ---------------------------------------------------------------- enumerations */
+/* boundary modes (reference include/types.h:30-33 hold them as strings) */
+enum mpcd_bc_mode {
+    MPCD_BC_UNKNOWN = -1,       /* any other string: error only if a particle crosses */
+    MPCD_BC_PERIODIC = 0,
+    MPCD_BC_THERMALIZE = 1,
+    MPCD_BC_BOUNCEBACK = 2,
+    MPCD_BC_SPECULAR = 3
+};
+/* highMode / lowMode (reference src/zone_pass.cpp:351,357): "1+coef" or anything else */
+enum mpcd_thr_mode { MPCD_THR_COEF = 0, MPCD_THR_ONE_PLUS_COEF = 1 };
+/* zone layout modes (reference src/zone_pass.cpp:178,193) */
+enum mpcd_layout_mode { MPCD_LAYOUT_BASE = 0, MPCD_LAYOUT_SHIFTED = 1, MPCD_LAYOUT_SINGLE_FULL = 2 };
+/* numeric forms of the step */
+enum mpcd_form { MPCD_FORM_PLAIN_F64 = 0 };
+
+/* ---------------------------------------------------------------- parameters */
+/* POD mirror of mpcd::Params (reference include/types.h:10-72); booleans are int32 0/1,
+ * strings are the enums above. Field order follows the reference struct. */
+typedef struct mpcd_params_c {
+    int32_t Nx, Ny, Nc, n;
+    double Lx, Ly, dt, a0;
+    double alpha, kBT, g, bodyForceX;
+    int32_t useThermostat, keepMeanFlow;
+    int32_t boundary_left, boundary_right, boundary_bottom, boundary_top;
+    double Utop, Ubottom, wallSigma;
+    int32_t noSurfaceCase, redistributionEnableSurfaceTopology, redistributionWallWettingEnabled;
+    int32_t useInterfaceVelocityReorientation, useIncompressibleRedistribution;
+    int32_t redistribAfterCollision, useZoneRedistribution;
+    int32_t zoneTileNx, zoneTileNy;
+    int32_t zoneUseShiftedSecondPass, zonePassthroughMode, zoneSingleFullDomainMode;
+    int32_t enableMomentumCorrectionPostRedistribution;
+    double gamma, coef;
+    int32_t highMode, lowMode;
+    int32_t maxRedistribPasses, useLocalFluidFractionThresholds;
+    double fluidFracGain, lowThrFloor, highThrFloor, lowThrBulkOverride;
+    int32_t useLiquidClosure, useOptimalBetaRepair;
+    double betaRepair, betaEOS, Kvirial;
+    int32_t smoothPdriveAtInterzone, smoothPdriveInterzoneWidthCells;
+    double smoothPdriveInterzoneBlend;
+    int32_t smoothPdriveIncludeShiftedLayouts, reserved0;
+} mpcd_params_c;
+
+/* ---------------------------------------------------------------- results */
+/* mpcd::WallInfo (reference include/types.h:97-111) */
+typedef struct mpcd_wallinfo_c {
+    int32_t nBot, nTop, nLeft, nRight;
+    double dEwall, dPxBot, dPxTop, dPyBot, dPyTop, dPxLeft, dPxRight, dPyLeft, dPyRight;
+} mpcd_wallinfo_c;
+
+/* mpcd::OpenMPPassMetrics (reference include/zone_pass_openmp.h:12-27). Times are device
+ * seconds; nThreadsUsed reports the number of zone blocks launched. */
+typedef struct mpcd_pass_metrics_c {
+    int32_t nZones, nThreadsRequested, nThreadsUsed, nParticlesMovedDense, nParticlesMovedSparse;
+    int32_t reserved0;
+    double corrRmsDU, corrMaxDU;
+    double timeLayout, timeZoneExtract, timeSnapshot, timeAlloc, timeKernel, timePack, timeMerge;
+} mpcd_pass_metrics_c;
+
+/* mpcd::LiquidClosureMetrics (reference include/liquid_closure.h:11-27) */
+typedef struct mpcd_closure_metrics_c {
+    double betaRepairOpt, betaRepairApplied, betaRepairNum, betaRepairDen, betaEOSApplied;
+    double meanPdriveRaw, meanPdrive, rmsRepairDU, meanAbsRepairDU, maxRepairDU;
+    double rmsEOSDU, maxEOSDU, momentumDeltaX, momentumDeltaY;
+    int32_t nMaskedInterzoneCells, reserved0;
+} mpcd_closure_metrics_c;
+
+/* mpcd::CellFields (reference include/types.h:81-95) as caller-owned host arrays of Nc
+ * entries each; any pointer may be NULL to skip that field. */
+typedef struct mpcd_cellfields_c {
+    int32_t* N;
+    double *Ux, *Uy, *Px, *Py, *T, *rho, *Pkin, *Pvir, *P, *rhoTarget;
+} mpcd_cellfields_c;
+
+/* Everything run_liquid_closure returns besides stateOut (reference
+ * include/liquid_closure.h:29-44); caller-owned host arrays, each pointer nullable.
+ * State arrays hold 2n doubles, grids Nc entries. */
+typedef struct mpcd_closure_detail_c {
+    double *repairedX, *repairedV;
+    mpcd_cellfields_c refFields, redFields, repairedFields, outFields;
+    double *pdriveRaw, *pdrive, *duRepairX, *duRepairY, *duEOSX, *duEOSY;
+    int32_t* interzoneMask;
+} mpcd_closure_detail_c;
+
+/* One row of the profiled benchmark's per-step metrics (reference
+ * src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:215,301-336). */
+typedef struct mpcd_step_metrics_c {
+    int64_t step;
+    mpcd_wallinfo_c wall;
+    mpcd_pass_metrics_c base, shifted;
+    mpcd_closure_metrics_c closure;
+    double occStd, outBand, meanKinetic, meanUx, meanUy, Qx;
+    double baseOccStd, baseOutBand, shiftedOccStd, shiftedOutBand;
+    double meanVelocityX, meanVelocityY;
+    double timeStepTotal, timeRefBuild, timeBase, timeShifted, timeClosure, timeDiagnostics;
+} mpcd_step_metrics_c;
+
+typedef struct mpcd_ctx mpcd_ctx;
+
+/* ---------------------------------------------------------------- library */
+const char* mpcd_last_error(void);
+/* 1 if a usable sm_100 device is present, else 0 (sets no error) */
+int mpcd_device_available(void);
+/* Parses a params.kv file (reference src/params_io.cpp:74-137; strict: every key required,
+ * unknown keys ignored). Benchmark keys are read separately (mpcd_read_kv_int / _string). */
+int mpcd_read_params_kv(const char* path, mpcd_params_c* out);
+
+/* ---------------------------------------------------------------- context */
+/* Allocates device buffers for params->n particles and params->Nc cells on `device`.
+ * Validates params (reference src/zone_pass.cpp:1100-1105, src/liquid_closure.cpp:332). */
+int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out);
+int mpcd_ctx_destroy(mpcd_ctx* ctx);
+/* The stream every kernel of this context runs on (a cudaStream_t). */
+void* mpcd_ctx_stream(mpcd_ctx* ctx);
+
+/* Host <-> device state, particle-id order. x and v: 2n doubles each (mpcd::State.x/.v). */
+int mpcd_set_state(mpcd_ctx* ctx, const double* x, const double* v, int64_t n);
+int mpcd_get_state(mpcd_ctx* ctx, double* x, double* v);
+/* Device-pointer variants (the same layout, already on the context's device). */
+int mpcd_set_state_device(mpcd_ctx* ctx, const double* d_x, const double* d_v, int64_t n);
+int mpcd_get_state_device(mpcd_ctx* ctx, double* d_x, double* d_v);
+
+/* ---------------------------------------------------------------- phases */
+/* v += (bodyForceX, g) dt; x += dt v
+ * (reference src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:242-247) */
+int mpcd_stream(mpcd_ctx* ctx);
+/* mpcd::apply_bc_general (reference src/boundary_conditions.cpp:19-203); info nullable */
+int mpcd_apply_bc(mpcd_ctx* ctx, uint64_t seed, mpcd_wallinfo_c* info);
+/* mpcd::srd_cell_id_with_random_shift (reference src/srd_collision.cpp:9-45). Keeps the
+ * cell ids on the device for mpcd_srd_collide; copies them to cid_out (n int32) if given. */
+int mpcd_srd_shift_cells(mpcd_ctx* ctx, uint64_t seed, int32_t* cid_out);
+/* mpcd::srd_collision_step (reference src/srd_collision.cpp:47-140) on the cell ids of the
+ * last mpcd_srd_shift_cells call. */
+int mpcd_srd_collide(mpcd_ctx* ctx, uint64_t seed);
+/* the same with caller-given cell ids (n int32 in [0, Nc), host memory) */
+int mpcd_srd_collide_cells(mpcd_ctx* ctx, const int32_t* cid, uint64_t seed);
+/* mpcd::compute_cell_fields (reference src/common_grid.cpp:32-100) of the current state */
+int mpcd_cell_fields(mpcd_ctx* ctx, double rho_target, mpcd_cellfields_c* out);
+/* Snapshot the current state as the closure's reference state ("stateRef"). */
+int mpcd_save_ref(mpcd_ctx* ctx);
+/* mpcd::run_zone_pass_openmp (reference src/zone_pass_openmp.cpp:176-182, snapshot
+ * semantics of :34-172). mode: mpcd_layout_mode. metrics nullable. */
+int mpcd_zone_pass(mpcd_ctx* ctx, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics);
+/* mpcd::run_liquid_closure (reference src/liquid_closure.cpp:329-444) with stateRef = the
+ * saved reference and stateRed = the current state; the current state becomes stateOut.
+ * metrics and detail nullable. */
+int mpcd_liquid_closure(mpcd_ctx* ctx, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail);
+/* Zone ownership map of a layout (reference src/zone_pass.cpp:1049-1063), Nc int32. */
+int mpcd_zone_owner_map(mpcd_ctx* ctx, int32_t mode, int32_t* owner_out);
+
+/* ---------------------------------------------------------------- the step */
+/* Runs steps step0+1 .. step0+nsteps of the profiled benchmark loop on the device
+ * (reference src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:237-279),
+ * with its per-step seed schedule. If `last` is given, fills the metrics row of the last
+ * step (costs extra device reductions and one synchronisation). */
+int mpcd_step(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* last);
+/* Device-side metrics row of the current state after a step (see mpcd_step). */
+int mpcd_step_metrics(mpcd_ctx* ctx, mpcd_step_metrics_c* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPCD_C_H */
