@@ -141,6 +141,12 @@ int mpcd_device_available(void);
 /* Parses a params.kv file (reference src/params_io.cpp:74-137; strict: every key required,
  * unknown keys ignored). Benchmark keys are read separately (mpcd_read_kv_int / _string). */
 int mpcd_read_params_kv(const char* path, mpcd_params_c* out);
+/* Any key of a params.kv file as a string (the reference driver reads benchmark_nSteps,
+ * benchmark_metricsEvery and benchmark_dumpSteps this way:
+ * src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:205-208). */
+int mpcd_read_kv_string(const char* path, const char* key, char* buf, int buflen);
+/* message of the last failed mpcd_read_params_kv / mpcd_read_kv_string on this thread */
+const char* mpcd_io_last_error(void);
 
 /* ---------------------------------------------------------------- context */
 /* Allocates device buffers for params->n particles and params->Nc cells on `device`.

@@ -1,0 +1,56 @@
+"""Builds libmpcd_b200.so in-tree with nvcc for sm_100a.
+
+FP64 kernels are compiled with -fmad=false (no FMA contraction, like the reference's x86-64
+build) and host code with -ffp-contract=off.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libmpcd_b200.so")
+
+SOURCES = ["capi.cu", "io.cpp"]
+DEPS = ["common.cuh", "ddmath.cuh", "logtab.inc", "sort.cuh", "bc.cuh", "cells.cuh", "zone.cuh", "closure.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path():
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(p):
+        raise RuntimeError("nvcc not found")
+    return p
+
+
+def needs_build():
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    files = [os.path.join(CSRC, f) for f in SOURCES + DEPS] + [os.path.join(ROOT, "include", "mpcd_c.h")]
+    return any(os.path.getmtime(f) > t for f in files if os.path.exists(f))
+
+
+def build(force=False, verbose=False):
+    if not force and not needs_build():
+        return OUT
+    cmd = [nvcc_path()] + ARCH + [
+        "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
+        "-Xcompiler", "-fPIC,-ffp-contract=off",
+        "-ccbin", shutil.which("g++") or "g++",
+        "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+        "-o", OUT + ".tmp",
+    ] + [os.path.join(CSRC, f) for f in SOURCES]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    os.replace(OUT + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,1194 @@
+// libmpcd_b200.so: the C-ABI of include/mpcd_c.h over the sm_100a kernels.
+//
+// The state lives on the device in "slots": x and v as double2, plus the particle id of each
+// slot. Slots are re-sorted by (cell, particle id) at the end of every step (inside the
+// closure kick), so per-cell work reads contiguous memory; every API that exchanges particle
+// arrays with the host uses particle-id order, as the reference does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mpcd_c.h"
+
+#include "bc.cuh"
+#include "cells.cuh"
+#include "closure.cuh"
+#include "common.cuh"
+#include "sort.cuh"
+#include "zone.cuh"
+
+using namespace mpcd_dev;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (expr);                                                                    \
+        if (e_ != cudaSuccess) return set_err(MPCD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kThreads = 256;
+inline int blocks_for(int64_t n, int t = kThreads) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
+
+struct CellIndex {
+    int* count = nullptr;      // Nc
+    uint64_t* packed = nullptr;// Nc   (count | (count >= 2) << 32)
+    uint64_t* start = nullptr; // Nc + 1 (exclusive scan of packed)
+    int* pos = nullptr;        // n
+    int* slots = nullptr;      // n
+};
+
+struct Layout {
+    int nZones = 0;
+    int maxArea = 0, maxTX = 0, maxTY = 0;
+    int4* rects = nullptr;
+    int* owner = nullptr;
+    std::vector<int4> hrects;
+    std::vector<int> howner;
+};
+
+}  // namespace
+
+struct mpcd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    mpcd_params_c pc{};
+    DevParams P{};
+    int n = 0, Nc = 0;
+    // state
+    double2* xb[2] = {nullptr, nullptr};
+    double2* vb[2] = {nullptr, nullptr};
+    int* pidb[2] = {nullptr, nullptr};
+    int xv = 0, pp = 0;
+    int* cidStd = nullptr;
+    int* cidSrd = nullptr;
+    bool cidStdValid = false;
+    bool srdCellsValid = false;
+    CellIndex idxStd, idxSrd;
+    bool idxStdValid = false;
+    uint64_t* blockSums = nullptr;
+    int blockSumsCap = 0;
+    // walls
+    BcWork W{};
+    int nwords = 0;
+    int bcBlocks = 0;
+    double* wallOut = nullptr;  // 9 doubles
+    // collision
+    uint8_t* signs = nullptr;
+    // zones
+    Layout lay[3];  // base, shifted, single_full
+    uint64_t* seeds = nullptr;
+    int2* zoneMoved = nullptr;
+    double2* zoneCorr = nullptr;
+    int* overflow = nullptr;
+    int* nOverflow = nullptr;
+    char* ovMem = nullptr;
+    size_t ovPerBlock = 0;
+    int ovBlocks = 2;
+    int zMaxCells = 0, zWinCap = 0, zNlocCap = 0, zArenaCap = 0;
+    size_t zSmem = 0;
+    int ovMaxCells = 0, ovWinCap = 0, ovNlocCap = 0, ovArenaCap = 0;
+    double* passOut = nullptr;  // 4 doubles
+    // closure
+    int* mask = nullptr;
+    int nMasked = 0;
+    double *refN = nullptr, *refPx = nullptr, *refPy = nullptr, *refUx = nullptr, *refUy = nullptr, *refT = nullptr,
+           *refRho = nullptr, *refPkin = nullptr, *refPvir = nullptr, *refP = nullptr;
+    int* refNi = nullptr;
+    bool refValid = false;
+    double *pdRaw = nullptr, *pdrive = nullptr, *eosX = nullptr, *eosY = nullptr, *duRX = nullptr, *duRY = nullptr;
+    double* cols = nullptr;     // Nc * kKickCols
+    double* partial = nullptr;  // reduction partials
+    int partialCap = 0;
+    double* red = nullptr;      // small results: [0..1] num,den  [2..] others
+    double* fieldTmp = nullptr; // 11 * Nc scratch for field outputs
+    int* fieldTmpN = nullptr;
+    double2* vrep = nullptr;
+    // status
+    DevStatus* st = nullptr;
+    DevStatus* hst = nullptr;
+    double* hred = nullptr;
+    // metrics
+    mpcd_step_metrics_c last{};
+    cudaEvent_t ev[8];
+};
+
+namespace {
+
+const char* dev_error_text(int code) {
+    switch (code) {
+        case kErrUnsupportedBcLeft: return "Unsupported boundary_left mode";
+        case kErrUnsupportedBcRight: return "Unsupported boundary_right mode";
+        case kErrUnsupportedBcBottom: return "Unsupported boundary_bottom mode";
+        case kErrUnsupportedBcTop: return "Unsupported boundary_top mode";
+        case kErrZoneCapacity: return "zone working set exceeded its capacity";
+        case kErrTableRange: return "minimal step outside the +-2 cell tables";
+        case kErrBcLateSweep: return "a particle crossed a wall again after the first boundary sweep (displacement larger than the box): not supported on the device path";
+        case kErrEventCapacity: return "more thermal wall hits than the event buffer holds";
+        case kErrCellId: return "cell id outside [0, Nc)";
+        case kErrTargetIsSource: return "a dense cell targeted itself (periodic axis shorter than 3 cells)";
+        case kErrRngCapacity: return "collision sign stream shorter than the number of cells with >= 2 particles";
+        default: return "device error";
+    }
+}
+
+// synchronise and turn a raised device flag into a status code
+int check_device(mpcd_ctx* c) {
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpy(c->hst, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost));
+    if (c->hst->code != 0) {
+        const int code = c->hst->code;
+        const int detail = c->hst->detail;
+        cudaMemset(c->st, 0, sizeof(DevStatus));
+        const int rc = (code >= kErrUnsupportedBcLeft && code <= kErrUnsupportedBcTop) ? MPCD_ERR_UNSUPPORTED_BC
+                       : (code == kErrZoneCapacity || code == kErrEventCapacity || code == kErrRngCapacity) ? MPCD_ERR_CAPACITY
+                       : (code == kErrCellId) ? MPCD_ERR_INVALID_ARG
+                                              : MPCD_ERR_DEVICE;
+        return set_err(rc, std::string(dev_error_text(code)) + " (detail " + std::to_string(detail) + ")");
+    }
+    return MPCD_OK;
+}
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+    return MPCD_OK;
+}
+
+// ---------------------------------------------------------------- layouts (host, static)
+std::vector<int> start_indices(int N, int tile, int off) {
+    std::vector<int> s{0};
+    for (int v = off; v < N; v += tile)
+        if (v > 0 && v < N) s.push_back(v);
+    return s;
+}
+
+// reference src/zone_pass.cpp:173-221
+void build_layout(const mpcd_params_c& p, int mode, Layout& L) {
+    L.hrects.clear();
+    L.howner.assign((size_t)p.Nc, 0);
+    if (mode == MPCD_LAYOUT_SINGLE_FULL) {
+        L.hrects.push_back(make_int4(0, p.Nx, 0, p.Ny));
+        std::fill(L.howner.begin(), L.howner.end(), 1);
+    } else {
+        const int offx = (mode == MPCD_LAYOUT_SHIFTED) ? p.zoneTileNx / 2 : 0;
+        const int offy = (mode == MPCD_LAYOUT_SHIFTED) ? p.zoneTileNy / 2 : 0;
+        const auto xs = start_indices(p.Nx, p.zoneTileNx, offx);
+        const auto ys = start_indices(p.Ny, p.zoneTileNy, offy);
+        int id = 0;
+        for (int y : ys)
+            for (int x : xs) {
+                const int xe = std::min(x + p.zoneTileNx, p.Nx), ye = std::min(y + p.zoneTileNy, p.Ny);
+                L.hrects.push_back(make_int4(x, xe, y, ye));
+                ++id;
+                for (int ix = x; ix < xe; ++ix)
+                    for (int iy = y; iy < ye; ++iy) L.howner[(size_t)iy + (size_t)p.Ny * ix] = id;
+            }
+    }
+    L.nZones = (int)L.hrects.size();
+    L.maxArea = L.maxTX = L.maxTY = 0;
+    for (const auto& r : L.hrects) {
+        L.maxTX = std::max(L.maxTX, r.y - r.x);
+        L.maxTY = std::max(L.maxTY, r.w - r.z);
+        L.maxArea = std::max(L.maxArea, (r.y - r.x) * (r.w - r.z));
+    }
+}
+
+bool periodic_x(const mpcd_params_c& p) { return p.boundary_left == MPCD_BC_PERIODIC && p.boundary_right == MPCD_BC_PERIODIC; }
+bool periodic_y(const mpcd_params_c& p) { return p.boundary_bottom == MPCD_BC_PERIODIC && p.boundary_top == MPCD_BC_PERIODIC; }
+
+// build_interzone_mask (reference src/liquid_closure.cpp:143-213), static per run
+std::vector<int> interzone_mask(const mpcd_params_c& p, const Layout& base, const Layout& shifted) {
+    std::vector<int> mask((size_t)p.Nc, 0);
+    if (!p.smoothPdriveAtInterzone || !p.useZoneRedistribution || p.zonePassthroughMode || p.zoneSingleFullDomainMode) return mask;
+    const bool px = periodic_x(p), py = periodic_y(p);
+    auto boundary = [&](const std::vector<int>& own) {
+        std::vector<int> b((size_t)p.Nc, 0);
+        for (int ix = 0; ix < p.Nx; ++ix)
+            for (int iy = 0; iy < p.Ny; ++iy) {
+                const int c = iy + p.Ny * ix;
+                const int right = (ix + 1 < p.Nx) ? iy + p.Ny * (ix + 1) : (px ? iy : -1);
+                const int up = (iy + 1 < p.Ny) ? (iy + 1) + p.Ny * ix : (py ? p.Ny * ix : -1);
+                b[(size_t)c] = (right >= 0 && own[(size_t)right] != own[(size_t)c]) || (up >= 0 && own[(size_t)up] != own[(size_t)c]);
+            }
+        return b;
+    };
+    auto dilate = [&](const std::vector<int>& in) {
+        const int w = p.smoothPdriveInterzoneWidthCells;
+        if (w <= 0) return in;
+        std::vector<int> out((size_t)p.Nc, 0);
+        for (int ix = 0; ix < p.Nx; ++ix)
+            for (int iy = 0; iy < p.Ny; ++iy) {
+                bool on = false;
+                for (int dx = -w; dx <= w && !on; ++dx)
+                    for (int dy = -w; dy <= w; ++dy) {
+                        int jx = ix + dx, jy = iy + dy;
+                        if (px) jx = ((jx % p.Nx) + p.Nx) % p.Nx;
+                        else if (jx < 0 || jx >= p.Nx) continue;
+                        if (py) jy = ((jy % p.Ny) + p.Ny) % p.Ny;
+                        else if (jy < 0 || jy >= p.Ny) continue;
+                        if (in[(size_t)jy + (size_t)p.Ny * jx]) { on = true; break; }
+                    }
+                out[(size_t)iy + (size_t)p.Ny * ix] = on;
+            }
+        return out;
+    };
+    mask = dilate(boundary(base.howner));
+    if (p.smoothPdriveIncludeShiftedLayouts) {
+        const auto s = dilate(boundary(shifted.howner));
+        for (size_t c = 0; c < mask.size(); ++c) mask[c] = (mask[c] || s[c]) ? 1 : 0;
+    }
+    return mask;
+}
+
+int validate(const mpcd_params_c& p) {
+    if (p.Nx < 1 || p.Ny < 1 || p.n < 0) return set_err(MPCD_ERR_INVALID_ARG, "Nx, Ny must be >= 1 and n >= 0");
+    if ((int64_t)p.Nx * p.Ny != p.Nc) return set_err(MPCD_ERR_INVALID_ARG, "Nc must equal Nx*Ny");
+    if ((int64_t)p.Nc >= (1LL << 31) || (int64_t)p.n * 2 >= (1LL << 31)) return set_err(MPCD_ERR_INVALID_ARG, "problem too large for 32-bit indices");
+    if (!(p.Lx > 0.0) || !(p.Ly > 0.0) || !(p.a0 > 0.0)) return set_err(MPCD_ERR_INVALID_ARG, "Lx, Ly, a0 must be > 0");
+    if (p.zoneTileNx < 1 || p.zoneTileNy < 1) return set_err(MPCD_ERR_INVALID_ARG, "zone tiles must be >= 1");
+    if (p.maxRedistribPasses < 0) return set_err(MPCD_ERR_INVALID_ARG, "maxRedistribPasses must be >= 0");
+    return MPCD_OK;
+}
+
+// Host-side derived constants; libm values where the reference calls libm.
+DevParams make_dev_params(const mpcd_params_c& p) {
+    DevParams d{};
+    d.Nx = p.Nx; d.Ny = p.Ny; d.Nc = p.Nc; d.n = p.n;
+    d.Lx = p.Lx; d.Ly = p.Ly; d.dt = p.dt; d.a0 = p.a0;
+    d.dx = p.Lx / (double)p.Nx;
+    d.dy = p.Ly / (double)p.Ny;
+    d.Vc = d.dx * d.dy;
+    d.alpha = p.alpha; d.kBT = p.kBT; d.g = p.g; d.bodyForceX = p.bodyForceX;
+    d.useThermostat = p.useThermostat; d.keepMeanFlow = p.keepMeanFlow;
+    d.bc[0] = p.boundary_left; d.bc[1] = p.boundary_right; d.bc[2] = p.boundary_bottom; d.bc[3] = p.boundary_top;
+    d.perx = periodic_x(p); d.pery = periodic_y(p);
+    d.Utop = p.Utop; d.Ubottom = p.Ubottom; d.wallSigma = p.wallSigma;
+    d.tileNx = p.zoneTileNx; d.tileNy = p.zoneTileNy;
+    d.momCorr = p.enableMomentumCorrectionPostRedistribution;
+    d.maxPasses = p.maxRedistribPasses;
+    d.useLFF = p.useLocalFluidFractionThresholds;
+    d.gamma = p.gamma; d.coef = p.coef;
+    // occupancy_thresholds (reference src/zone_pass.cpp:347-366)
+    d.highThr = (p.highMode == MPCD_THR_ONE_PLUS_COEF) ? p.gamma * (1.0 + p.coef) : p.gamma + p.gamma * p.coef;
+    d.lowThrBulk = (p.lowMode == MPCD_THR_ONE_PLUS_COEF) ? p.gamma / (1.0 + p.coef) : p.gamma - p.gamma * p.coef;
+    if (std::isfinite(p.lowThrBulkOverride)) d.lowThrBulk = p.lowThrBulkOverride;
+    d.lowFrac = 1.0 / (1.0 + p.coef);
+    d.highFrac = 1.0 + p.coef;
+    d.fluidFracGain = p.fluidFracGain; d.lowThrFloor = p.lowThrFloor; d.highThrFloor = p.highThrFloor;
+    d.lowThrBulkInt = (int)std::ceil(d.lowThrBulk);
+    d.useLiquidClosure = p.useLiquidClosure; d.useOptimalBetaRepair = p.useOptimalBetaRepair;
+    d.smoothWidth = p.smoothPdriveInterzoneWidthCells;
+    d.betaRepair = p.betaRepair; d.betaEOS = p.betaEOS; d.Kvirial = p.Kvirial;
+    d.smoothBlend = p.smoothPdriveInterzoneBlend;
+    d.rhoTarget = p.gamma / ((p.Lx / (double)p.Nx) * (p.Ly / (double)p.Ny));
+    // rotation constants (reference src/srd_collision.cpp:93-94 evaluates cos/sin of theta)
+    const double th[3] = {0.0, p.alpha * 1.0, p.alpha * -1.0};
+    for (int k = 0; k < 3; ++k) {
+        d.rotCos[k] = std::cos(th[k]);
+        d.rotSin[k] = std::sin(th[k]);
+    }
+    // angular bins and step lengths of small integer steps (reference src/zone_pass.cpp:451-459)
+    for (int b = -2; b <= 2; ++b)
+        for (int a = -2; a <= 2; ++a) {
+            const double ang = std::atan2((double)b, (double)a);
+            int ib = (int)std::floor((ang + M_PI) / (2.0 * M_PI / 8.0));
+            ib = ((ib % 8) + 8) % 8;
+            d.atanBin[(a + 2) + 5 * (b + 2)] = ib;
+            d.hypotTab[(a + 2) + 5 * (b + 2)] = std::hypot((double)a, (double)b);
+        }
+    return d;
+}
+
+// ---------------------------------------------------------------- index sort
+int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out) {
+    const int nb = (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile);
+    if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
+    k_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums);
+    k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb);
+    k_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums, out);
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+int build_index(mpcd_ctx* c, const int* cid, CellIndex& I) {
+    CUDA_TRY(cudaMemsetAsync(I.count, 0, sizeof(int) * (size_t)c->Nc, c->stream));
+    if (c->n > 0) k_histogram<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
+    k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed);
+    int rc = scan_u64(c, I.packed, c->Nc, I.start);
+    if (rc) return rc;
+    if (c->n > 0) {
+        k_scatter<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, I.pos, c->n, I.start, I.slots);
+        k_cell_sort<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(I.start, c->Nc, c->pidb[c->pp], I.slots);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+__global__ void k_std_cells(DevParams P, const double2* __restrict__ x, int* __restrict__ cid) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < P.n) cid[s] = cell_of(x[s].x, x[s].y, P);
+}
+
+int ensure_std_index(mpcd_ctx* c) {
+    if (c->idxStdValid) return MPCD_OK;
+    if (!c->cidStdValid) {
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd);
+        c->cidStdValid = true;
+    }
+    const int rc = build_index(c, c->cidStd, c->idxStd);
+    if (!rc) c->idxStdValid = true;
+    return rc;
+}
+
+void invalidate_positions(mpcd_ctx* c) {
+    c->cidStdValid = false;
+    c->idxStdValid = false;
+    c->srdCellsValid = false;
+}
+
+// ---------------------------------------------------------------- host <-> device in id order
+__global__ void k_gather_by_pid(const double2* __restrict__ x, const double2* __restrict__ v, const int* __restrict__ pid,
+                                int n, double2* __restrict__ xo, double2* __restrict__ vo) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int p = pid[s];
+    if (xo) xo[p] = x[s];
+    if (vo) vo[p] = v[s];
+}
+
+__global__ void k_int_by_pid(const int* __restrict__ a, const int* __restrict__ pid, int n, int* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[pid[s]] = a[s];
+}
+
+__global__ void k_int_to_slots(const int* __restrict__ byPid, const int* __restrict__ pid, int n, int Nc,
+                               int* __restrict__ out, DevStatus* st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int c = byPid[pid[s]];
+    if (c < 0 || c >= Nc) raise_error(st, kErrCellId, pid[s]);
+    out[s] = (c < 0) ? 0 : ((c >= Nc) ? Nc - 1 : c);
+}
+
+__global__ void k_stream_only(DevParams P, double2* __restrict__ x, double2* __restrict__ v) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    double2 xs = x[s], vs = v[s];
+    vs.x = __dadd_rn(vs.x, __dmul_rn(P.bodyForceX, P.dt));
+    vs.y = __dadd_rn(vs.y, __dmul_rn(P.g, P.dt));
+    xs.x = __dadd_rn(xs.x, __dmul_rn(P.dt, vs.x));
+    xs.y = __dadd_rn(xs.y, __dmul_rn(P.dt, vs.y));
+    x[s] = xs;
+    v[s] = vs;
+}
+
+__global__ void k_srd_cells(DevParams P, const double2* __restrict__ x, const double* __restrict__ shift, int* __restrict__ cid) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < P.n) cid[s] = srd_cell(x[s].x, x[s].y, shift[0], shift[1], P);
+}
+
+__global__ void k_sub_mean(double2* __restrict__ v, int n, const double* __restrict__ sums) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double mx = __ddiv_rn(sums[1], (double)n), my = __ddiv_rn(sums[2], (double)n);
+    v[s] = make_double2(__dsub_rn(v[s].x, mx), __dsub_rn(v[s].y, my));
+}
+
+int reduce_cols(mpcd_ctx* c, const double* cols, int64_t rows, int K, unsigned maxMask, double* out) {
+    const int rowsPerBlock = 8192;
+    const int nb = (int)std::max<int64_t>(1, (rows + rowsPerBlock - 1) / rowsPerBlock);
+    if ((int64_t)nb * K > c->partialCap) return set_err(MPCD_ERR_CAPACITY, "reduction buffer too small");
+    k_reduce_partial<<<nb, kRedThreads, 0, c->stream>>>(cols, rows, K, maxMask, rowsPerBlock, c->partial);
+    k_reduce_final<<<1, kRedThreads, 0, c->stream>>>(c->partial, nb, K, maxMask, out);
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+// ---------------------------------------------------------------- phases
+int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo) {
+    BcWork& W = c->W;
+    CUDA_TRY(cudaMemsetAsync(W.bitsX, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
+    CUDA_TRY(cudaMemsetAsync(W.bitsY, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
+    CUDA_TRY(cudaMemsetAsync(W.nEvents, 0, sizeof(int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(W.ints, 0, sizeof(int) * 4, c->stream));
+    k_stream_bc<<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp],
+                                                         cidStd, cidSrd, W, c->st);
+    k_word_counts<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount);
+    int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix);
+    if (rc) return rc;
+    k_wall_normals<<<1, kNormThreads, 0, c->stream>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st);
+    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, c->stream>>>(c->P, c->vb[c->xv], W, c->st);
+    if (wantInfo)
+        k_wall_reduce<<<1, 32, 0, c->stream>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut);
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+int run_collide(mpcd_ctx* c, uint64_t seed) {
+    int rc = build_index(c, c->cidSrd, c->idxSrd);
+    if (rc) return rc;
+    k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs);
+    k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, c->signs, c->Nc,
+                                                                 c->vb[c->xv], c->st);
+    if (c->P.keepMeanFlow) {
+        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols);
+        rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
+        if (rc) return rc;
+        k_sub_mean<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->red + 8);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+// reference fields of the current state + pdrive + EOS kick (depend on the reference only)
+int run_save_ref(mpcd_ctx* c) {
+    int rc = ensure_std_index(c);
+    if (rc) return rc;
+    FieldsOut o{};
+    o.N = c->refNi; o.Ux = c->refUx; o.Uy = c->refUy; o.Px = c->refPx; o.Py = c->refPy; o.T = c->refT;
+    o.rho = c->refRho; o.Pkin = c->refPkin; o.Pvir = c->refPvir; o.P = c->refP;
+    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
+                                                                 c->P.rhoTarget, o);
+    k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw);
+    k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive);
+    k_eos<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdrive, c->eosX, c->eosY);
+    CUDA_TRY(cudaGetLastError());
+    c->refValid = true;
+    return MPCD_OK;
+}
+
+int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase) {
+    if (!c->cidStdValid) {
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd);
+        c->cidStdValid = true;
+    }
+    int rc = ensure_std_index(c);
+    if (rc) return rc;
+    if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
+    if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
+    Layout& L = c->lay[mode];
+    k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
+        seedBase, L.nZones, c->seeds);
+    CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
+    ZoneArgs A{};
+    A.P = c->P;
+    A.rects = L.rects;
+    A.owner = L.owner;
+    A.start = c->idxStd.start;
+    A.slots = c->idxStd.slots;
+    A.xin = c->xb[c->xv];
+    A.vin = c->vb[c->xv];
+    A.xout = c->xb[c->xv ^ 1];
+    A.vout = c->vb[c->xv ^ 1];
+    A.cid = c->cidStd;
+    A.seeds = c->seeds;
+    A.nZones = L.nZones;
+    A.maxCells = c->zMaxCells;
+    A.winCap = c->zWinCap;
+    A.nlocCap = c->zNlocCap;
+    A.arenaCap = c->zArenaCap;
+    A.overflow = c->overflow;
+    A.nOverflow = c->nOverflow;
+    A.zoneMoved = c->zoneMoved;
+    A.zoneCorr = c->zoneCorr;
+    A.st = c->st;
+    k_zone_pass<<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+    CUDA_TRY(cudaGetLastError());
+    ZoneArgs B = A;
+    B.maxCells = c->ovMaxCells;
+    B.winCap = c->ovWinCap;
+    B.nlocCap = c->ovNlocCap;
+    B.arenaCap = c->ovArenaCap;
+    k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0));
+    CUDA_TRY(cudaGetLastError());
+    c->xv ^= 1;
+    c->idxStdValid = false;  // cid was updated for moved particles; positions changed
+    c->srdCellsValid = false;
+    return MPCD_OK;
+}
+
+// closure on the current (red) state; permute: write particles in (cell, id) order into the
+// other buffers (next step's layout); vrep: repaired velocities wanted
+int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats) {
+    if (!c->refValid) return set_err(MPCD_ERR_STATE, "liquid closure needs a saved reference state (mpcd_save_ref)");
+    int rc = ensure_std_index(c);
+    if (rc) return rc;
+    RedFields rf{};
+    k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
+                                                                   c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
+                                                                   c->duRY, c->cols);
+    rc = reduce_cols(c, c->cols, c->Nc, 2, 0u, c->red);
+    if (rc) return rc;
+    const int nx = c->xv, np = c->pp;
+    k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
+        c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
+        c->pidb[np], permute ? c->xb[nx ^ 1] : nullptr, permute ? c->vb[nx ^ 1] : nullptr,
+        permute ? c->pidb[np ^ 1] : nullptr, wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    if (wantStats) {
+        // sum, max, sum, sum, max, sum, sum, sum, sum
+        rc = reduce_cols(c, c->cols, c->Nc, kKickCols, (1u << 1) | (1u << 4), c->red + 2);
+        if (rc) return rc;
+    }
+    if (permute) {
+        c->xv ^= 1;
+        c->pp ^= 1;
+        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n);
+        CUDA_TRY(cudaGetLastError());
+        // the standard index stays valid (same cells, identity slots); per-slot cell ids and
+        // SRD cells refer to the old layout
+        c->cidStdValid = false;
+        c->srdCellsValid = false;
+    }
+    return MPCD_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C-ABI
+extern "C" {
+
+const char* mpcd_last_error(void) { return g_err.c_str(); }
+
+int mpcd_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, 0) != cudaSuccess) return 0;
+    return pr.major >= 10 ? 1 : 0;
+}
+
+int mpcd_ctx_destroy(mpcd_ctx* c) {
+    if (!c) return MPCD_OK;
+    cudaSetDevice(c->device);
+    void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd,
+                    c->idxStd.count, c->idxStd.packed, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
+                    c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
+                    c->blockSums, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
+                    c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
+                    c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
+                    c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
+                    c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
+                    c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->st};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (int k = 0; k < 3; ++k) {
+        if (c->lay[k].rects) cudaFree(c->lay[k].rects);
+        if (c->lay[k].owner) cudaFree(c->lay[k].owner);
+    }
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->hst) cudaFreeHost(c->hst);
+    if (c->hred) cudaFreeHost(c->hred);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MPCD_OK;
+}
+
+int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
+    if (!params || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    int rc = validate(*params);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(MPCD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return set_err(MPCD_ERR_INVALID_ARG, "device index out of range");
+    mpcd_ctx* c = new mpcd_ctx();
+    std::memset(c->ev, 0, sizeof(c->ev));
+    c->device = device;
+    c->pc = *params;
+    c->P = make_dev_params(*params);
+    c->n = params->n;
+    c->Nc = params->Nc;
+    auto fail = [&](int code) {
+        mpcd_ctx_destroy(c);
+        return code;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "stream"));
+    const int n = c->n, Nc = c->Nc;
+#define ALLOC(p, cnt) \
+    if ((rc = dalloc(&(p), (cnt)))) return fail(rc)
+    for (int k = 0; k < 2; ++k) {
+        ALLOC(c->xb[k], (size_t)n);
+        ALLOC(c->vb[k], (size_t)n);
+        ALLOC(c->pidb[k], (size_t)n);
+    }
+    ALLOC(c->cidStd, (size_t)n);
+    ALLOC(c->cidSrd, (size_t)n);
+    for (CellIndex* I : {&c->idxStd, &c->idxSrd}) {
+        ALLOC(I->count, (size_t)Nc);
+        ALLOC(I->packed, (size_t)Nc);
+        ALLOC(I->start, (size_t)Nc + 1);
+        ALLOC(I->pos, (size_t)n);
+        ALLOC(I->slots, (size_t)n);
+    }
+    c->nwords = (n + 31) / 32 + 1;
+    c->blockSumsCap = (int)std::max<int64_t>(1, ((int64_t)std::max(Nc, c->nwords) + kScanTile - 1) / kScanTile) + 1;
+    ALLOC(c->blockSums, (size_t)c->blockSumsCap);
+    c->bcBlocks = blocks_for(n);
+    BcWork& W = c->W;
+    ALLOC(W.bitsX, (size_t)c->nwords);
+    ALLOC(W.bitsY, (size_t)c->nwords);
+    ALLOC(W.wordCount, (size_t)c->nwords);
+    ALLOC(W.wordPrefix, (size_t)c->nwords + 1);
+    W.eventCap = std::max(4096, std::min(n, std::max(65536, n / 8)));
+    W.normalCap = 2 * W.eventCap;
+    ALLOC(W.events, (size_t)W.eventCap);
+    ALLOC(W.nEvents, 1);
+    ALLOC(W.normals, 2 * (size_t)W.normalCap);
+    ALLOC(W.contrib, (size_t)kWallDoubles * W.normalCap);
+    ALLOC(W.blockPartial, (size_t)kWallDoubles * c->bcBlocks);
+    ALLOC(W.ints, 4);
+    ALLOC(W.srdShift, 2);
+    ALLOC(c->wallOut, kWallDoubles);
+    ALLOC(c->signs, (size_t)Nc);
+    // zone layouts
+    build_layout(*params, MPCD_LAYOUT_BASE, c->lay[0]);
+    build_layout(*params, MPCD_LAYOUT_SHIFTED, c->lay[1]);
+    build_layout(*params, MPCD_LAYOUT_SINGLE_FULL, c->lay[2]);
+    int maxZones = 0, maxArea = 0, maxTX = 0, maxTY = 0;
+    for (int k = 0; k < 3; ++k) {
+        Layout& L = c->lay[k];
+        ALLOC(L.rects, L.hrects.size());
+        ALLOC(L.owner, (size_t)Nc);
+        if (cudaMemcpy(L.rects, L.hrects.data(), L.hrects.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.owner, L.howner.data(), (size_t)Nc * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_err(MPCD_ERR_CUDA, "layout upload"));
+        maxZones = std::max(maxZones, L.nZones);
+        maxArea = std::max(maxArea, L.maxArea);
+        maxTX = std::max(maxTX, L.maxTX);
+        maxTY = std::max(maxTY, L.maxTY);
+    }
+    ALLOC(c->seeds, (size_t)maxZones * kMtN);
+    ALLOC(c->zoneMoved, (size_t)maxZones);
+    ALLOC(c->zoneCorr, (size_t)maxZones);
+    ALLOC(c->overflow, (size_t)maxZones);
+    ALLOC(c->nOverflow, 1);
+    ALLOC(c->passOut, 8);
+    // fast path: tiles of the base/shifted layouts in shared memory
+    {
+        const Layout& B = c->lay[0];
+        const Layout& S = c->lay[1];
+        const int area = std::max(B.maxArea, S.maxArea);
+        const int tx = std::max(B.maxTX, S.maxTX), ty = std::max(B.maxTY, S.maxTY);
+        c->zMaxCells = std::max(1, area);
+        c->zWinCap = (tx + 4) * (ty + 4);
+        const double g = std::max(1.0, params->gamma);
+        c->zNlocCap = ((int)std::ceil(1.6 * g * area) + 64 + 31) / 32 * 32;
+        c->zArenaCap = c->zNlocCap + 1024;
+        c->zSmem = ZoneMem<uint16_t>::bytes(c->zMaxCells, c->zWinCap, c->zNlocCap, c->zArenaCap);
+        if (c->zNlocCap > 65535 || c->zSmem > 200 * 1024) {
+            // too large for the shared-memory path: every zone takes the overflow path
+            c->zMaxCells = 0;
+            c->zSmem = ZoneMem<uint16_t>::bytes(0, 0, 0, 0);
+        }
+        if (c->zSmem > 48 * 1024 &&
+            cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess)
+            return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
+        c->ovMaxCells = maxArea;
+        c->ovWinCap = (maxTX + 4) * (maxTY + 4);
+        c->ovNlocCap = std::max(1, params->zoneSingleFullDomainMode ? n : std::min(n, std::max(65536, 16 * std::max(c->zNlocCap, 1))));
+        c->ovArenaCap = c->ovNlocCap + 4096;
+        c->ovPerBlock = (ZoneMem<uint32_t>::bytes(c->ovMaxCells, c->ovWinCap, c->ovNlocCap, c->ovArenaCap) + 255) / 256 * 256;
+        ALLOC(c->ovMem, c->ovPerBlock * (size_t)c->ovBlocks);
+    }
+    // closure
+    const auto mask = interzone_mask(*params, c->lay[params->zoneSingleFullDomainMode ? 2 : 0],
+                                     c->lay[params->zoneSingleFullDomainMode ? 2 : 1]);
+    c->nMasked = 0;
+    for (int m : mask) c->nMasked += (m == 1);
+    ALLOC(c->mask, (size_t)Nc);
+    if (cudaMemcpy(c->mask, mask.data(), (size_t)Nc * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(set_err(MPCD_ERR_CUDA, "mask upload"));
+    for (double** p : {&c->refPx, &c->refPy, &c->refUx, &c->refUy, &c->refT, &c->refRho, &c->refPkin, &c->refPvir,
+                       &c->refP, &c->pdRaw, &c->pdrive, &c->eosX, &c->eosY, &c->duRX, &c->duRY})
+        ALLOC(*p, (size_t)Nc);
+    ALLOC(c->refNi, (size_t)Nc);
+    ALLOC(c->cols, (size_t)std::max<int64_t>((int64_t)Nc * kKickCols, 3LL * n));
+    c->partialCap = (int)(((int64_t)std::max(Nc, n) + 8191) / 8192 + 1) * kRedMaxCols;
+    ALLOC(c->partial, (size_t)c->partialCap);
+    ALLOC(c->red, 32);
+    ALLOC(c->fieldTmp, 11 * (size_t)Nc);
+    ALLOC(c->fieldTmpN, (size_t)Nc);
+    ALLOC(c->vrep, (size_t)n);
+    ALLOC(c->st, 1);
+#undef ALLOC
+    if (cudaMemset(c->st, 0, sizeof(DevStatus)) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "memset"));
+    if (cudaMallocHost((void**)&c->hst, sizeof(DevStatus)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->hred, 32 * sizeof(double)) != cudaSuccess)
+        return fail(set_err(MPCD_ERR_CUDA, "pinned host"));
+    for (auto& e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "event"));
+    *out = c;
+    return MPCD_OK;
+}
+
+void* mpcd_ctx_stream(mpcd_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t n, cudaMemcpyKind kind) {
+    if (!c || !x || !v) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (n != c->n) return set_err(MPCD_ERR_INVALID_ARG, "state size does not match params.n");
+    CUDA_TRY(cudaSetDevice(c->device));
+    c->xv = 0;
+    c->pp = 0;
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(c->xb[0], x, sizeof(double2) * (size_t)n, kind, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(c->vb[0], v, sizeof(double2) * (size_t)n, kind, c->stream));
+        k_iota<<<blocks_for(n), kThreads, 0, c->stream>>>(c->pidb[0], (int)n);
+        CUDA_TRY(cudaGetLastError());
+    }
+    invalidate_positions(c);
+    c->refValid = false;
+    return check_device(c);
+}
+
+int mpcd_set_state(mpcd_ctx* c, const double* x, const double* v, int64_t n) {
+    return set_state_impl(c, x, v, n, cudaMemcpyHostToDevice);
+}
+int mpcd_set_state_device(mpcd_ctx* c, const double* x, const double* v, int64_t n) {
+    return set_state_impl(c, x, v, n, cudaMemcpyDeviceToDevice);
+}
+
+static int get_state_impl(mpcd_ctx* c, double* x, double* v, bool toHost) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (c->n == 0) return MPCD_OK;
+    double2* tx = c->xb[c->xv ^ 1];
+    double2* tv = c->vb[c->xv ^ 1];
+    k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv);
+    CUDA_TRY(cudaGetLastError());
+    const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (x) CUDA_TRY(cudaMemcpyAsync(x, tx, sizeof(double2) * (size_t)c->n, k, c->stream));
+    if (v) CUDA_TRY(cudaMemcpyAsync(v, tv, sizeof(double2) * (size_t)c->n, k, c->stream));
+    return check_device(c);
+}
+
+int mpcd_get_state(mpcd_ctx* c, double* x, double* v) { return get_state_impl(c, x, v, true); }
+int mpcd_get_state_device(mpcd_ctx* c, double* x, double* v) { return get_state_impl(c, x, v, false); }
+
+int mpcd_stream(mpcd_ctx* c) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->vb[c->xv]);
+    CUDA_TRY(cudaGetLastError());
+    invalidate_positions(c);
+    return check_device(c);
+}
+
+int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = run_bc(c, false, seed, nullptr, nullptr, info != nullptr);
+    if (rc) return rc;
+    invalidate_positions(c);
+    rc = check_device(c);
+    if (rc) return rc;
+    if (info) {
+        int ints[4];
+        double d[kWallDoubles];
+        CUDA_TRY(cudaMemcpy(ints, c->W.ints, sizeof ints, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(d, c->wallOut, sizeof d, cudaMemcpyDeviceToHost));
+        info->nBot = ints[0]; info->nTop = ints[1]; info->nLeft = ints[2]; info->nRight = ints[3];
+        info->dEwall = d[0]; info->dPxBot = d[1]; info->dPxTop = d[2]; info->dPyBot = d[3]; info->dPyTop = d[4];
+        info->dPxLeft = d[5]; info->dPxRight = d[6]; info->dPyLeft = d[7]; info->dPyRight = d[8];
+    }
+    return MPCD_OK;
+}
+
+int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift);
+    k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd);
+    CUDA_TRY(cudaGetLastError());
+    c->srdCellsValid = true;
+    if (cid_out && c->n > 0) {
+        int* tmp = c->idxSrd.pos;  // scratch: particle-id order
+        k_int_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->cidSrd, c->pidb[c->pp], c->n, tmp);
+        CUDA_TRY(cudaMemcpyAsync(cid_out, tmp, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    return check_device(c);
+}
+
+int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (!c->srdCellsValid) return set_err(MPCD_ERR_STATE, "no SRD cell ids: call mpcd_srd_shift_cells first");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = run_collide(c, seed);
+    if (rc) return rc;
+    c->refValid = false;
+    return check_device(c);
+}
+
+int mpcd_srd_collide_cells(mpcd_ctx* c, const int32_t* cid, uint64_t seed) {
+    if (!c || !cid) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (c->n > 0) {
+        int* tmp = c->idxSrd.pos;
+        CUDA_TRY(cudaMemcpyAsync(tmp, cid, sizeof(int) * (size_t)c->n, cudaMemcpyHostToDevice, c->stream));
+        k_int_to_slots<<<blocks_for(c->n), kThreads, 0, c->stream>>>(tmp, c->pidb[c->pp], c->n, c->Nc, c->cidSrd, c->st);
+        CUDA_TRY(cudaGetLastError());
+        int rc = check_device(c);
+        if (rc) return rc;
+    }
+    c->srdCellsValid = true;
+    return mpcd_srd_collide(c, seed);
+}
+
+static int fields_to_host(mpcd_ctx* c, const FieldsOut& o, mpcd_cellfields_c* out) {
+    const size_t nc = (size_t)c->Nc;
+    if (out->N) CUDA_TRY(cudaMemcpyAsync(out->N, o.N, nc * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    const double* src[10] = {o.Ux, o.Uy, o.Px, o.Py, o.T, o.rho, o.Pkin, o.Pvir, o.P, o.rhoTarget};
+    double* dst[10] = {out->Ux, out->Uy, out->Px, out->Py, out->T, out->rho, out->Pkin, out->Pvir, out->P, out->rhoTarget};
+    for (int k = 0; k < 10; ++k)
+        if (dst[k]) CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return MPCD_OK;
+}
+
+static FieldsOut tmp_fields(mpcd_ctx* c) {
+    FieldsOut o{};
+    double* b = c->fieldTmp;
+    const size_t nc = (size_t)c->Nc;
+    o.N = c->fieldTmpN;
+    o.Ux = b; o.Uy = b + nc; o.Px = b + 2 * nc; o.Py = b + 3 * nc; o.T = b + 4 * nc; o.rho = b + 5 * nc;
+    o.Pkin = b + 6 * nc; o.Pvir = b + 7 * nc; o.P = b + 8 * nc; o.rhoTarget = b + 9 * nc;
+    return o;
+}
+
+int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
+    if (!c || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = ensure_std_index(c);
+    if (rc) return rc;
+    const FieldsOut o = tmp_fields(c);
+    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], rho_target, o);
+    CUDA_TRY(cudaGetLastError());
+    rc = fields_to_host(c, o, out);
+    if (rc) return rc;
+    return check_device(c);
+}
+
+int mpcd_save_ref(mpcd_ctx* c) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = run_save_ref(c);
+    if (rc) return rc;
+    return check_device(c);
+}
+
+static int pass_metrics_to_host(mpcd_ctx* c, int mode, mpcd_pass_metrics_c* m) {
+    double d[4];
+    CUDA_TRY(cudaMemcpy(d, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0), sizeof d, cudaMemcpyDeviceToHost));
+    std::memset(m, 0, sizeof *m);
+    const Layout& L = c->lay[c->pc.zoneSingleFullDomainMode ? 2 : mode];
+    m->nZones = L.nZones;
+    m->nThreadsRequested = 1;
+    m->nThreadsUsed = L.nZones;
+    m->nParticlesMovedDense = (int)d[0];
+    m->nParticlesMovedSparse = (int)d[1];
+    m->corrRmsDU = d[2];
+    m->corrMaxDU = d[3];
+    return MPCD_OK;
+}
+
+int mpcd_zone_pass(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
+    if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (mode < 0 || mode > 2) mode = MPCD_LAYOUT_BASE;
+    CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+    int rc = run_zone_pass(c, mode, seed_base);
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+    rc = check_device(c);
+    if (rc) return rc;
+    if (metrics) {
+        rc = pass_metrics_to_host(c, mode, metrics);
+        if (rc) return rc;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        metrics->timeKernel = ms * 1e-3;
+    }
+    return MPCD_OK;
+}
+
+int mpcd_zone_owner_map(mpcd_ctx* c, int32_t mode, int32_t* owner_out) {
+    if (!c || !owner_out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (mode < 0 || mode > 2) mode = MPCD_LAYOUT_BASE;
+    if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
+    std::memcpy(owner_out, c->lay[mode].howner.data(), sizeof(int32_t) * (size_t)c->Nc);
+    return MPCD_OK;
+}
+
+static void closure_metrics_from(mpcd_ctx* c, const double* r, mpcd_closure_metrics_c* m) {
+    // r: [0] num [1] den [2..10] kick columns
+    std::memset(m, 0, sizeof *m);
+    const double num = r[0], den = r[1];
+    double opt = 0.0;
+    if (std::isfinite(num) && std::isfinite(den) && den > 0.0) opt = std::max(num / den, 0.0);
+    m->betaRepairNum = num;
+    m->betaRepairDen = den;
+    m->betaRepairOpt = opt;
+    if (!c->pc.useOptimalBetaRepair || !std::isfinite(opt) || !std::isfinite(den) || den < 1e-20)
+        m->betaRepairApplied = c->pc.betaRepair;
+    else
+        m->betaRepairApplied = std::clamp(opt, 0.0, 2.0);
+    m->betaEOSApplied = c->pc.betaEOS;
+    const double nn = (double)std::max(c->n, 1);
+    m->rmsRepairDU = (c->n > 0) ? std::sqrt(r[2] / nn) : 0.0;
+    m->maxRepairDU = (c->n > 0) ? r[3] : 0.0;
+    m->meanAbsRepairDU = r[4] / (double)std::max(c->Nc, 1);
+    m->rmsEOSDU = (c->n > 0) ? std::sqrt(r[5] / nn) : 0.0;
+    m->maxEOSDU = (c->n > 0) ? r[6] : 0.0;
+    m->momentumDeltaX = r[9] - r[7];
+    m->momentumDeltaY = r[10] - r[8];
+    m->nMaskedInterzoneCells = c->nMasked;
+}
+
+int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (!c->pc.useLiquidClosure) return set_err(MPCD_ERR_INVALID_ARG, "run_liquid_closure requires useLiquidClosure=true");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const bool wantRep = detail && (detail->repairedV || detail->repairedX || detail->repairedFields.N ||
+                                    detail->repairedFields.Px || detail->repairedFields.Ux || detail->repairedFields.T);
+    int rc;
+    if (detail) {  // fields of the red state, before the kicks
+        if (!c->refValid) return set_err(MPCD_ERR_STATE, "liquid closure needs a saved reference state (mpcd_save_ref)");
+        rc = ensure_std_index(c);
+        if (rc) return rc;
+        const FieldsOut o = tmp_fields(c);
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        rc = fields_to_host(c, o, &detail->redFields);
+        if (rc) return rc;
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+    rc = run_closure(c, false, wantRep, true);
+    if (rc) return rc;
+    // pdrive sums for the means
+    rc = reduce_cols(c, c->pdRaw, c->Nc, 1, 0u, c->red + 16);
+    if (rc) return rc;
+    rc = reduce_cols(c, c->pdrive, c->Nc, 1, 0u, c->red + 17);
+    if (rc) return rc;
+    rc = check_device(c);
+    if (rc) return rc;
+    double r[18];
+    CUDA_TRY(cudaMemcpy(r, c->red, sizeof r, cudaMemcpyDeviceToHost));
+    mpcd_closure_metrics_c m;
+    closure_metrics_from(c, r, &m);
+    m.meanPdriveRaw = (c->Nc > 0) ? r[16] / (double)c->Nc : 0.0;
+    m.meanPdrive = (c->Nc > 0) ? r[17] / (double)c->Nc : 0.0;
+    if (metrics) *metrics = m;
+    if (detail) {
+        const size_t nc = (size_t)c->Nc;
+        FieldsOut ref{};
+        ref.N = c->refNi; ref.Ux = c->refUx; ref.Uy = c->refUy; ref.Px = c->refPx; ref.Py = c->refPy; ref.T = c->refT;
+        ref.rho = c->refRho; ref.Pkin = c->refPkin; ref.Pvir = c->refPvir; ref.P = c->refP; ref.rhoTarget = nullptr;
+        mpcd_cellfields_c rf = detail->refFields;
+        if (rf.rhoTarget) {
+            std::vector<double> t(nc, c->P.rhoTarget);
+            std::memcpy(rf.rhoTarget, t.data(), nc * sizeof(double));
+            rf.rhoTarget = nullptr;
+        }
+        rc = fields_to_host(c, ref, &rf);
+        if (rc) return rc;
+        const double* src[6] = {c->pdRaw, c->pdrive, c->duRX, c->duRY, c->eosX, c->eosY};
+        double* dst[6] = {detail->pdriveRaw, detail->pdrive, detail->duRepairX, detail->duRepairY, detail->duEOSX, detail->duEOSY};
+        for (int k = 0; k < 6; ++k)
+            if (dst[k]) CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (detail->interzoneMask) CUDA_TRY(cudaMemcpyAsync(detail->interzoneMask, c->mask, nc * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        const FieldsOut o = tmp_fields(c);
+        if (wantRep) {
+            // repaired state: positions unchanged, velocities = vrep
+            if (detail->repairedX || detail->repairedV) {
+                k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vrep, c->pidb[c->pp], c->n,
+                                                                              c->xb[c->xv ^ 1], c->vb[c->xv ^ 1]);
+                if (detail->repairedX) CUDA_TRY(cudaMemcpyAsync(detail->repairedX, c->xb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+                if (detail->repairedV) CUDA_TRY(cudaMemcpyAsync(detail->repairedV, c->vb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+                CUDA_TRY(cudaStreamSynchronize(c->stream));
+            }
+            k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vrep, c->P.rhoTarget, o);
+            rc = fields_to_host(c, o, &detail->repairedFields);
+            if (rc) return rc;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+        }
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        rc = fields_to_host(c, o, &detail->outFields);
+        if (rc) return rc;
+        rc = check_device(c);
+        if (rc) return rc;
+    }
+    return MPCD_OK;
+}
+
+
+// ---------------------------------------------------------------- the step
+static int count_metrics(mpcd_ctx* c, double* dst /* device: 3 doubles */) {
+    k_count_cols<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->P.highThr, c->P.lowThrBulk, c->cols);
+    CUDA_TRY(cudaGetLastError());
+    return reduce_cols(c, c->cols, c->Nc, 3, 0u, dst);
+}
+
+// One iteration of the profiled benchmark loop (reference
+// src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:241-279) with its seeds.
+static int step_once(mpcd_ctx* c, int64_t step, bool metrics) {
+    const uint64_t s = (uint64_t)step;
+    int rc;
+    if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift);
+    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics);
+    if (rc) return rc;
+    c->cidStdValid = true;
+    c->srdCellsValid = true;
+    c->idxStdValid = false;
+    rc = run_collide(c, 433494437ULL + 10007ULL * s);
+    if (rc) return rc;
+    rc = run_save_ref(c);
+    if (rc) return rc;
+    if (metrics) CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+    rc = run_zone_pass(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s);
+    if (rc) return rc;
+    if (metrics) {
+        CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
+        rc = ensure_std_index(c);
+        if (rc) return rc;
+        rc = count_metrics(c, c->red + 20);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
+    }
+    rc = run_zone_pass(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s);
+    if (rc) return rc;
+    if (metrics) {
+        CUDA_TRY(cudaEventRecord(c->ev[4], c->stream));
+        rc = ensure_std_index(c);
+        if (rc) return rc;
+        rc = count_metrics(c, c->red + 23);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(c->ev[5], c->stream));
+    }
+    rc = run_closure(c, true, false, metrics);
+    if (rc) return rc;
+    if (metrics) {
+        CUDA_TRY(cudaEventRecord(c->ev[6], c->stream));
+        rc = reduce_cols(c, c->pdRaw, c->Nc, 1, 0u, c->red + 16);
+        if (rc) return rc;
+        rc = reduce_cols(c, c->pdrive, c->Nc, 1, 0u, c->red + 17);
+        if (rc) return rc;
+        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols);
+        rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 26);
+        if (rc) return rc;
+        FieldsOut o{};
+        o.Ux = c->fieldTmp;
+        o.Uy = c->fieldTmp + c->Nc;
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        rc = reduce_cols(c, c->fieldTmp, c->Nc, 1, 0u, c->red + 29);
+        if (rc) return rc;
+        rc = reduce_cols(c, c->fieldTmp + c->Nc, c->Nc, 1, 0u, c->red + 30);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(c->ev[7], c->stream));
+    }
+    return MPCD_OK;
+}
+
+static void occ_from(const mpcd_ctx* c, const double* r, double* occ, double* ob) {
+    const double N = (double)std::max(1, c->Nc);
+    const double mean = r[0] / N;
+    double var = r[1] / N - mean * mean;
+    if (var < 0.0) var = 0.0;
+    *occ = std::sqrt(var) / std::max(c->pc.gamma, 1e-12);
+    *ob = r[2] / N;
+}
+
+int mpcd_step(mpcd_ctx* c, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* last) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (nsteps < 0) return set_err(MPCD_ERR_INVALID_ARG, "nsteps must be >= 0");
+    if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution || !c->pc.useLiquidClosure)
+        return set_err(MPCD_ERR_INVALID_ARG, "the benchmark step needs useIncompressibleRedistribution, useZoneRedistribution and useLiquidClosure");
+    if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (int64_t k = 1; k <= nsteps; ++k) {
+        const bool m = (last != nullptr) && (k == nsteps);
+        int rc = step_once(c, step0 + k, m);
+        if (rc) return rc;
+    }
+    int rc = check_device(c);
+    if (rc) return rc;
+    if (last && nsteps > 0) {
+        mpcd_step_metrics_c& M = *last;
+        std::memset(&M, 0, sizeof M);
+        M.step = step0 + nsteps;
+        double r[32];
+        int ints[4];
+        double wd[kWallDoubles];
+        CUDA_TRY(cudaMemcpy(r, c->red, sizeof r, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(ints, c->W.ints, sizeof ints, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(wd, c->wallOut, sizeof wd, cudaMemcpyDeviceToHost));
+        M.wall.nBot = ints[0]; M.wall.nTop = ints[1]; M.wall.nLeft = ints[2]; M.wall.nRight = ints[3];
+        M.wall.dEwall = wd[0]; M.wall.dPxBot = wd[1]; M.wall.dPxTop = wd[2]; M.wall.dPyBot = wd[3]; M.wall.dPyTop = wd[4];
+        M.wall.dPxLeft = wd[5]; M.wall.dPxRight = wd[6]; M.wall.dPyLeft = wd[7]; M.wall.dPyRight = wd[8];
+        rc = pass_metrics_to_host(c, MPCD_LAYOUT_BASE, &M.base);
+        if (rc) return rc;
+        rc = pass_metrics_to_host(c, MPCD_LAYOUT_SHIFTED, &M.shifted);
+        if (rc) return rc;
+        closure_metrics_from(c, r, &M.closure);
+        M.closure.meanPdriveRaw = r[16] / (double)std::max(1, c->Nc);
+        M.closure.meanPdrive = r[17] / (double)std::max(1, c->Nc);
+        occ_from(c, r + 20, &M.baseOccStd, &M.baseOutBand);
+        occ_from(c, r + 23, &M.shiftedOccStd, &M.shiftedOutBand);
+        M.occStd = M.shiftedOccStd;
+        M.outBand = M.shiftedOutBand;
+        const double nn = (double)std::max(c->n, 1);
+        M.meanKinetic = r[26] / nn;
+        M.meanVelocityX = r[27] / nn;
+        M.meanVelocityY = r[28] / nn;
+        M.meanUx = r[29] / (double)std::max(1, c->Nc);
+        M.meanUy = r[30] / (double)std::max(1, c->Nc);
+        M.Qx = M.meanUx * c->pc.Ly;
+        float t[7];
+        for (int k = 0; k < 7; ++k) cudaEventElapsedTime(&t[k], c->ev[k], c->ev[k + 1]);
+        M.timeRefBuild = t[0] * 1e-3;
+        M.timeBase = t[1] * 1e-3;
+        M.timeShifted = t[3] * 1e-3;
+        M.timeClosure = t[5] * 1e-3;
+        M.timeDiagnostics = (t[2] + t[4] + t[6]) * 1e-3;
+        M.timeStepTotal = M.timeRefBuild + M.timeBase + M.timeShifted + M.timeClosure + M.timeDiagnostics;
+        M.base.timeKernel = M.timeBase;
+        M.shifted.timeKernel = M.timeShifted;
+        c->last = M;
+    }
+    return MPCD_OK;
+}
+
+int mpcd_step_metrics(mpcd_ctx* c, mpcd_step_metrics_c* out) {
+    if (!c || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    *out = c->last;
+    return MPCD_OK;
+}
+
+}  // extern "C"

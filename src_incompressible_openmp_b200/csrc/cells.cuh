@@ -1,0 +1,148 @@
+// Per-cell kernels over a cell index (slots of each cell in ascending particle id):
+// the SRD rotation collision and compute_cell_fields.
+#pragma once
+
+#include "common.cuh"
+
+namespace mpcd_dev {
+
+// The collision's rotation-sign stream: draw r of mt19937_64(seed) belongs to the r-th cell
+// (in cell order) holding >= 2 particles (src/srd_collision.cpp:77-83); sign[r] = 1 when
+// U(0,1) < 0.5 (theta = -alpha). One block generates `count` draws, one twist at a time.
+constexpr int kSignThreads = 320;
+__global__ void __launch_bounds__(kSignThreads) k_srd_signs(uint64_t seed, int count, uint8_t* __restrict__ sign) {
+    __shared__ uint64_t mt[kMtN];
+    const int t = threadIdx.x;
+    if (t == 0) {
+        uint64_t w = seed;
+        mt[0] = w;
+        for (int i = 1; i < kMtN; ++i) {
+            w = mt_seed_next(w, i);
+            mt[i] = w;
+        }
+    }
+    __syncthreads();
+    for (int base = 0; base < count; base += kMtN) {
+        uint64_t nv = 0;
+        if (t < kMtN - kMtM) nv = mt[t + kMtM] ^ mt_mix(mt[t], mt[t + 1]);
+        __syncthreads();
+        if (t < kMtN - kMtM) mt[t] = nv;
+        __syncthreads();
+        if (t >= kMtN - kMtM && t < kMtN) {
+            const uint64_t nxt = (t + 1 < kMtN) ? mt[t + 1] : mt[0];
+            nv = mt[t - (kMtN - kMtM)] ^ mt_mix(mt[t], nxt);
+        }
+        __syncthreads();
+        if (t >= kMtN - kMtM && t < kMtN) mt[t] = nv;
+        __syncthreads();
+        if (t < kMtN && base + t < count) sign[base + t] = (canon(mt_temper(mt[t])) < 0.5) ? 1 : 0;
+        __syncthreads();
+    }
+}
+
+// srd_collision_step (src/srd_collision.cpp:47-124) for one SRD cell per thread. start:
+// packed (segment start | rank among cells with >= 2 particles << 32).
+__global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
+                              const uint8_t* __restrict__ sign, int signCount, double2* __restrict__ v,
+                              DevStatus* st) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    const uint64_t s0 = start[c];
+    const int a = (int)(uint32_t)s0, b = (int)(uint32_t)start[c + 1];
+    const int m = b - a;
+    if (m == 0) return;
+    double sx = 0.0, sy = 0.0;
+    for (int j = a; j < b; ++j) {
+        const double2 w = v[slots[j]];
+        sx = __dadd_rn(sx, w.x);
+        sy = __dadd_rn(sy, w.y);
+    }
+    const double ux = __ddiv_rn(sx, (double)m), uy = __ddiv_rn(sy, (double)m);
+    int rot = 0;
+    if (m >= 2) {
+        const int r = (int)(s0 >> 32);
+        if (r >= signCount) {
+            raise_error(st, kErrRngCapacity, r);
+            return;
+        }
+        rot = sign[r] ? 2 : 1;
+    }
+    const double ct = P.rotCos[rot], sn = P.rotSin[rot];
+    double lam = 1.0;
+    if (P.useThermostat) {
+        double sr = 0.0;
+        for (int j = a; j < b; ++j) {
+            const double2 w = v[slots[j]];
+            const double xr = __dsub_rn(w.x, ux), yr = __dsub_rn(w.y, uy);
+            const double x2 = __dsub_rn(__dmul_rn(ct, xr), __dmul_rn(sn, yr));
+            const double y2 = __dadd_rn(__dmul_rn(sn, xr), __dmul_rn(ct, yr));
+            sr = __dadd_rn(sr, __dadd_rn(__dmul_rn(x2, x2), __dmul_rn(y2, y2)));
+        }
+        if (m > 1 && sr > 0.0) lam = sqrt(__ddiv_rn(__dmul_rn((double)(2 * (m - 1)), P.kBT), sr));
+    }
+    for (int j = a; j < b; ++j) {
+        const int s = slots[j];
+        const double2 w = v[s];
+        const double xr = __dsub_rn(w.x, ux), yr = __dsub_rn(w.y, uy);
+        double x2 = __dsub_rn(__dmul_rn(ct, xr), __dmul_rn(sn, yr));
+        double y2 = __dadd_rn(__dmul_rn(sn, xr), __dmul_rn(ct, yr));
+        if (P.useThermostat) {
+            x2 = __dmul_rn(x2, lam);
+            y2 = __dmul_rn(y2, lam);
+        }
+        v[s] = make_double2(__dadd_rn(ux, x2), __dadd_rn(uy, y2));
+    }
+}
+
+// Output arrays of compute_cell_fields; any pointer may be null.
+struct FieldsOut {
+    int* N;
+    double *Ux, *Uy, *Px, *Py, *T, *rho, *Pkin, *Pvir, *P, *rhoTarget;
+};
+
+// compute_cell_fields (src/common_grid.cpp:32-100), one cell per thread.
+__global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, const int* __restrict__ slots,
+                              const double2* __restrict__ v, double rhoTarget, FieldsOut o) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Pm.Nc) return;
+    const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
+    const int m = b - a;
+    double px = 0.0, py = 0.0;
+    for (int j = a; j < b; ++j) {
+        const double2 w = v[slots[j]];
+        px = __dadd_rn(px, w.x);
+        py = __dadd_rn(py, w.y);
+    }
+    double ux = 0.0, uy = 0.0;
+    if (m > 0) {
+        ux = __ddiv_rn(px, (double)m);
+        uy = __ddiv_rn(py, (double)m);
+    }
+    const double rho = __ddiv_rn((double)m, Pm.Vc);
+    double T = 0.0, pk = 0.0;
+    const int dof = 2 * max(m - 1, 0);
+    if (dof > 0 && (o.T || o.Pkin || o.P)) {
+        double s2 = 0.0;
+        for (int j = a; j < b; ++j) {
+            const double2 w = v[slots[j]];
+            const double ax = __dsub_rn(w.x, ux), ay = __dsub_rn(w.y, uy);
+            s2 = __dadd_rn(s2, __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
+        }
+        T = __ddiv_rn(s2, (double)dof);
+        pk = __dmul_rn(rho, T);
+    }
+    const double pv = __dmul_rn(Pm.Kvirial, __dsub_rn(rho, rhoTarget));
+    if (o.N) o.N[c] = m;
+    if (o.Ux) o.Ux[c] = ux;
+    if (o.Uy) o.Uy[c] = uy;
+    if (o.Px) o.Px[c] = px;
+    if (o.Py) o.Py[c] = py;
+    if (o.T) o.T[c] = T;
+    if (o.rho) o.rho[c] = rho;
+    if (o.Pkin) o.Pkin[c] = pk;
+    if (o.Pvir) o.Pvir[c] = pv;
+    if (o.P) o.P[c] = __dadd_rn(pk, pv);
+    if (o.rhoTarget) o.rhoTarget[c] = rhoTarget;
+}
+
+}  // namespace mpcd_dev

@@ -1,0 +1,254 @@
+// Liquid closure (reference src/liquid_closure.cpp:329-444).
+//
+//   ref fields  : cell fields of the post-collision state (computed before the zone passes)
+//   k_pdrive    : pdriveRaw = Pkin + Pvir of ref, blended with the 5-point cross smoothing on
+//                 the static interzone mask (:401-419, local_cross_smooth :215-241)
+//   k_eos       : boundary-aware central gradient and the EOS kick (:243-295, :424-430)
+//   k_closure_cells : red-state momenta per cell, duRepair and the beta_opt terms (:343-360)
+//   k_reduce_*  : fixed-order reductions (num, den and diagnostics)
+//   k_kick      : v <- (v + beta*duRepair[c]) + duEOS[c] per particle (:380-389, :432-436),
+//                 writing particles in (cell, particle id) order into the next buffer
+#pragma once
+
+#include "common.cuh"
+
+namespace mpcd_dev {
+
+// local_cross_smooth at one cell (acc = centre, then left, right, down, up)
+__device__ __forceinline__ double cross_smooth(const double* raw, int ix, int iy, const DevParams& P) {
+    double acc = raw[iy + P.Ny * ix];
+    int cnt = 1;
+    const int jj[4][2] = {{iy, ix - 1}, {iy, ix + 1}, {iy - 1, ix}, {iy + 1, ix}};
+    for (int q = 0; q < 4; ++q) {
+        int jy = jj[q][0], jx = jj[q][1];
+        if (P.perx) jx = wrap_index(jx, P.Nx);
+        else if (jx < 0 || jx >= P.Nx) continue;
+        if (P.pery) jy = wrap_index(jy, P.Ny);
+        else if (jy < 0 || jy >= P.Ny) continue;
+        acc = __dadd_rn(acc, raw[jy + P.Ny * jx]);
+        ++cnt;
+    }
+    return __ddiv_rn(acc, (double)cnt);
+}
+
+__global__ void k_pdrive(DevParams P, const double* __restrict__ pkin, const double* __restrict__ pvir, double* __restrict__ raw) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    raw[c] = __dadd_rn(pkin[c], pvir[c]);
+}
+
+__global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, const int* __restrict__ mask, int anyMask,
+                               double* __restrict__ pdrive) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    double v = raw[c];
+    if (anyMask && mask[c] != 0) {
+        const int ix = c / P.Ny, iy = c - ix * P.Ny;
+        const double ps = cross_smooth(raw, ix, iy, P);
+        v = __dadd_rn(__dmul_rn(__dsub_rn(1.0, P.smoothBlend), raw[c]), __dmul_rn(P.smoothBlend, ps));
+    }
+    pdrive[c] = v;
+}
+
+__global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __restrict__ eosX, double* __restrict__ eosY) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    const int ix = c / P.Ny, iy = c - ix * P.Ny;
+    double gx, gy;
+    if (P.perx) gx = __ddiv_rn(__dsub_rn(pd[iy + P.Ny * wrap_index(ix + 1, P.Nx)], pd[iy + P.Ny * wrap_index(ix - 1, P.Nx)]), __dmul_rn(2.0, P.dx));
+    else if (ix == 0) gx = __ddiv_rn(__dsub_rn(pd[iy + P.Ny * (ix + 1)], pd[c]), P.dx);
+    else if (ix == P.Nx - 1) gx = __ddiv_rn(__dsub_rn(pd[c], pd[iy + P.Ny * (ix - 1)]), P.dx);
+    else gx = __ddiv_rn(__dsub_rn(pd[iy + P.Ny * (ix + 1)], pd[iy + P.Ny * (ix - 1)]), __dmul_rn(2.0, P.dx));
+    if (P.pery) gy = __ddiv_rn(__dsub_rn(pd[wrap_index(iy + 1, P.Ny) + P.Ny * ix], pd[wrap_index(iy - 1, P.Ny) + P.Ny * ix]), __dmul_rn(2.0, P.dy));
+    else if (iy == 0) gy = __ddiv_rn(__dsub_rn(pd[(iy + 1) + P.Ny * ix], pd[c]), P.dy);
+    else if (iy == P.Ny - 1) gy = __ddiv_rn(__dsub_rn(pd[c], pd[(iy - 1) + P.Ny * ix]), P.dy);
+    else gy = __ddiv_rn(__dsub_rn(pd[(iy + 1) + P.Ny * ix], pd[(iy - 1) + P.Ny * ix]), __dmul_rn(2.0, P.dy));
+    const double k = -__ddiv_rn(P.dt, P.rhoTarget);
+    eosX[c] = __dmul_rn(__dmul_rn(k, gx), P.betaEOS);
+    eosY[c] = __dmul_rn(__dmul_rn(k, gy), P.betaEOS);
+}
+
+// Per cell of the red (post-redistribution) state: momenta in particle-id order, velocity,
+// duRepair = (P_ref - P_red) / gamma and the beta_opt terms. cols: 2 doubles per cell
+// (num term, den term) for the fixed-order reduction.
+struct RedFields {
+    int* N;
+    double *Px, *Py, *Ux, *Uy;
+};
+__global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
+                                const double2* __restrict__ v, const double* __restrict__ refPx,
+                                const double* __restrict__ refPy, const double* __restrict__ refUx,
+                                const double* __restrict__ refUy, RedFields red, double* __restrict__ duRX,
+                                double* __restrict__ duRY, double* __restrict__ cols) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
+    const int m = b - a;
+    double px = 0.0, py = 0.0;
+    for (int j = a; j < b; ++j) {
+        const double2 w = v[slots[j]];
+        px = __dadd_rn(px, w.x);
+        py = __dadd_rn(py, w.y);
+    }
+    double ux = 0.0, uy = 0.0;
+    if (m > 0) {
+        ux = __ddiv_rn(px, (double)m);
+        uy = __ddiv_rn(py, (double)m);
+    }
+    const double ax = __ddiv_rn(__dsub_rn(refPx[c], px), P.gamma);
+    const double ay = __ddiv_rn(__dsub_rn(refPy[c], py), P.gamma);
+    const double ex = __dsub_rn(ux, refUx[c]), ey = __dsub_rn(uy, refUy[c]);
+    duRX[c] = ax;
+    duRY[c] = ay;
+    cols[2 * (size_t)c] = -__dadd_rn(__dmul_rn(ex, ax), __dmul_rn(ey, ay));
+    cols[2 * (size_t)c + 1] = __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay));
+    if (red.N) red.N[c] = m;
+    if (red.Px) red.Px[c] = px;
+    if (red.Py) red.Py[c] = py;
+    if (red.Ux) red.Ux[c] = ux;
+    if (red.Uy) red.Uy[c] = uy;
+}
+
+// ---------------------------------------------------------------- fixed-order reductions
+// K interleaved columns over n rows; kind bit k set -> max instead of sum for column k.
+constexpr int kRedThreads = 256;
+constexpr int kRedMaxCols = 16;
+__global__ void __launch_bounds__(kRedThreads) k_reduce_partial(const double* __restrict__ in, int64_t n, int K,
+                                                                unsigned maxMask, int rowsPerBlock,
+                                                                double* __restrict__ partial) {
+    __shared__ double sh[kRedMaxCols][kRedThreads];
+    const int t = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * rowsPerBlock;
+    const int64_t r1 = min((int64_t)n, r0 + rowsPerBlock);
+    for (int k = 0; k < K; ++k) {
+        double a = 0.0;
+        for (int64_t r = r0 + t; r < r1; r += kRedThreads) {
+            const double x = in[r * K + k];
+            a = ((maxMask >> k) & 1u) ? smax(a, x) : __dadd_rn(a, x);
+        }
+        sh[k][t] = a;
+    }
+    __syncthreads();
+    for (int o = kRedThreads / 2; o > 0; o >>= 1) {
+        if (t < o)
+            for (int k = 0; k < K; ++k)
+                sh[k][t] = ((maxMask >> k) & 1u) ? smax(sh[k][t], sh[k][t + o]) : __dadd_rn(sh[k][t], sh[k][t + o]);
+        __syncthreads();
+    }
+    if (t < K) partial[(size_t)blockIdx.x * K + t] = sh[t][0];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_reduce_final(const double* __restrict__ partial, int nb, int K,
+                                                              unsigned maxMask, double* __restrict__ out) {
+    __shared__ double sh[kRedMaxCols][kRedThreads];
+    const int t = threadIdx.x;
+    for (int k = 0; k < K; ++k) {
+        double a = 0.0;
+        for (int b = t; b < nb; b += kRedThreads) {
+            const double x = partial[(size_t)b * K + k];
+            a = ((maxMask >> k) & 1u) ? smax(a, x) : __dadd_rn(a, x);
+        }
+        sh[k][t] = a;
+    }
+    __syncthreads();
+    for (int o = kRedThreads / 2; o > 0; o >>= 1) {
+        if (t < o)
+            for (int k = 0; k < K; ++k)
+                sh[k][t] = ((maxMask >> k) & 1u) ? smax(sh[k][t], sh[k][t + o]) : __dadd_rn(sh[k][t], sh[k][t + o]);
+        __syncthreads();
+    }
+    if (t < K) out[t] = sh[t][0];
+}
+
+// beta_applied from num/den (src/liquid_closure.cpp:364-377)
+__device__ __forceinline__ double beta_applied(const DevParams& P, double num, double den) {
+    double opt = 0.0;
+    if (isfinite(num) && isfinite(den) && den > 0.0) opt = smax(__ddiv_rn(num, den), 0.0);
+    if (!P.useOptimalBetaRepair) return P.betaRepair;
+    if (!isfinite(opt) || !isfinite(den) || den < 1e-20) return P.betaRepair;
+    return (opt < 0.0) ? 0.0 : ((2.0 < opt) ? 2.0 : opt);
+}
+
+// The two kicks, one cell per thread in particle-id order. If xo/vo/pido are given the
+// particles are written in (cell, id) order starting at the cell's segment (the next
+// step's layout); otherwise v is updated in place. vrep (optional, slot order) receives the
+// repaired velocities. stats: 8 columns per cell for the diagnostics reduction:
+// sum kn_rep^2, max kn_rep, hypot(beta*duR), sum kn_eos^2, max kn_eos, sum vin.x, sum vin.y,
+// sum vout.x - not used (momentum delta from vout sums) -> see column list in k_kick.
+constexpr int kKickCols = 9;
+__global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
+                       const double* __restrict__ numden, const double* __restrict__ duRX,
+                       const double* __restrict__ duRY, const double* __restrict__ eosX,
+                       const double* __restrict__ eosY, const double2* __restrict__ x, double2* __restrict__ v,
+                       const int* __restrict__ pid, double2* __restrict__ xo, double2* __restrict__ vo,
+                       int* __restrict__ pido, double2* __restrict__ vrep, double* __restrict__ stats) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.Nc) return;
+    const double beta = beta_applied(P, numden[0], numden[1]);
+    const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
+    const double ex = eosX[c], ey = eosY[c];
+    const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
+    double sinx = 0.0, siny = 0.0, soutx = 0.0, souty = 0.0;
+    for (int j = a; j < b; ++j) {
+        const int s = slots[j];
+        const double2 w = v[s];
+        const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
+        const double2 o = make_double2(__dadd_rn(r.x, ex), __dadd_rn(r.y, ey));
+        if (vrep) vrep[s] = r;
+        if (vo) {
+            xo[j] = x[s];
+            vo[j] = o;
+            pido[j] = pid[s];
+        } else {
+            v[s] = o;
+        }
+        sinx = __dadd_rn(sinx, w.x);
+        siny = __dadd_rn(siny, w.y);
+        soutx = __dadd_rn(soutx, o.x);
+        souty = __dadd_rn(souty, o.y);
+    }
+    if (stats) {
+        const int m = b - a;
+        const double knr = sqrt(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)));
+        const double kne = sqrt(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)));
+        double* s = stats + (size_t)c * kKickCols;
+        s[0] = __dmul_rn((double)m, __dmul_rn(knr, knr));
+        s[1] = (m > 0) ? knr : 0.0;
+        s[2] = mpcd_dd::hypot_cr(kx, ky);
+        s[3] = __dmul_rn((double)m, __dmul_rn(kne, kne));
+        s[4] = (m > 0) ? kne : 0.0;
+        s[5] = sinx;
+        s[6] = siny;
+        s[7] = soutx;
+        s[8] = souty;
+    }
+}
+
+// identity cell index after a permuting kick: slots[j] = j
+__global__ void k_iota(int* __restrict__ a, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+// per-particle sums for the step metrics: 0.5|v|^2, vx, vy (slot order; fixed reduction)
+__global__ void k_particle_cols(const double2* __restrict__ v, int n, double* __restrict__ cols) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 w = v[i];
+    cols[3 * (size_t)i] = __dmul_rn(0.5, __dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y)));
+    cols[3 * (size_t)i + 1] = w.x;
+    cols[3 * (size_t)i + 2] = w.y;
+}
+
+// per-cell columns for occStd / outBand from a cell index (counts), and mean Ux / Uy
+__global__ void k_count_cols(const uint64_t* __restrict__ start, int Nc, double highThr, double lowThr,
+                             double* __restrict__ cols) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nc) return;
+    const double n = (double)((uint32_t)start[c + 1] - (uint32_t)start[c]);
+    cols[3 * (size_t)c] = n;
+    cols[3 * (size_t)c + 1] = __dmul_rn(n, n);
+    cols[3 * (size_t)c + 2] = ((n > highThr) || (n > 0.0 && n < lowThr)) ? 1.0 : 0.0;
+}
+
+}  // namespace mpcd_dev

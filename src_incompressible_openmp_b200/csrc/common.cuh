@@ -1,0 +1,274 @@
+// Shared device definitions: the parameter block, error flags, MT19937-64 and the
+// libstdc++-13 distributions restated for warp-uniform use on sm_100a.
+//
+// All FP64 arithmetic in this library is compiled with -fmad=false: every a*b+c rounds
+// twice, exactly like the reference's x86-64 build (no FMA contraction).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ddmath.cuh"
+
+namespace mpcd_dev {
+
+constexpr int kWarp = 32;
+
+// Device-side error codes (written to DevStatus::code with atomicCAS: first error wins).
+enum DevError : int {
+    kDevOk = 0,
+    kErrUnsupportedBcLeft = 1,
+    kErrUnsupportedBcRight = 2,
+    kErrUnsupportedBcBottom = 3,
+    kErrUnsupportedBcTop = 4,
+    kErrZoneCapacity = 5,       // a zone list exceeded its provable bound
+    kErrTableRange = 6,         // a minimal step outside the 5x5 tables
+    kErrBcLateSweep = 7,        // a particle crossed a wall again after the first sweep
+    kErrEventCapacity = 8,      // more wall events than the event buffer holds
+    kErrCellId = 9,             // a caller-given cell id outside [0, Nc)
+    kErrTargetIsSource = 10,    // a dense cell targeting itself (periodic axis shorter than 3)
+    kErrRngCapacity = 11        // the collision sign stream was shorter than needed
+};
+
+struct DevStatus {
+    int code;
+    int detail;
+    unsigned long long count;
+};
+
+__device__ __forceinline__ void raise_error(DevStatus* st, int code, int detail) {
+    if (atomicCAS(&st->code, 0, code) == 0) st->detail = detail;
+}
+
+// Parameter block passed by value to every kernel. Derived constants are computed on the
+// host once per context, with the host libm where the reference calls libm (cos, sin,
+// atan2 and hypot of small integer steps).
+struct DevParams {
+    int Nx, Ny, Nc, n;
+    double Lx, Ly, dt, a0, dx, dy, Vc;
+    double alpha, kBT, g, bodyForceX;
+    int useThermostat, keepMeanFlow;
+    int bc[4];  // left, right, bottom, top (mpcd_bc_mode)
+    int perx, pery;
+    double Utop, Ubottom, wallSigma;
+    int tileNx, tileNy, momCorr, maxPasses, useLFF, lowThrBulkInt, listBound, reserved0;
+    double gamma, coef, highThr, lowThrBulk, lowFrac, highFrac, fluidFracGain, lowThrFloor, highThrFloor;
+    int useLiquidClosure, useOptimalBetaRepair, smoothWidth, reserved1;
+    double betaRepair, betaEOS, Kvirial, smoothBlend, rhoTarget;
+    // rotation: index 0 -> theta = 0, 1 -> +alpha, 2 -> -alpha
+    double rotCos[3], rotSin[3];
+    // (ddx+2) + 5*(ddy+2) -> angular bin of atan2(ddy, ddx) and hypot(ddx, ddy)
+    int atanBin[25];
+    double hypotTab[25];
+};
+
+__device__ __forceinline__ int wrap_index(int i, int n) {
+    int r = i % n;
+    return (r < 0) ? r + n : r;
+}
+
+// std::max / std::min / std::clamp argument-order semantics (NaN-faithful)
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+// reference src/common_grid.cpp:9-19
+__device__ __forceinline__ int cell_of(double x, double y, const DevParams& P) {
+    int ix = (int)floor(x / P.dx), iy = (int)floor(y / P.dy);
+    if (ix < 0) ix = 0;
+    if (ix >= P.Nx) ix = P.Nx - 1;
+    if (iy < 0) iy = 0;
+    if (iy >= P.Ny) iy = P.Ny - 1;
+    return iy + P.Ny * ix;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ------------------------------------------------------------------ MT19937-64
+constexpr int kMtN = 312;
+constexpr int kMtM = 156;
+constexpr uint64_t kMtUM = 0xFFFFFFFF80000000ULL;
+constexpr uint64_t kMtLM = 0x7FFFFFFFULL;
+constexpr uint64_t kMtA = 0xB5026F5AA96619E9ULL;
+
+__host__ __device__ __forceinline__ uint64_t mt_temper(uint64_t z) {
+    z ^= (z >> 29) & 0x5555555555555555ULL;
+    z ^= (z << 17) & 0x71D67FFFEDA60000ULL;
+    z ^= (z << 37) & 0xFFF7EEE000000000ULL;
+    z ^= z >> 43;
+    return z;
+}
+
+__host__ __device__ __forceinline__ uint64_t mt_mix(uint64_t a, uint64_t b) {
+    const uint64_t y = (a & kMtUM) | (b & kMtLM);
+    return (y >> 1) ^ ((y & 1ULL) ? kMtA : 0ULL);
+}
+
+// Sequential seeding recurrence (one thread).
+__host__ __device__ __forceinline__ uint64_t mt_seed_next(uint64_t prev, int i) {
+    return 6364136223846793005ULL * (prev ^ (prev >> 62)) + (uint64_t)i;
+}
+
+// Out-of-place twist of a 312-word state A into B by one warp (A is left intact).
+__device__ __forceinline__ void mt_twist_warp(const uint64_t* A, uint64_t* B, int lane) {
+    for (int i = lane; i < kMtN - kMtM; i += kWarp) B[i] = A[i + kMtM] ^ mt_mix(A[i], A[i + 1]);
+    __syncwarp();
+    for (int i = kMtN - kMtM + lane; i < kMtN - 1; i += kWarp) B[i] = B[i - (kMtN - kMtM)] ^ mt_mix(A[i], A[i + 1]);
+    if (lane == 0) B[kMtN - 1] = B[kMtM - 1] ^ mt_mix(A[kMtN - 1], B[0]);
+    __syncwarp();
+}
+
+// generate_canonical<double, 53> of one 64-bit draw
+__device__ __forceinline__ double canon(uint64_t u) {
+    double c = __dmul_rn(__ull2double_rn(u), 0x1p-64);  // exact scaling
+    if (c >= 1.0) c = 0x1.fffffffffffffp-1;  // nextafter(1, 0)
+    return c;
+}
+
+// Warp-uniform MT19937-64 stream over a double-buffered state in shared memory. Every lane
+// of the warp must call the member functions with identical arguments (uniform control
+// flow); the buffers are only written inside mt_twist_warp.
+struct WarpMt {
+    uint64_t* buf;  // 2 * 312 words: buffers 0 and 1
+    int cur;        // buffer holding draws pos..311 of the current block
+    int pos;        // next draw within the current block
+    int nextReady;  // buffer cur^1 holds the following block
+    int lane;
+
+    __device__ __forceinline__ void init_from_seeded(int lane_) {
+        lane = lane_;
+        cur = 0;
+        pos = kMtN;
+        nextReady = 0;
+    }
+    // make draws pos .. pos+k-1 available (k <= 312)
+    __device__ __forceinline__ void ensure(int k) {
+        if (pos + k > kMtN && !nextReady) {
+            mt_twist_warp(buf + cur * kMtN, buf + (cur ^ 1) * kMtN, lane);
+            nextReady = 1;
+        }
+    }
+    // draw i (0-based) past the current position; requires ensure(i+1) first
+    __device__ __forceinline__ uint64_t peek(int i) const {
+        const int j = pos + i;
+        return mt_temper((j < kMtN) ? buf[cur * kMtN + j] : buf[(cur ^ 1) * kMtN + (j - kMtN)]);
+    }
+    // pos == 312 means the block is exhausted; a swap happens only once a draw past the
+    // block end was taken (ensure() produced the next block before it was peeked)
+    __device__ __forceinline__ void consume(int k) {
+        pos += k;
+        if (pos > kMtN) {
+            cur ^= 1;
+            pos -= kMtN;
+            nextReady = 0;
+        }
+    }
+    __device__ __forceinline__ uint64_t next() {
+        ensure(1);
+        const uint64_t u = peek(0);
+        consume(1);
+        return u;
+    }
+    __device__ __forceinline__ double u01() { return canon(next()); }
+    // uniform_int_distribution on [lo, hi] (Lemire downscaling with 128-bit products)
+    __device__ __forceinline__ uint64_t uint_in(uint64_t lo, uint64_t hi) {
+        const uint64_t range = hi - lo + 1ULL;
+        uint64_t u = next();
+        uint64_t low = u * range;
+        uint64_t high = __umul64hi(u, range);
+        if (low < range) {
+            const uint64_t thr = (0ULL - range) % range;
+            while (low < thr) {
+                u = next();
+                low = u * range;
+                high = __umul64hi(u, range);
+            }
+        }
+        return high + lo;
+    }
+};
+
+// normal_distribution<double>(0, 1): Marsaglia polar method with one cached deviate
+struct PolarNormal {
+    double saved;
+    int has;
+    __device__ __forceinline__ void reset() { has = 0; saved = 0.0; }
+    __device__ __forceinline__ double next(WarpMt& r) {
+        if (has) {
+            has = 0;
+            return saved;
+        }
+        double x, y, r2;
+        do {
+            x = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
+            y = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
+            r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+        } while (r2 > 1.0 || r2 == 0.0);
+        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, mpcd_dd::log_cr(r2)), r2));
+        saved = __dmul_rn(x, mult);
+        has = 1;
+        return __dmul_rn(y, mult);
+    }
+};
+
+// std::shuffle of m entries at a (warp-uniform; lane 0 performs the swaps)
+template <typename T>
+__device__ __forceinline__ void warp_shuffle(T* a, int m, WarpMt& r, int lane) {
+    if (m <= 0) return;
+    int i = 1;
+    if ((m % 2) == 0) {
+        const int j = (int)r.uint_in(0, 1);
+        if (lane == 0) {
+            const T t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+        ++i;
+    }
+    while (i != m) {
+        const uint64_t sr = (uint64_t)i + 1ULL;
+        const uint64_t x = r.uint_in(0, sr * (sr + 1ULL) - 1ULL);
+        const int p1 = (int)(x / (sr + 1ULL)), p2 = (int)(x % (sr + 1ULL));
+        if (lane == 0) {
+            T t = a[i];
+            a[i] = a[p1];
+            a[p1] = t;
+            t = a[i + 1];
+            a[i + 1] = a[p2];
+            a[p2] = t;
+        }
+        i += 2;
+    }
+    __syncwarp();
+}
+
+// Block-wide exclusive scan of one u64 per thread (blockDim a multiple of 32, <= 1024).
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* sh, uint64_t* total) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        uint64_t s = (lane < nw) ? sh[lane] : 0ULL;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) sh[lane] = s;
+    }
+    __syncthreads();
+    const uint64_t warpPrefix = (wid > 0) ? sh[wid - 1] : 0ULL;
+    if (total) *total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warpPrefix + x - v;
+}
+
+}  // namespace mpcd_dev

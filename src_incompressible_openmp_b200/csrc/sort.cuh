@@ -1,0 +1,142 @@
+// Cell index: for every cell, the slots of its particles in ascending particle id.
+//
+// The reference walks particles in id order whenever it accumulates per-cell sums
+// (src/common_grid.cpp:62-67, src/srd_collision.cpp:61-66) or builds per-cell lists
+// (src/zone_pass.cpp:112-118). Ordering each cell's slots by particle id makes every
+// per-cell FP64 sum on the device run in exactly that order, so sums are bit-identical.
+//
+// Build: warp-aggregated histogram with atomics (one atomic per run of equal cell ids in a
+// warp), exclusive scan of the counts, scatter of slots, then an insertion sort of each
+// cell's short segment by particle id.
+#pragma once
+
+#include "common.cuh"
+
+namespace mpcd_dev {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// ------------------------------------------------------------------ exclusive scan (u64)
+__global__ void k_scan_reduce(const uint64_t* __restrict__ in, int64_t n, uint64_t* __restrict__ blockSums) {
+    __shared__ uint64_t sh[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint64_t tot;
+    block_exclusive_scan(s, sh, &tot);
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = tot;
+}
+
+// single block: exclusive scan of nb block sums in place
+__global__ void k_scan_blocks(uint64_t* __restrict__ blockSums, int nb) {
+    __shared__ uint64_t sh[32];
+    uint64_t carry = 0;
+    for (int base = 0; base < nb; base += kScanThreads) {
+        const int i = base + threadIdx.x;
+        const uint64_t v = (i < nb) ? blockSums[i] : 0ULL;
+        uint64_t tot;
+        const uint64_t ex = block_exclusive_scan(v, sh, &tot);
+        if (i < nb) blockSums[i] = carry + ex;
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+// out[i] = exclusive prefix of in; out[n] = total (out has n+1 entries)
+__global__ void k_scan_apply(const uint64_t* __restrict__ in, int64_t n, const uint64_t* __restrict__ blockSums,
+                             uint64_t* __restrict__ out) {
+    __shared__ uint64_t sh[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint64_t v[kScanItems];
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0ULL;
+        s += v[k];
+    }
+    uint64_t tot;
+    uint64_t ex = block_exclusive_scan(s, sh, &tot) + blockSums[blockIdx.x];
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (base + kScanItems >= n && base < n) out[n] = ex;  // the thread holding the last element
+}
+
+// ------------------------------------------------------------------ cell index
+// pack (count, count >= 2) so one scan yields both the segment starts and the rank of each
+// cell among cells holding at least two particles (the SRD sign stream index).
+__global__ void k_pack_counts(const int* __restrict__ count, int Nc, uint64_t* __restrict__ packed) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < Nc) {
+        const int k = count[c];
+        packed[c] = (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+    }
+}
+
+// pos[s] = arrival order of slot s within its cell (any order; fixed later by k_cell_sort)
+__global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict__ count, int* __restrict__ pos) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned active = __ballot_sync(0xffffffffu, s < n);
+    if (s >= n) return;
+    const int c = cid[s];
+    const unsigned same = __match_any_sync(active, c);
+    const int leader = __ffs(same) - 1;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&count[c], __popc(same));
+    base = __shfl_sync(same, base, leader);
+    pos[s] = base + __popc(same & lanemask_lt());
+}
+
+__global__ void k_scatter(const int* __restrict__ cid, const int* __restrict__ pos, int n,
+                          const uint64_t* __restrict__ start, int* __restrict__ slots) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) slots[(uint32_t)start[cid[s]] + pos[s]] = s;
+}
+
+// sort each cell's slots by particle id (segments are short: ~ particles per cell)
+__global__ void k_cell_sort(const uint64_t* __restrict__ start, int Nc, const int* __restrict__ pid,
+                            int* __restrict__ slots) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nc) return;
+    const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
+    const int m = b - a;
+    if (m <= 1) return;
+    constexpr int kLocal = 48;
+    if (m <= kLocal) {
+        uint64_t key[kLocal];
+        for (int i = 0; i < m; ++i) {
+            const int s = slots[a + i];
+            key[i] = ((uint64_t)(uint32_t)pid[s] << 32) | (uint32_t)s;
+        }
+        for (int i = 1; i < m; ++i) {
+            const uint64_t v = key[i];
+            int j = i;
+            while (j > 0 && key[j - 1] > v) {
+                key[j] = key[j - 1];
+                --j;
+            }
+            key[j] = v;
+        }
+        for (int i = 0; i < m; ++i) slots[a + i] = (int)(uint32_t)key[i];
+    } else {
+        // long segment: insertion sort in place in global memory
+        for (int i = a + 1; i < b; ++i) {
+            const int v = slots[i];
+            const int pv = pid[v];
+            int j = i;
+            while (j > a && pid[slots[j - 1]] > pv) {
+                slots[j] = slots[j - 1];
+                --j;
+            }
+            slots[j] = v;
+        }
+    }
+}
+
+}  // namespace mpcd_dev

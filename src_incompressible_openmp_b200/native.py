@@ -1,0 +1,223 @@
+"""Python binding of the C-ABI (include/mpcd_c.h) in libmpcd_b200.so.
+
+There is no CPU fallback: if the CUDA library is not built, or no sm_100 device is present,
+every entry point raises. ``Context`` mirrors the reference's phase functions on a
+device-resident state:
+
+    reference (namespace mpcd)                       Context method
+    main_...shifted_profiled.cpp:242-247 (stream)    stream()
+    apply_bc_general                                 apply_bc(seed)
+    srd_cell_id_with_random_shift                    srd_shift_cells(seed)
+    srd_collision_step                               srd_collide(seed) / srd_collide_cells(cid, seed)
+    compute_cell_fields                              cell_fields(rho_target)
+    run_zone_pass_openmp                             zone_pass(mode, seed_base)
+    run_liquid_closure(stateRef, stateRed)           save_ref() before the passes, then liquid_closure()
+    the benchmark loop body                          step(step0, nsteps)
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from .cases import to_c
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpcd_b200.so")
+
+_lib = None
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class MpcdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libmpcd_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    sig = {
+        "mpcd_last_error": ([], C.c_char_p),
+        "mpcd_io_last_error": ([], C.c_char_p),
+        "mpcd_device_available": ([], C.c_int),
+        "mpcd_read_params_kv": ([C.c_char_p, P(_abi.ParamsC)], C.c_int),
+        "mpcd_read_kv_string": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_int], C.c_int),
+        "mpcd_ctx_create": ([P(_abi.ParamsC), C.c_int, P(C.c_void_p)], C.c_int),
+        "mpcd_ctx_destroy": ([C.c_void_p], C.c_int),
+        "mpcd_ctx_stream": ([C.c_void_p], C.c_void_p),
+        "mpcd_set_state": ([C.c_void_p, _dp, _dp, C.c_int64], C.c_int),
+        "mpcd_get_state": ([C.c_void_p, _dp, _dp], C.c_int),
+        "mpcd_set_state_device": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+        "mpcd_get_state_device": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+        "mpcd_stream": ([C.c_void_p], C.c_int),
+        "mpcd_apply_bc": ([C.c_void_p, C.c_uint64, P(_abi.WallInfoC)], C.c_int),
+        "mpcd_srd_shift_cells": ([C.c_void_p, C.c_uint64, C.c_void_p], C.c_int),
+        "mpcd_srd_collide": ([C.c_void_p, C.c_uint64], C.c_int),
+        "mpcd_srd_collide_cells": ([C.c_void_p, _ip, C.c_uint64], C.c_int),
+        "mpcd_cell_fields": ([C.c_void_p, C.c_double, P(_abi.CellFieldsC)], C.c_int),
+        "mpcd_save_ref": ([C.c_void_p], C.c_int),
+        "mpcd_zone_pass": ([C.c_void_p, C.c_int32, C.c_uint64, P(_abi.PassMetricsC)], C.c_int),
+        "mpcd_liquid_closure": ([C.c_void_p, P(_abi.ClosureMetricsC), P(_abi.ClosureDetailC)], C.c_int),
+        "mpcd_zone_owner_map": ([C.c_void_p, C.c_int32, _ip], C.c_int),
+        "mpcd_step": ([C.c_void_p, C.c_int64, C.c_int64, P(_abi.StepMetricsC)], C.c_int),
+        "mpcd_step_metrics": ([C.c_void_p, P(_abi.StepMetricsC)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def device_available():
+    return bool(lib().mpcd_device_available())
+
+
+def _check(rc):
+    if rc != 0:
+        raise MpcdError(rc, lib().mpcd_last_error().decode())
+
+
+def read_params_kv(path):
+    p = _abi.ParamsC()
+    rc = lib().mpcd_read_params_kv(path.encode(), C.byref(p))
+    if rc != 0:
+        raise MpcdError(rc, lib().mpcd_io_last_error().decode())
+    return p
+
+
+def _fields_struct(Nc):
+    arrs = {k: np.zeros(Nc) for k in _abi.FIELD_NAMES}
+    arrs["N"] = np.zeros(Nc, np.int32)
+    s = _abi.CellFieldsC()
+    s.N = arrs["N"].ctypes.data_as(C.POINTER(C.c_int32))
+    for k in _abi.FIELD_NAMES:
+        setattr(s, k, arrs[k].ctypes.data_as(C.POINTER(C.c_double)))
+    return s, arrs
+
+
+class Context:
+    """A device-resident MPCD state for one parameter set (one GPU)."""
+
+    def __init__(self, params, device=0):
+        self.params = dict(params)
+        self.n = int(params["n"])
+        self.Nc = int(params["Nc"])
+        self._pc = to_c(params)
+        h = C.c_void_p()
+        _check(lib().mpcd_ctx_create(C.byref(self._pc), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mpcd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state -------------------------------------------------------------------------
+    def set_state(self, x, v):
+        x = np.ascontiguousarray(x, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        _check(lib().mpcd_set_state(self.h, x, v, self.n))
+
+    def get_state(self):
+        x = np.empty(2 * self.n)
+        v = np.empty(2 * self.n)
+        _check(lib().mpcd_get_state(self.h, x, v))
+        return x, v
+
+    def set_state_device(self, x_ptr, v_ptr):
+        _check(lib().mpcd_set_state_device(self.h, C.c_void_p(x_ptr), C.c_void_p(v_ptr), self.n))
+
+    def get_state_device(self, x_ptr, v_ptr):
+        _check(lib().mpcd_get_state_device(self.h, C.c_void_p(x_ptr), C.c_void_p(v_ptr)))
+
+    @property
+    def stream_handle(self):
+        return lib().mpcd_ctx_stream(self.h)
+
+    # phases ------------------------------------------------------------------------
+    def stream(self):
+        _check(lib().mpcd_stream(self.h))
+
+    def apply_bc(self, seed):
+        w = _abi.WallInfoC()
+        _check(lib().mpcd_apply_bc(self.h, seed, C.byref(w)))
+        return _abi.struct_to_dict(w)
+
+    def srd_shift_cells(self, seed, want_cells=True):
+        cid = np.empty(self.n, np.int32) if want_cells else None
+        _check(lib().mpcd_srd_shift_cells(self.h, seed, cid.ctypes.data if want_cells else None))
+        return cid
+
+    def srd_collide(self, seed):
+        _check(lib().mpcd_srd_collide(self.h, seed))
+
+    def srd_collide_cells(self, cid, seed):
+        _check(lib().mpcd_srd_collide_cells(self.h, np.ascontiguousarray(cid, np.int32), seed))
+
+    def cell_fields(self, rho_target):
+        s, arrs = _fields_struct(self.Nc)
+        _check(lib().mpcd_cell_fields(self.h, rho_target, C.byref(s)))
+        return arrs
+
+    def save_ref(self):
+        _check(lib().mpcd_save_ref(self.h))
+
+    def zone_pass(self, mode, seed_base):
+        m = _abi.PassMetricsC()
+        _check(lib().mpcd_zone_pass(self.h, _abi.LAYOUT_MODES[mode] if isinstance(mode, str) else mode, seed_base, C.byref(m)))
+        return _abi.struct_to_dict(m)
+
+    def liquid_closure(self, detail=False):
+        m = _abi.ClosureMetricsC()
+        d = None
+        out = None
+        if detail:
+            d = _abi.ClosureDetailC()
+            out = {}
+            for k in ("repairedX", "repairedV"):
+                out[k] = np.zeros(2 * self.n)
+                setattr(d, k, out[k].ctypes.data_as(C.POINTER(C.c_double)))
+            for k in ("refFields", "redFields", "repairedFields", "outFields"):
+                s, arrs = _fields_struct(self.Nc)
+                setattr(d, k, s)
+                out[k] = arrs
+            for k in ("pdriveRaw", "pdrive", "duRepairX", "duRepairY", "duEOSX", "duEOSY"):
+                out[k] = np.zeros(self.Nc)
+                setattr(d, k, out[k].ctypes.data_as(C.POINTER(C.c_double)))
+            out["interzoneMask"] = np.zeros(self.Nc, np.int32)
+            d.interzoneMask = out["interzoneMask"].ctypes.data_as(C.POINTER(C.c_int32))
+        _check(lib().mpcd_liquid_closure(self.h, C.byref(m), C.byref(d) if d is not None else None))
+        return (_abi.struct_to_dict(m), out) if detail else _abi.struct_to_dict(m)
+
+    def zone_owner_map(self, mode):
+        o = np.zeros(self.Nc, np.int32)
+        _check(lib().mpcd_zone_owner_map(self.h, _abi.LAYOUT_MODES[mode], o))
+        return o
+
+    def step(self, step0, nsteps, metrics=False):
+        m = _abi.StepMetricsC() if metrics else None
+        _check(lib().mpcd_step(self.h, step0, nsteps, C.byref(m) if m is not None else None))
+        return _abi.struct_to_dict(m) if metrics else None
