@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the SRC/MPCD time step on B200: particle-steps/s of the FP64 plain form.
+
+Workload: the large plain-FP64 Poiseuille channel, 2048 x 512 cells (a = 0.2), 10 particles
+per cell (10,485,760 particles), dt = 0.1, alpha = 130 deg, body force 1e-3 along +x,
+periodic x, thermalising walls at y = 0 and y = Ly, 10 x 10 redistribution tiles with a
+shifted second pass, closure stiffness 1. Synthetic seeded state (uniform positions,
+Maxwellian velocities with kT = 1, mean removed). The state (378 MB) is larger than L2
+(126 MB), so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours: W warm-up steps, then K steps timed with CUDA events on the context's stream,
+bracketed by a barrier and a device synchronisation on every rank; value = all ranks'
+particle-steps / max-over-ranks time. Under torchrun every rank advances its own replica on
+its own GPU (the step has no cross-replica exchange).
+
+reference: the unmodified reference (oracle/_ref/ref_sampled, built from the reference's
+own sources) on the host cores, on a bounded sample of the same workload: one full step of
+everything but the zone passes, plus a sample of zones per pass scaled to all zones.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200: FP64 plain vs FP32+learned closure, at ≤1% profile err"
+UNIT = "particle-steps/s"
+WORKLOAD = dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10)
+DATA = "synthetic: seeded uniform positions, Maxwellian velocities (kT=1, mean removed)"
+# algorithmic bytes per particle (P) and per cell (C) of one launch of each phase's main
+# kernel, FP64 plain form ("Roofline")
+PHASE_BYTES = {
+    "stream_bc": (72, 0),       # read x,v 32 B; write x,v 32 B; write 2 cell ids 8 B
+    "zone_pass": (68, 8),       # read slot 4, x 16, v 16; write x 16, v 16 | counts 8 per cell
+    "kick_resort": (76, 32),    # read slot 4, x,v 32, pid 4; write x,v,pid 36 | duR, duEOS 32 per cell
+    "collide": (36, 16),        # read slot 4, v 16; write v 16 | segment starts 16 per cell
+    "cell_index": (32, 24),     # cid 2x4, pos 2x4, slots 2x4, pid 4, slot rewrite 4 | count, scan 24
+    "ref_fields": (20, 96),     # read slot 4, v 16 | 10 field arrays + start
+    "closure_cells": (20, 64),
+}
+LAUNCHES_PER_STEP = {"zone_pass": 2, "cell_index": 4}
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self):
+        return time.time()
+
+    def stop(self, t0, t1):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [l for (t, l) in self.lines if t0 - 0.15 <= t <= t1 + 0.15] or [l for (_, l) in self.lines[-3:]]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            f = [x.strip() for x in r.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, val in zip(names, f[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return world, rank, local, dist, torch
+    return 1, 0, 0, None, None
+
+
+def barrier(dist, torch):
+    if dist is not None:
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def reduce_max(x, dist, torch):
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def config_dict(p, world):
+    return {
+        "workload": WORKLOAD["name"], "Nx": p["Nx"], "Ny": p["Ny"], "particles_per_cell": WORKLOAD["ppc"],
+        "n_particles": p["n"], "n_cells": p["Nc"], "form": "plain_f64", "dt": p["dt"],
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "l2_policy": "state (378 MB) larger than L2 (126 MB); no flush",
+    }
+
+
+def cpu_baseline_port(p, x, v):
+    """The oracle port (single thread) on one full step of the workload."""
+    from tests.oracle_libs import Oracle
+    O = Oracle()
+    t0 = time.perf_counter()
+    O.step(p, x, v, 1)
+    dt = time.perf_counter() - t0
+    return {"value": p["n"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one full step of {WORKLOAD['name']} ({p['n']} particles) with the C oracle, one thread: {dt:.1f} s"}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def measured_traffic(kernel):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        e = d.get(kernel)
+        if e and e.get("workload") == WORKLOAD["name"]:
+            return float(e["bytes_per_launch"])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def run_ours(args):
+    from src_incompressible_openmp_b200 import native
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
+
+    world, rank, local, dist, torch = dist_setup(args.gpus)
+    p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
+    x, v = uniform_state(p, 1 + rank)
+    ctx = native.Context(p, device=local)
+    ctx.set_state(x, v)
+    W, K = args.warmup, args.steps
+    ctx.step(0, W)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ctx.launch_count()
+    barrier(dist, torch)
+    t_wall0 = time.time()
+    t_dev = ctx.step_timed(W, K)
+    barrier(dist, torch)
+    t_wall1 = time.time()
+    l1 = ctx.launch_count()
+    clocks = sampler.stop(t_wall0, t_wall1)
+    t_max = reduce_max(t_dev, dist, torch)
+    value = world * p["n"] * K / t_max
+    # live per-phase timing (separate run: one synchronisation per step)
+    KP = max(1, min(K, args.profile_steps))
+    phases = ctx.step_profile(W + K, KP)
+    # end-to-end through the C-ABI with pinned host buffers: every step uploads its input
+    # state and downloads the resulting state
+    KE = max(1, min(K, args.e2e_steps))
+    hx = native.PinnedArray(2 * p["n"])
+    hv = native.PinnedArray(2 * p["n"])
+    hx.array[:] = x
+    hv.array[:] = v
+    barrier(dist, torch)
+    t0 = time.perf_counter()
+    for k in range(KE):
+        ctx.set_state(hx.array, hv.array)
+        ctx.step(W + K + KP + k, 1)
+        ctx.get_state(hx.array, hv.array)
+    barrier(dist, torch)
+    te = reduce_max(time.perf_counter() - t0, dist, torch)
+    hx.close()
+    hv.close()
+    e2e = {"value": world * p["n"] * KE / te, "unit": UNIT, "h2d_bytes_per_step": 32 * p["n"],
+           "d2h_bytes_per_step": 32 * p["n"], "steps": KE,
+           "note": "per step: state upload from pinned host memory, one step, state download (C-ABI)"}
+    ctx.close()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    # roofline of the dominant kernel
+    peak, peak_src = measured_peaks()
+    dom = max((k for k in phases if k in PHASE_BYTES), key=lambda k: phases[k])
+    per_launch_s = phases[dom] / (KP * LAUNCHES_PER_STEP.get(dom, 1))
+    bp, bc = PHASE_BYTES[dom]
+    alg = bp * p["n"] + bc * p["Nc"]
+    achieved = alg / per_launch_s / 1e9
+    step_bytes = 256 * p["n"] + 128 * p["Nc"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": DATA, "config": config_dict(p, world),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": measured_traffic(dom),
+                     "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
+                     "avg_launch_ms": 1e3 * per_launch_s},
+        "step_hbm": {"algorithmic_bytes_per_step": step_bytes,
+                     "achieved_GBps": step_bytes * K / t_max / 1e9 * world,
+                     "note": "256 B per particle + 128 B per cell per step"},
+        "phases_ms_per_step": {k: 1e3 * t / KP for k, t in phases.items()},
+        "e2e": e2e,
+        "gpu_launches": int((l1 - l0) * world),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port(p, x, v)
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state, write_case
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_sampled")
+    threads = os.cpu_count() or 1
+    x, v = uniform_state(p, 1)
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_sampled was not built (reference sources absent at build time)"}))
+        return
+    budget = args.reference_budget_s
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as d:
+        write_case(d, p, x, v, {"benchmark_nSteps": 1, "benchmark_metricsEvery": 1, "benchmark_dumpSteps": ""})
+        runs = []
+        t_start = time.time()
+        n_warm = min(args.warmup, 1)
+        k = 0
+        while True:
+            r = subprocess.run([exe, os.path.join(d, "params.kv"), os.path.join(d, "in_x.bin"), os.path.join(d, "in_v.bin"),
+                                str(threads), "1", str(k + 1)], capture_output=True, text=True)
+            if r.returncode != 0:
+                print(json.dumps({"impl": "reference", "unavailable": "reference harness failed: " + r.stderr.strip()[-200:]}))
+                return
+            runs.append(json.loads(r.stdout))
+            k += 1
+            elapsed = time.time() - t_start
+            timed = len(runs) - n_warm
+            per = elapsed / len(runs)
+            if timed >= args.steps or (timed >= 1 and elapsed + per > budget):
+                break
+    timed_runs = runs[n_warm:]
+    t_step = statistics.mean(r["t_step_extrapolated"] for r in timed_runs)
+    value = p["n"] / t_step
+    sample = (f"{len(timed_runs)} sampled steps of {WORKLOAD['name']} on {threads} threads: full stream/BC/SRD and closure, "
+              f"{timed_runs[0]['base_sampled']}/{timed_runs[0]['base_zones']} base and {timed_runs[0]['shifted_sampled']}/"
+              f"{timed_runs[0]['shifted_zones']} shifted zones per step through the reference's own per-zone body, "
+              f"scaled to all zones")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": len(timed_runs), "warmup": n_warm, "ms_per_step": 1e3 * t_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA, "config": config_dict(p, 1),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "phases_s": {k: statistics.mean(r[k] for r in timed_runs) for k in ("t_refbuild", "base_extrapolated", "shifted_extrapolated", "t_closure")},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,7 @@
 #ifndef MPCD_C_H
 #define MPCD_C_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -199,6 +200,18 @@ int mpcd_zone_owner_map(mpcd_ctx* ctx, int32_t mode, int32_t* owner_out);
 int mpcd_step(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* last);
 /* Device-side metrics row of the current state after a step (see mpcd_step). */
 int mpcd_step_metrics(mpcd_ctx* ctx, mpcd_step_metrics_c* out);
+/* mpcd_step without metrics, timed with CUDA events recorded on the context's stream
+ * around the whole loop (device seconds). */
+int mpcd_step_timed(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* device_seconds);
+/* Per-phase device seconds of nsteps steps (phase list in the implementation's comment:
+ * stream+BC, walls, SRD index, SRD signs, collision, cell index, reference fields, zone seeds,
+ * zone passes, closure cells, kick + re-sort). */
+int mpcd_step_profile(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* phase_seconds, int nphase);
+/* Page-locked host memory (for staging states); NULL on failure. */
+void* mpcd_host_alloc(size_t bytes);
+void mpcd_host_free(void* p);
+/* Number of kernels this context has launched so far. */
+int64_t mpcd_launch_count(mpcd_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,14 @@ struct Layout {
     std::vector<int> howner;
 };
 
+// Phase boundaries recorded on the context's stream (profiling runs only).
+constexpr int kProfMarks = 24;
+struct Prof {
+    cudaEvent_t ev[kProfMarks];
+    int label[kProfMarks];  // phase label of the interval ending at this mark
+    int n;
+};
+
 }  // namespace
 
 struct mpcd_ctx {
@@ -122,6 +130,7 @@ struct mpcd_ctx {
     double* hred = nullptr;
     // metrics
     mpcd_step_metrics_c last{};
+    int64_t launches = 0;
     cudaEvent_t ev[8];
 };
 
@@ -145,6 +154,12 @@ const char* dev_error_text(int code) {
 }
 
 // synchronise and turn a raised device flag into a status code
+void mark(mpcd_ctx* c, Prof* p, int label) {
+    if (!p || p->n >= kProfMarks) return;
+    p->label[p->n] = label;
+    cudaEventRecord(p->ev[p->n++], c->stream);
+}
+
 int check_device(mpcd_ctx* c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     CUDA_TRY(cudaMemcpy(c->hst, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost));
@@ -318,24 +333,28 @@ DevParams make_dev_params(const mpcd_params_c& p) {
 int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out) {
     const int nb = (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile);
     if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
-    k_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums);
-    k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb);
-    k_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums, out);
+    k_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums); ++c->launches;
+    k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb); ++c->launches;
+    k_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums, out); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     return MPCD_OK;
 }
 
-int build_index(mpcd_ctx* c, const int* cid, CellIndex& I) {
+int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, int label = -1) {
     CUDA_TRY(cudaMemsetAsync(I.count, 0, sizeof(int) * (size_t)c->Nc, c->stream));
-    if (c->n > 0) k_histogram<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
-    k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed);
+    if (c->n > 0) {
+        k_histogram<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
+        ++c->launches;
+    }
+    k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed); ++c->launches;
     int rc = scan_u64(c, I.packed, c->Nc, I.start);
     if (rc) return rc;
     if (c->n > 0) {
-        k_scatter<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, I.pos, c->n, I.start, I.slots);
-        k_cell_sort<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(I.start, c->Nc, c->pidb[c->pp], I.slots);
+        k_scatter<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, I.pos, c->n, I.start, I.slots); ++c->launches;
+        k_cell_sort<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(I.start, c->Nc, c->pidb[c->pp], I.slots); ++c->launches;
     }
     CUDA_TRY(cudaGetLastError());
+    mark(c, pf, label);
     return MPCD_OK;
 }
 
@@ -344,13 +363,13 @@ __global__ void k_std_cells(DevParams P, const double2* __restrict__ x, int* __r
     if (s < P.n) cid[s] = cell_of(x[s].x, x[s].y, P);
 }
 
-int ensure_std_index(mpcd_ctx* c) {
+int ensure_std_index(mpcd_ctx* c, Prof* pf = nullptr) {
     if (c->idxStdValid) return MPCD_OK;
     if (!c->cidStdValid) {
-        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd);
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
         c->cidStdValid = true;
     }
-    const int rc = build_index(c, c->cidStd, c->idxStd);
+    const int rc = build_index(c, c->cidStd, c->idxStd, pf, 5);
     if (!rc) c->idxStdValid = true;
     return rc;
 }
@@ -413,77 +432,83 @@ int reduce_cols(mpcd_ctx* c, const double* cols, int64_t rows, int K, unsigned m
     const int rowsPerBlock = 8192;
     const int nb = (int)std::max<int64_t>(1, (rows + rowsPerBlock - 1) / rowsPerBlock);
     if ((int64_t)nb * K > c->partialCap) return set_err(MPCD_ERR_CAPACITY, "reduction buffer too small");
-    k_reduce_partial<<<nb, kRedThreads, 0, c->stream>>>(cols, rows, K, maxMask, rowsPerBlock, c->partial);
-    k_reduce_final<<<1, kRedThreads, 0, c->stream>>>(c->partial, nb, K, maxMask, out);
+    k_reduce_partial<<<nb, kRedThreads, 0, c->stream>>>(cols, rows, K, maxMask, rowsPerBlock, c->partial); ++c->launches;
+    k_reduce_final<<<1, kRedThreads, 0, c->stream>>>(c->partial, nb, K, maxMask, out); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     return MPCD_OK;
 }
 
 // ---------------------------------------------------------------- phases
-int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo) {
+int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo, Prof* pf = nullptr) {
     BcWork& W = c->W;
     CUDA_TRY(cudaMemsetAsync(W.bitsX, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
     CUDA_TRY(cudaMemsetAsync(W.bitsY, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
     CUDA_TRY(cudaMemsetAsync(W.nEvents, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaMemsetAsync(W.ints, 0, sizeof(int) * 4, c->stream));
     k_stream_bc<<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp],
-                                                         cidStd, cidSrd, W, c->st);
-    k_word_counts<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount);
+                                                         cidStd, cidSrd, W, c->st); ++c->launches;
+    mark(c, pf, 0);
+    k_word_counts<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount); ++c->launches;
     int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix);
     if (rc) return rc;
-    k_wall_normals<<<1, kNormThreads, 0, c->stream>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st);
-    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, c->stream>>>(c->P, c->vb[c->xv], W, c->st);
+    k_wall_normals<<<1, kNormThreads, 0, c->stream>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st); ++c->launches;
+    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, c->stream>>>(c->P, c->vb[c->xv], W, c->st); ++c->launches;
     if (wantInfo)
-        k_wall_reduce<<<1, 32, 0, c->stream>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut);
+        k_wall_reduce<<<1, 32, 0, c->stream>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut); ++c->launches;
     CUDA_TRY(cudaGetLastError());
+    mark(c, pf, 1);
     return MPCD_OK;
 }
 
-int run_collide(mpcd_ctx* c, uint64_t seed) {
-    int rc = build_index(c, c->cidSrd, c->idxSrd);
+int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr) {
+    int rc = build_index(c, c->cidSrd, c->idxSrd, pf, 2);
     if (rc) return rc;
-    k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs);
+    k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs); ++c->launches;
+    mark(c, pf, 3);
     k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, c->signs, c->Nc,
-                                                                 c->vb[c->xv], c->st);
+                                                                 c->vb[c->xv], c->st); ++c->launches;
     if (c->P.keepMeanFlow) {
-        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols);
+        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
         if (rc) return rc;
-        k_sub_mean<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->red + 8);
+        k_sub_mean<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->red + 8); ++c->launches;
     }
     CUDA_TRY(cudaGetLastError());
+    mark(c, pf, 4);
     return MPCD_OK;
 }
 
 // reference fields of the current state + pdrive + EOS kick (depend on the reference only)
-int run_save_ref(mpcd_ctx* c) {
-    int rc = ensure_std_index(c);
+int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr) {
+    int rc = ensure_std_index(c, pf);
     if (rc) return rc;
     FieldsOut o{};
     o.N = c->refNi; o.Ux = c->refUx; o.Uy = c->refUy; o.Px = c->refPx; o.Py = c->refPy; o.T = c->refT;
     o.rho = c->refRho; o.Pkin = c->refPkin; o.Pvir = c->refPvir; o.P = c->refP;
     k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
-                                                                 c->P.rhoTarget, o);
-    k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw);
-    k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive);
-    k_eos<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdrive, c->eosX, c->eosY);
+                                                                 c->P.rhoTarget, o); ++c->launches;
+    k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw); ++c->launches;
+    k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive); ++c->launches;
+    k_eos<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdrive, c->eosX, c->eosY); ++c->launches;
     CUDA_TRY(cudaGetLastError());
+    mark(c, pf, 6);
     c->refValid = true;
     return MPCD_OK;
 }
 
-int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase) {
+int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) {
     if (!c->cidStdValid) {
-        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd);
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
         c->cidStdValid = true;
     }
-    int rc = ensure_std_index(c);
+    int rc = ensure_std_index(c, pf);
     if (rc) return rc;
     if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
     if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
     Layout& L = c->lay[mode];
     k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
-        seedBase, L.nZones, c->seeds);
+        seedBase, L.nZones, c->seeds); ++c->launches;
+    mark(c, pf, 7);
     CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
     ZoneArgs A{};
     A.P = c->P;
@@ -507,16 +532,17 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase) {
     A.zoneMoved = c->zoneMoved;
     A.zoneCorr = c->zoneCorr;
     A.st = c->st;
-    k_zone_pass<<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+    k_zone_pass<<<L.nZones, 32, c->zSmem, c->stream>>>(A); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     ZoneArgs B = A;
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
     B.nlocCap = c->ovNlocCap;
     B.arenaCap = c->ovArenaCap;
-    k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0));
+    k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
     CUDA_TRY(cudaGetLastError());
+    mark(c, pf, 8);
     c->xv ^= 1;
     c->idxStdValid = false;  // cid was updated for moved particles; positions changed
     c->srdCellsValid = false;
@@ -525,21 +551,22 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase) {
 
 // closure on the current (red) state; permute: write particles in (cell, id) order into the
 // other buffers (next step's layout); vrep: repaired velocities wanted
-int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats) {
+int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* pf = nullptr) {
     if (!c->refValid) return set_err(MPCD_ERR_STATE, "liquid closure needs a saved reference state (mpcd_save_ref)");
-    int rc = ensure_std_index(c);
+    int rc = ensure_std_index(c, pf);
     if (rc) return rc;
     RedFields rf{};
     k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
                                                                    c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
-                                                                   c->duRY, c->cols);
+                                                                   c->duRY, c->cols); ++c->launches;
     rc = reduce_cols(c, c->cols, c->Nc, 2, 0u, c->red);
     if (rc) return rc;
+    mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
     k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
         c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
         c->pidb[np], permute ? c->xb[nx ^ 1] : nullptr, permute ? c->vb[nx ^ 1] : nullptr,
-        permute ? c->pidb[np ^ 1] : nullptr, wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr);
+        permute ? c->pidb[np ^ 1] : nullptr, wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     if (wantStats) {
         // sum, max, sum, sum, max, sum, sum, sum, sum
@@ -549,8 +576,9 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats) {
     if (permute) {
         c->xv ^= 1;
         c->pp ^= 1;
-        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n);
+        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
         CUDA_TRY(cudaGetLastError());
+        mark(c, pf, 10);
         // the standard index stays valid (same cells, identity slots); per-slot cell ids and
         // SRD cells refer to the old layout
         c->cidStdValid = false;
@@ -757,7 +785,7 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
     if (n > 0) {
         CUDA_TRY(cudaMemcpyAsync(c->xb[0], x, sizeof(double2) * (size_t)n, kind, c->stream));
         CUDA_TRY(cudaMemcpyAsync(c->vb[0], v, sizeof(double2) * (size_t)n, kind, c->stream));
-        k_iota<<<blocks_for(n), kThreads, 0, c->stream>>>(c->pidb[0], (int)n);
+        k_iota<<<blocks_for(n), kThreads, 0, c->stream>>>(c->pidb[0], (int)n); ++c->launches;
         CUDA_TRY(cudaGetLastError());
     }
     invalidate_positions(c);
@@ -778,7 +806,7 @@ static int get_state_impl(mpcd_ctx* c, double* x, double* v, bool toHost) {
     if (c->n == 0) return MPCD_OK;
     double2* tx = c->xb[c->xv ^ 1];
     double2* tv = c->vb[c->xv ^ 1];
-    k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv);
+    k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (x) CUDA_TRY(cudaMemcpyAsync(x, tx, sizeof(double2) * (size_t)c->n, k, c->stream));
@@ -792,7 +820,7 @@ int mpcd_get_state_device(mpcd_ctx* c, double* x, double* v) { return get_state_
 int mpcd_stream(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
-    k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->vb[c->xv]);
+    k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->vb[c->xv]); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     invalidate_positions(c);
     return check_device(c);
@@ -821,13 +849,13 @@ int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
 int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
-    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift);
-    k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd);
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift); ++c->launches;
+    k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     c->srdCellsValid = true;
     if (cid_out && c->n > 0) {
         int* tmp = c->idxSrd.pos;  // scratch: particle-id order
-        k_int_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->cidSrd, c->pidb[c->pp], c->n, tmp);
+        k_int_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->cidSrd, c->pidb[c->pp], c->n, tmp); ++c->launches;
         CUDA_TRY(cudaMemcpyAsync(cid_out, tmp, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
     }
     return check_device(c);
@@ -849,7 +877,7 @@ int mpcd_srd_collide_cells(mpcd_ctx* c, const int32_t* cid, uint64_t seed) {
     if (c->n > 0) {
         int* tmp = c->idxSrd.pos;
         CUDA_TRY(cudaMemcpyAsync(tmp, cid, sizeof(int) * (size_t)c->n, cudaMemcpyHostToDevice, c->stream));
-        k_int_to_slots<<<blocks_for(c->n), kThreads, 0, c->stream>>>(tmp, c->pidb[c->pp], c->n, c->Nc, c->cidSrd, c->st);
+        k_int_to_slots<<<blocks_for(c->n), kThreads, 0, c->stream>>>(tmp, c->pidb[c->pp], c->n, c->Nc, c->cidSrd, c->st); ++c->launches;
         CUDA_TRY(cudaGetLastError());
         int rc = check_device(c);
         if (rc) return rc;
@@ -884,7 +912,7 @@ int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
     int rc = ensure_std_index(c);
     if (rc) return rc;
     const FieldsOut o = tmp_fields(c);
-    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], rho_target, o);
+    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], rho_target, o); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     rc = fields_to_host(c, o, out);
     if (rc) return rc;
@@ -983,7 +1011,7 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
         rc = ensure_std_index(c);
         if (rc) return rc;
         const FieldsOut o = tmp_fields(c);
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
         rc = fields_to_host(c, o, &detail->redFields);
         if (rc) return rc;
         CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1027,17 +1055,17 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
             // repaired state: positions unchanged, velocities = vrep
             if (detail->repairedX || detail->repairedV) {
                 k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vrep, c->pidb[c->pp], c->n,
-                                                                              c->xb[c->xv ^ 1], c->vb[c->xv ^ 1]);
+                                                                              c->xb[c->xv ^ 1], c->vb[c->xv ^ 1]); ++c->launches;
                 if (detail->repairedX) CUDA_TRY(cudaMemcpyAsync(detail->repairedX, c->xb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
                 if (detail->repairedV) CUDA_TRY(cudaMemcpyAsync(detail->repairedV, c->vb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
                 CUDA_TRY(cudaStreamSynchronize(c->stream));
             }
-            k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vrep, c->P.rhoTarget, o);
+            k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vrep, c->P.rhoTarget, o); ++c->launches;
             rc = fields_to_host(c, o, &detail->repairedFields);
             if (rc) return rc;
             CUDA_TRY(cudaStreamSynchronize(c->stream));
         }
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
         rc = fields_to_host(c, o, &detail->outFields);
         if (rc) return rc;
         rc = check_device(c);
@@ -1049,29 +1077,30 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
 
 // ---------------------------------------------------------------- the step
 static int count_metrics(mpcd_ctx* c, double* dst /* device: 3 doubles */) {
-    k_count_cols<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->P.highThr, c->P.lowThrBulk, c->cols);
+    k_count_cols<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->P.highThr, c->P.lowThrBulk, c->cols); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     return reduce_cols(c, c->cols, c->Nc, 3, 0u, dst);
 }
 
 // One iteration of the profiled benchmark loop (reference
 // src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:241-279) with its seeds.
-static int step_once(mpcd_ctx* c, int64_t step, bool metrics) {
+static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr) {
     const uint64_t s = (uint64_t)step;
     int rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
-    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift);
-    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics);
+    mark(c, pf, -1);
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift); ++c->launches;
+    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf);
     if (rc) return rc;
     c->cidStdValid = true;
     c->srdCellsValid = true;
     c->idxStdValid = false;
-    rc = run_collide(c, 433494437ULL + 10007ULL * s);
+    rc = run_collide(c, 433494437ULL + 10007ULL * s, pf);
     if (rc) return rc;
-    rc = run_save_ref(c);
+    rc = run_save_ref(c, pf);
     if (rc) return rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
-    rc = run_zone_pass(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s);
+    rc = run_zone_pass(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s, pf);
     if (rc) return rc;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
@@ -1081,7 +1110,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics) {
         if (rc) return rc;
         CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
     }
-    rc = run_zone_pass(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s);
+    rc = run_zone_pass(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s, pf);
     if (rc) return rc;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[4], c->stream));
@@ -1091,7 +1120,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics) {
         if (rc) return rc;
         CUDA_TRY(cudaEventRecord(c->ev[5], c->stream));
     }
-    rc = run_closure(c, true, false, metrics);
+    rc = run_closure(c, true, false, metrics, pf);
     if (rc) return rc;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[6], c->stream));
@@ -1099,13 +1128,13 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics) {
         if (rc) return rc;
         rc = reduce_cols(c, c->pdrive, c->Nc, 1, 0u, c->red + 17);
         if (rc) return rc;
-        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols);
+        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 26);
         if (rc) return rc;
         FieldsOut o{};
         o.Ux = c->fieldTmp;
         o.Uy = c->fieldTmp + c->Nc;
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o);
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
         rc = reduce_cols(c, c->fieldTmp, c->Nc, 1, 0u, c->red + 29);
         if (rc) return rc;
         rc = reduce_cols(c, c->fieldTmp + c->Nc, c->Nc, 1, 0u, c->red + 30);
@@ -1189,6 +1218,75 @@ int mpcd_step_metrics(mpcd_ctx* c, mpcd_step_metrics_c* out) {
     if (!c || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
     *out = c->last;
     return MPCD_OK;
+}
+
+
+int mpcd_step_timed(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* device_seconds) {
+    if (!c || !device_seconds) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaEventRecord(a, c->stream));
+    int rc = MPCD_OK;
+    for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) rc = step_once(c, step0 + k, false);
+    CUDA_TRY(cudaEventRecord(b, c->stream));
+    CUDA_TRY(cudaEventSynchronize(b));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    *device_seconds = ms * 1e-3;
+    return check_device(c);
+}
+
+int64_t mpcd_launch_count(mpcd_ctx* c) { return c ? c->launches : 0; }
+
+
+// Per-phase device time over nsteps steps (events at phase boundaries on the context's
+// stream; one synchronisation per step). phase_seconds[k] accumulates phase k:
+// 0 stream+BC, 1 thermal walls, 2 SRD cell index, 3 SRD sign stream, 4 collision,
+// 5 standard cell index (3 per step), 6 reference fields + pdrive + EOS kick,
+// 7 zone seeds (2), 8 zone passes (2), 9 closure cells + beta reduction, 10 kick + re-sort.
+int mpcd_step_profile(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* phase_seconds, int nphase) {
+    if (!c || !phase_seconds) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (int k = 0; k < nphase; ++k) phase_seconds[k] = 0.0;
+    Prof pf;
+    for (auto& e : pf.ev) CUDA_TRY(cudaEventCreate(&e));
+    int rc = MPCD_OK;
+    for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) {
+        pf.n = 0;
+        rc = step_once(c, step0 + k, false, &pf);
+        if (rc) break;
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int i = 1; i < pf.n; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, pf.ev[i - 1], pf.ev[i]);
+            const int lab = pf.label[i];
+            if (lab >= 0 && lab < nphase) phase_seconds[lab] += ms * 1e-3;
+        }
+    }
+    for (auto& e : pf.ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    return check_device(c);
+}
+
+
+// Page-locked host memory for callers that stage states (the end-to-end benchmark).
+void* mpcd_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(MPCD_ERR_CUDA, "cudaMallocHost failed");
+        return nullptr;
+    }
+    return p;
+}
+void mpcd_host_free(void* p) {
+    if (p) cudaFreeHost(p);
 }
 
 }  // extern "C"

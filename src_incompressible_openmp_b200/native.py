@@ -70,6 +70,11 @@ def lib():
         "mpcd_zone_owner_map": ([C.c_void_p, C.c_int32, _ip], C.c_int),
         "mpcd_step": ([C.c_void_p, C.c_int64, C.c_int64, P(_abi.StepMetricsC)], C.c_int),
         "mpcd_step_metrics": ([C.c_void_p, P(_abi.StepMetricsC)], C.c_int),
+        "mpcd_step_timed": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
+        "mpcd_step_profile": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double), C.c_int], C.c_int),
+        "mpcd_launch_count": ([C.c_void_p], C.c_int64),
+        "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
+        "mpcd_host_free": ([C.c_void_p], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -77,6 +82,21 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+class PinnedArray:
+    """A float64 numpy view of page-locked host memory (freed with close())."""
+
+    def __init__(self, count):
+        self.ptr = lib().mpcd_host_alloc(8 * count)
+        if not self.ptr:
+            raise MpcdError(2, lib().mpcd_last_error().decode())
+        self.array = np.ctypeslib.as_array((C.c_double * count).from_address(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            lib().mpcd_host_free(self.ptr)
+            self.ptr = None
 
 
 def device_available():
@@ -141,9 +161,10 @@ class Context:
         v = np.ascontiguousarray(v, np.float64)
         _check(lib().mpcd_set_state(self.h, x, v, self.n))
 
-    def get_state(self):
-        x = np.empty(2 * self.n)
-        v = np.empty(2 * self.n)
+    def get_state(self, x=None, v=None):
+        """Particle-id-ordered copies of x and v (into the given float64 arrays if any)."""
+        x = np.empty(2 * self.n) if x is None else x
+        v = np.empty(2 * self.n) if v is None else v
         _check(lib().mpcd_get_state(self.h, x, v))
         return x, v
 
@@ -216,6 +237,24 @@ class Context:
         o = np.zeros(self.Nc, np.int32)
         _check(lib().mpcd_zone_owner_map(self.h, _abi.LAYOUT_MODES[mode], o))
         return o
+
+    PHASES = ("stream_bc", "walls", "srd_index", "srd_signs", "collide", "cell_index", "ref_fields",
+              "zone_seeds", "zone_pass", "closure_cells", "kick_resort")
+
+    def step_timed(self, step0, nsteps):
+        """Runs the steps; returns device seconds (CUDA events on the context's stream)."""
+        t = C.c_double()
+        _check(lib().mpcd_step_timed(self.h, step0, nsteps, C.byref(t)))
+        return t.value
+
+    def step_profile(self, step0, nsteps):
+        """Runs the steps with phase-boundary events; returns {phase: device seconds}."""
+        arr = (C.c_double * len(self.PHASES))()
+        _check(lib().mpcd_step_profile(self.h, step0, nsteps, arr, len(self.PHASES)))
+        return dict(zip(self.PHASES, list(arr)))
+
+    def launch_count(self):
+        return int(lib().mpcd_launch_count(self.h))
 
     def step(self, step0, nsteps, metrics=False):
         m = _abi.StepMetricsC() if metrics else None
