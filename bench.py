@@ -34,7 +34,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200: FP64 plain vs FP32+learned closure, at ≤1% profile err"
 UNIT = "particle-steps/s"
-WORKLOAD = dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10)
+WORKLOADS = {
+    # the benchmark workload: the large plain-FP64 channel
+    "channel_2048x512_ppc10": dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10),
+    # a smaller channel of the same physics, for profiler captures (state 47 MB)
+    "channel_512x256_ppc10": dict(name="channel_512x256_ppc10", Nx=512, Ny=256, ppc=10),
+}
+WORKLOAD = WORKLOADS["channel_2048x512_ppc10"]
 DATA = "synthetic: seeded uniform positions, Maxwellian velocities (kT=1, mean removed)"
 # algorithmic bytes per particle (P) and per cell (C) of one launch of each phase's main
 # kernel, FP64 plain form ("Roofline")
@@ -145,7 +151,7 @@ def config_dict(p, world):
         "workload": WORKLOAD["name"], "Nx": p["Nx"], "Ny": p["Ny"], "particles_per_cell": WORKLOAD["ppc"],
         "n_particles": p["n"], "n_cells": p["Nc"], "form": "plain_f64", "dt": p["dt"],
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        "l2_policy": "state (378 MB) larger than L2 (126 MB); no flush",
+        "l2_policy": f"state ({36 * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
     }
 
 
@@ -326,7 +332,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel_2048x512_ppc10")
     args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

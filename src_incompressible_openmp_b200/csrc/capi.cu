@@ -93,8 +93,14 @@ struct mpcd_ctx {
     int nwords = 0;
     int bcBlocks = 0;
     double* wallOut = nullptr;  // 9 doubles
-    // collision
-    uint8_t* signs = nullptr;
+    // collision: rotation-sign streams, double-buffered; step s+1's stream is generated on a
+    // side stream while step s's zone passes run
+    uint8_t* signs = nullptr;       // synchronous use (phase API)
+    uint8_t* signsBuf[2] = {nullptr, nullptr};
+    int64_t signsStep[2] = {-1, -1};
+    cudaStream_t side = nullptr;
+    cudaEvent_t signsReady[2] = {nullptr, nullptr};
+    cudaEvent_t collDone = nullptr;
     // zones
     Layout lay[3];  // base, shifted, single_full
     uint64_t* seeds = nullptr;
@@ -105,9 +111,9 @@ struct mpcd_ctx {
     char* ovMem = nullptr;
     size_t ovPerBlock = 0;
     int ovBlocks = 2;
-    int zMaxCells = 0, zWinCap = 0, zNlocCap = 0, zArenaCap = 0;
+    int zMaxCells = 0, zWinCap = 0, zArenaCap = 0;
     size_t zSmem = 0;
-    int ovMaxCells = 0, ovWinCap = 0, ovNlocCap = 0, ovArenaCap = 0;
+    int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0;
     double* passOut = nullptr;  // 4 doubles
     // closure
     int* mask = nullptr;
@@ -162,6 +168,7 @@ void mark(mpcd_ctx* c, Prof* p, int label) {
 
 int check_device(mpcd_ctx* c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->side) CUDA_TRY(cudaStreamSynchronize(c->side));
     CUDA_TRY(cudaMemcpy(c->hst, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost));
     if (c->hst->code != 0) {
         const int code = c->hst->code;
@@ -460,12 +467,26 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     return MPCD_OK;
 }
 
-int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr) {
+// step < 0: phase API (sign stream generated here, synchronously); otherwise the stream of
+// that step from the double buffer (generated ahead on the side stream when possible)
+int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -1) {
     int rc = build_index(c, c->cidSrd, c->idxSrd, pf, 2);
     if (rc) return rc;
-    k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs); ++c->launches;
+    const uint8_t* signs = c->signs;
+    if (step < 0) {
+        k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs); ++c->launches;
+    } else {
+        const int b = (int)(step & 1);
+        if (c->signsStep[b] != step) {
+            k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signsBuf[b]); ++c->launches;
+            c->signsStep[b] = step;
+        } else {
+            CUDA_TRY(cudaStreamWaitEvent(c->stream, c->signsReady[b], 0));
+        }
+        signs = c->signsBuf[b];
+    }
     mark(c, pf, 3);
-    k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, c->signs, c->Nc,
+    k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc,
                                                                  c->vb[c->xv], c->st); ++c->launches;
     if (c->P.keepMeanFlow) {
         k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
@@ -475,6 +496,18 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr) {
     }
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 4);
+    if (step >= 0) {
+        // generate the next step's sign stream on the side stream, after this collision
+        // (which is the last reader of the buffer it overwrites' previous contents)
+        const int b = (int)((step + 1) & 1);
+        CUDA_TRY(cudaEventRecord(c->collDone, c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->side, c->collDone, 0));
+        const uint64_t next = 433494437ULL + 10007ULL * (uint64_t)(step + 1);
+        k_srd_signs<<<1, kSignThreads, 0, c->side>>>(next, c->Nc, c->signsBuf[b]); ++c->launches;
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(c->signsReady[b], c->side));
+        c->signsStep[b] = step + 1;
+    }
     return MPCD_OK;
 }
 
@@ -510,13 +543,15 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
         seedBase, L.nZones, c->seeds); ++c->launches;
     mark(c, pf, 7);
     CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
+    // out of place: outputs start as a copy of the inputs; zones write what they change
+    CUDA_TRY(cudaMemcpyAsync(c->xb[c->xv ^ 1], c->xb[c->xv], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->vb[c->xv ^ 1], c->vb[c->xv], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
     ZoneArgs A{};
     A.P = c->P;
     A.rects = L.rects;
     A.owner = L.owner;
     A.start = c->idxStd.start;
     A.slots = c->idxStd.slots;
-    A.xin = c->xb[c->xv];
     A.vin = c->vb[c->xv];
     A.xout = c->xb[c->xv ^ 1];
     A.vout = c->vb[c->xv ^ 1];
@@ -525,7 +560,6 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     A.nZones = L.nZones;
     A.maxCells = c->zMaxCells;
     A.winCap = c->zWinCap;
-    A.nlocCap = c->zNlocCap;
     A.arenaCap = c->zArenaCap;
     A.overflow = c->overflow;
     A.nOverflow = c->nOverflow;
@@ -537,7 +571,6 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     ZoneArgs B = A;
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
-    B.nlocCap = c->ovNlocCap;
     B.arenaCap = c->ovArenaCap;
     k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock); ++c->launches;
     k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
@@ -625,6 +658,12 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     }
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    if (c->side) cudaStreamSynchronize(c->side);
+    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone})
+        if (e) cudaEventDestroy(e);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->signsBuf[0]) cudaFree(c->signsBuf[0]);
+    if (c->signsBuf[1]) cudaFree(c->signsBuf[1]);
     if (c->hst) cudaFreeHost(c->hst);
     if (c->hred) cudaFreeHost(c->hred);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -693,6 +732,13 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     ALLOC(W.srdShift, 2);
     ALLOC(c->wallOut, kWallDoubles);
     ALLOC(c->signs, (size_t)Nc);
+    ALLOC(c->signsBuf[0], (size_t)Nc);
+    ALLOC(c->signsBuf[1], (size_t)Nc);
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->signsReady[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->signsReady[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->collDone, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_err(MPCD_ERR_CUDA, "side stream"));
     // zone layouts
     build_layout(*params, MPCD_LAYOUT_BASE, c->lay[0]);
     build_layout(*params, MPCD_LAYOUT_SHIFTED, c->lay[1]);
@@ -725,22 +771,24 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
         c->zMaxCells = std::max(1, area);
         c->zWinCap = (tx + 4) * (ty + 4);
         const double g = std::max(1.0, params->gamma);
-        c->zNlocCap = ((int)std::ceil(1.6 * g * area) + 64 + 31) / 32 * 32;
-        c->zArenaCap = c->zNlocCap + 1024;
-        c->zSmem = ZoneMem<uint16_t>::bytes(c->zMaxCells, c->zWinCap, c->zNlocCap, c->zArenaCap);
-        if (c->zNlocCap > 65535 || c->zSmem > 200 * 1024) {
+        // arena for the lists a zone materialises (receivers, donors): ~0.8 of the zone's
+        // particles covers typical passes; a zone that runs out is re-run on the overflow path
+        c->zArenaCap = ((int)std::ceil(0.8 * g * area) + 128 + 31) / 32 * 32;
+        c->zSmem = ZoneMem::bytes(c->zMaxCells, c->zWinCap, c->zArenaCap);
+        if (c->zSmem > 200 * 1024) {
             // too large for the shared-memory path: every zone takes the overflow path
             c->zMaxCells = 0;
-            c->zSmem = ZoneMem<uint16_t>::bytes(0, 0, 0, 0);
+            c->zSmem = ZoneMem::bytes(0, 0, 0);
         }
         if (c->zSmem > 48 * 1024 &&
             cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess)
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
         c->ovWinCap = (maxTX + 4) * (maxTY + 4);
-        c->ovNlocCap = std::max(1, params->zoneSingleFullDomainMode ? n : std::min(n, std::max(65536, 16 * std::max(c->zNlocCap, 1))));
-        c->ovArenaCap = c->ovNlocCap + 4096;
-        c->ovPerBlock = (ZoneMem<uint32_t>::bytes(c->ovMaxCells, c->ovWinCap, c->ovNlocCap, c->ovArenaCap) + 255) / 256 * 256;
+        // every materialised list fits in (particles of the zone + 4 per cell) entries after
+        // compaction; bound the zone's particles by all particles
+        c->ovArenaCap = (int)std::min<int64_t>((int64_t)n + 4LL * maxArea + 4096, (1LL << 31) - 1);
+        c->ovPerBlock = (ZoneMem::bytes(c->ovMaxCells, c->ovWinCap, c->ovArenaCap) + 255) / 256 * 256;
         ALLOC(c->ovMem, c->ovPerBlock * (size_t)c->ovBlocks);
     }
     // closure
@@ -1095,7 +1143,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     c->cidStdValid = true;
     c->srdCellsValid = true;
     c->idxStdValid = false;
-    rc = run_collide(c, 433494437ULL + 10007ULL * s, pf);
+    rc = run_collide(c, 433494437ULL + 10007ULL * s, pf, step);
     if (rc) return rc;
     rc = run_save_ref(c, pf);
     if (rc) return rc;

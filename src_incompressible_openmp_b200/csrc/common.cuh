@@ -112,8 +112,9 @@ __host__ __device__ __forceinline__ uint64_t mt_seed_next(uint64_t prev, int i) 
     return 6364136223846793005ULL * (prev ^ (prev >> 62)) + (uint64_t)i;
 }
 
-// Out-of-place twist of a 312-word state A into B by one warp (A is left intact).
-__device__ __forceinline__ void mt_twist_warp(const uint64_t* A, uint64_t* B, int lane) {
+// Out-of-place twist of a 312-word state A into B by one warp (A is left intact). Not
+// inlined: it is reached from every RNG call site and would otherwise bloat the zone kernel.
+__device__ __noinline__ void mt_twist_warp(const uint64_t* A, uint64_t* B, int lane) {
     for (int i = lane; i < kMtN - kMtM; i += kWarp) B[i] = A[i + kMtM] ^ mt_mix(A[i], A[i + 1]);
     __syncwarp();
     for (int i = kMtN - kMtM + lane; i < kMtN - 1; i += kWarp) B[i] = B[i - (kMtN - kMtM)] ^ mt_mix(A[i], A[i + 1]);
@@ -191,6 +192,9 @@ struct WarpMt {
     }
 };
 
+// log_cr as an out-of-line device function (shared by all call sites)
+__device__ __noinline__ double log_cr_dev(double x) { return mpcd_dd::log_cr(x); }
+
 // normal_distribution<double>(0, 1): Marsaglia polar method with one cached deviate
 struct PolarNormal {
     double saved;
@@ -207,7 +211,7 @@ struct PolarNormal {
             y = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
             r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
         } while (r2 > 1.0 || r2 == 0.0);
-        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, mpcd_dd::log_cr(r2)), r2));
+        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log_cr_dev(r2)), r2));
         saved = __dmul_rn(x, mult);
         has = 1;
         return __dmul_rn(y, mult);

@@ -148,7 +148,11 @@ MPCD_HD double log_cr(double x) {
     const double c = (double)j * 0.0078125;
     const double num = mant - c;                  // exact (Sterbenz)
     const dd den = two_sum(mant, c);              // exact
-    const dd u = dd_div(dd{num, 0.0}, den);       // |u| < 2^-8.4
+    // u = num / den to ~2^-100: one division for the reciprocal, then an fma residual
+    const double inv = 1.0 / den.hi;
+    const double uh = num * inv;
+    const double res = fma_(-uh, den.hi, num) - uh * den.lo;
+    const dd u = fast_two_sum(uh, res * inv);     // |u| < 2^-8.4
     // u^2 and u^3 to ~2^-100 relative
     const dd u2 = dd_mul(u, u);
     const dd u3 = dd_mul(u2, u);

@@ -110,10 +110,9 @@ __global__ void k_cell_sort(const uint64_t* __restrict__ start, int Nc, const in
     constexpr int kLocal = 48;
     if (m <= kLocal) {
         uint64_t key[kLocal];
-        for (int i = 0; i < m; ++i) {
-            const int s = slots[a + i];
-            key[i] = ((uint64_t)(uint32_t)pid[s] << 32) | (uint32_t)s;
-        }
+        int sl[kLocal];
+        for (int i = 0; i < m; ++i) sl[i] = slots[a + i];
+        for (int i = 0; i < m; ++i) key[i] = ((uint64_t)(uint32_t)pid[sl[i]] << 32) | (uint32_t)sl[i];
         for (int i = 1; i < m; ++i) {
             const uint64_t v = key[i];
             int j = i;

@@ -15,20 +15,30 @@
 // The merge writes each particle from the LAST zone whose rectangle holds the particle's
 // input cell (zone ids grow in merge order), i.e. from ownerMap[input cell]. Shifted layouts
 // overlap (tiles start at 0 and at tile/2, src/zone_pass.cpp:160-221), so every zone
-// processes its full rectangle but writes only the particles it owns, out of place.
+// processes its full rectangle and writes only the particles it owns. The pass is out of
+// place: the output buffers start as a copy of the input, and a zone writes only what it
+// changes (positions of moved particles, velocities of corrected cells).
 //
-// Warp discipline: every lane runs the same control flow with identical scalar values
-// (the RNG stream is warp-uniform); lane-parallel sections are candidate evaluation,
-// position sampling, list copies and the final per-particle writes. Shared-memory scalars
-// written by lane 0 are followed by __syncwarp() before any lane reads them.
+// Lists: a cell's list starts as its input segment of the cell index (ascending id) and
+// stays implicit -- a head offset into that segment -- until the cell receives particles or
+// is shuffled; then it is materialised in a small arena. List entries encode
+// (input cell << 20 | position in its input segment), so a particle's slot is read from the
+// cell index when needed.
+//
+// Warp discipline: every lane runs the same control flow with identical scalar values (the
+// RNG stream is warp-uniform); lane-parallel sections are candidate evaluation, position
+// sampling, list copies and the final momentum correction. Shared-memory scalars written by
+// lane 0 are followed by __syncwarp() before any lane reads them.
 #pragma once
 
 #include "common.cuh"
 
 namespace mpcd_dev {
 
-constexpr uint8_t kPMoved = 1, kPOwned = 2;
-constexpr uint8_t kCRecv = 1, kCBulkBulk = 2, kCSkip = 4, kCBulkBefore = 8, kCChanged = 16, kCApply = 32;
+// cell flags
+constexpr uint8_t kCRecv = 1, kCBulkBulk = 2, kCSkip = 4, kCBulkBefore = 8, kCChanged = 16, kCOwned = 32,
+                  kCMat = 64;
+constexpr int kEntryShift = 20;  // entry = cell << 20 | position (cells < 4096, positions < 2^20)
 
 struct ZoneArgs {
     DevParams P;
@@ -36,14 +46,13 @@ struct ZoneArgs {
     const int* owner;         // ownerMap of the layout
     const uint64_t* start;    // cell index of the pass input (packed starts)
     const int* slots;
-    const double2* xin;
     const double2* vin;
-    double2* xout;
-    double2* vout;
+    double2* xout;            // pre-filled with the input positions
+    double2* vout;            // pre-filled with the input velocities
     int* cid;                 // standard-grid cell per slot; moved owned particles updated
     const uint64_t* seeds;    // seeded MT19937-64 state per zone (312 words each)
     int nZones;
-    int maxCells, winCap, nlocCap, arenaCap;  // capacities of the per-zone working set
+    int maxCells, winCap, arenaCap;  // capacities of the per-zone working set
     int* overflow;            // zones left to the overflow kernel
     int* nOverflow;
     int2* zoneMoved;          // (dense, sparse) per zone
@@ -52,49 +61,42 @@ struct ZoneArgs {
 };
 
 // Working set of one zone; carved from shared memory (fast path) or global memory.
-template <typename Idx>
 struct ZoneMem {
-    uint64_t* mt;      // 2 * 312
-    double* lowA;      // maxCells (reused as du.x at the end)
-    double* highA;     // maxCells (reused as du.y)
-    double* nsm;       // (TX+2)(TY+2) <= winCap (reused as dU2)
-    int* slot;         // nlocCap
-    int* win;          // winCap: pass-input counts around the zone (-1 = outside)
-    int* cnt;          // maxCells: live counts
-    int* cnt0;         // maxCells
-    int* base0;        // maxCells: first local index of the cell's input list
-    int* abase;        // maxCells: list storage start in the arena
-    int* head;         // maxCells
-    int* len;          // maxCells
-    int* cap;          // maxCells
-    Idx* arena;        // arenaCap
-    Idx* scratch;      // nlocCap: compaction buffer, then final cell per local particle
-    uint8_t* pflags;   // nlocCap
-    uint8_t* cflags;   // maxCells
-    Idx* list;         // maxCells: dense / low cell order
+    uint64_t* mt;      // 312: MT19937-64 state
+    uint64_t* carry;   // 64: untwisted words of the previous block still to be drawn
+    double* nsm;       // (TX+2)(TY+2): smoothed occupancy; reused for dU2 at the end
+    int* win;          // (TX+4)(TY+4): pass-input counts around the zone (-1 = outside)
+    int* gstart;       // cell: start of its input segment in the cell index
+    int* cnt;          // cell: live count
+    int* cnt0;         // cell: input count
+    int* head;         // cell: list head (implicit: offset into the input segment)
+    int* len;          // cell
+    int* abase;        // cell: arena start of a materialised list
+    int* cap;          // cell: arena capacity of a materialised list
+    uint8_t* cflags;   // cell
+    uint16_t* list;    // cell: dense / low cell order
+    uint16_t* order;   // cell: arena order of materialised lists (compaction)
+    uint32_t* arena;   // arenaCap
     int* small;        // 128 ints: candidates, targets, receivers, donors
     double* smallD;    // 16 doubles: donor scores
 
-    __host__ __device__ static size_t bytes(int maxCells, int winCap, int nlocCap, int arenaCap) {
+    __host__ __device__ static size_t bytes(int maxCells, int winCap, int arenaCap) {
         size_t b = 0;
         auto add = [&](size_t n, size_t a) { b = (b + a - 1) / a * a + n; };
-        add(2 * kMtN * 8, 8);
-        add((size_t)maxCells * 8, 8);
-        add((size_t)maxCells * 8, 8);
+        add((size_t)kMtN * 8, 8);
+        add(64 * 8, 8);
         add((size_t)winCap * 8, 8);
-        add((size_t)nlocCap * 4, 4);
         add((size_t)winCap * 4, 4);
         for (int k = 0; k < 7; ++k) add((size_t)maxCells * 4, 4);
-        add((size_t)arenaCap * sizeof(Idx), sizeof(Idx));
-        add((size_t)nlocCap * sizeof(Idx), sizeof(Idx));
-        add((size_t)nlocCap, 1);
         add((size_t)maxCells, 1);
-        add((size_t)maxCells * sizeof(Idx), sizeof(Idx));
+        add((size_t)maxCells * 2, 2);
+        add((size_t)maxCells * 2, 2);
+        add((size_t)arenaCap * 4, 4);
         add(128 * 4, 4);
         add(16 * 8, 8);
         return (b + 15) / 16 * 16;
     }
-    __device__ void carve(char* base, int maxCells, int winCap, int nlocCap, int arenaCap) {
+    __device__ void carve(char* base, int maxCells, int winCap, int arenaCap) {
         size_t b = 0;
         auto take = [&](size_t n, size_t a) {
             b = (b + a - 1) / a * a;
@@ -102,40 +104,176 @@ struct ZoneMem {
             b += n;
             return p;
         };
-        mt = (uint64_t*)take(2 * kMtN * 8, 8);
-        lowA = (double*)take((size_t)maxCells * 8, 8);
-        highA = (double*)take((size_t)maxCells * 8, 8);
+        mt = (uint64_t*)take((size_t)kMtN * 8, 8);
+        carry = (uint64_t*)take(64 * 8, 8);
         nsm = (double*)take((size_t)winCap * 8, 8);
-        slot = (int*)take((size_t)nlocCap * 4, 4);
         win = (int*)take((size_t)winCap * 4, 4);
+        gstart = (int*)take((size_t)maxCells * 4, 4);
         cnt = (int*)take((size_t)maxCells * 4, 4);
         cnt0 = (int*)take((size_t)maxCells * 4, 4);
-        base0 = (int*)take((size_t)maxCells * 4, 4);
-        abase = (int*)take((size_t)maxCells * 4, 4);
         head = (int*)take((size_t)maxCells * 4, 4);
         len = (int*)take((size_t)maxCells * 4, 4);
+        abase = (int*)take((size_t)maxCells * 4, 4);
         cap = (int*)take((size_t)maxCells * 4, 4);
-        arena = (Idx*)take((size_t)arenaCap * sizeof(Idx), sizeof(Idx));
-        scratch = (Idx*)take((size_t)nlocCap * sizeof(Idx), sizeof(Idx));
-        pflags = (uint8_t*)take((size_t)nlocCap, 1);
         cflags = (uint8_t*)take((size_t)maxCells, 1);
-        list = (Idx*)take((size_t)maxCells * sizeof(Idx), sizeof(Idx));
+        list = (uint16_t*)take((size_t)maxCells * 2, 2);
+        order = (uint16_t*)take((size_t)maxCells * 2, 2);
+        arena = (uint32_t*)take((size_t)arenaCap * 4, 4);
         small = (int*)take(128 * 4, 4);
         smallD = (double*)take(16 * 8, 8);
     }
 };
 
+// In-place twist of a 312-word MT19937-64 state by one warp (reads of each half are staged
+// in registers before its writes).
+__device__ __noinline__ void mt_twist_inplace_warp(uint64_t* A, int lane) {
+    uint64_t nv[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int i = lane + k * kWarp;
+        nv[k] = (i < kMtN - kMtM) ? (A[i + kMtM] ^ mt_mix(A[i], A[i + 1])) : 0ULL;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int i = lane + k * kWarp;
+        if (i < kMtN - kMtM) A[i] = nv[k];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int i = kMtN - kMtM + lane + k * kWarp;
+        nv[k] = 0ULL;
+        if (i < kMtN - 1) nv[k] = A[i - (kMtN - kMtM)] ^ mt_mix(A[i], A[i + 1]);
+        else if (i == kMtN - 1) nv[k] = A[kMtM - 1] ^ mt_mix(A[kMtN - 1], A[0]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int i = kMtN - kMtM + lane + k * kWarp;
+        if (i < kMtN) A[i] = nv[k];
+    }
+    __syncwarp();
+}
+
+// Warp-uniform MT19937-64 stream with a single state buffer. Batches of up to 64 draws
+// may cross a block boundary: the words left in the old block move to `carry` first.
+struct ZoneMt {
+    uint64_t* buf;
+    uint64_t* carry;
+    int pos;     // next draw: carry[ncarry + pos] if pos < 0, else buf[pos]
+    int ncarry;
+    int lane;
+
+    __device__ __forceinline__ void init(uint64_t* b, uint64_t* c, int lane_) {
+        buf = b;
+        carry = c;
+        pos = kMtN;
+        ncarry = 0;
+        lane = lane_;
+    }
+    __device__ __forceinline__ void ensure(int k) {  // k <= 64
+        if (pos + k <= kMtN) return;
+        const int left = kMtN - pos;  // 0..63 words still to draw from the old block
+        for (int i = lane; i < left; i += kWarp) carry[i] = buf[pos + i];
+        __syncwarp();
+        mt_twist_inplace_warp(buf, lane);
+        ncarry = left;
+        pos = -left;
+    }
+    __device__ __forceinline__ uint64_t peek(int i) const {
+        const int j = pos + i;
+        return mt_temper((j < 0) ? carry[ncarry + j] : buf[j]);
+    }
+    __device__ __forceinline__ void consume(int k) { pos += k; }
+    __device__ __forceinline__ uint64_t next() {
+        ensure(1);
+        const uint64_t u = peek(0);
+        consume(1);
+        return u;
+    }
+    __device__ __forceinline__ double u01() { return canon(next()); }
+    __device__ __forceinline__ uint64_t uint_in(uint64_t lo, uint64_t hi) {
+        const uint64_t range = hi - lo + 1ULL;
+        uint64_t u = next();
+        uint64_t low = u * range;
+        uint64_t high = __umul64hi(u, range);
+        if (low < range) {
+            const uint64_t thr = (0ULL - range) % range;
+            while (low < thr) {
+                u = next();
+                low = u * range;
+                high = __umul64hi(u, range);
+            }
+        }
+        return high + lo;
+    }
+};
+
+// std::shuffle of m entries at a (warp-uniform; lane 0 performs the swaps)
+template <typename T>
+__device__ __forceinline__ void zone_shuffle(T* a, int m, ZoneMt& r, int lane) {
+    if (m <= 0) return;
+    int i = 1;
+    if ((m % 2) == 0) {
+        const int j = (int)r.uint_in(0, 1);
+        if (lane == 0) {
+            const T t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+        ++i;
+    }
+    while (i != m) {
+        const uint64_t sr = (uint64_t)i + 1ULL;
+        const uint64_t x = r.uint_in(0, sr * (sr + 1ULL) - 1ULL);
+        const int p1 = (int)(x / (sr + 1ULL)), p2 = (int)(x % (sr + 1ULL));
+        if (lane == 0) {
+            T t = a[i];
+            a[i] = a[p1];
+            a[p1] = t;
+            t = a[i + 1];
+            a[i + 1] = a[p2];
+            a[p2] = t;
+        }
+        i += 2;
+    }
+    __syncwarp();
+}
+
+// polar-method normal deviate (libstdc++ normal_distribution), one cached value
+struct ZoneNormal {
+    double saved;
+    int has;
+    __device__ __forceinline__ double next(ZoneMt& r) {
+        if (has) {
+            has = 0;
+            return saved;
+        }
+        double x, y, r2;
+        do {
+            x = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
+            y = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
+            r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+        } while (r2 > 1.0 || r2 == 0.0);
+        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log_cr_dev(r2)), r2));
+        saved = __dmul_rn(x, mult);
+        has = 1;
+        return __dmul_rn(y, mult);
+    }
+};
+
 // Scalar (warp-uniform) state of one zone.
-template <typename Idx>
 struct ZoneState {
-    ZoneMem<Idx> M;
-    WarpMt rng;
+    ZoneMem M;
+    ZoneMt rng;
     const ZoneArgs* A;
     int lane, zone;
-    int xs, xe, ys, ye, TX, TY, nl, WY;  // rectangle, sizes, window height
-    int nloc, arenaTop;
+    int xs, xe, ys, ye, TX, TY, nl, WY;
+    int arenaTop, arenaCap;
     int movedDense, movedSparse;
-    bool failed;
+    bool failed;   // capacity exhausted: the zone is handed to the overflow path
+    bool fatal;    // a device error was raised
 
     __device__ __forceinline__ const DevParams& P() const { return A->P; }
     __device__ __forceinline__ bool in_zone(int ix, int iy) const { return ix >= xs && ix < xe && iy >= ys && iy < ye; }
@@ -143,7 +281,6 @@ struct ZoneState {
     __device__ __forceinline__ int gx_of(int l) const { return xs + l / TY; }
     __device__ __forceinline__ int gy_of(int l) const { return ys + l % TY; }
 
-    // pass-input or live count of an in-range cell within two cells of the zone
     __device__ __forceinline__ int cnt_at(int ix, int iy) const {
         if (in_zone(ix, iy)) return M.cnt[loc(ix, iy)];
         int wx = ix - (xs - 2), wy = iy - (ys - 2);
@@ -161,7 +298,6 @@ struct ZoneState {
         if (ly >= TY + 2) ly -= P().Ny;
         return lx * (TY + 2) + ly;
     }
-    // src/zone_pass.cpp:246-261
     __device__ __forceinline__ bool shift_index(int iy, int ix, int dy, int dx, int& jy, int& jx) const {
         jy = iy + dy;
         if (P().pery) jy = wrap_index(jy, P().Ny);
@@ -171,7 +307,6 @@ struct ZoneState {
         else if (jx < 0 || jx >= P().Nx) return false;
         return true;
     }
-    // src/zone_pass.cpp:229-244 -> index into the 5x5 step tables (-1 if outside)
     __device__ __forceinline__ int step_index(int sx, int sy, int tx, int ty, int& ddx, int& ddy) const {
         int a = tx - sx, b = ty - sy;
         if (P().perx) {
@@ -187,6 +322,27 @@ struct ZoneState {
         if (a < -2 || a > 2 || b < -2 || b > 2) return -1;
         return (a + 2) + 5 * (b + 2);
     }
+
+    // threshold maps (src/zone_pass.cpp:321-345, :715-725) from the cell's bulk flag at
+    // the last map build and the smoothed occupancy then
+    __device__ __forceinline__ double frac(int l) const {
+        const DevParams& p = P();
+        if (!p.useLFF) return 1.0;
+        const double fraw = __ddiv_rn(M.nsm[nsm_index(gx_of(l), gy_of(l))], smax(p.gamma, 1e-12));
+        const double g = __dmul_rn(p.fluidFracGain, fraw);
+        return (g < 0.0) ? 0.0 : ((1.0 < g) ? 1.0 : g);
+    }
+    __device__ __forceinline__ double map_low(int l) const {
+        const DevParams& p = P();
+        if (M.cflags[l] & kCBulkBefore) return p.lowThrBulk;
+        return smax(__dmul_rn(p.lowFrac, __dmul_rn(p.gamma, frac(l))), p.lowThrFloor);
+    }
+    __device__ __forceinline__ double map_high(int l) const {
+        const DevParams& p = P();
+        if (M.cflags[l] & kCBulkBefore) return p.highThr;
+        return smax(__dmul_rn(p.highFrac, __dmul_rn(p.gamma, frac(l))), p.highThrFloor);
+    }
+    __device__ __forceinline__ double map_val(int l, bool low) const { return low ? map_low(l) : map_high(l); }
 
     // ------------------------------------------------------------------ smoothing, maps
     __device__ void compute_nsm() {
@@ -214,32 +370,15 @@ struct ZoneState {
         __syncwarp();
     }
 
-    // threshold maps of zone cells (src/zone_pass.cpp:321-345, :715-725) + bulk flags
-    __device__ void build_maps() {
-        const DevParams& p = P();
+    // start of a map build: record which cells are bulk (cnt > 0)
+    __device__ void mark_bulk() {
         for (int l = lane; l < nl; l += kWarp) {
-            double f = 1.0;
-            if (p.useLFF) {
-                const double fraw = __ddiv_rn(M.nsm[nsm_index(gx_of(l), gy_of(l))], smax(p.gamma, 1e-12));
-                const double g = __dmul_rn(p.fluidFracGain, fraw);
-                f = (g < 0.0) ? 0.0 : ((1.0 < g) ? 1.0 : g);
-            }
-            const double gl = __dmul_rn(p.gamma, f);
-            double lo = smax(__dmul_rn(p.lowFrac, gl), p.lowThrFloor);
-            double hi = smax(__dmul_rn(p.highFrac, gl), p.highThrFloor);
-            const bool bulk = M.cnt[l] > 0;
-            if (bulk) {
-                lo = p.lowThrBulk;
-                hi = p.highThr;
-            }
-            M.lowA[l] = lo;
-            M.highA[l] = hi;
-            M.cflags[l] = (uint8_t)((M.cflags[l] & ~kCBulkBefore) | (bulk ? kCBulkBefore : 0));
+            const uint8_t f = M.cflags[l];
+            M.cflags[l] = (uint8_t)((f & ~kCBulkBefore) | ((M.cnt[l] > 0) ? kCBulkBefore : 0));
         }
         __syncwarp();
     }
 
-    // ordered list of zone cells satisfying pred (ascending cell index); returns the count
     template <typename Pred>
     __device__ int collect(Pred pred) {
         int total = 0;
@@ -247,27 +386,45 @@ struct ZoneState {
             const int l = b + lane;
             const bool ok = (l < nl) && pred(l);
             const unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (ok) M.list[total + __popc(m & lanemask_lt())] = (Idx)l;
+            if (ok) M.list[total + __popc(m & lanemask_lt())] = (uint16_t)l;
             total += __popc(m);
         }
         __syncwarp();
         return total;
     }
 
-    // ------------------------------------------------------------------ arena lists
-    // tightly repack every list into the arena (rare: only when the arena top is reached)
+    // ------------------------------------------------------------------ lists
+    __device__ __forceinline__ uint32_t elem(int l, int i) const {
+        if (M.cflags[l] & kCMat) return M.arena[M.abase[l] + M.head[l] + i];
+        return ((uint32_t)l << kEntryShift) | (uint32_t)(M.head[l] + i);
+    }
+
+    // repack the materialised lists at the bottom of the arena (in arena order)
     __device__ void compact() {
-        int off = 0;
-        for (int l = 0; l < nl; ++l) {
-            const int a = M.abase[l] + M.head[l], n = M.len[l];
-            for (int j = lane; j < n; j += kWarp) M.scratch[off + j] = M.arena[a + j];
-            off += n;
+        for (int l = lane; l < nl; l += kWarp) {
+            int r = 0;
+            if (M.cflags[l] & kCMat)
+                for (int q = 0; q < nl; ++q)
+                    if ((M.cflags[q] & kCMat) && (M.abase[q] < M.abase[l] || (M.abase[q] == M.abase[l] && q < l))) ++r;
+            M.order[l] = (uint16_t)r;
         }
         __syncwarp();
-        off = 0;
-        for (int l = 0; l < nl; ++l) {
-            const int n = M.len[l];
-            for (int j = lane; j < n; j += kWarp) M.arena[off + j] = M.scratch[off + j];
+        int nmat = 0;
+        for (int l = 0; l < nl; ++l) nmat += (M.cflags[l] & kCMat) ? 1 : 0;
+        int off = 0;
+        for (int r = 0; r < nmat; ++r) {
+            int l = 0;
+            for (int q = 0; q < nl; ++q)
+                if ((M.cflags[q] & kCMat) && M.order[q] == r) l = q;
+            const int a = M.abase[l] + M.head[l], n = M.len[l];
+            // off <= a: copy down in ascending chunks (reads of a chunk precede its writes)
+            for (int j0 = 0; j0 < n; j0 += kWarp) {
+                const int j = j0 + lane;
+                const uint32_t v = (j < n) ? M.arena[a + j] : 0u;
+                __syncwarp();
+                if (j < n) M.arena[off + j] = v;
+                __syncwarp();
+            }
             if (lane == 0) {
                 M.abase[l] = off;
                 M.head[l] = 0;
@@ -279,56 +436,54 @@ struct ZoneState {
         __syncwarp();
     }
 
-    // make room to append `extra` entries to list t (may relocate or repack lists)
+    // materialise or grow list t so that `extra` entries can be appended
     __device__ bool ensure_room(int t, int extra) {
-        if (M.head[t] + M.len[t] + extra <= M.cap[t]) return true;
-        const int want = M.len[t] + extra + 8;
-        if (arenaTop + want > A->arenaCap) {
+        const bool mat = (M.cflags[t] & kCMat) != 0;
+        if (mat && M.head[t] + M.len[t] + extra <= M.cap[t]) return true;
+        const int n = M.len[t];
+        const int want = n + extra + 4;
+        if (arenaTop + want > arenaCap) {
             compact();
-            if (arenaTop + want > A->arenaCap) {
-                if (lane == 0) raise_error(A->st, kErrZoneCapacity, zone);
+            if (arenaTop + want > arenaCap) {
                 failed = true;
                 return false;
             }
         }
-        const int a = M.abase[t] + M.head[t], n = M.len[t];
-        for (int j = lane; j < n; j += kWarp) M.arena[arenaTop + j] = M.arena[a + j];
+        for (int j = lane; j < n; j += kWarp) M.arena[arenaTop + j] = elem(t, j);
         __syncwarp();
         if (lane == 0) {
             M.abase[t] = arenaTop;
             M.head[t] = 0;
             M.cap[t] = want;
+            M.cflags[t] |= kCMat;
         }
         arenaTop += want;
         __syncwarp();
         return true;
     }
 
-    // Move `nt` particles from list position srcPos (arena index, read before any
-    // relocation) into cell t, drawing their positions with sample_in_cell
-    // (src/zone_pass.cpp:280-294): per particle U for x then U for y.
+    // Move `nt` particles from positions srcOff.. of list s into cell t, drawing positions
+    // with sample_in_cell (src/zone_pass.cpp:280-294): per particle U for x then U for y.
     __device__ bool move_into(int s, int srcOff, int nt, int t) {
         if (!ensure_room(t, nt)) return false;
         const DevParams& p = P();
-        const int tix = gx_of(t), tiy = gy_of(t);
-        const double x0 = __dmul_rn((double)tix, p.dx), y0 = __dmul_rn((double)tiy, p.dy);
-        const int src = M.abase[s] + M.head[s] + srcOff;
+        const double x0 = __dmul_rn((double)gx_of(t), p.dx), y0 = __dmul_rn((double)gy_of(t), p.dy);
         const int dst = M.abase[t] + M.head[t] + M.len[t];
-        for (int q0 = 0; q0 < nt; q0 += 128) {
-            const int c = min(128, nt - q0);
+        for (int q0 = 0; q0 < nt; q0 += kWarp) {
+            const int c = min(kWarp, nt - q0);
             rng.ensure(2 * c);
-            for (int q = q0 + lane; q < q0 + c; q += kWarp) {
-                const int k = (int)M.arena[src + q];
-                const double px = __dadd_rn(x0, __dmul_rn(p.dx, canon(rng.peek(2 * (q - q0)))));
-                const double py = __dadd_rn(y0, __dmul_rn(p.dy, canon(rng.peek(2 * (q - q0) + 1))));
-                const uint8_t fl = M.pflags[k];
-                if (fl & kPOwned) {
-                    const int sl = M.slot[k];
+            const int q = q0 + lane;
+            if (lane < c) {
+                const uint32_t e = elem(s, srcOff + q);
+                const double px = __dadd_rn(x0, __dmul_rn(p.dx, canon(rng.peek(2 * lane))));
+                const double py = __dadd_rn(y0, __dmul_rn(p.dy, canon(rng.peek(2 * lane + 1))));
+                const int lc = (int)(e >> kEntryShift);
+                if (M.cflags[lc] & kCOwned) {
+                    const int sl = A->slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
                     A->xout[sl] = make_double2(px, py);
                     A->cid[sl] = cell_of(px, py, p);
                 }
-                M.pflags[k] = fl | kPMoved;
-                M.arena[dst + q] = (Idx)k;
+                M.arena[dst + q] = e;
             }
             rng.consume(2 * c);
             __syncwarp();
@@ -353,7 +508,6 @@ struct ZoneState {
 
     // update_transfer_correction_masks (src/zone_pass.cpp:492-525), forceSkip = false
     __device__ void update_masks(int src, const int* recv, int nrecv) {
-        // touched = unique_stable([src] + recv); src is never a receiver here
         bool allBulk = (M.cflags[src] & kCBulkBefore) != 0;
         for (int q = 0; q < nrecv; ++q) allBulk &= (M.cflags[recv[q]] & kCBulkBefore) != 0;
         if (lane <= nrecv) {
@@ -367,9 +521,8 @@ struct ZoneState {
     }
 
     // ------------------------------------------------------------------ dense phase
-    // admissible_dense_targets_rangeR (src/zone_pass.cpp:413-434) + the zone filter;
-    // writes the ordered candidates to cand and returns their number
-    __device__ int admissible(int l, const double* map, int* cand) {
+    // admissible_dense_targets_rangeR (src/zone_pass.cpp:413-434) + the zone filter
+    __device__ int admissible(int l, bool low, int* cand) {
         const int ix = gx_of(l), iy = gy_of(l);
         int nb = -1;
         if (lane < 24) {
@@ -378,7 +531,7 @@ struct ZoneState {
             int jy, jx;
             if (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy)) {
                 const int t = loc(jx, jy);
-                if ((double)M.cnt[t] < map[t]) nb = t;
+                if ((double)M.cnt[t] < map_val(t, low)) nb = t;
             }
         }
         const unsigned m0 = __ballot_sync(0xffffffffu, nb >= 0);
@@ -390,14 +543,14 @@ struct ZoneState {
         return __popc(mk);
     }
 
-    // rank_dense_targets_unified (src/zone_pass.cpp:436-490) with inwardWeight = 0:
-    // per-bin insertion sort (stable) on (-deficit, cnt, cheb, dist2, U01), round robin
-    __device__ int rank_dense(int l, const int* cand, int m, const double* map, int* T) {
+    // rank_dense_targets_unified (src/zone_pass.cpp:436-490), inwardWeight = 0: per-bin
+    // stable insertion sort on (-deficit, cnt, cheb, dist2, U01), then round robin
+    __device__ int rank_dense(int l, const int* cand, int m, bool low, int* T) {
         if (m == 0) return 0;
         const DevParams& p = P();
         const int startBin = (int)rng.uint_in(1, 8) - 1;
         rng.ensure(m);
-        int nb = -1, bin = -1, key2 = 0, cheb = 0, d2 = 0;
+        int nb = -1, bin = -1, key2 = 0;
         double dneg = 0.0, tie = 0.0;
         if (lane < m) {
             nb = cand[lane];
@@ -409,10 +562,9 @@ struct ZoneState {
             } else {
                 bin = p.atanBin[idx];
             }
-            dneg = -smax(0.0, __dsub_rn(map[nb], (double)M.cnt[nb]));
-            key2 = M.cnt[nb];
-            cheb = max(abs(ddx), abs(ddy));
-            d2 = ddx * ddx + ddy * ddy;
+            dneg = -smax(0.0, __dsub_rn(map_val(nb, low), (double)M.cnt[nb]));
+            const int cheb = max(abs(ddx), abs(ddy)), d2 = ddx * ddx + ddy * ddy;
+            key2 = (M.cnt[nb] << 8) | (cheb << 4) | d2;  // lexicographic (cnt, cheb, dist2)
             tie = canon(rng.peek(lane));
         }
         rng.consume(m);
@@ -420,16 +572,12 @@ struct ZoneState {
         for (int j = 0; j < m; ++j) {
             const int bj = __shfl_sync(0xffffffffu, bin, j);
             const double dj = __shfl_sync(0xffffffffu, dneg, j);
-            const int cj = __shfl_sync(0xffffffffu, key2, j);
-            const int hj = __shfl_sync(0xffffffffu, cheb, j);
-            const int ej = __shfl_sync(0xffffffffu, d2, j);
+            const int kj = __shfl_sync(0xffffffffu, key2, j);
             const double tj = __shfl_sync(0xffffffffu, tie, j);
             if (lane < m && j != lane && bj == bin) {
                 bool less, eq = false;
                 if (dj != dneg) less = dj < dneg;
-                else if (cj != key2) less = cj < key2;
-                else if (hj != cheb) less = hj < cheb;
-                else if (ej != d2) less = ej < d2;
+                else if (kj != key2) less = kj < key2;
                 else if (tj != tie) less = tj < tie;
                 else { less = false; eq = true; }
                 if (less || (eq && j < lane)) ++r;
@@ -450,7 +598,7 @@ struct ZoneState {
     }
 
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589)
-    __device__ int spread(int s, const int* T, int nT, const double* map, int needOut, int* recv, int& nrecv) {
+    __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int* recv, int& nrecv) {
         if (needOut <= 0 || nT == 0) return 0;
         const int srcLen = M.len[s];
         if (srcLen == 0) return 0;
@@ -461,7 +609,7 @@ struct ZoneState {
                 int defj = 0;
                 if (lane < nT) {
                     const int t = T[lane];
-                    defj = max(0, (int)floor(__dsub_rn(map[t], (double)M.cnt[t])));
+                    defj = max(0, (int)floor(__dsub_rn(map_val(t, low), (double)M.cnt[t])));
                 }
                 const unsigned pm = __ballot_sync(0xffffffffu, lane < nT && defj > 0);
                 const int deficit = __shfl_sync(0xffffffffu, defj, kk);
@@ -472,7 +620,7 @@ struct ZoneState {
                 const int t = T[kk];
                 if (t == s) {
                     if (lane == 0) raise_error(A->st, kErrTargetIsSource, zone);
-                    failed = true;
+                    fatal = true;
                     return moved;
                 }
                 if (!move_into(s, taken, nt, t)) return moved;
@@ -496,26 +644,26 @@ struct ZoneState {
 
     // one dense cell (src/zone_pass.cpp:734-753 calling :591-634)
     __device__ void dense_cell(int l) {
-        int* cand = M.small;        // 24
-        int* T = M.small + 32;      // 24
-        int* recv = M.small + 64;   // <= 24 unique
+        int* cand = M.small;
+        int* T = M.small + 32;
+        int* recv = M.small + 64;
         const int ncc = M.cnt[l];
         if (ncc <= 0) return;
-        const double hl = M.highA[l];
+        const double hl = map_high(l);
         if ((double)ncc <= hl) return;
         int nrecv = 0, moved = 0;
         const int needOut = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
         if (needOut > 0) {
-            int m = admissible(l, M.lowA, cand);
-            int nT = rank_dense(l, cand, m, M.lowA, T);
-            moved += spread(l, T, nT, M.lowA, needOut, recv, nrecv);
-            if (failed) return;
+            int m = admissible(l, true, cand);
+            int nT = rank_dense(l, cand, m, true, T);
+            moved += spread(l, T, nT, true, needOut, recv, nrecv);
+            if (failed || fatal) return;
             const int rem = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
             if (rem > 0) {
-                m = admissible(l, M.highA, cand);
-                nT = rank_dense(l, cand, m, M.highA, T);
-                moved += spread(l, T, nT, M.highA, rem, recv, nrecv);
-                if (failed) return;
+                m = admissible(l, false, cand);
+                nT = rank_dense(l, cand, m, false, T);
+                moved += spread(l, T, nT, false, rem, recv, nrecv);
+                if (failed || fatal) return;
             }
         }
         if (lane < nrecv) M.cflags[recv[lane]] |= (kCRecv | kCChanged);
@@ -526,7 +674,6 @@ struct ZoneState {
     }
 
     // ------------------------------------------------------------------ sparse phase
-    // inward_direction_from_local_gradient (src/zone_pass.cpp:375-411)
     __device__ void inward(int l, double& gx, double& gy) const {
         const DevParams& p = P();
         const int ix = gx_of(l), iy = gy_of(l);
@@ -545,11 +692,10 @@ struct ZoneState {
     // one sparse cell (src/zone_pass.cpp:804-854)
     __device__ void sparse_cell(int l) {
         const DevParams& p = P();
-        int* don = M.small + 96;  // <= 8
+        int* don = M.small + 96;
         const int ncc = M.cnt[l];
         if (ncc <= 0) return;
         if (M.len[l] == 0) return;
-        // local_neighbors_in_zone, range 1 (src/zone_pass.cpp:263-278)
         const int ix = gx_of(l), iy = gy_of(l);
         int nb = -1;
         if (lane < 8) {
@@ -571,13 +717,13 @@ struct ZoneState {
         if (nd == 0) return;
         if (isDonor) don[__popc(md & lanemask_lt())] = nb;
         __syncwarp();
-        // rank_admissible_neighbors_inward (src/zone_pass.cpp:636-667)
         double gx, gy;
         inward(l, gx, gy);
-        warp_shuffle(don, nd, rng, lane);
+        zone_shuffle(don, nd, rng, lane);
         const double ndir = mpcd_dd::hypot_cr(gx, gy);
-        PolarNormal N;
-        N.reset();
+        ZoneNormal N;
+        N.has = 0;
+        N.saved = 0.0;
         double* score = M.smallD;
         for (int k = 0; k < nd; ++k) {
             const int d = don[k];
@@ -615,7 +761,8 @@ struct ZoneState {
             if (avail <= 0) continue;
             const int nt = min(min(need, avail), ld);
             if (nt <= 0) continue;
-            warp_shuffle(M.arena + M.abase[d] + M.head[d], ld, rng, lane);
+            if (!ensure_room(d, 0)) return;  // materialise the donor list to shuffle it
+            zone_shuffle(M.arena + M.abase[d] + M.head[d], ld, rng, lane);
             if (!move_into(d, 0, nt, l)) return;
             if (lane == 0) {
                 M.head[d] += nt;
@@ -635,13 +782,14 @@ struct ZoneState {
 };
 
 // ------------------------------------------------------------------ the zone body
-template <typename Idx>
-__device__ void zone_body(const ZoneArgs& A, int z, char* mem, bool overflowPath) {
-    ZoneState<Idx> S;
+// Returns false if the zone must be re-run on the overflow path.
+__device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap) {
+    ZoneState S;
     S.A = &A;
     S.lane = threadIdx.x & 31;
     S.zone = z;
     S.failed = false;
+    S.fatal = false;
     S.movedDense = S.movedSparse = 0;
     const int lane = S.lane;
     const DevParams& p = A.P;
@@ -649,129 +797,147 @@ __device__ void zone_body(const ZoneArgs& A, int z, char* mem, bool overflowPath
     S.xs = R.x; S.xe = R.y; S.ys = R.z; S.ye = R.w;
     S.TX = S.xe - S.xs; S.TY = S.ye - S.ys; S.nl = S.TX * S.TY; S.WY = S.TY + 4;
     const int W = (S.TX + 4) * S.WY;
-    if (S.nl > A.maxCells || W > A.winCap || (S.TX + 2) * (S.TY + 2) > A.winCap) {
-        if (!overflowPath && lane == 0) A.overflow[atomicAdd(A.nOverflow, 1)] = z;
-        if (overflowPath && lane == 0) raise_error(A.st, kErrZoneCapacity, z);
-        return;
-    }
-    S.M.carve(mem, A.maxCells, A.winCap, A.nlocCap, A.arenaCap);
-    ZoneMem<Idx>& M = S.M;
+    if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > winCap || S.nl >= (1 << (32 - kEntryShift))) return false;
+    S.M.carve(mem, maxCells, winCap, arenaCap);
+    S.arenaCap = arenaCap;
+    S.arenaTop = 0;
+    ZoneMem& M = S.M;
     // pass-input counts around the zone
-    for (int w = lane; w < W; w += kWarp) {
-        int ix = S.xs - 2 + w / S.WY, iy = S.ys - 2 + w % S.WY;
-        if (p.perx) ix = wrap_index(ix, p.Nx);
-        if (p.pery) iy = wrap_index(iy, p.Ny);
-        int c = -1;
-        if (ix >= 0 && ix < p.Nx && iy >= 0 && iy < p.Ny) {
-            const int cc = iy + p.Ny * ix;
-            c = (int)((uint32_t)A.start[cc + 1] - (uint32_t)A.start[cc]);
+    for (int w0 = 0; w0 < W; w0 += 4 * kWarp) {
+        uint64_t a[4], b[4];
+        bool ok[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int w = w0 + lane + k * kWarp;
+            int ix = S.xs - 2 + w / S.WY, iy = S.ys - 2 + w % S.WY;
+            if (p.perx) ix = wrap_index(ix, p.Nx);
+            if (p.pery) iy = wrap_index(iy, p.Ny);
+            ok[k] = w < W && ix >= 0 && ix < p.Nx && iy >= 0 && iy < p.Ny;
+            const int cc = ok[k] ? iy + p.Ny * ix : 0;
+            a[k] = ok[k] ? A.start[cc] : 0ULL;
+            b[k] = ok[k] ? A.start[cc + 1] : 0ULL;
         }
-        M.win[w] = c;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int w = w0 + lane + k * kWarp;
+            if (w < W) M.win[w] = ok[k] ? (int)((uint32_t)b[k] - (uint32_t)a[k]) : -1;
+        }
     }
-    __syncwarp();
-    // zone cell counts and their prefix (local particle numbering in input order)
-    int total = 0;
-    for (int b = 0; b < S.nl; b += kWarp) {
-        const int l = b + lane;
-        int c = 0;
-        if (l < S.nl) c = M.win[(l / S.TY + 2) * S.WY + (l % S.TY + 2)];
-        int x = c;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (l < S.nl) {
-            M.cnt0[l] = c;
-            M.cnt[l] = c;
-            M.base0[l] = total + x - c;
-            M.len[l] = c;
-            M.head[l] = 0;
-            M.cflags[l] = 0;
-        }
-        total += __shfl_sync(0xffffffffu, x, 31);
+    // zone cells: segment starts and ownership
+    for (int l = lane; l < S.nl; l += kWarp) {
+        const int c = S.gy_of(l) + p.Ny * S.gx_of(l);
+        const int own = A.owner[c];
+        M.gstart[l] = (int)(uint32_t)A.start[c];
+        M.cflags[l] = (own == z + 1) ? kCOwned : 0;
     }
-    S.nloc = total;
-    if (total > A.nlocCap || total > A.arenaCap) {
-        if (!overflowPath && lane == 0) A.overflow[atomicAdd(A.nOverflow, 1)] = z;
-        if (overflowPath && lane == 0) raise_error(A.st, kErrZoneCapacity, z);
-        return;
+    {
+        uint64_t w[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            const int i = lane + k * kWarp;
+            w[k] = (i < kMtN) ? A.seeds[(size_t)z * kMtN + i] : 0ULL;
+        }
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            const int i = lane + k * kWarp;
+            if (i < kMtN) M.mt[i] = w[k];
+        }
     }
     __syncwarp();
     for (int l = lane; l < S.nl; l += kWarp) {
-        M.abase[l] = M.base0[l];
-        M.cap[l] = M.cnt0[l];
+        const int c = M.win[(l / S.TY + 2) * S.WY + (l % S.TY + 2)];
+        M.cnt0[l] = c;
+        M.cnt[l] = c;
+        M.len[l] = c;
+        M.head[l] = 0;
+        M.abase[l] = 0;
+        M.cap[l] = 0;
     }
-    S.arenaTop = total;
-    // slots of the zone's particles: one contiguous run of the cell index per zone column
-    for (int col = 0; col < S.TX; ++col) {
-        const int c0 = S.ys + p.Ny * (S.xs + col);
-        const int g0 = (int)(uint32_t)A.start[c0], g1 = (int)(uint32_t)A.start[c0 + S.TY];
-        const int b0 = M.base0[col * S.TY];
-        for (int j = lane; j < g1 - g0; j += kWarp) M.slot[b0 + j] = A.slots[g0 + j];
-    }
-    for (int k = lane; k < total; k += kWarp) M.arena[k] = (Idx)k;
     __syncwarp();
-    for (int l = 0; l < S.nl; ++l) {
-        const int c = S.gy_of(l) + p.Ny * S.gx_of(l);
-        const uint8_t fl = (A.owner[c] == z + 1) ? kPOwned : 0;
-        for (int j = lane; j < M.cnt0[l]; j += kWarp) M.pflags[M.base0[l] + j] = fl;
-    }
-    for (int i = lane; i < kMtN; i += kWarp) M.mt[i] = A.seeds[(size_t)z * kMtN + i];
-    __syncwarp();
-    S.rng.buf = M.mt;
-    S.rng.init_from_seeded(lane);
+    S.rng.init(M.mt, M.carry, lane);
 
     // dense passes (src/zone_pass.cpp:708-781)
-    for (int pass = 0; pass < p.maxPasses && !S.failed; ++pass) {
+    for (int pass = 0; pass < p.maxPasses && !S.failed && !S.fatal; ++pass) {
         if (p.useLFF) S.compute_nsm();
-        S.build_maps();
-        const int nd = S.collect([&](int l) { return (double)M.cnt[l] > M.highA[l]; });
-        warp_shuffle(M.list, nd, S.rng, lane);
-        for (int q = 0; q < nd && !S.failed; ++q) S.dense_cell((int)M.list[q]);
+        S.mark_bulk();
+        const int nd = S.collect([&](int l) { return (double)M.cnt[l] > S.map_high(l); });
+        zone_shuffle(M.list, nd, S.rng, lane);
+        for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
     }
     // sparse phase (src/zone_pass.cpp:783-854)
-    if (!S.failed) {
+    if (!S.failed && !S.fatal) {
         S.compute_nsm();
-        S.build_maps();
-        const int nlow = S.collect([&](int l) { return M.cnt[l] > 0 && (double)M.cnt[l] < M.lowA[l]; });
-        warp_shuffle(M.list, nlow, S.rng, lane);
-        for (int q = 0; q < nlow && !S.failed; ++q) S.sparse_cell((int)M.list[q]);
+        S.mark_bulk();
+        const int nlow = S.collect([&](int l) { return M.cnt[l] > 0 && (double)M.cnt[l] < S.map_low(l); });
+        zone_shuffle(M.list, nlow, S.rng, lane);
+        for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
     }
-    if (S.failed) return;
+    if (S.fatal) return true;
+    if (S.failed) return false;
 
-    // momentum correction (src/zone_pass.cpp:870-922)
-    double* dux = M.lowA;
-    double* duy = M.highA;
+    // momentum correction (src/zone_pass.cpp:870-922): per changed cell, the momentum of
+    // its input list and of its final list, both in list order; owned particles of
+    // corrected cells get v + du
     double* du2 = M.nsm;
     for (int l = lane; l < S.nl; l += kWarp) {
-        double d2 = 0.0, ux = 0.0, uy = 0.0;
-        uint8_t f = M.cflags[l] & ~kCApply;
+        double d2 = 0.0;
+        const uint8_t f = M.cflags[l];
         const int n = M.len[l];
         if ((f & kCChanged) && n > 0) {
             double bx = 0.0, by = 0.0, axs = 0.0, ays = 0.0;
-            for (int j = 0; j < M.cnt0[l]; ++j) {
-                const double2 w = A.vin[M.slot[M.base0[l] + j]];
-                bx = __dadd_rn(bx, w.x);
-                by = __dadd_rn(by, w.y);
+            const int n0 = M.cnt0[l], g0 = M.gstart[l];
+            for (int j0 = 0; j0 < n0; j0 += 8) {
+                int sl[8];
+                double2 w[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) sl[u] = (j0 + u < n0) ? A.slots[g0 + j0 + u] : 0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n0) ? A.vin[sl[u]] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (j0 + u < n0) {
+                        bx = __dadd_rn(bx, w[u].x);
+                        by = __dadd_rn(by, w[u].y);
+                    }
             }
-            const int a = M.abase[l] + M.head[l];
-            for (int j = 0; j < n; ++j) {
-                const double2 w = A.vin[M.slot[(int)M.arena[a + j]]];
-                axs = __dadd_rn(axs, w.x);
-                ays = __dadd_rn(ays, w.y);
+            for (int j0 = 0; j0 < n; j0 += 8) {
+                int sl[8];
+                double2 w[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    sl[u] = 0;
+                    if (j0 + u < n) {
+                        const uint32_t e = S.elem(l, j0 + u);
+                        sl[u] = A.slots[M.gstart[e >> kEntryShift] + (int)(e & ((1u << kEntryShift) - 1))];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n) ? A.vin[sl[u]] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (j0 + u < n) {
+                        axs = __dadd_rn(axs, w[u].x);
+                        ays = __dadd_rn(ays, w[u].y);
+                    }
             }
-            ux = __ddiv_rn(__dsub_rn(bx, axs), (double)n);
-            uy = __ddiv_rn(__dsub_rn(by, ays), (double)n);
+            const double ux = __ddiv_rn(__dsub_rn(bx, axs), (double)n);
+            const double uy = __ddiv_rn(__dsub_rn(by, ays), (double)n);
             d2 = __dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy));
             bool doCorr = p.momCorr != 0;
             if (doCorr && (f & kCSkip)) doCorr = false;
             if (doCorr && (f & kCRecv) && !(f & kCBulkBulk)) doCorr = false;
-            if (doCorr && (ux != 0.0 || uy != 0.0)) f |= kCApply;
+            if (doCorr && (ux != 0.0 || uy != 0.0)) {
+                for (int j = 0; j < n; ++j) {
+                    const uint32_t e = S.elem(l, j);
+                    const int lc = (int)(e >> kEntryShift);
+                    if (!(M.cflags[lc] & kCOwned)) continue;
+                    const int sl = A.slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
+                    const double2 w = A.vin[sl];
+                    A.vout[sl] = make_double2(__dadd_rn(w.x, ux), __dadd_rn(w.y, uy));
+                }
+            }
         }
-        dux[l] = ux;
-        duy[l] = uy;
         du2[l] = d2;
-        M.cflags[l] = f;
     }
     __syncwarp();
     // zone stats[4], stats[5] in ascending cell order (src/zone_pass.cpp:911-922)
@@ -789,37 +955,25 @@ __device__ void zone_body(const ZoneArgs& A, int z, char* mem, bool overflowPath
         A.zoneCorr[z] = make_double2((cntDU > 0) ? sqrt(__ddiv_rn(acc, (double)cntDU)) : 0.0, (cntDU > 0) ? mx : 0.0);
         A.zoneMoved[z] = make_int2(S.movedDense, S.movedSparse);
     }
-    // final cell of every local particle
-    for (int l = lane; l < S.nl; l += kWarp) {
-        const int a = M.abase[l] + M.head[l];
-        for (int j = 0; j < M.len[l]; ++j) M.scratch[(int)M.arena[a + j]] = (Idx)l;
-    }
-    __syncwarp();
-    // owned particles: corrected velocities, unmoved positions copied
-    for (int k = lane; k < S.nloc; k += kWarp) {
-        const uint8_t fl = M.pflags[k];
-        if (!(fl & kPOwned)) continue;
-        const int sl = M.slot[k];
-        const int fc = (int)M.scratch[k];
-        double2 w = A.vin[sl];
-        if (M.cflags[fc] & kCApply) w = make_double2(__dadd_rn(w.x, dux[fc]), __dadd_rn(w.y, duy[fc]));
-        A.vout[sl] = w;
-        if (!(fl & kPMoved)) A.xout[sl] = A.xin[sl];
-    }
+    return true;
 }
 
 __global__ void __launch_bounds__(32) k_zone_pass(ZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int z = blockIdx.x;
     if (z >= A.nZones) return;
-    zone_body<uint16_t>(A, z, smem, false);
+    if (!zone_body(A, z, smem, A.maxCells, A.winCap, A.arenaCap) && (threadIdx.x & 31) == 0)
+        A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
-// zones that did not fit the shared-memory working set, one at a time per block, with a
-// global-memory working set per block
+// zones that did not fit the shared-memory working set, re-run from their seed with a
+// global-memory working set per block (deterministic: identical decisions and writes)
 __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock) {
     const int nov = *A.nOverflow;
-    for (int i = blockIdx.x; i < nov; i += gridDim.x) zone_body<uint32_t>(A, A.overflow[i], gmem + perBlock * blockIdx.x, true);
+    for (int i = blockIdx.x; i < nov; i += gridDim.x)
+        if (!zone_body(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap) &&
+            (threadIdx.x & 31) == 0)
+            raise_error(A.st, kErrZoneCapacity, A.overflow[i]);
 }
 
 // Seeded MT19937-64 state of every zone: seed = seedBase + 104729 (iz + 1)
