@@ -46,7 +46,7 @@ struct BcWork {
 // One particle through the four sweeps. kDry: thermal hits leave velocities undefined and
 // only count; otherwise pair (firstPair + k) serves the particle's k-th thermal hit.
 // Returns false on an unsupported mode (error code in *err).
-template <bool kDry>
+template <bool kDry, bool kInfo = true>
 __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, double& vy, const DevParams& P,
                                           const double* __restrict__ normals, int firstPair, int pairCap, int& thermX0,
                                           int& thermY0, int& late, double* acc, int* nhit, int* err) {
@@ -75,12 +75,14 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
                 } else {
                     vx = fabs(vx);
                 }
-                const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
-                nhit[2] += 1;
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
-                                                                  __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
-                acc[5] = __dadd_rn(acc[5], fabs(dvx));
-                acc[7] = __dadd_rn(acc[7], dvy);
+                if (kInfo) {
+                    const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
+                    nhit[2] += 1;
+                    acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
+                                                                      __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
+                    acc[5] = __dadd_rn(acc[5], fabs(dvx));
+                    acc[7] = __dadd_rn(acc[7], dvy);
+                }
             } else {
                 *err = kErrUnsupportedBcLeft;
                 return false;
@@ -106,12 +108,14 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
                 } else {
                     vx = -fabs(vx);
                 }
-                const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
-                nhit[3] += 1;
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
-                                                                  __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
-                acc[6] = __dadd_rn(acc[6], fabs(dvx));
-                acc[8] = __dadd_rn(acc[8], dvy);
+                if (kInfo) {
+                    const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
+                    nhit[3] += 1;
+                    acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
+                                                                      __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
+                    acc[6] = __dadd_rn(acc[6], fabs(dvx));
+                    acc[8] = __dadd_rn(acc[8], dvy);
+                }
             } else {
                 *err = kErrUnsupportedBcRight;
                 return false;
@@ -137,12 +141,14 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
                 } else {
                     vy = fabs(vy);
                 }
-                const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
-                nhit[0] += 1;
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
-                                                                  __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
-                acc[1] = __dadd_rn(acc[1], dvx);
-                acc[3] = __dadd_rn(acc[3], fabs(dvy));
+                if (kInfo) {
+                    const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
+                    nhit[0] += 1;
+                    acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
+                                                                      __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
+                    acc[1] = __dadd_rn(acc[1], dvx);
+                    acc[3] = __dadd_rn(acc[3], fabs(dvy));
+                }
             } else {
                 *err = kErrUnsupportedBcBottom;
                 return false;
@@ -168,12 +174,14 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
                 } else {
                     vy = -fabs(vy);
                 }
-                const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
-                nhit[1] += 1;
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
-                                                                  __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
-                acc[2] = __dadd_rn(acc[2], dvx);
-                acc[4] = __dadd_rn(acc[4], fabs(dvy));
+                if (kInfo) {
+                    const double dvx = __dsub_rn(vx, ox), dvy = __dsub_rn(vy, oy);
+                    nhit[1] += 1;
+                    acc[0] = __dadd_rn(acc[0], __dmul_rn(0.5, __dsub_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)),
+                                                                      __dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)))));
+                    acc[2] = __dadd_rn(acc[2], dvx);
+                    acc[4] = __dadd_rn(acc[4], fabs(dvy));
+                }
             } else {
                 *err = kErrUnsupportedBcTop;
                 return false;
@@ -236,6 +244,7 @@ __global__ void k_srd_shift(DevParams P, uint64_t seed, double* out) {
 
 // Streams (optional), replays the sweeps, and computes the cell ids the next phases need.
 // x, v: slot-ordered state. cidStd: cell on the standard grid; cidSrd (optional): SRD cell.
+template <bool kInfo>
 __global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, double2* __restrict__ v,
                             const int* __restrict__ pid, int* __restrict__ cidStd, int* __restrict__ cidSrd,
                             BcWork W, DevStatus* st) {
@@ -256,7 +265,7 @@ __global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, 
         double a2[kWallDoubles];
         int h2[4] = {0, 0, 0, 0};
         for (int k = 0; k < kWallDoubles; ++k) a2[k] = 0.0;
-        const bool ok = bc_replay<true>(xs.x, xs.y, vs.x, vs.y, P, nullptr, 0, 1, tx, ty, late, a2, h2, &err);
+        const bool ok = bc_replay<true, kInfo>(xs.x, xs.y, vs.x, vs.y, P, nullptr, 0, 1, tx, ty, late, a2, h2, &err);
         if (!ok) {
             raise_error(st, err, s);
         } else if (tx + ty == 0 && !late) {
@@ -286,6 +295,7 @@ __global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, 
         if (cidStd) cidStd[s] = cell_of(xs.x, xs.y, P);
         if (cidSrd) cidSrd[s] = srd_cell(xs.x, xs.y, W.srdShift[0], W.srdShift[1], P);
     }
+    if (!kInfo) return;
     // block partial WallInfo of particles finished here (fixed reduction order)
     __shared__ double sh[kWallDoubles][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

@@ -130,6 +130,7 @@ struct mpcd_ctx {
     double* fieldTmp = nullptr; // 11 * Nc scratch for field outputs
     int* fieldTmpN = nullptr;
     double2* vrep = nullptr;
+    int* cellOf = nullptr;      // n: cell of each cell-index position (flat kick)
     // status
     DevStatus* st = nullptr;
     DevStatus* hst = nullptr;
@@ -452,8 +453,13 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     CUDA_TRY(cudaMemsetAsync(W.bitsY, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
     CUDA_TRY(cudaMemsetAsync(W.nEvents, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaMemsetAsync(W.ints, 0, sizeof(int) * 4, c->stream));
-    k_stream_bc<<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp],
-                                                         cidStd, cidSrd, W, c->st); ++c->launches;
+    if (wantInfo)
+        k_stream_bc<true><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv],
+                                                                   c->pidb[c->pp], cidStd, cidSrd, W, c->st);
+    else
+        k_stream_bc<false><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv],
+                                                                    c->pidb[c->pp], cidStd, cidSrd, W, c->st);
+    ++c->launches;
     mark(c, pf, 0);
     k_word_counts<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount); ++c->launches;
     int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix);
@@ -589,13 +595,20 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     int rc = ensure_std_index(c, pf);
     if (rc) return rc;
     RedFields rf{};
+    const bool flat = permute && !wantRep && !wantStats;  // the step's fast path
     k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
                                                                    c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
-                                                                   c->duRY, c->cols); ++c->launches;
+                                                                   c->duRY, c->cols, flat ? c->cellOf : nullptr); ++c->launches;
     rc = reduce_cols(c, c->cols, c->Nc, 2, 0u, c->red);
     if (rc) return rc;
     mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
+    if (flat) {
+        k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX,
+                                                                   c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
+                                                                   c->pidb[np], c->xb[nx ^ 1], c->vb[nx ^ 1],
+                                                                   c->pidb[np ^ 1]); ++c->launches;
+    } else
     k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
         c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
         c->pidb[np], permute ? c->xb[nx ^ 1] : nullptr, permute ? c->vb[nx ^ 1] : nullptr,
@@ -649,7 +662,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
-                    c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->st};
+                    c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 3; ++k) {
@@ -810,6 +823,7 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     ALLOC(c->fieldTmp, 11 * (size_t)Nc);
     ALLOC(c->fieldTmpN, (size_t)Nc);
     ALLOC(c->vrep, (size_t)n);
+    ALLOC(c->cellOf, (size_t)n);
     ALLOC(c->st, 1);
 #undef ALLOC
     if (cudaMemset(c->st, 0, sizeof(DevStatus)) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "memset"));

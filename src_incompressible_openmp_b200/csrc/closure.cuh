@@ -79,7 +79,7 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
                                 const double2* __restrict__ v, const double* __restrict__ refPx,
                                 const double* __restrict__ refPy, const double* __restrict__ refUx,
                                 const double* __restrict__ refUy, RedFields red, double* __restrict__ duRX,
-                                double* __restrict__ duRY, double* __restrict__ cols) {
+                                double* __restrict__ duRY, double* __restrict__ cols, int* __restrict__ cellOf) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
@@ -89,6 +89,7 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
         const double2 w = v[slots[j]];
         px = __dadd_rn(px, w.x);
         py = __dadd_rn(py, w.y);
+        if (cellOf) cellOf[j] = c;
     }
     double ux = 0.0, uy = 0.0;
     if (m > 0) {
@@ -222,6 +223,27 @@ __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const in
         s[7] = soutx;
         s[8] = souty;
     }
+}
+
+// The two kicks for one index position j (flat, coalesced), writing the particle at
+// position j of the next step's layout: (cell, particle id) order.
+__global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, const int* __restrict__ slots,
+                            const double* __restrict__ numden, const double* __restrict__ duRX,
+                            const double* __restrict__ duRY, const double* __restrict__ eosX,
+                            const double* __restrict__ eosY, const double2* __restrict__ x,
+                            const double2* __restrict__ v, const int* __restrict__ pid, double2* __restrict__ xo,
+                            double2* __restrict__ vo, int* __restrict__ pido) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double beta = beta_applied(P, numden[0], numden[1]);
+    const int c = cellOf[j];
+    const int s = slots[j];
+    const double2 w = v[s];
+    const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
+    const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
+    vo[j] = make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c]));
+    xo[j] = x[s];
+    pido[j] = pid[s];
 }
 
 // identity cell index after a permuting kick: slots[j] = j

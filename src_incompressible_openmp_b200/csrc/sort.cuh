@@ -78,25 +78,65 @@ __global__ void k_pack_counts(const int* __restrict__ count, int Nc, uint64_t* _
     }
 }
 
-// pos[s] = arrival order of slot s within its cell (any order; fixed later by k_cell_sort)
+// pos[s] = arrival order of slot s within its cell (any order; fixed later by k_cell_sort).
+// One atomic per run of equal cell ids among consecutive lanes: after the end-of-step
+// re-sort, slots are ordered by cell, so a warp's lanes form a few long runs.
 __global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict__ count, int* __restrict__ pos) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned active = __ballot_sync(0xffffffffu, s < n);
-    if (s >= n) return;
-    const int c = cid[s];
-    const unsigned same = __match_any_sync(active, c);
-    const int leader = __ffs(same) - 1;
     const int lane = threadIdx.x & 31;
+    const int c = (s < n) ? cid[s] : -1;
+    const int prev = __shfl_up_sync(0xffffffffu, c, 1);
+    const bool headOfRun = (lane == 0) || (prev != c);
+    const unsigned heads = __ballot_sync(0xffffffffu, headOfRun);
+    // run start = highest head lane <= lane; run end = next head lane
+    const unsigned upTo = heads & (0xffffffffu >> (31 - lane));
+    const int runStart = 31 - __clz(upTo);
+    const unsigned after = heads & ~(0xffffffffu >> (31 - lane));
+    const int runEnd = after ? (__ffs(after) - 1) : 32;
     int base = 0;
-    if (lane == leader) base = atomicAdd(&count[c], __popc(same));
-    base = __shfl_sync(same, base, leader);
-    pos[s] = base + __popc(same & lanemask_lt());
+    if (headOfRun && c >= 0) base = atomicAdd(&count[c], runEnd - runStart);
+    base = __shfl_sync(0xffffffffu, base, runStart);
+    if (s < n) pos[s] = base + (lane - runStart);
 }
 
 __global__ void k_scatter(const int* __restrict__ cid, const int* __restrict__ pos, int n,
                           const uint64_t* __restrict__ start, int* __restrict__ slots) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < n) slots[(uint32_t)start[cid[s]] + pos[s]] = s;
+}
+
+// Bitonic sort of 16 or 32 keys held in registers (fully unrolled, no local memory).
+template <int N>
+__device__ __forceinline__ void bitonic_regs(uint64_t (&k)[N]) {
+#pragma unroll
+    for (int size = 2; size <= N; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = ((i & size) == 0);
+                    const uint64_t a = k[i], b = k[j];
+                    const bool sw = up ? (a > b) : (a < b);
+                    k[i] = sw ? b : a;
+                    k[j] = sw ? a : b;
+                }
+            }
+}
+
+template <int N>
+__device__ __forceinline__ void sort_segment_regs(int a, int m, const int* __restrict__ pid, int* __restrict__ slots) {
+    uint64_t k[N];
+    int sl[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) sl[i] = (i < m) ? slots[a + i] : 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) k[i] = (i < m) ? (((uint64_t)(uint32_t)pid[sl[i]] << 32) | (uint32_t)sl[i]) : ~0ULL;
+    bitonic_regs<N>(k);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (i < m) slots[a + i] = (int)(uint32_t)k[i];
 }
 
 // sort each cell's slots by particle id (segments are short: ~ particles per cell)
@@ -107,22 +147,10 @@ __global__ void k_cell_sort(const uint64_t* __restrict__ start, int Nc, const in
     const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
     const int m = b - a;
     if (m <= 1) return;
-    constexpr int kLocal = 48;
-    if (m <= kLocal) {
-        uint64_t key[kLocal];
-        int sl[kLocal];
-        for (int i = 0; i < m; ++i) sl[i] = slots[a + i];
-        for (int i = 0; i < m; ++i) key[i] = ((uint64_t)(uint32_t)pid[sl[i]] << 32) | (uint32_t)sl[i];
-        for (int i = 1; i < m; ++i) {
-            const uint64_t v = key[i];
-            int j = i;
-            while (j > 0 && key[j - 1] > v) {
-                key[j] = key[j - 1];
-                --j;
-            }
-            key[j] = v;
-        }
-        for (int i = 0; i < m; ++i) slots[a + i] = (int)(uint32_t)key[i];
+    if (m <= 16) {
+        sort_segment_regs<16>(a, m, pid, slots);
+    } else if (m <= 32) {
+        sort_segment_regs<32>(a, m, pid, slots);
     } else {
         // long segment: insertion sort in place in global memory
         for (int i = a + 1; i < b; ++i) {

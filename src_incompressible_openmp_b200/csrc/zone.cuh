@@ -156,24 +156,46 @@ __device__ __noinline__ void mt_twist_inplace_warp(uint64_t* A, int lane) {
     __syncwarp();
 }
 
+// copy a seeded 312-word state from global memory (one warp, 10 loads per lane in flight)
+__device__ __noinline__ void mt_load_warp(uint64_t* buf, const uint64_t* seeded, int lane) {
+    uint64_t w[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        const int i = lane + k * kWarp;
+        w[k] = (i < kMtN) ? seeded[i] : 0ULL;
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        const int i = lane + k * kWarp;
+        if (i < kMtN) buf[i] = w[k];
+    }
+    __syncwarp();
+}
+
 // Warp-uniform MT19937-64 stream with a single state buffer. Batches of up to 64 draws
 // may cross a block boundary: the words left in the old block move to `carry` first.
 struct ZoneMt {
     uint64_t* buf;
     uint64_t* carry;
+    const uint64_t* seeded;  // the zone's seeded state, loaded at the first draw
     int pos;     // next draw: carry[ncarry + pos] if pos < 0, else buf[pos]
     int ncarry;
     int lane;
 
-    __device__ __forceinline__ void init(uint64_t* b, uint64_t* c, int lane_) {
+    __device__ __forceinline__ void init(uint64_t* b, uint64_t* c, const uint64_t* s, int lane_) {
         buf = b;
         carry = c;
+        seeded = s;
         pos = kMtN;
         ncarry = 0;
         lane = lane_;
     }
     __device__ __forceinline__ void ensure(int k) {  // k <= 64
         if (pos + k <= kMtN) return;
+        if (seeded) {
+            mt_load_warp(buf, seeded, lane);
+            seeded = nullptr;
+        }
         const int left = kMtN - pos;  // 0..63 words still to draw from the old block
         for (int i = lane; i < left; i += kWarp) carry[i] = buf[pos + i];
         __syncwarp();
@@ -227,7 +249,17 @@ __device__ __forceinline__ void zone_shuffle(T* a, int m, ZoneMt& r, int lane) {
     while (i != m) {
         const uint64_t sr = (uint64_t)i + 1ULL;
         const uint64_t x = r.uint_in(0, sr * (sr + 1ULL) - 1ULL);
-        const int p1 = (int)(x / (sr + 1ULL)), p2 = (int)(x % (sr + 1ULL));
+        // x < sr (sr + 1) < 2^32 for the list sizes here: 32-bit division is exact
+        int p1, p2;
+        if (sr < 65535ULL) {
+            const uint32_t x32 = (uint32_t)x, b1 = (uint32_t)sr + 1u;
+            const uint32_t q = x32 / b1;
+            p1 = (int)q;
+            p2 = (int)(x32 - q * b1);
+        } else {
+            p1 = (int)(x / (sr + 1ULL));
+            p2 = (int)(x % (sr + 1ULL));
+        }
         if (lane == 0) {
             T t = a[i];
             a[i] = a[p1];
@@ -824,23 +856,23 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         }
     }
     // zone cells: segment starts and ownership
-    for (int l = lane; l < S.nl; l += kWarp) {
-        const int c = S.gy_of(l) + p.Ny * S.gx_of(l);
-        const int own = A.owner[c];
-        M.gstart[l] = (int)(uint32_t)A.start[c];
-        M.cflags[l] = (own == z + 1) ? kCOwned : 0;
-    }
-    {
-        uint64_t w[10];
+    for (int l0 = 0; l0 < S.nl; l0 += 4 * kWarp) {
+        int own[4];
+        uint64_t st[4];
 #pragma unroll
-        for (int k = 0; k < 10; ++k) {
-            const int i = lane + k * kWarp;
-            w[k] = (i < kMtN) ? A.seeds[(size_t)z * kMtN + i] : 0ULL;
+        for (int k = 0; k < 4; ++k) {
+            const int l = l0 + lane + k * kWarp;
+            const int c = (l < S.nl) ? S.gy_of(l) + p.Ny * S.gx_of(l) : 0;
+            own[k] = (l < S.nl) ? A.owner[c] : 0;
+            st[k] = (l < S.nl) ? A.start[c] : 0ULL;
         }
 #pragma unroll
-        for (int k = 0; k < 10; ++k) {
-            const int i = lane + k * kWarp;
-            if (i < kMtN) M.mt[i] = w[k];
+        for (int k = 0; k < 4; ++k) {
+            const int l = l0 + lane + k * kWarp;
+            if (l < S.nl) {
+                M.gstart[l] = (int)(uint32_t)st[k];
+                M.cflags[l] = (own[k] == z + 1) ? kCOwned : 0;
+            }
         }
     }
     __syncwarp();
@@ -854,7 +886,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         M.cap[l] = 0;
     }
     __syncwarp();
-    S.rng.init(M.mt, M.carry, lane);
+    S.rng.init(M.mt, M.carry, A.seeds + (size_t)z * kMtN, lane);
 
     // dense passes (src/zone_pass.cpp:708-781)
     for (int pass = 0; pass < p.maxPasses && !S.failed && !S.fatal; ++pass) {
@@ -866,9 +898,12 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     }
     // sparse phase (src/zone_pass.cpp:783-854)
     if (!S.failed && !S.fatal) {
-        S.compute_nsm();
+        // the smoothed occupancy feeds the maps only with local fluid-fraction thresholds;
+        // otherwise it is needed only if some cell is sparse (inward gradient, donor scores)
+        if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
         const int nlow = S.collect([&](int l) { return M.cnt[l] > 0 && (double)M.cnt[l] < S.map_low(l); });
+        if (!p.useLFF && nlow > 0) S.compute_nsm();
         zone_shuffle(M.list, nlow, S.rng, lane);
         for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
     }
@@ -940,18 +975,24 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         du2[l] = d2;
     }
     __syncwarp();
-    // zone stats[4], stats[5] in ascending cell order (src/zone_pass.cpp:911-922)
-    if (lane == 0) {
-        double acc = 0.0, mx = 0.0;
-        int cntDU = 0;
-        for (int l = 0; l < S.nl; ++l) {
-            const double d2 = du2[l];
-            mx = smax(mx, sqrt(d2));
-            if (d2 > 0.0) {
-                acc = __dadd_rn(acc, d2);
-                ++cntDU;
-            }
+    // zone stats[4], stats[5] (src/zone_pass.cpp:911-922): the sum of positive dU2 in
+    // ascending cell order and their maximum (zero entries change neither)
+    double acc = 0.0, mx = 0.0;
+    int cntDU = 0;
+    for (int b = 0; b < S.nl; b += kWarp) {
+        const int l = b + lane;
+        const double d2 = (l < S.nl) ? du2[l] : 0.0;
+        unsigned pos = __ballot_sync(0xffffffffu, d2 > 0.0);
+        while (pos) {
+            const int q = __ffs(pos) - 1;
+            pos &= pos - 1;
+            const double v = __shfl_sync(0xffffffffu, d2, q);
+            acc = __dadd_rn(acc, v);
+            mx = smax(mx, sqrt(v));
+            ++cntDU;
         }
+    }
+    if (lane == 0) {
         A.zoneCorr[z] = make_double2((cntDU > 0) ? sqrt(__ddiv_rn(acc, (double)cntDU)) : 0.0, (cntDU > 0) ? mx : 0.0);
         A.zoneMoved[z] = make_int2(S.movedDense, S.movedSparse);
     }
