@@ -180,6 +180,23 @@ int mpcd_srd_collide(mpcd_ctx* ctx, uint64_t seed);
 int mpcd_srd_collide_cells(mpcd_ctx* ctx, const int32_t* cid, uint64_t seed);
 /* mpcd::compute_cell_fields (reference src/common_grid.cpp:32-100) of the current state */
 int mpcd_cell_fields(mpcd_ctx* ctx, double rho_target, mpcd_cellfields_c* out);
+/* No counterpart in the reference: mpcd_cell_fields on a caller-owned device state, for
+ * callers that must not allocate device memory (a host code that drives its own time loop
+ * from a memory pool reserved up front; cudaFree would also synchronise its other streams).
+ * No context is needed and nothing is allocated: the working memory is one static device
+ * array of 4 * MPCD_STATIC_FIELDS_MAX_CELLS doubles (32 MiB) per device.
+ *   params   grid and cell constants (Nx, Ny, Nc, Lx, Ly, Kvirial, ...); params->n is not used
+ *   d_x, d_v 2n doubles each, particle-id order, on the current device
+ *   d_out    DEVICE arrays of Nc entries on the current device, any pointer NULL to skip
+ *   stream   a cudaStream_t (NULL: the legacy default stream); the call only enqueues work
+ * Returns MPCD_ERR_CAPACITY if Nc > MPCD_STATIC_FIELDS_MAX_CELLS. The first call on a device
+ * looks up the array's device address (and may load the module there): make that first call
+ * before any stream capture. Every call on a device shares the array and zeroes it first;
+ * calls that overlap on the GPU race. Sums are accumulated with atomics, so the fields may
+ * differ from mpcd_cell_fields in the last bits (counts are exact). */
+#define MPCD_STATIC_FIELDS_MAX_CELLS 1048576
+int mpcd_cell_fields_static(const mpcd_params_c* params, const double* d_x, const double* d_v, int64_t n,
+                            double rho_target, const mpcd_cellfields_c* d_out, void* stream);
 /* Snapshot the current state as the closure's reference state ("stateRef"). */
 int mpcd_save_ref(mpcd_ctx* ctx);
 /* mpcd::run_zone_pass_openmp (reference src/zone_pass_openmp.cpp:176-182, snapshot

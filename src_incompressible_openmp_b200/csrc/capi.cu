@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1352,3 +1353,151 @@ void mpcd_host_free(void* p) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// mpcd_cell_fields_static: compute_cell_fields (reference src/common_grid.cpp:32-100) of a
+// caller-owned device state, without a context and without allocating device memory.
+//
+// It serves callers that must not allocate: a host code that embeds the MPCD state in its own
+// time loop, has reserved the device memory it may use up front (its own pool sized to the
+// GPU), and needs the cell fields between steps. Creating a context would allocate; and
+// cudaFree synchronises the whole device, which would stall the caller's other streams.
+//
+// Its only working memory is the file-scope array below: per cell, the particle count, the two
+// momentum sums and the sum of squared peculiar speeds. The array is shared by every call on
+// a device, so calls whose work overlaps on the GPU (two streams, two host threads) race on it
+// and must be serialised by the caller.
+namespace mpcd_dev {
+
+constexpr int kStaticMaxDevices = 64;
+
+// 4 doubles per cell: [count | sum vx | sum vy | sum |v - u|^2], each block Nc long.
+__global__ void k_static_accumulate(DevParams P, const double* __restrict__ x, const double* __restrict__ v,
+                                    int n, double* __restrict__ acc) {
+    const size_t nc = (size_t)P.Nc;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = cell_of(x[2 * (size_t)i], x[2 * (size_t)i + 1], P);
+        atomicAdd(acc + c, 1.0);
+        atomicAdd(acc + nc + c, v[2 * (size_t)i]);
+        atomicAdd(acc + 2 * nc + c, v[2 * (size_t)i + 1]);
+    }
+}
+
+__global__ void k_static_peculiar(DevParams P, const double* __restrict__ x, const double* __restrict__ v,
+                                  int n, double* __restrict__ acc) {
+    const size_t nc = (size_t)P.Nc;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = cell_of(x[2 * (size_t)i], x[2 * (size_t)i + 1], P);
+        const double m = acc[c];
+        if (m < 2.0) continue;  // a cell of one particle has no thermal degrees of freedom
+        const double ux = __ddiv_rn(acc[nc + c], m), uy = __ddiv_rn(acc[2 * nc + c], m);
+        const double ax = __dsub_rn(v[2 * (size_t)i], ux), ay = __dsub_rn(v[2 * (size_t)i + 1], uy);
+        atomicAdd(acc + 3 * nc + c, __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
+    }
+}
+
+// The per-cell formulas of k_cell_fields, from the accumulated sums.
+__global__ void k_static_finish(DevParams Pm, const double* __restrict__ acc, double rhoTarget, FieldsOut o) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Pm.Nc) return;
+    const size_t nc = (size_t)Pm.Nc;
+    const int m = (int)acc[c];
+    const double px = acc[nc + c], py = acc[2 * nc + c];
+    double ux = 0.0, uy = 0.0;
+    if (m > 0) {
+        ux = __ddiv_rn(px, (double)m);
+        uy = __ddiv_rn(py, (double)m);
+    }
+    const double rho = __ddiv_rn((double)m, Pm.Vc);
+    double T = 0.0, pk = 0.0;
+    const int dof = 2 * max(m - 1, 0);
+    if (dof > 0) {
+        T = __ddiv_rn(acc[3 * nc + c], (double)dof);
+        pk = __dmul_rn(rho, T);
+    }
+    const double pv = __dmul_rn(Pm.Kvirial, __dsub_rn(rho, rhoTarget));
+    if (o.N) o.N[c] = m;
+    if (o.Ux) o.Ux[c] = ux;
+    if (o.Uy) o.Uy[c] = uy;
+    if (o.Px) o.Px[c] = px;
+    if (o.Py) o.Py[c] = py;
+    if (o.T) o.T[c] = T;
+    if (o.rho) o.rho[c] = rho;
+    if (o.Pkin) o.Pkin[c] = pk;
+    if (o.Pvir) o.Pvir[c] = pv;
+    if (o.P) o.P[c] = __dadd_rn(pk, pv);
+    if (o.rhoTarget) o.rhoTarget[c] = rhoTarget;
+}
+
+}  // namespace mpcd_dev
+
+// The scratch of mpcd_cell_fields_static: 4 * MPCD_STATIC_FIELDS_MAX_CELLS doubles (32 MiB),
+// part of the module's static device memory on every device the library is loaded on.
+static __device__ __align__(256) double g_static_fields_scratch[4 * (size_t)MPCD_STATIC_FIELDS_MAX_CELLS];
+
+namespace {
+
+std::mutex g_static_mu;
+double* g_static_ptr[mpcd_dev::kStaticMaxDevices] = {};
+
+// Set-up, once per device, with that device current: the device address of the scratch array.
+// This is the first call's extra work (it may also load the module onto the device).
+int static_scratch(int dev, double** out) {
+    if (dev < 0 || dev >= mpcd_dev::kStaticMaxDevices)
+        return set_err(MPCD_ERR_INVALID_ARG, "mpcd_cell_fields_static: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_fields_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return set_err(MPCD_ERR_CUDA, std::string("mpcd_cell_fields_static: cudaGetSymbolAddress failed: ") +
+                                              cudaGetErrorString(e));
+        }
+        g_static_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_static_ptr[dev];
+    return MPCD_OK;
+}
+
+}  // namespace
+
+extern "C" int mpcd_cell_fields_static(const mpcd_params_c* params, const double* d_x, const double* d_v, int64_t n,
+                                       double rho_target, const mpcd_cellfields_c* d_out, void* stream) {
+    if (!params || !d_out || (n > 0 && (!d_x || !d_v)))
+        return set_err(MPCD_ERR_INVALID_ARG, "mpcd_cell_fields_static: null argument");
+    int rc = validate(*params);
+    if (rc) return rc;
+    if (n < 0 || 2 * n >= (1LL << 31)) return set_err(MPCD_ERR_INVALID_ARG, "mpcd_cell_fields_static: n out of range");
+    if (params->Nc > MPCD_STATIC_FIELDS_MAX_CELLS)
+        return set_err(MPCD_ERR_CAPACITY, "mpcd_cell_fields_static: Nc = " + std::to_string(params->Nc) +
+                                              " exceeds the static scratch maximum of " +
+                                              std::to_string(MPCD_STATIC_FIELDS_MAX_CELLS) + " cells");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    double* acc = nullptr;
+    rc = static_scratch(dev, &acc);
+    if (rc) return rc;
+    const DevParams P = make_dev_params(*params);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t nc = (size_t)params->Nc;
+    // everything the kernels accumulate into starts at zero
+    CUDA_TRY(cudaMemsetAsync(acc, 0, 4 * nc * sizeof(double), s));
+    const bool wantT = d_out->T || d_out->Pkin || d_out->P;
+    if (n > 0) {
+        const int grid = (int)std::min<int64_t>(blocks_for(n), 148 * 16);
+        k_static_accumulate<<<grid, kThreads, 0, s>>>(P, d_x, d_v, (int)n, acc);
+        CUDA_TRY(cudaGetLastError());
+        if (wantT) {
+            k_static_peculiar<<<grid, kThreads, 0, s>>>(P, d_x, d_v, (int)n, acc);
+            CUDA_TRY(cudaGetLastError());
+        }
+    }
+    FieldsOut o{};
+    o.N = d_out->N;
+    o.Ux = d_out->Ux; o.Uy = d_out->Uy; o.Px = d_out->Px; o.Py = d_out->Py; o.T = d_out->T;
+    o.rho = d_out->rho; o.Pkin = d_out->Pkin; o.Pvir = d_out->Pvir; o.P = d_out->P; o.rhoTarget = d_out->rhoTarget;
+    k_static_finish<<<blocks_for(params->Nc), kThreads, 0, s>>>(P, acc, rho_target, o);
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}

@@ -73,6 +73,8 @@ def lib():
         "mpcd_step_timed": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
         "mpcd_step_profile": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double), C.c_int], C.c_int),
         "mpcd_launch_count": ([C.c_void_p], C.c_int64),
+        "mpcd_cell_fields_static": ([P(_abi.ParamsC), C.c_void_p, C.c_void_p, C.c_int64, C.c_double,
+                                     P(_abi.CellFieldsC), C.c_void_p], C.c_int),
         "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
         "mpcd_host_free": ([C.c_void_p], None),
     }
@@ -124,6 +126,19 @@ def _fields_struct(Nc):
     for k in _abi.FIELD_NAMES:
         setattr(s, k, arrs[k].ctypes.data_as(C.POINTER(C.c_double)))
     return s, arrs
+
+
+def cell_fields_static(params, x_ptr, v_ptr, n, rho_target, out_ptrs, stream=0):
+    """mpcd_cell_fields_static: cell fields of a caller-owned device state (device pointers
+    x_ptr, v_ptr of 2n doubles) into caller-owned device arrays out_ptrs {field: pointer}
+    (fields of mpcd_cellfields_c; missing ones are skipped), enqueued on `stream`."""
+    s = _abi.CellFieldsC()
+    for k, ptr in out_ptrs.items():
+        t = C.c_int32 if k == "N" else C.c_double
+        setattr(s, k, C.cast(C.c_void_p(ptr), C.POINTER(t)))
+    pc = to_c(params)
+    _check(lib().mpcd_cell_fields_static(C.byref(pc), C.c_void_p(x_ptr), C.c_void_p(v_ptr), n, rho_target,
+                                         C.byref(s), C.c_void_p(stream)))
 
 
 class Context:
