@@ -295,6 +295,46 @@ struct ZoneNormal {
     }
 };
 
+// Repacks the materialised lists of a zone at the bottom of its arena, in arena order;
+// returns the new arena top. Out of line: it runs only when the arena is full.
+__device__ __noinline__ int zone_compact(uint8_t* cflags, int* abase, int* head, const int* len, int* cap,
+                                         uint16_t* order, uint32_t* arena, int nl, int lane) {
+    for (int l = lane; l < nl; l += kWarp) {
+        int r = 0;
+        if (cflags[l] & kCMat)
+            for (int q = 0; q < nl; ++q)
+                if ((cflags[q] & kCMat) && (abase[q] < abase[l] || (abase[q] == abase[l] && q < l))) ++r;
+        order[l] = (uint16_t)r;
+    }
+    __syncwarp();
+    int nmat = 0;
+    for (int l = 0; l < nl; ++l) nmat += (cflags[l] & kCMat) ? 1 : 0;
+    int off = 0;
+    for (int r = 0; r < nmat; ++r) {
+        int l = 0;
+        for (int q = 0; q < nl; ++q)
+            if ((cflags[q] & kCMat) && order[q] == r) l = q;
+        const int a = abase[l] + head[l], n = len[l];
+        // off <= a: copy down in ascending chunks (reads of a chunk precede its writes)
+        for (int j0 = 0; j0 < n; j0 += kWarp) {
+            const int j = j0 + lane;
+            const uint32_t v = (j < n) ? arena[a + j] : 0u;
+            __syncwarp();
+            if (j < n) arena[off + j] = v;
+            __syncwarp();
+        }
+        if (lane == 0) {
+            abase[l] = off;
+            head[l] = 0;
+            cap[l] = n;
+        }
+        off += n;
+        __syncwarp();
+    }
+    __syncwarp();
+    return off;
+}
+
 // Scalar (warp-uniform) state of one zone.
 struct ZoneState {
     ZoneMem M;
@@ -431,41 +471,9 @@ struct ZoneState {
         return ((uint32_t)l << kEntryShift) | (uint32_t)(M.head[l] + i);
     }
 
-    // repack the materialised lists at the bottom of the arena (in arena order)
+    // repack the materialised lists at the bottom of the arena (rare: out of line)
     __device__ void compact() {
-        for (int l = lane; l < nl; l += kWarp) {
-            int r = 0;
-            if (M.cflags[l] & kCMat)
-                for (int q = 0; q < nl; ++q)
-                    if ((M.cflags[q] & kCMat) && (M.abase[q] < M.abase[l] || (M.abase[q] == M.abase[l] && q < l))) ++r;
-            M.order[l] = (uint16_t)r;
-        }
-        __syncwarp();
-        int nmat = 0;
-        for (int l = 0; l < nl; ++l) nmat += (M.cflags[l] & kCMat) ? 1 : 0;
-        int off = 0;
-        for (int r = 0; r < nmat; ++r) {
-            int l = 0;
-            for (int q = 0; q < nl; ++q)
-                if ((M.cflags[q] & kCMat) && M.order[q] == r) l = q;
-            const int a = M.abase[l] + M.head[l], n = M.len[l];
-            // off <= a: copy down in ascending chunks (reads of a chunk precede its writes)
-            for (int j0 = 0; j0 < n; j0 += kWarp) {
-                const int j = j0 + lane;
-                const uint32_t v = (j < n) ? M.arena[a + j] : 0u;
-                __syncwarp();
-                if (j < n) M.arena[off + j] = v;
-                __syncwarp();
-            }
-            if (lane == 0) {
-                M.abase[l] = off;
-                M.head[l] = 0;
-                M.cap[l] = n;
-            }
-            off += n;
-        }
-        arenaTop = off;
-        __syncwarp();
+        arenaTop = zone_compact(M.cflags, M.abase, M.head, M.len, M.cap, M.order, M.arena, nl, lane);
     }
 
     // materialise or grow list t so that `extra` entries can be appended
@@ -684,19 +692,17 @@ struct ZoneState {
         const double hl = map_high(l);
         if ((double)ncc <= hl) return;
         int nrecv = 0, moved = 0;
-        const int needOut = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
-        if (needOut > 0) {
-            int m = admissible(l, true, cand);
-            int nT = rank_dense(l, cand, m, true, T);
-            moved += spread(l, T, nT, true, needOut, recv, nrecv);
+        // first towards the low-threshold map, then whatever is left towards the high one
+        // (one copy of the code for both rounds)
+#pragma unroll 1
+        for (int round = 0; round < 2; ++round) {
+            const int need = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
+            if (need <= 0) break;
+            const bool low = (round == 0);
+            const int m = admissible(l, low, cand);
+            const int nT = rank_dense(l, cand, m, low, T);
+            moved += spread(l, T, nT, low, need, recv, nrecv);
             if (failed || fatal) return;
-            const int rem = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
-            if (rem > 0) {
-                m = admissible(l, false, cand);
-                nT = rank_dense(l, cand, m, false, T);
-                moved += spread(l, T, nT, false, rem, recv, nrecv);
-                if (failed || fatal) return;
-            }
         }
         if (lane < nrecv) M.cflags[recv[lane]] |= (kCRecv | kCChanged);
         if (lane == 0 && moved > 0) M.cflags[l] |= kCChanged;
