@@ -172,6 +172,22 @@ __device__ __noinline__ void mt_load_warp(uint64_t* buf, const uint64_t* seeded,
     __syncwarp();
 }
 
+// 64-bit division and remainder on rare paths, out of line to keep the zone kernel small
+__device__ __noinline__ uint64_t umod64_slow(uint64_t a, uint64_t b) { return a % b; }
+__device__ __noinline__ uint64_t udiv64_slow(uint64_t a, uint64_t b) { return a / b; }
+
+// Next block of a zone's stream (out of line, once per 312 draws): loads the seeded state
+// on first use, keeps the kMtN - pos words not yet drawn in `carry`, twists in place.
+// Returns the number of carried words.
+__device__ __noinline__ int mt_refill(uint64_t* buf, uint64_t* carry, const uint64_t* seeded, int pos, int lane) {
+    if (seeded) mt_load_warp(buf, seeded, lane);
+    const int left = kMtN - pos;  // 0..63 words still to draw from the old block
+    for (int i = lane; i < left; i += kWarp) carry[i] = buf[pos + i];
+    __syncwarp();
+    mt_twist_inplace_warp(buf, lane);
+    return left;
+}
+
 // Warp-uniform MT19937-64 stream with a single state buffer. Batches of up to 64 draws
 // may cross a block boundary: the words left in the old block move to `carry` first.
 struct ZoneMt {
@@ -192,14 +208,8 @@ struct ZoneMt {
     }
     __device__ __forceinline__ void ensure(int k) {  // k <= 64
         if (pos + k <= kMtN) return;
-        if (seeded) {
-            mt_load_warp(buf, seeded, lane);
-            seeded = nullptr;
-        }
-        const int left = kMtN - pos;  // 0..63 words still to draw from the old block
-        for (int i = lane; i < left; i += kWarp) carry[i] = buf[pos + i];
-        __syncwarp();
-        mt_twist_inplace_warp(buf, lane);
+        const int left = mt_refill(buf, carry, seeded, pos, lane);
+        seeded = nullptr;
         ncarry = left;
         pos = -left;
     }
@@ -221,7 +231,7 @@ struct ZoneMt {
         uint64_t low = u * range;
         uint64_t high = __umul64hi(u, range);
         if (low < range) {
-            const uint64_t thr = (0ULL - range) % range;
+            const uint64_t thr = umod64_slow(0ULL - range, range);
             while (low < thr) {
                 u = next();
                 low = u * range;
@@ -257,8 +267,9 @@ __device__ __forceinline__ void zone_shuffle(T* a, int m, ZoneMt& r, int lane) {
             p1 = (int)q;
             p2 = (int)(x32 - q * b1);
         } else {
-            p1 = (int)(x / (sr + 1ULL));
-            p2 = (int)(x % (sr + 1ULL));
+            const uint64_t q = udiv64_slow(x, sr + 1ULL);
+            p1 = (int)q;
+            p2 = (int)(x - q * (sr + 1ULL));
         }
         if (lane == 0) {
             T t = a[i];
