@@ -284,6 +284,9 @@ __device__ __forceinline__ void zone_shuffle(T* a, int m, ZoneMt& r, int lane) {
     __syncwarp();
 }
 
+// sqrt(-2 ln r2 / r2) of the polar method, out of line
+__device__ __noinline__ double polar_scale(double r2) { return sqrt(__ddiv_rn(__dmul_rn(-2.0, log_cr_dev(r2)), r2)); }
+
 // polar-method normal deviate (libstdc++ normal_distribution), one cached value
 struct ZoneNormal {
     double saved;
@@ -299,7 +302,7 @@ struct ZoneNormal {
             y = __dsub_rn(__dmul_rn(2.0, r.u01()), 1.0);
             r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
         } while (r2 > 1.0 || r2 == 0.0);
-        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log_cr_dev(r2)), r2));
+        const double mult = polar_scale(r2);
         saved = __dmul_rn(x, mult);
         has = 1;
         return __dmul_rn(y, mult);
@@ -345,6 +348,48 @@ __device__ __noinline__ int zone_compact(uint8_t* cflags, int* abase, int* head,
     __syncwarp();
     return off;
 }
+
+// smoothed occupancy on the zone plus a one-cell ring (src/zone_pass.cpp:296-319):
+// 3x3 binomial weights, renormalised over the in-domain neighbours. Out of line (called at
+// most twice per pass).
+__device__ __noinline__ void zone_compute_nsm(double* nsm, const int* win, const int* cnt, int xs, int ys, int TX,
+                                              int TY, int Nx, int Ny, int perx, int pery, int lane) {
+    const int GX = TX + 2, GY = TY + 2, WY = TY + 4;
+    for (int g = lane; g < GX * GY; g += kWarp) {
+        int ix = xs - 1 + g / GY, iy = ys - 1 + g % GY;
+        if (perx) ix = wrap_index(ix, Nx);
+        if (pery) iy = wrap_index(iy, Ny);
+        double val = 0.0;
+        if (ix >= 0 && ix < Nx && iy >= 0 && iy < Ny) {
+            double acc = 0.0, ws = 0.0;
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int jy = iy + dy, jx = ix + dx;
+                    if (jy < 0 || jy >= Ny || jx < 0 || jx >= Nx) continue;
+                    const double w = ((dx == 0) ? 2.0 : 1.0) * ((dy == 0) ? 2.0 : 1.0) * 0.0625;
+                    int c;
+                    if (jx >= xs && jx < xs + TX && jy >= ys && jy < ys + TY) {
+                        c = cnt[(jx - xs) * TY + (jy - ys)];
+                    } else {
+                        int wx = jx - (xs - 2), wy = jy - (ys - 2);
+                        if (wx < 0) wx += Nx;
+                        else if (wx >= TX + 4) wx -= Nx;
+                        if (wy < 0) wy += Ny;
+                        else if (wy >= WY) wy -= Ny;
+                        c = win[wx * WY + wy];
+                    }
+                    acc = __dadd_rn(acc, __dmul_rn(w, (double)c));
+                    ws = __dadd_rn(ws, w);
+                }
+            val = __ddiv_rn(acc, smax(ws, 1e-30));
+        }
+        nsm[g] = val;
+    }
+    __syncwarp();
+}
+
+// hypot, out of line (once per sparse cell)
+__device__ __noinline__ double zone_hypot(double a, double b) { return mpcd_dd::hypot_cr(a, b); }
 
 // Scalar (warp-uniform) state of one zone.
 struct ZoneState {
@@ -429,28 +474,7 @@ struct ZoneState {
 
     // ------------------------------------------------------------------ smoothing, maps
     __device__ void compute_nsm() {
-        const DevParams& p = P();
-        const int GX = TX + 2, GY = TY + 2;
-        for (int g = lane; g < GX * GY; g += kWarp) {
-            int ix = xs - 1 + g / GY, iy = ys - 1 + g % GY;
-            if (p.perx) ix = wrap_index(ix, p.Nx);
-            if (p.pery) iy = wrap_index(iy, p.Ny);
-            double val = 0.0;
-            if (ix >= 0 && ix < p.Nx && iy >= 0 && iy < p.Ny) {
-                double acc = 0.0, ws = 0.0;
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        const int jy = iy + dy, jx = ix + dx;
-                        if (jy < 0 || jy >= p.Ny || jx < 0 || jx >= p.Nx) continue;
-                        const double w = ((dx == 0) ? 2.0 : 1.0) * ((dy == 0) ? 2.0 : 1.0) * 0.0625;
-                        acc = __dadd_rn(acc, __dmul_rn(w, (double)cnt_at(jx, jy)));
-                        ws = __dadd_rn(ws, w);
-                    }
-                val = __ddiv_rn(acc, smax(ws, 1e-30));
-            }
-            M.nsm[g] = val;
-        }
-        __syncwarp();
+        zone_compute_nsm(M.nsm, M.win, M.cnt, xs, ys, TX, TY, P().Nx, P().Ny, P().perx, P().pery, lane);
     }
 
     // start of a map build: record which cells are bulk (cnt > 0)
@@ -648,27 +672,34 @@ struct ZoneState {
         return m;
     }
 
-    // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589)
+    // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589). Lane k holds
+    // target k's map value and deficit; a move changes only the deficit of its own target, so
+    // each round walks the targets whose deficit was positive at the start of the round.
     __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int* recv, int& nrecv) {
         if (needOut <= 0 || nT == 0) return 0;
         const int srcLen = M.len[s];
         if (srcLen == 0) return 0;
+        int tl = -1, defj = 0;
+        double mv = 0.0;
+        if (lane < nT) {
+            tl = T[lane];
+            mv = map_val(tl, low);
+            defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
+        }
         int taken = 0, moved = 0;
-        while (needOut > 0 && taken < srcLen) {
-            bool progressed = false;
-            for (int kk = 0; kk < nT; ++kk) {
-                int defj = 0;
-                if (lane < nT) {
-                    const int t = T[lane];
-                    defj = max(0, (int)floor(__dsub_rn(map_val(t, low), (double)M.cnt[t])));
-                }
-                const unsigned pm = __ballot_sync(0xffffffffu, lane < nT && defj > 0);
+        bool stop = false;
+        while (!stop && needOut > 0 && taken < srcLen) {
+            const unsigned pm = __ballot_sync(0xffffffffu, lane < nT && defj > 0);
+            if (pm == 0) break;  // no target can take a particle: no progress
+            unsigned rest = pm;
+            while (rest) {
+                const int kk = __ffs(rest) - 1;
+                rest &= rest - 1;
                 const int deficit = __shfl_sync(0xffffffffu, defj, kk);
-                if (deficit <= 0) continue;
+                const int t = __shfl_sync(0xffffffffu, tl, kk);
                 const int remaining = __popc(pm >> kk);
                 const int quota = max(1, (int)ceil(__ddiv_rn((double)needOut, (double)max(1, remaining))));
                 const int nt = max(1, min(min(quota, deficit), min(needOut, srcLen - taken)));
-                const int t = T[kk];
                 if (t == s) {
                     if (lane == 0) raise_error(A->st, kErrTargetIsSource, zone);
                     fatal = true;
@@ -676,13 +707,15 @@ struct ZoneState {
                 }
                 if (!move_into(s, taken, nt, t)) return moved;
                 push_recv(recv, nrecv, t);
+                if (lane == kk) defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
                 taken += nt;
                 moved += nt;
                 needOut -= nt;
-                progressed = true;
-                if (needOut <= 0 || taken >= srcLen) break;
+                if (needOut <= 0 || taken >= srcLen) {
+                    stop = true;
+                    break;
+                }
             }
-            if (!progressed) break;
         }
         if (moved > 0 && lane == 0) {
             M.head[s] += taken;
@@ -769,7 +802,7 @@ struct ZoneState {
         double gx, gy;
         inward(l, gx, gy);
         zone_shuffle(don, nd, rng, lane);
-        const double ndir = mpcd_dd::hypot_cr(gx, gy);
+        const double ndir = zone_hypot(gx, gy);
         ZoneNormal N;
         N.has = 0;
         N.saved = 0.0;
