@@ -140,7 +140,7 @@ const char* mpcd_last_error(void);
 /* 1 if a usable sm_100 device is present, else 0 (sets no error) */
 int mpcd_device_available(void);
 /* Parses a params.kv file (reference src/params_io.cpp:74-137; strict: every key required,
- * unknown keys ignored). Benchmark keys are read separately (mpcd_read_kv_int / _string). */
+ * unknown keys ignored). Other keys are read with mpcd_read_kv_string. */
 int mpcd_read_params_kv(const char* path, mpcd_params_c* out);
 /* Any key of a params.kv file as a string (the reference driver reads benchmark_nSteps,
  * benchmark_metricsEvery and benchmark_dumpSteps this way:
@@ -197,7 +197,9 @@ int mpcd_cell_fields(mpcd_ctx* ctx, double rho_target, mpcd_cellfields_c* out);
 #define MPCD_STATIC_FIELDS_MAX_CELLS 1048576
 int mpcd_cell_fields_static(const mpcd_params_c* params, const double* d_x, const double* d_v, int64_t n,
                             double rho_target, const mpcd_cellfields_c* d_out, void* stream);
-/* Snapshot the current state as the closure's reference state ("stateRef"). */
+/* Snapshot the current state as the closure's reference state ("stateRef"): its cell fields,
+ * pressure drive and EOS kick. The snapshot stays until the next mpcd_save_ref (setting a new
+ * state does not clear it), so stateRef and stateRed may come from separate uploads. */
 int mpcd_save_ref(mpcd_ctx* ctx);
 /* mpcd::run_zone_pass_openmp (reference src/zone_pass_openmp.cpp:176-182, snapshot
  * semantics of :34-172). mode: mpcd_layout_mode. metrics nullable. */

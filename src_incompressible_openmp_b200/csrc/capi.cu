@@ -852,7 +852,6 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
         CUDA_TRY(cudaGetLastError());
     }
     invalidate_positions(c);
-    c->refValid = false;
     return check_device(c);
 }
 
@@ -930,7 +929,6 @@ int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_collide(c, seed);
     if (rc) return rc;
-    c->refValid = false;
     return check_device(c);
 }
 

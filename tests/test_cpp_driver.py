@@ -1,0 +1,136 @@
+"""The reference's own caller on the GPU library, and mpcd_bench, against the reference.
+
+Three runs of the profiled Poiseuille benchmark on the same case files:
+  A. oracle/_ref/ref_bench:      the reference driver on the reference library (CPU);
+  B. oracle/_ref/ref_main_b200:  the reference driver, unmodified, compiled against the C++ shim
+                                 (include/compat -> include/mpcd_b200.hpp) and linked to
+                                 libmpcd_b200.so: every phase call runs on the GPU;
+  C. src_incompressible_openmp_b200/bin/mpcd_bench: this library's device-resident driver with
+                                 the same command line.
+The runs are free (no teacher forcing), so the one-ulp differences of thermal-wall draws may
+propagate: states must agree within 1e-9 relative, integer columns exactly and the printed
+metrics (6 significant digits) within 1e-5 relative.
+"""
+import csv
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state, write_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+REF_ON_B200 = os.path.join(ROOT, "oracle", "_ref", "ref_main_b200")
+MPCD_BENCH = os.path.join(ROOT, "src_incompressible_openmp_b200", "bin", "mpcd_bench")
+
+INT_COLS = ("step", "particlesMovedDense", "particlesMovedSparse", "nMaskedInterzoneCells")
+SKIP_COLS = ("nThreadsUsedBase", "nThreadsUsedShifted", "timeStepTotal", "timeRefBuild", "timeBase", "timeShifted",
+             "timeClosure", "timeDiagnostics", "timeDump")
+N_STEPS = 6
+
+
+def run_driver(exe, case, out_prefix):
+    args = [exe, os.path.join(case, "params.kv"), os.path.join(case, "in_x.bin"), os.path.join(case, "in_v.bin"),
+            os.path.join(case, "in_type.bin"), os.path.join(case, "in_r0.bin"), out_prefix, "1", "1", "2"]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, f"{os.path.basename(exe)} failed: {r.stderr[-500:]}"
+
+
+def read_csv(path):
+    with open(path) as f:
+        return list(csv.DictReader(f))
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+
+@pytest.fixture(scope="module")
+def runs(tmp_path_factory):
+    for exe in (REF_BENCH, REF_ON_B200, MPCD_BENCH):
+        if not os.path.exists(exe):
+            pytest.fail(f"not built: {exe} (run __graft_entry__.build())")
+    d = str(tmp_path_factory.mktemp("driver"))
+    p = poiseuille_params(40, 20, 10)
+    x, v = uniform_state(p, 5)
+    case = os.path.join(d, "case")
+    write_case(case, p, x, v, {"benchmark_nSteps": N_STEPS, "benchmark_metricsEvery": 2, "benchmark_dumpSteps": "0,3,6"})
+    out = {}
+    for key, exe in (("ref", REF_BENCH), ("shim", REF_ON_B200), ("ours", MPCD_BENCH)):
+        prefix = os.path.join(d, key, "run")
+        os.makedirs(os.path.dirname(prefix))
+        run_driver(exe, case, prefix)
+        out[key] = prefix
+    return p, out
+
+
+def load_state(prefix, step, n):
+    s = f"{prefix}_step{step:04d}"
+    x = np.fromfile(s + "_x.bin", np.float64)
+    v = np.fromfile(s + "_v.bin", np.float64)
+    assert x.size == 2 * n and v.size == 2 * n
+    return x, v
+
+
+def load_cellfields(prefix, step):
+    raw = open(f"{prefix}_step{step:04d}_cellfields.bin", "rb").read()
+    Nx, Ny = np.frombuffer(raw[:8], np.int32)
+    Nc = int(Nx) * int(Ny)
+    N = np.frombuffer(raw[8:8 + 4 * Nc], np.int32)
+    rest = np.frombuffer(raw[8 + 4 * Nc:], np.float64).reshape(10, Nc)
+    return int(Nx), int(Ny), N, rest
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", ["shim", "ours"])
+def test_driver_states_match_reference(runs, key):
+    p, out = runs
+    for step in (0, 3, 6):
+        xr, vr = load_state(out["ref"], step, p["n"])
+        xg, vg = load_state(out[key], step, p["n"])
+        assert rel(xg, xr) <= 1e-9, (key, step, "x")
+        assert rel(vg, vr) <= 1e-9, (key, step, "v")
+        Nx, Ny, Nr, Fr = load_cellfields(out["ref"], step)
+        gx, gy, Ng, Fg = load_cellfields(out[key], step)
+        assert (gx, gy) == (Nx, Ny)
+        assert np.array_equal(Ng, Nr), (key, step, "N")
+        assert rel(Fg, Fr) <= 1e-9, (key, step, "fields")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", ["shim", "ours"])
+def test_driver_metrics_match_reference(runs, key):
+    p, out = runs
+    R = read_csv(out["ref"] + "_metrics.csv")
+    G = read_csv(out[key] + "_metrics.csv")
+    assert list(G[0].keys()) == list(R[0].keys())
+    assert [r["step"] for r in G] == [r["step"] for r in R] == ["2", "4", "6"]
+    for rr, rg in zip(R, G):
+        for k in rr:
+            if k in SKIP_COLS:
+                continue
+            if k in INT_COLS:
+                assert rg[k] == rr[k], (key, rr["step"], k)
+            else:
+                a, b = float(rg[k]), float(rr[k])
+                assert abs(a - b) <= 1e-5 * max(abs(b), 1e-7) + 1e-12, (key, rr["step"], k, a, b)
+
+
+@pytest.mark.gpu
+def test_driver_runout_keys(runs):
+    _, out = runs
+
+    def kv(path):
+        return dict(line.rstrip("\n").split("=", 1) for line in open(path) if "=" in line)
+
+    R = kv(out["ref"] + "_runout.kv")
+    G = kv(out["ours"] + "_runout.kv")
+    assert set(G) >= {k for k in R if not k.startswith(("timeBase", "timeShifted", "fracBase", "fracShifted"))} - {
+        "timeBaseLayout"}
+    for k in ("totalParticlesMovedDense", "totalParticlesMovedSparse", "benchmark_nSteps"):
+        assert G[k] == R[k], k
+    for k in ("finalOccStd", "finalQx", "finalMeanKinetic"):
+        assert abs(float(G[k]) - float(R[k])) <= 1e-5 * abs(float(R[k])) + 1e-12, k
