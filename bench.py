@@ -135,15 +135,23 @@ def dist_setup(gpus):
 def barrier(dist, torch):
     if dist is not None:
         dist.barrier()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
 
 def reduce_max(x, dist, torch):
+    """Max over ranks (every rank times its own replica; the job takes the slowest)."""
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(world, n_per_rank, steps, t_max):
+    """particle-steps/s of the whole job: every rank advances its own n-particle replica."""
+    return world * n_per_rank * steps / t_max
 
 
 def config_dict(p, world):
@@ -210,7 +218,7 @@ def run_ours(args):
     l1 = ctx.launch_count()
     clocks = sampler.stop(t_wall0, t_wall1)
     t_max = reduce_max(t_dev, dist, torch)
-    value = world * p["n"] * K / t_max
+    value = whole_job_value(world, p["n"], K, t_max)
     # live per-phase timing (separate run: one synchronisation per step)
     KP = max(1, min(K, args.profile_steps))
     phases = ctx.step_profile(W + K, KP)
@@ -231,7 +239,7 @@ def run_ours(args):
     te = reduce_max(time.perf_counter() - t0, dist, torch)
     hx.close()
     hv.close()
-    e2e = {"value": world * p["n"] * KE / te, "unit": UNIT, "h2d_bytes_per_step": 32 * p["n"],
+    e2e = {"value": whole_job_value(world, p["n"], KE, te), "unit": UNIT, "h2d_bytes_per_step": 32 * p["n"],
            "d2h_bytes_per_step": 32 * p["n"], "steps": KE,
            "note": "per step: state upload from pinned host memory, one step, state download (C-ABI)"}
     ctx.close()
