@@ -400,6 +400,9 @@ struct ZoneState {
     int xs, xe, ys, ye, TX, TY, nl, WY;
     int arenaTop, arenaCap;
     int movedDense, movedSparse;
+    int atanLane;   // lane k < 25 holds the angular bin of step k (DevParams::atanBin)
+    bool dupNb5;    // a periodic axis shorter than 5 cells: range-2 neighbours can coincide
+    bool dupNb3;    // a periodic axis shorter than 3 cells: 8-neighbours can coincide
     bool failed;   // capacity exhausted: the zone is handed to the overflow path
     bool fatal;    // a device error was raised
 
@@ -539,7 +542,9 @@ struct ZoneState {
 
     // Move `nt` particles from positions srcOff.. of list s into cell t, drawing positions
     // with sample_in_cell (src/zone_pass.cpp:280-294): per particle U for x then U for y.
-    __device__ bool move_into(int s, int srcOff, int nt, int t) {
+    // slotPre/preOff: lane k holds the slot of entry preOff + k of list s if it was loaded
+    // ahead (owned entries only); entries outside that window are loaded here.
+    __device__ bool move_into(int s, int srcOff, int nt, int t, int slotPre = -1, int preOff = 1 << 29) {
         if (!ensure_room(t, nt)) return false;
         const DevParams& p = P();
         const double x0 = __dmul_rn((double)gx_of(t), p.dx), y0 = __dmul_rn((double)gy_of(t), p.dy);
@@ -548,13 +553,15 @@ struct ZoneState {
             const int c = min(kWarp, nt - q0);
             rng.ensure(2 * c);
             const int q = q0 + lane;
+            const int w = preOff + srcOff + q;  // position in the prefetched window
+            const int pre = __shfl_sync(0xffffffffu, slotPre, w & (kWarp - 1));
             if (lane < c) {
                 const uint32_t e = elem(s, srcOff + q);
                 const double px = __dadd_rn(x0, __dmul_rn(p.dx, canon(rng.peek(2 * lane))));
                 const double py = __dadd_rn(y0, __dmul_rn(p.dy, canon(rng.peek(2 * lane + 1))));
                 const int lc = (int)(e >> kEntryShift);
                 if (M.cflags[lc] & kCOwned) {
-                    const int sl = A->slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
+                    const int sl = (w < kWarp) ? pre : A->slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
                     A->xout[sl] = make_double2(px, py);
                     A->cid[sl] = cell_of(px, py, p);
                 }
@@ -609,9 +616,12 @@ struct ZoneState {
                 if ((double)M.cnt[t] < map_val(t, low)) nb = t;
             }
         }
-        const unsigned m0 = __ballot_sync(0xffffffffu, nb >= 0);
-        const unsigned same = __match_any_sync(0xffffffffu, nb >= 0 ? nb : -1 - lane);
-        const bool keep = (nb >= 0) && ((same & m0 & lanemask_lt()) == 0);
+        bool keep = nb >= 0;
+        if (dupNb5) {  // wrapped offsets can coincide: keep the first occurrence of each cell
+            const unsigned m0 = __ballot_sync(0xffffffffu, nb >= 0);
+            const unsigned same = __match_any_sync(0xffffffffu, nb >= 0 ? nb : -1 - lane);
+            keep = keep && ((same & m0 & lanemask_lt()) == 0);
+        }
         const unsigned mk = __ballot_sync(0xffffffffu, keep);
         if (keep) cand[__popc(mk & lanemask_lt())] = nb;
         __syncwarp();
@@ -622,34 +632,33 @@ struct ZoneState {
     // stable insertion sort on (-deficit, cnt, cheb, dist2, U01), then round robin
     __device__ int rank_dense(int l, const int* cand, int m, bool low, int* T) {
         if (m == 0) return 0;
-        const DevParams& p = P();
         const int startBin = (int)rng.uint_in(1, 8) - 1;
         rng.ensure(m);
-        int nb = -1, bin = -1, key2 = 0;
+        int nb = -1, key2 = 0, idx = 0, ddx = 0, ddy = 0;
         double dneg = 0.0, tie = 0.0;
         if (lane < m) {
             nb = cand[lane];
-            int ddx, ddy;
-            const int idx = step_index(gx_of(l), gy_of(l), gx_of(nb), gy_of(nb), ddx, ddy);
-            if (idx < 0) {
-                raise_error(A->st, kErrTableRange, zone);
-                bin = 0;
-            } else {
-                bin = p.atanBin[idx];
-            }
+            idx = step_index(gx_of(l), gy_of(l), gx_of(nb), gy_of(nb), ddx, ddy);
+            if (idx < 0) raise_error(A->st, kErrTableRange, zone);
             dneg = -smax(0.0, __dsub_rn(map_val(nb, low), (double)M.cnt[nb]));
             const int cheb = max(abs(ddx), abs(ddy)), d2 = ddx * ddx + ddy * ddy;
             key2 = (M.cnt[nb] << 8) | (cheb << 4) | d2;  // lexicographic (cnt, cheb, dist2)
             tie = canon(rng.peek(lane));
         }
         rng.consume(m);
+        // angular bin of the step (table held in lanes 0..24)
+        const int tb = __shfl_sync(0xffffffffu, atanLane, idx < 0 ? 0 : idx);
+        const int bin = (lane < m) ? ((idx < 0) ? 0 : tb) : 8 + lane;
+        // rank within the bin: compare only with the other lanes of the same bin
+        unsigned others = __match_any_sync(0xffffffffu, bin) & ~(1u << lane);
         int r = 0;
-        for (int j = 0; j < m; ++j) {
-            const int bj = __shfl_sync(0xffffffffu, bin, j);
+        while (__any_sync(0xffffffffu, others != 0u)) {
+            const int j = others ? (__ffs(others) - 1) : lane;
+            others &= others - 1u;
             const double dj = __shfl_sync(0xffffffffu, dneg, j);
             const int kj = __shfl_sync(0xffffffffu, key2, j);
             const double tj = __shfl_sync(0xffffffffu, tie, j);
-            if (lane < m && j != lane && bj == bin) {
+            if (j != lane) {
                 bool less, eq = false;
                 if (dj != dneg) less = dj < dneg;
                 else if (kj != key2) less = kj < key2;
@@ -658,9 +667,11 @@ struct ZoneState {
                 if (less || (eq && j < lane)) ++r;
             }
         }
+        // round robin over the bins from startBin: position = entries of rank < r in every
+        // bin, plus the bins before this one (in rotated order) that still hold rank r
         int pos = 0;
         for (int b = 0; b < 8; ++b) {
-            const int cb = __popc(__ballot_sync(0xffffffffu, lane < m && bin == b));
+            const int cb = __popc(__ballot_sync(0xffffffffu, bin == b));
             if (lane < m) {
                 pos += min(cb, r);
                 const int rb = (b - startBin + 8) & 7, rq = (bin - startBin + 8) & 7;
@@ -675,7 +686,8 @@ struct ZoneState {
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589). Lane k holds
     // target k's map value and deficit; a move changes only the deficit of its own target, so
     // each round walks the targets whose deficit was positive at the start of the round.
-    __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int* recv, int& nrecv) {
+    __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int* recv, int& nrecv, int slotPre,
+                          int preOff) {
         if (needOut <= 0 || nT == 0) return 0;
         const int srcLen = M.len[s];
         if (srcLen == 0) return 0;
@@ -705,7 +717,7 @@ struct ZoneState {
                     fatal = true;
                     return moved;
                 }
-                if (!move_into(s, taken, nt, t)) return moved;
+                if (!move_into(s, taken, nt, t, slotPre, preOff)) return moved;
                 push_recv(recv, nrecv, t);
                 if (lane == kk) defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
                 taken += nt;
@@ -736,6 +748,17 @@ struct ZoneState {
         const double hl = map_high(l);
         if ((double)ncc <= hl) return;
         int nrecv = 0, moved = 0;
+        // The two rounds take at most ceil(cnt - high) entries from the front of the list:
+        // load the slots of the owned ones now, so the loads overlap the target ranking.
+        int slotPre = -1;
+        {
+            const int take = min(min(M.len[l], max(0, (int)ceil(__dsub_rn((double)ncc, hl)))), kWarp);
+            if (lane < take) {
+                const uint32_t e = elem(l, lane);
+                const int lc = (int)(e >> kEntryShift);
+                if (M.cflags[lc] & kCOwned) slotPre = A->slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
+            }
+        }
         // first towards the low-threshold map, then whatever is left towards the high one
         // (one copy of the code for both rounds)
 #pragma unroll 1
@@ -745,7 +768,7 @@ struct ZoneState {
             const bool low = (round == 0);
             const int m = admissible(l, low, cand);
             const int nT = rank_dense(l, cand, m, low, T);
-            moved += spread(l, T, nT, low, need, recv, nrecv);
+            moved += spread(l, T, nT, low, need, recv, nrecv, slotPre, moved);
             if (failed || fatal) return;
         }
         if (lane < nrecv) M.cflags[recv[lane]] |= (kCRecv | kCChanged);
@@ -788,8 +811,11 @@ struct ZoneState {
         }
         const unsigned m0 = __ballot_sync(0xffffffffu, nb >= 0);
         if (m0 == 0) return;
-        const unsigned same = __match_any_sync(0xffffffffu, nb >= 0 ? nb : -1 - lane);
-        const bool uniq = (nb >= 0) && ((same & m0 & lanemask_lt()) == 0);
+        bool uniq = nb >= 0;
+        if (dupNb3) {  // wrapped offsets can coincide: keep the first occurrence of each cell
+            const unsigned same = __match_any_sync(0xffffffffu, nb >= 0 ? nb : -1 - lane);
+            uniq = uniq && ((same & m0 & lanemask_lt()) == 0);
+        }
         const int lowInt = p.lowThrBulkInt;
         int need = max(0, lowInt - ncc);
         if (need <= 0) return;
@@ -878,6 +904,9 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     const int4 R = A.rects[z];
     S.xs = R.x; S.xe = R.y; S.ys = R.z; S.ye = R.w;
     S.TX = S.xe - S.xs; S.TY = S.ye - S.ys; S.nl = S.TX * S.TY; S.WY = S.TY + 4;
+    S.atanLane = (lane < 25) ? p.atanBin[lane] : 0;
+    S.dupNb5 = (p.perx && p.Nx < 5) || (p.pery && p.Ny < 5);
+    S.dupNb3 = (p.perx && p.Nx < 3) || (p.pery && p.Ny < 3);
     const int W = (S.TX + 4) * S.WY;
     if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > winCap || S.nl >= (1 << (32 - kEntryShift))) return false;
     S.M.carve(mem, maxCells, winCap, arenaCap);
