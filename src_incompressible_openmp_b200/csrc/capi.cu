@@ -109,6 +109,9 @@ struct mpcd_ctx {
     double2* zoneCorr = nullptr;
     int* overflow = nullptr;
     int* nOverflow = nullptr;
+    int* zoneCost = nullptr;   // per zone: cost bucket
+    int* zoneHist = nullptr;   // kCostBuckets
+    int* zoneOrder = nullptr;  // launch order, heaviest first
     char* ovMem = nullptr;
     size_t ovPerBlock = 0;
     int ovBlocks = 2;
@@ -573,9 +576,15 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     A.zoneMoved = c->zoneMoved;
     A.zoneCorr = c->zoneCorr;
     A.st = c->st;
+    CUDA_TRY(cudaMemsetAsync(c->zoneHist, 0, sizeof(int) * kCostBuckets, c->stream));
+    k_zone_cost<<<blocks_for(L.nZones), kThreads, 0, c->stream>>>(c->P, L.rects, c->idxStd.start, L.nZones, c->zoneCost,
+                                                                   c->zoneHist); ++c->launches;
+    k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
+    A.order = c->zoneOrder;
     k_zone_pass<<<L.nZones, 32, c->zSmem, c->stream>>>(A); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     ZoneArgs B = A;
+    B.order = nullptr;
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
@@ -661,6 +670,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->blockSums, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
+                    c->zoneCost, c->zoneHist, c->zoneOrder,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -774,6 +784,9 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     ALLOC(c->zoneMoved, (size_t)maxZones);
     ALLOC(c->zoneCorr, (size_t)maxZones);
     ALLOC(c->overflow, (size_t)maxZones);
+    ALLOC(c->zoneCost, (size_t)maxZones);
+    ALLOC(c->zoneHist, (size_t)kCostBuckets);
+    ALLOC(c->zoneOrder, (size_t)maxZones);
     ALLOC(c->nOverflow, 1);
     ALLOC(c->passOut, 8);
     // fast path: tiles of the base/shifted layouts in shared memory

@@ -57,6 +57,7 @@ struct ZoneArgs {
     int* nOverflow;
     int2* zoneMoved;          // (dense, sparse) per zone
     double2* zoneCorr;        // (stats[4], stats[5]) per zone
+    const int* order;         // launch order of the zones (heaviest first); nullptr = by id
     DevStatus* st;
 };
 
@@ -1080,10 +1081,47 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
 
 __global__ void __launch_bounds__(32) k_zone_pass(ZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
-    const int z = blockIdx.x;
-    if (z >= A.nZones) return;
+    if ((int)blockIdx.x >= A.nZones) return;
+    const int z = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
     if (!zone_body(A, z, smem, A.maxCells, A.winCap, A.arenaCap) && (threadIdx.x & 31) == 0)
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
+}
+
+// Launch order of the zones, heaviest first, so that the last wave of blocks holds the
+// cheapest zones. The cost estimate is the number of particles above the bulk high threshold
+// in the zone's cells (the dense-phase work); ties keep no particular order, which is fine:
+// a zone's result does not depend on when it runs.
+constexpr int kCostBuckets = 256;
+__global__ void k_zone_cost(DevParams P, const int4* __restrict__ rects, const uint64_t* __restrict__ start, int nZones,
+                            int* __restrict__ cost, int* __restrict__ hist) {
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nZones) return;
+    const int4 R = rects[z];
+    double ex = 0.0;
+    for (int ix = R.x; ix < R.y; ++ix)
+        for (int iy = R.z; iy < R.w; ++iy) {
+            const int c = iy + P.Ny * ix;
+            const double n = (double)(int)((uint32_t)start[c + 1] - (uint32_t)start[c]);
+            if (n > P.highThr) ex += n - P.highThr;
+        }
+    const int b = min(kCostBuckets - 1, (int)ex);
+    cost[z] = b;
+    atomicAdd(hist + b, 1);
+}
+
+// one block: bucket offsets in descending cost, then each zone takes a place in its bucket
+__global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cost, int* __restrict__ hist, int nZones,
+                                                     int* __restrict__ order) {
+    __shared__ int off[kCostBuckets];
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int b = kCostBuckets - 1; b >= 0; --b) {
+            off[b] = acc;
+            acc += hist[b];
+        }
+    }
+    __syncthreads();
+    for (int z = threadIdx.x; z < nZones; z += blockDim.x) order[atomicAdd(&off[cost[z]], 1)] = z;
 }
 
 // zones that did not fit the shared-memory working set, re-run from their seed with a
