@@ -285,6 +285,58 @@ __device__ __forceinline__ void zone_shuffle(T* a, int m, ZoneMt& r, int lane) {
     __syncwarp();
 }
 
+// The same shuffle for m <= 32 entries, with every draw taken from the stream at once: lane
+// k computes draw k, and the swaps are applied in draw order to one value per lane. If some
+// draw would need Lemire's rejection step (probability ~ range / 2^64), nothing is consumed
+// and the sequential version runs instead.
+template <typename T>
+__device__ __forceinline__ void zone_shuffle_fast(T* a, int m, ZoneMt& r, int lane) {
+    if (m <= 1) return;
+    if (m > kWarp) {
+        zone_shuffle(a, m, r, lane);
+        return;
+    }
+    const bool even = (m % 2) == 0;
+    const int D = (even ? 1 : 0) + (m - (even ? 2 : 1)) / 2;  // <= 16 draws
+    r.ensure(D);
+    int i = 0, p1 = 0, p2 = -1;
+    bool rej = false;
+    if (lane < D) {
+        const bool first2 = even && lane == 0;
+        i = first2 ? 1 : (even ? 2 : 1) + 2 * (lane - (even ? 1 : 0));
+        const uint64_t R = first2 ? 2ULL : (uint64_t)(i + 1) * (uint64_t)(i + 2);
+        const uint64_t u = r.peek(lane);
+        const uint64_t low = u * R;
+        if (low < R) rej = low < umod64_slow(0ULL - R, R);
+        const uint32_t x = (uint32_t)__umul64hi(u, R);
+        if (first2) {
+            p1 = (int)x;
+        } else {
+            const uint32_t b1 = (uint32_t)(i + 2), q = x / b1;
+            p1 = (int)q;
+            p2 = (int)(x - q * b1);
+        }
+    }
+    if (__any_sync(0xffffffffu, rej)) {
+        zone_shuffle(a, m, r, lane);
+        return;
+    }
+    r.consume(D);
+    unsigned v = (lane < m) ? (unsigned)a[lane] : 0u;
+    for (int k = 0; k < D; ++k) {
+        const int ik = __shfl_sync(0xffffffffu, i, k);
+        const int a1 = __shfl_sync(0xffffffffu, p1, k);
+        const int a2 = __shfl_sync(0xffffffffu, p2, k);
+        v = __shfl_sync(0xffffffffu, v, (lane == ik) ? a1 : ((lane == a1) ? ik : lane));
+        if (a2 >= 0) {
+            const int i2 = ik + 1;
+            v = __shfl_sync(0xffffffffu, v, (lane == i2) ? a2 : ((lane == a2) ? i2 : lane));
+        }
+    }
+    if (lane < m) a[lane] = (T)v;
+    __syncwarp();
+}
+
 // sqrt(-2 ln r2 / r2) of the polar method, out of line
 __device__ __noinline__ double polar_scale(double r2) { return sqrt(__ddiv_rn(__dmul_rn(-2.0, log_cr_dev(r2)), r2)); }
 
@@ -392,6 +444,35 @@ __device__ __noinline__ void zone_compute_nsm(double* nsm, const int* win, const
 // hypot, out of line (once per sparse cell)
 __device__ __noinline__ double zone_hypot(double a, double b) { return mpcd_dd::hypot_cr(a, b); }
 
+// cnt deviates of one fresh normal_distribution (polar method: pairs of uniforms in stream
+// order until r2 is in (0, 1]; each accepted pair gives y*m, then the cached x*m) into out[].
+// Lane c examines candidate pair c of the batch; the accepted ones are ranked by ballot.
+__device__ __forceinline__ void zone_normals(double* out, int cnt, ZoneMt& r, int lane) {
+    int got = 0;
+    while (got < cnt) {
+        r.ensure(2 * kWarp);
+        const double x = __dsub_rn(__dmul_rn(2.0, canon(r.peek(2 * lane))), 1.0);
+        const double y = __dsub_rn(__dmul_rn(2.0, canon(r.peek(2 * lane + 1))), 1.0);
+        const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+        const bool acc = !(r2 > 1.0 || r2 == 0.0);
+        const unsigned am = __ballot_sync(0xffffffffu, acc);
+        const int need = (cnt - got + 1) / 2;
+        const int rank = __popc(am & lanemask_lt());
+        const int used = min(__popc(am), need);
+        int last = kWarp - 1;
+        if (__popc(am) >= need) last = __ffs(__ballot_sync(0xffffffffu, acc && rank == need - 1)) - 1;
+        if (acc && rank < need) {
+            const double mult = polar_scale(r2);
+            const int k0 = got + 2 * rank;
+            out[k0] = __dmul_rn(y, mult);
+            if (k0 + 1 < cnt) out[k0 + 1] = __dmul_rn(x, mult);
+        }
+        r.consume(2 * (last + 1));
+        got += 2 * used;
+    }
+    __syncwarp();
+}
+
 // Scalar (warp-uniform) state of one zone.
 struct ZoneState {
     ZoneMem M;
@@ -402,6 +483,7 @@ struct ZoneState {
     int arenaTop, arenaCap;
     int movedDense, movedSparse;
     int atanLane;   // lane k < 25 holds the angular bin of step k (DevParams::atanBin)
+    double hypLane; // lane k < 25 holds the length of step k (DevParams::hypotTab)
     bool dupNb5;    // a periodic axis shorter than 5 cells: range-2 neighbours can coincide
     bool dupNb3;    // a periodic axis shorter than 3 cells: 8-neighbours can coincide
     bool failed;   // capacity exhausted: the zone is handed to the overflow path
@@ -828,39 +910,34 @@ struct ZoneState {
         __syncwarp();
         double gx, gy;
         inward(l, gx, gy);
-        zone_shuffle(don, nd, rng, lane);
+        zone_shuffle_fast(don, nd, rng, lane);
         const double ndir = zone_hypot(gx, gy);
-        ZoneNormal N;
-        N.has = 0;
-        N.saved = 0.0;
-        double* score = M.smallD;
-        for (int k = 0; k < nd; ++k) {
-            const int d = don[k];
-            int ddx, ddy;
-            const int idx = step_index(ix, iy, gx_of(d), gy_of(d), ddx, ddy);
-            const double nstep = (idx >= 0) ? p.hypotTab[idx] : 0.0;
+        // one N(0,1) per donor in shuffled order, then scores in parallel (lane k = donor k)
+        double* nrm = M.smallD;
+        zone_normals(nrm, nd, rng, lane);
+        int dk = -1, idx = 0, ddx = 0, ddy = 0;
+        if (lane < nd) {
+            dk = don[lane];
+            idx = step_index(ix, iy, gx_of(dk), gy_of(dk), ddx, ddy);
+        }
+        const double hs = __shfl_sync(0xffffffffu, hypLane, idx < 0 ? 0 : idx);
+        double sc = 0.0;
+        if (lane < nd) {
+            const double nstep = (idx >= 0) ? hs : 0.0;
             double align = 0.0;
             if (ndir >= 1e-14 && nstep >= 1e-14)
                 align = __ddiv_rn(__dadd_rn(__dmul_rn((double)ddx, gx), __dmul_rn((double)ddy, gy)), __dmul_rn(ndir, nstep));
-            const double noise = __dmul_rn(1e-9, N.next(rng));
-            const double sc = __dadd_rn(__dadd_rn(__dmul_rn(100.0, align), M.nsm[nsm_index(gx_of(d), gy_of(d))]), noise);
-            if (lane == 0) score[k] = sc;
+            const double noise = __dmul_rn(1e-9, nrm[lane]);
+            sc = __dadd_rn(__dadd_rn(__dmul_rn(100.0, align), M.nsm[nsm_index(gx_of(dk), gy_of(dk))]), noise);
+        }
+        // descending, ties in shuffled order (std::sort of <= 16 elements is an insertion sort)
+        int rk = 0;
+        for (int j = 0; j < nd; ++j) {
+            const double sj = __shfl_sync(0xffffffffu, sc, j);
+            if (lane < nd && j != lane && (sj > sc || (sj == sc && j < lane))) ++rk;
         }
         __syncwarp();
-        if (lane == 0) {  // stable insertion sort, descending
-            for (int i = 1; i < nd; ++i) {
-                const double sv = score[i];
-                const int ov = don[i];
-                int j = i;
-                while (j > 0 && sv > score[j - 1]) {
-                    score[j] = score[j - 1];
-                    don[j] = don[j - 1];
-                    --j;
-                }
-                score[j] = sv;
-                don[j] = ov;
-            }
-        }
+        if (lane < nd) don[rk] = dk;
         __syncwarp();
         for (int k = 0; k < nd; ++k) {
             const int d = don[k];
@@ -871,7 +948,7 @@ struct ZoneState {
             const int nt = min(min(need, avail), ld);
             if (nt <= 0) continue;
             if (!ensure_room(d, 0)) return;  // materialise the donor list to shuffle it
-            zone_shuffle(M.arena + M.abase[d] + M.head[d], ld, rng, lane);
+            zone_shuffle_fast(M.arena + M.abase[d] + M.head[d], ld, rng, lane);
             if (!move_into(d, 0, nt, l)) return;
             if (lane == 0) {
                 M.head[d] += nt;
@@ -906,6 +983,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     S.xs = R.x; S.xe = R.y; S.ys = R.z; S.ye = R.w;
     S.TX = S.xe - S.xs; S.TY = S.ye - S.ys; S.nl = S.TX * S.TY; S.WY = S.TY + 4;
     S.atanLane = (lane < 25) ? p.atanBin[lane] : 0;
+    S.hypLane = (lane < 25) ? p.hypotTab[lane] : 0.0;
     S.dupNb5 = (p.perx && p.Nx < 5) || (p.pery && p.Ny < 5);
     S.dupNb3 = (p.perx && p.Nx < 3) || (p.pery && p.Ny < 3);
     const int W = (S.TX + 4) * S.WY;
@@ -973,7 +1051,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
         const int nd = S.collect([&](int l) { return (double)M.cnt[l] > S.map_high(l); });
-        zone_shuffle(M.list, nd, S.rng, lane);
+        zone_shuffle_fast(M.list, nd, S.rng, lane);
         for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
     }
     // sparse phase (src/zone_pass.cpp:783-854)
@@ -984,7 +1062,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         S.mark_bulk();
         const int nlow = S.collect([&](int l) { return M.cnt[l] > 0 && (double)M.cnt[l] < S.map_low(l); });
         if (!p.useLFF && nlow > 0) S.compute_nsm();
-        zone_shuffle(M.list, nlow, S.rng, lane);
+        zone_shuffle_fast(M.list, nlow, S.rng, lane);
         for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
     }
     if (S.fatal) return true;
