@@ -88,6 +88,7 @@ struct mpcd_ctx {
     CellIndex idxStd, idxSrd;
     bool idxStdValid = false;
     uint64_t* blockSums = nullptr;
+    uint64_t* blockSumsWalls = nullptr;  // the walls' scan runs beside the index scans
     int blockSumsCap = 0;
     // walls
     BcWork W{};
@@ -100,6 +101,11 @@ struct mpcd_ctx {
     uint8_t* signsBuf[2] = {nullptr, nullptr};
     int64_t signsStep[2] = {-1, -1};
     cudaStream_t side = nullptr;
+    // thermal-wall velocities of a step (they need the post-BC positions only) run on their
+    // own stream, beside the SRD index build, and join before the collision
+    cudaStream_t walls = nullptr;
+    cudaEvent_t bcDone = nullptr, wallsDone = nullptr;
+    bool wallsPending = false;
     cudaEvent_t signsReady[2] = {nullptr, nullptr};
     cudaEvent_t collDone = nullptr;
     // zones
@@ -174,6 +180,7 @@ void mark(mpcd_ctx* c, Prof* p, int label) {
 int check_device(mpcd_ctx* c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (c->side) CUDA_TRY(cudaStreamSynchronize(c->side));
+    if (c->walls) CUDA_TRY(cudaStreamSynchronize(c->walls));
     CUDA_TRY(cudaMemcpy(c->hst, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost));
     if (c->hst->code != 0) {
         const int code = c->hst->code;
@@ -342,12 +349,15 @@ DevParams make_dev_params(const mpcd_params_c& p) {
 }
 
 // ---------------------------------------------------------------- index sort
-int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out) {
+int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out, cudaStream_t s = nullptr,
+             uint64_t* sums = nullptr) {
+    if (!s) s = c->stream;
+    if (!sums) sums = c->blockSums;
     const int nb = (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile);
     if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
-    k_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums); ++c->launches;
-    k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb); ++c->launches;
-    k_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(in, n, c->blockSums, out); ++c->launches;
+    k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, sums); ++c->launches;
+    k_scan_blocks<<<1, kScanThreads, 0, s>>>(sums, nb); ++c->launches;
+    k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, sums, out); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     return MPCD_OK;
 }
@@ -451,7 +461,10 @@ int reduce_cols(mpcd_ctx* c, const double* cols, int64_t rows, int K, unsigned m
 }
 
 // ---------------------------------------------------------------- phases
-int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo, Prof* pf = nullptr) {
+// overlap: the wall-velocity kernels go to c->walls and run_collide joins them before the
+// collision (the step's path); otherwise everything stays on the context's stream
+int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo, Prof* pf = nullptr,
+           bool overlap = false) {
     BcWork& W = c->W;
     CUDA_TRY(cudaMemsetAsync(W.bitsX, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
     CUDA_TRY(cudaMemsetAsync(W.bitsY, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
@@ -465,14 +478,26 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
                                                                     c->pidb[c->pp], cidStd, cidSrd, W, c->st);
     ++c->launches;
     mark(c, pf, 0);
-    k_word_counts<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount); ++c->launches;
-    int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix);
+    cudaStream_t ws = c->stream;
+    uint64_t* sums = c->blockSums;
+    if (overlap && c->walls) {
+        CUDA_TRY(cudaEventRecord(c->bcDone, c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->walls, c->bcDone, 0));
+        ws = c->walls;
+        sums = c->blockSumsWalls;
+    }
+    k_word_counts<<<blocks_for(c->nwords), kThreads, 0, ws>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount); ++c->launches;
+    int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix, ws, sums);
     if (rc) return rc;
-    k_wall_normals<<<1, kNormThreads, 0, c->stream>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st); ++c->launches;
-    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, c->stream>>>(c->P, c->vb[c->xv], W, c->st); ++c->launches;
+    k_wall_normals<<<1, kNormThreads, 0, ws>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st); ++c->launches;
+    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, ws>>>(c->P, c->vb[c->xv], W, c->st); ++c->launches;
     if (wantInfo)
-        k_wall_reduce<<<1, 32, 0, c->stream>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut); ++c->launches;
+        k_wall_reduce<<<1, 32, 0, ws>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut); ++c->launches;
     CUDA_TRY(cudaGetLastError());
+    if (ws != c->stream) {
+        CUDA_TRY(cudaEventRecord(c->wallsDone, ws));
+        c->wallsPending = true;
+    }
     mark(c, pf, 1);
     return MPCD_OK;
 }
@@ -496,6 +521,10 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         signs = c->signsBuf[b];
     }
     mark(c, pf, 3);
+    if (c->wallsPending) {  // the collision reads the wall-updated velocities
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->wallsDone, 0));
+        c->wallsPending = false;
+    }
     k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc,
                                                                  c->vb[c->xv], c->st); ++c->launches;
     if (c->P.keepMeanFlow) {
@@ -667,7 +696,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd,
                     c->idxStd.count, c->idxStd.packed, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
                     c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
-                    c->blockSums, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
+                    c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->zoneCost, c->zoneHist, c->zoneOrder,
@@ -683,9 +712,11 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->side) cudaStreamSynchronize(c->side);
-    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone})
+    if (c->walls) cudaStreamSynchronize(c->walls);
+    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone})
         if (e) cudaEventDestroy(e);
     if (c->side) cudaStreamDestroy(c->side);
+    if (c->walls) cudaStreamDestroy(c->walls);
     if (c->signsBuf[0]) cudaFree(c->signsBuf[0]);
     if (c->signsBuf[1]) cudaFree(c->signsBuf[1]);
     if (c->hst) cudaFreeHost(c->hst);
@@ -739,6 +770,7 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     c->nwords = (n + 31) / 32 + 1;
     c->blockSumsCap = (int)std::max<int64_t>(1, ((int64_t)std::max(Nc, c->nwords) + kScanTile - 1) / kScanTile) + 1;
     ALLOC(c->blockSums, (size_t)c->blockSumsCap);
+    ALLOC(c->blockSumsWalls, (size_t)c->blockSumsCap);
     c->bcBlocks = blocks_for(n);
     BcWork& W = c->W;
     ALLOC(W.bitsX, (size_t)c->nwords);
@@ -761,7 +793,10 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->signsReady[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->signsReady[1], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->collDone, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->collDone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->walls, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->bcDone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->wallsDone, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_err(MPCD_ERR_CUDA, "side stream"));
     // zone layouts
     build_layout(*params, MPCD_LAYOUT_BASE, c->lay[0]);
@@ -1164,7 +1199,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
     mark(c, pf, -1);
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift); ++c->launches;
-    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf);
+    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
     if (rc) return rc;
     c->cidStdValid = true;
     c->srdCellsValid = true;
