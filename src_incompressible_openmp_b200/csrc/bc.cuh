@@ -230,8 +230,9 @@ __device__ __forceinline__ int srd_cell(double x, double y, double sx, double sy
 
 // The two shift draws U(-a0/2, a0/2) of srd_cell_id_with_random_shift: outputs 0 and 1 of
 // mt19937_64(seed), which need seeded words 0, 1, 2, 156, 157 only. One thread.
-__global__ void k_srd_shift(DevParams P, uint64_t seed, double* out) {
+__global__ void k_srd_shift(DevParams P, uint64_t seed, double* out, const uint64_t* seedDev) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (seedDev) seed = seedDev[kSeedSrdShift];
     uint64_t w[kMtM + 2];
     w[0] = seed;
     for (int i = 1; i < kMtM + 2; ++i) w[i] = mt_seed_next(w[i - 1], i);
@@ -328,7 +329,9 @@ __global__ void k_word_counts(const uint32_t* __restrict__ bx, const uint32_t* _
 // order; pair p = (y*mult, x*mult) = (first deviate, cached second deviate).
 constexpr int kNormThreads = 320;
 __global__ void __launch_bounds__(kNormThreads) k_wall_normals(uint64_t seed, const uint64_t* __restrict__ totalPairs,
-                                                             int cap, double* __restrict__ normals, DevStatus* st) {
+                                                             int cap, double* __restrict__ normals, DevStatus* st,
+                                                             const uint64_t* seedDev) {
+    if (seedDev) seed = seedDev[kSeedBc];
     __shared__ uint64_t mt[kMtN];
     __shared__ uint64_t scanSh[32];
     const int t = threadIdx.x;

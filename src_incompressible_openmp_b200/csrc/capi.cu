@@ -106,6 +106,19 @@ struct mpcd_ctx {
     cudaStream_t walls = nullptr;
     cudaEvent_t bcDone = nullptr, wallsDone = nullptr;
     bool wallsPending = false;
+    // CUDA-graph replay of the plain step: the step number and its seeds live on the device
+    // (k_step_begin); one graph per entry parity of the ping-pong buffers
+    bool graphMode = false;            // true while a step is being captured
+    bool useGraphs = true;
+    long long* dStep = nullptr;        // device: number of the last step begun
+    uint64_t* stepSeeds = nullptr;     // device: kStepSeeds
+    cudaEvent_t sideDone = nullptr;    // the captured step joins its sign prefetch
+    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t gkernels[4] = {0, 0, 0, 0};
+    struct HostFlags {
+        int xv, pp;
+        bool cidStdValid, srdCellsValid, idxStdValid, refValid;
+    } gpost[4];
     cudaEvent_t signsReady[2] = {nullptr, nullptr};
     cudaEvent_t collDone = nullptr;
     // zones
@@ -380,6 +393,10 @@ int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, i
     return MPCD_OK;
 }
 
+__global__ void k_set_step(long long* step, long long value) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *step = value;
+}
+
 __global__ void k_std_cells(DevParams P, const double2* __restrict__ x, int* __restrict__ cid) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < P.n) cid[s] = cell_of(x[s].x, x[s].y, P);
@@ -489,7 +506,8 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     k_word_counts<<<blocks_for(c->nwords), kThreads, 0, ws>>>(W.bitsX, W.bitsY, c->nwords, W.wordCount); ++c->launches;
     int rc = scan_u64(c, W.wordCount, c->nwords, W.wordPrefix, ws, sums);
     if (rc) return rc;
-    k_wall_normals<<<1, kNormThreads, 0, ws>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st); ++c->launches;
+    k_wall_normals<<<1, kNormThreads, 0, ws>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st,
+                                               c->graphMode ? c->stepSeeds : nullptr); ++c->launches;
     k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, ws>>>(c->P, c->vb[c->xv], W, c->st); ++c->launches;
     if (wantInfo)
         k_wall_reduce<<<1, 32, 0, ws>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut); ++c->launches;
@@ -508,12 +526,15 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
     int rc = build_index(c, c->cidSrd, c->idxSrd, pf, 2);
     if (rc) return rc;
     const uint8_t* signs = c->signs;
-    if (step < 0) {
-        k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs); ++c->launches;
+    const uint64_t* gs = c->graphMode ? c->stepSeeds : nullptr;
+    if (c->graphMode) {
+        signs = c->signsBuf[0];  // or signsBuf[1]: k_srd_collide picks by the step's parity
+    } else if (step < 0) {
+        k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signs, nullptr, nullptr); ++c->launches;
     } else {
         const int b = (int)(step & 1);
         if (c->signsStep[b] != step) {
-            k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signsBuf[b]); ++c->launches;
+            k_srd_signs<<<1, kSignThreads, 0, c->stream>>>(seed, c->Nc, c->signsBuf[b], nullptr, nullptr); ++c->launches;
             c->signsStep[b] = step;
         } else {
             CUDA_TRY(cudaStreamWaitEvent(c->stream, c->signsReady[b], 0));
@@ -526,7 +547,7 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         c->wallsPending = false;
     }
     k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc,
-                                                                 c->vb[c->xv], c->st); ++c->launches;
+                                                                 c->vb[c->xv], c->st, gs, c->signsBuf[1]); ++c->launches;
     if (c->P.keepMeanFlow) {
         k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
@@ -535,14 +556,21 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
     }
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 4);
-    if (step >= 0) {
+    if (c->graphMode) {
+        // the next step's sign stream on the side stream; the captured step joins it at its end
+        CUDA_TRY(cudaEventRecord(c->collDone, c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->side, c->collDone, 0));
+        k_srd_signs<<<1, kSignThreads, 0, c->side>>>(0, c->Nc, c->signsBuf[0], gs, c->signsBuf[1]); ++c->launches;
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(c->sideDone, c->side));
+    } else if (step >= 0) {
         // generate the next step's sign stream on the side stream, after this collision
         // (which is the last reader of the buffer it overwrites' previous contents)
         const int b = (int)((step + 1) & 1);
         CUDA_TRY(cudaEventRecord(c->collDone, c->stream));
         CUDA_TRY(cudaStreamWaitEvent(c->side, c->collDone, 0));
         const uint64_t next = 433494437ULL + 10007ULL * (uint64_t)(step + 1);
-        k_srd_signs<<<1, kSignThreads, 0, c->side>>>(next, c->Nc, c->signsBuf[b]); ++c->launches;
+        k_srd_signs<<<1, kSignThreads, 0, c->side>>>(next, c->Nc, c->signsBuf[b], nullptr, nullptr); ++c->launches;
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaEventRecord(c->signsReady[b], c->side));
         c->signsStep[b] = step + 1;
@@ -579,7 +607,8 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
     Layout& L = c->lay[mode];
     k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
-        seedBase, L.nZones, c->seeds); ++c->launches;
+        seedBase, L.nZones, c->seeds, c->graphMode ? c->stepSeeds : nullptr,
+        mode == MPCD_LAYOUT_SHIFTED ? kSeedShifted : kSeedBase); ++c->launches;
     mark(c, pf, 7);
     CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
     // out of place: outputs start as a copy of the inputs; zones write what they change
@@ -699,7 +728,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
-                    c->zoneCost, c->zoneHist, c->zoneOrder,
+                    c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -713,8 +742,10 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
         if (e) cudaEventDestroy(e);
     if (c->side) cudaStreamSynchronize(c->side);
     if (c->walls) cudaStreamSynchronize(c->walls);
-    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone})
+    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone, c->sideDone})
         if (e) cudaEventDestroy(e);
+    for (auto& g : c->gexec)
+        if (g) cudaGraphExecDestroy(g);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->walls) cudaStreamDestroy(c->walls);
     if (c->signsBuf[0]) cudaFree(c->signsBuf[0]);
@@ -796,8 +827,11 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
         cudaEventCreateWithFlags(&c->collDone, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->walls, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->bcDone, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->wallsDone, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->wallsDone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->sideDone, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_err(MPCD_ERR_CUDA, "side stream"));
+    ALLOC(c->dStep, 1);
+    ALLOC(c->stepSeeds, (size_t)kStepSeeds);
     // zone layouts
     build_layout(*params, MPCD_LAYOUT_BASE, c->lay[0]);
     build_layout(*params, MPCD_LAYOUT_SHIFTED, c->lay[1]);
@@ -959,7 +993,7 @@ int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
 int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
-    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift); ++c->launches;
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift, nullptr); ++c->launches;
     k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     c->srdCellsValid = true;
@@ -1198,7 +1232,11 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     int rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
     mark(c, pf, -1);
-    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift); ++c->launches;
+    if (c->graphMode) {
+        k_step_begin<<<1, 1, 0, c->stream>>>(c->dStep, c->stepSeeds); ++c->launches;
+    }
+    k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift,
+                                        c->graphMode ? c->stepSeeds : nullptr); ++c->launches;
     rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
     if (rc) return rc;
     c->cidStdValid = true;
@@ -1250,6 +1288,70 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
         if (rc) return rc;
         CUDA_TRY(cudaEventRecord(c->ev[7], c->stream));
     }
+    if (c->graphMode) CUDA_TRY(cudaStreamWaitEvent(c->stream, c->sideDone, 0));  // join the sign prefetch
+    return MPCD_OK;
+}
+
+// A step replayed from a CUDA graph. The graph of each entry parity of the ping-pong
+// buffers is captured from step_once on first use; the step number and seeds come from the
+// device (k_step_begin increments *dStep), so one graph serves every step. Needs the step's
+// sign stream prefetched by the step before (signsStep), like the eager path's fast case.
+static int graph_step(mpcd_ctx* c, int64_t step) {
+    const int key = c->xv * 2 + c->pp;
+    if (!c->gexec[key]) {
+        const int64_t l0 = c->launches;
+        CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->graphMode = true;
+        const int rc = step_once(c, step, false);
+        c->graphMode = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (rc != MPCD_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != MPCD_OK ? rc : set_err(MPCD_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&c->gexec[key], g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            c->gexec[key] = nullptr;
+            cudaGetLastError();
+            return set_err(MPCD_ERR_CUDA, std::string("step graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        c->gkernels[key] = c->launches - l0;
+        c->launches = l0;
+        c->gpost[key] = {c->xv, c->pp, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
+    } else {
+        const auto& f = c->gpost[key];  // host-side state after the step, as step_once leaves it
+        c->xv = f.xv;
+        c->pp = f.pp;
+        c->cidStdValid = f.cidStdValid;
+        c->srdCellsValid = f.srdCellsValid;
+        c->idxStdValid = f.idxStdValid;
+        c->refValid = f.refValid;
+    }
+    // the sign stream of this step may come from an eager step's prefetch on the side stream
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->signsReady[step & 1], 0));
+    k_set_step<<<1, 1, 0, c->stream>>>(c->dStep, (long long)(step - 1)); ++c->launches;
+    CUDA_TRY(cudaGraphLaunch(c->gexec[key], c->stream));
+    c->launches += c->gkernels[key];
+    c->signsStep[(step + 1) & 1] = step + 1;
+    return MPCD_OK;
+}
+
+// steps step0+1 .. step0+nsteps; the metrics step (if any) and steps whose sign stream was
+// not prefetched run eagerly, the others from graphs
+static int run_steps(mpcd_ctx* c, int64_t step0, int64_t nsteps, bool metricsLast) {
+    for (int64_t k = 1; k <= nsteps; ++k) {
+        const int64_t s = step0 + k;
+        const bool m = metricsLast && k == nsteps;
+        int rc;
+        if (c->useGraphs && !m && c->signsStep[s & 1] == s)
+            rc = graph_step(c, s);
+        else
+            rc = step_once(c, s, m);
+        if (rc) return rc;
+    }
     return MPCD_OK;
 }
 
@@ -1270,9 +1372,8 @@ int mpcd_step(mpcd_ctx* c, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* l
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
     CUDA_TRY(cudaSetDevice(c->device));
-    for (int64_t k = 1; k <= nsteps; ++k) {
-        const bool m = (last != nullptr) && (k == nsteps);
-        int rc = step_once(c, step0 + k, m);
+    {
+        const int rc = run_steps(c, step0, nsteps, last != nullptr);
         if (rc) return rc;
     }
     int rc = check_device(c);
@@ -1339,7 +1440,7 @@ int mpcd_step_timed(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* device_s
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     CUDA_TRY(cudaEventRecord(a, c->stream));
     int rc = MPCD_OK;
-    for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) rc = step_once(c, step0 + k, false);
+    rc = run_steps(c, step0, nsteps, false);
     CUDA_TRY(cudaEventRecord(b, c->stream));
     CUDA_TRY(cudaEventSynchronize(b));
     float ms = 0.f;

@@ -10,7 +10,13 @@ namespace mpcd_dev {
 // (in cell order) holding >= 2 particles (src/srd_collision.cpp:77-83); sign[r] = 1 when
 // U(0,1) < 0.5 (theta = -alpha). One block generates `count` draws, one twist at a time.
 constexpr int kSignThreads = 320;
-__global__ void __launch_bounds__(kSignThreads) k_srd_signs(uint64_t seed, int count, uint8_t* __restrict__ sign) {
+// seedDev (graph replay): the next step's seed and output buffer (sign, sign1 by its parity)
+__global__ void __launch_bounds__(kSignThreads) k_srd_signs(uint64_t seed, int count, uint8_t* __restrict__ sign,
+                                                           const uint64_t* seedDev, uint8_t* sign1) {
+    if (seedDev) {
+        seed = seedDev[kSeedSignsNext];
+        if (seedDev[kSeedNextParity]) sign = sign1;
+    }
     __shared__ uint64_t mt[kMtN];
     const int t = threadIdx.x;
     if (t == 0) {
@@ -42,9 +48,11 @@ __global__ void __launch_bounds__(kSignThreads) k_srd_signs(uint64_t seed, int c
 
 // srd_collision_step (src/srd_collision.cpp:47-124) for one SRD cell per thread. start:
 // packed (segment start | rank among cells with >= 2 particles << 32).
+// seedDev (graph replay): the signs are sign or sign1 by the step's parity
 __global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
                               const uint8_t* __restrict__ sign, int signCount, double2* __restrict__ v,
-                              DevStatus* st) {
+                              DevStatus* st, const uint64_t* seedDev, const uint8_t* __restrict__ sign1) {
+    if (seedDev && seedDev[kSeedParity]) sign = sign1;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const uint64_t s0 = start[c];

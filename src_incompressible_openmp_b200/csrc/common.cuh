@@ -62,6 +62,26 @@ struct DevParams {
     double hypotTab[25];
 };
 
+// Device-side seed table of one step (CUDA-graph replay: the step number lives on the
+// device and every seeded kernel reads its seed here instead of from its arguments).
+// Seeds follow the benchmark schedule (src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:249-266).
+enum StepSeed { kSeedBc = 0, kSeedSrdShift, kSeedSignsNext, kSeedBase, kSeedShifted, kSeedParity, kSeedNextParity,
+                kStepSeeds };
+
+__global__ void k_step_begin(long long* __restrict__ step, uint64_t* __restrict__ seeds) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const long long s = *step + 1;
+    *step = s;
+    const uint64_t u = (uint64_t)s;
+    seeds[kSeedBc] = 104729ULL + 10007ULL * u;
+    seeds[kSeedSrdShift] = 130363ULL + 10007ULL * u;
+    seeds[kSeedSignsNext] = 433494437ULL + 10007ULL * (u + 1ULL);
+    seeds[kSeedBase] = 88172645463325252ULL + 10007ULL * u;
+    seeds[kSeedShifted] = 88172645463325252ULL + 4099ULL + 10007ULL * u;
+    seeds[kSeedParity] = u & 1ULL;
+    seeds[kSeedNextParity] = (u + 1ULL) & 1ULL;
+}
+
 __device__ __forceinline__ int wrap_index(int i, int n) {
     int r = i % n;
     return (r < 0) ? r + n : r;

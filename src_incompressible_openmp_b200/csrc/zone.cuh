@@ -1216,7 +1216,9 @@ __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, si
 // (src/zone_pass_openmp.cpp:78). One thread per zone runs the sequential seeding
 // recurrence; states are staged in shared memory and written zone-major, coalesced.
 constexpr int kSeedZonesPerBlock = 16;
-__global__ void __launch_bounds__(kSeedZonesPerBlock * 2) k_zone_seeds(uint64_t seedBase, int nZones, uint64_t* out) {
+__global__ void __launch_bounds__(kSeedZonesPerBlock * 2) k_zone_seeds(uint64_t seedBase, int nZones, uint64_t* out,
+                                                                       const uint64_t* seedDev, int which) {
+    if (seedDev) seedBase = seedDev[which];
     __shared__ uint64_t st[kSeedZonesPerBlock][kMtN];
     const int t = threadIdx.x;
     const int z0 = blockIdx.x * kSeedZonesPerBlock;
