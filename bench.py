@@ -39,6 +39,11 @@ WORKLOADS = {
     "channel_2048x512_ppc10": dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10),
     # a smaller channel of the same physics, for profiler captures (state 47 MB)
     "channel_512x256_ppc10": dict(name="channel_512x256_ppc10", Nx=512, Ny=256, ppc=10),
+    # the reference's own benchmark case (50x50 cells, 25,000 particles)
+    "channel_50x50_ppc10": dict(name="channel_50x50_ppc10", Nx=50, Ny=50, ppc=10),
+    # batched ensemble: 256 independent channels, Nx ~ U[32,512], Ny ~ U[16,128],
+    # ppc ~ U[5,20], bodyForceX log-uniform in [1e-4, 1e-2], one initial-state seed each
+    "ensemble_256": dict(name="ensemble_256", replicas=256, seed=2024),
 }
 WORKLOAD = WORKLOADS["channel_2048x512_ppc10"]
 DATA = "synthetic: seeded uniform positions, Maxwellian velocities (kT=1, mean removed)"
@@ -278,6 +283,64 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def ensemble_params(W):
+    """Parameters and initial states of the batched ensemble (seeded)."""
+    import numpy as np
+
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
+
+    rng = np.random.default_rng(W["seed"])
+    out = []
+    for r in range(W["replicas"]):
+        Nx = int(rng.integers(32, 513))
+        Ny = int(rng.integers(16, 129))
+        ppc = int(rng.integers(5, 21))
+        force = float(10.0 ** rng.uniform(-4.0, -2.0))
+        p = poiseuille_params(Nx, Ny, ppc, bodyForceX=force)
+        out.append((p, 1000 + r))
+    return out
+
+
+def run_ensemble(args):
+    """Aggregate particle-steps/s of the batched ensemble (one GPU; rank 0 only)."""
+    from src_incompressible_openmp_b200 import native
+    from src_incompressible_openmp_b200.cases import uniform_state
+
+    if env_int("RANK", 0) != 0:
+        return
+    reps = ensemble_params(WORKLOAD)
+    B = native.Batch([p for p, _ in reps])
+    for i, (p, seed) in enumerate(reps):
+        x, v = uniform_state(p, seed)
+        B.member(i).set_state(x, v)
+    W, K = args.warmup, args.steps
+    B.step(0, W)
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = sum(B.member(i).launch_count() for i in range(len(reps)))
+    t_wall0 = time.time()
+    t_dev = B.step(W, K)
+    t_wall1 = time.time()
+    l1 = sum(B.member(i).launch_count() for i in range(len(reps)))
+    clocks = sampler.stop(t_wall0, t_wall1)
+    n_tot = sum(p["n"] for p, _ in reps)
+    nc_tot = sum(p["Nc"] for p, _ in reps)
+    B.close()
+    line = {
+        "metric": METRIC, "value": n_tot * K / t_dev, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: per replica seeded uniform positions, Maxwellian velocities",
+        "config": {"workload": WORKLOAD["name"], "replicas": len(reps), "n_particles": n_tot, "n_cells": nc_tot,
+                   "form": "plain_f64, one context and stream per replica, steps replayed from CUDA graphs",
+                   "parallelism": "single GPU"},
+        "step_hbm": {"algorithmic_bytes_per_step": 256 * n_tot + 128 * nc_tot,
+                     "achieved_GBps": (256 * n_tot + 128 * nc_tot) * K / t_dev / 1e9},
+        "e2e": None, "gpu_launches": int(l1 - l0), "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
 def run_reference(args):
     from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state, write_case
 
@@ -348,6 +411,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif "replicas" in WORKLOAD:
+        run_ensemble(args)
     else:
         run_ours(args)
 

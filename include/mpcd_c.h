@@ -226,6 +226,24 @@ int mpcd_step_timed(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* device
  * stream+BC, walls, SRD index, SRD signs, collision, cell index, reference fields, zone seeds,
  * zone passes, closure cells, kick + re-sort). */
 int mpcd_step_profile(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* phase_seconds, int nphase);
+/* Step replay from CUDA graphs (default on): after the first step, plain steps without a
+ * metrics row are replayed from a captured graph with device-side seeds. 0 turns it off. */
+int mpcd_ctx_set_graphs(mpcd_ctx* ctx, int enable);
+
+/* ---------------------------------------------------------------- batched replicas */
+/* Independent replicas (reference: one run of the benchmark driver per replica), each with
+ * its own parameters, size, state and zone layout, advanced together: every step is issued
+ * for all replicas before the next one, each on its own streams, so their kernels overlap on
+ * the GPU. Members are ordinary contexts for state I/O and metrics (mpcd_batch_member). */
+typedef struct mpcd_batch mpcd_batch;
+int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_batch** out);
+int mpcd_batch_destroy(mpcd_batch* batch);
+int mpcd_batch_size(mpcd_batch* batch);
+mpcd_ctx* mpcd_batch_member(mpcd_batch* batch, int index);
+/* steps step0+1 .. step0+nsteps for every replica; device_seconds (nullable): CUDA-event time
+ * of the whole batch */
+int mpcd_batch_step(mpcd_batch* batch, int64_t step0, int64_t nsteps, double* device_seconds);
+
 /* Page-locked host memory (for staging states); NULL on failure. */
 void* mpcd_host_alloc(size_t bytes);
 void mpcd_host_free(void* p);

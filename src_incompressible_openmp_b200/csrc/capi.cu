@@ -1648,3 +1648,109 @@ extern "C" int mpcd_cell_fields_static(const mpcd_params_c* params, const double
     CUDA_TRY(cudaGetLastError());
     return MPCD_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Batched replicas: independent contexts (own parameters, sizes, states and zone layouts) that
+// advance together. Each step is issued for every replica before the next step, each replica
+// on its own streams and from its own step graph, so their kernels run side by side on the GPU.
+struct mpcd_batch {
+    int device = 0;
+    std::vector<mpcd_ctx*> members;
+    cudaStream_t stream = nullptr;  // timing and the fork/join of the members' streams
+    cudaEvent_t start = nullptr, stop = nullptr;
+    std::vector<cudaEvent_t> done;
+};
+
+extern "C" {
+
+int mpcd_ctx_set_graphs(mpcd_ctx* c, int enable) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    c->useGraphs = enable != 0;
+    return MPCD_OK;
+}
+
+int mpcd_batch_destroy(mpcd_batch* b) {
+    if (!b) return MPCD_OK;
+    cudaSetDevice(b->device);
+    for (mpcd_ctx* c : b->members) mpcd_ctx_destroy(c);
+    for (cudaEvent_t e : b->done)
+        if (e) cudaEventDestroy(e);
+    if (b->start) cudaEventDestroy(b->start);
+    if (b->stop) cudaEventDestroy(b->stop);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return MPCD_OK;
+}
+
+int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_batch** out) {
+    if (!params || !out || count < 1) return set_err(MPCD_ERR_INVALID_ARG, "null argument or empty batch");
+    *out = nullptr;
+    mpcd_batch* b = new mpcd_batch();
+    b->device = device;
+    for (int i = 0; i < count; ++i) {
+        mpcd_ctx* c = nullptr;
+        const int rc = mpcd_ctx_create(params + i, device, &c);
+        if (rc) {
+            const std::string msg = "replica " + std::to_string(i) + ": " + g_err;
+            mpcd_batch_destroy(b);
+            return set_err(rc, msg);
+        }
+        b->members.push_back(c);
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->start) != cudaSuccess || cudaEventCreate(&b->stop) != cudaSuccess) {
+        cudaGetLastError();
+        mpcd_batch_destroy(b);
+        return set_err(MPCD_ERR_CUDA, "batch stream");
+    }
+    b->done.assign((size_t)count, nullptr);
+    for (auto& e : b->done)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            mpcd_batch_destroy(b);
+            return set_err(MPCD_ERR_CUDA, "batch events");
+        }
+    *out = b;
+    return MPCD_OK;
+}
+
+int mpcd_batch_size(mpcd_batch* b) { return b ? (int)b->members.size() : 0; }
+
+mpcd_ctx* mpcd_batch_member(mpcd_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->members.size()) return nullptr;
+    return b->members[(size_t)i];
+}
+
+int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device_seconds) {
+    if (!b) return set_err(MPCD_ERR_INVALID_ARG, "null batch");
+    if (nsteps < 0) return set_err(MPCD_ERR_INVALID_ARG, "nsteps must be >= 0");
+    for (mpcd_ctx* c : b->members)
+        if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution || !c->pc.useLiquidClosure)
+            return set_err(MPCD_ERR_INVALID_ARG, "the benchmark step needs useIncompressibleRedistribution, useZoneRedistribution and useLiquidClosure");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaEventRecord(b->start, b->stream));
+    for (mpcd_ctx* c : b->members) CUDA_TRY(cudaStreamWaitEvent(c->stream, b->start, 0));
+    for (int64_t k = 1; k <= nsteps; ++k)
+        for (mpcd_ctx* c : b->members) {
+            const int rc = run_steps(c, step0 + k - 1, 1, false);
+            if (rc) return rc;
+        }
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        mpcd_ctx* c = b->members[i];
+        CUDA_TRY(cudaEventRecord(b->done[i], c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(b->stream, b->done[i], 0));
+        if (c->side) CUDA_TRY(cudaStreamWaitEvent(b->stream, c->signsReady[(step0 + nsteps + 1) & 1], 0));
+    }
+    CUDA_TRY(cudaEventRecord(b->stop, b->stream));
+    CUDA_TRY(cudaEventSynchronize(b->stop));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, b->start, b->stop));
+    if (device_seconds) *device_seconds = ms * 1e-3;
+    for (mpcd_ctx* c : b->members) {
+        const int rc = check_device(c);
+        if (rc) return rc;
+    }
+    return MPCD_OK;
+}
+
+}  // extern "C"

@@ -73,6 +73,12 @@ def lib():
         "mpcd_step_timed": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
         "mpcd_step_profile": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double), C.c_int], C.c_int),
         "mpcd_launch_count": ([C.c_void_p], C.c_int64),
+        "mpcd_ctx_set_graphs": ([C.c_void_p, C.c_int], C.c_int),
+        "mpcd_batch_create": ([P(_abi.ParamsC), C.c_int, C.c_int, P(C.c_void_p)], C.c_int),
+        "mpcd_batch_destroy": ([C.c_void_p], C.c_int),
+        "mpcd_batch_size": ([C.c_void_p], C.c_int),
+        "mpcd_batch_member": ([C.c_void_p, C.c_int], C.c_void_p),
+        "mpcd_batch_step": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
         "mpcd_cell_fields_static": ([P(_abi.ParamsC), C.c_void_p, C.c_void_p, C.c_int64, C.c_double,
                                      P(_abi.CellFieldsC), C.c_void_p], C.c_int),
         "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
@@ -271,7 +277,65 @@ class Context:
     def launch_count(self):
         return int(lib().mpcd_launch_count(self.h))
 
+    def set_graphs(self, enable):
+        """Step replay from CUDA graphs (on by default)."""
+        _check(lib().mpcd_ctx_set_graphs(self.h, 1 if enable else 0))
+
     def step(self, step0, nsteps, metrics=False):
         m = _abi.StepMetricsC() if metrics else None
         _check(lib().mpcd_step(self.h, step0, nsteps, C.byref(m) if m is not None else None))
         return _abi.struct_to_dict(m) if metrics else None
+
+
+class _Member(Context):
+    """A replica of a Batch: a context the batch owns (not destroyed on its own)."""
+
+    def __init__(self, params, handle):
+        self.params = dict(params)
+        self.n = int(params["n"])
+        self.Nc = int(params["Nc"])
+        self.h = handle
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Independent replicas advanced together (mpcd_batch_*): each keeps its own parameters,
+    size, state and zone layout; member(i) is the i-th replica's context."""
+
+    def __init__(self, params_list, device=0):
+        self.params = [dict(p) for p in params_list]
+        arr = (_abi.ParamsC * len(self.params))(*[to_c(p) for p in self.params])
+        h = C.c_void_p()
+        _check(lib().mpcd_batch_create(arr, len(self.params), device, C.byref(h)))
+        self.h = h
+        self.members = [_Member(p, lib().mpcd_batch_member(self.h, i)) for i, p in enumerate(self.params)]
+
+    def member(self, i):
+        return self.members[i]
+
+    def step(self, step0, nsteps):
+        """Advances every replica; returns the device seconds of the whole batch."""
+        t = C.c_double()
+        _check(lib().mpcd_batch_step(self.h, step0, nsteps, C.byref(t)))
+        return t.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.close()
+            lib().mpcd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
