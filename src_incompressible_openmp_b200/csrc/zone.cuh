@@ -661,22 +661,21 @@ struct ZoneState {
         return true;
     }
 
-    __device__ __forceinline__ void push_recv(int* recv, int& nrecv, int c) {
-        bool seen = false;
-        for (int q = 0; q < nrecv; ++q) seen |= (recv[q] == c);
-        if (!seen) {
-            if (lane == 0) recv[nrecv] = c;
+    // receivers of a source cell, lane k < nrecv holding the k-th (at most 24 targets)
+    __device__ __forceinline__ void push_recv(int& recvReg, int& nrecv, int c) {
+        if (!__any_sync(0xffffffffu, lane < nrecv && recvReg == c)) {
+            if (lane == nrecv) recvReg = c;
             ++nrecv;
         }
-        __syncwarp();
     }
 
     // update_transfer_correction_masks (src/zone_pass.cpp:492-525), forceSkip = false
-    __device__ void update_masks(int src, const int* recv, int nrecv) {
-        bool allBulk = (M.cflags[src] & kCBulkBefore) != 0;
-        for (int q = 0; q < nrecv; ++q) allBulk &= (M.cflags[recv[q]] & kCBulkBefore) != 0;
+    __device__ void update_masks(int src, int recvReg, int nrecv) {
+        const bool ok = lane >= nrecv || (M.cflags[recvReg] & kCBulkBefore) != 0;
+        const bool allBulk = ((M.cflags[src] & kCBulkBefore) != 0) && __all_sync(0xffffffffu, ok);
+        const int prevRecv = __shfl_up_sync(0xffffffffu, recvReg, 1);
         if (lane <= nrecv) {
-            const int c = (lane == 0) ? src : recv[lane - 1];
+            const int c = (lane == 0) ? src : prevRecv;
             uint8_t f = M.cflags[c];
             if (allBulk) f |= kCBulkBulk;
             else f = (uint8_t)((f | kCSkip) & ~kCBulkBulk);
@@ -686,10 +685,14 @@ struct ZoneState {
     }
 
     // ------------------------------------------------------------------ dense phase
-    // admissible_dense_targets_rangeR (src/zone_pass.cpp:413-434) + the zone filter
-    __device__ int admissible(int l, bool low, int* cand) {
+    // Targets of dense cell l, ranked, into T[0..m): admissible_dense_targets_rangeR
+    // (src/zone_pass.cpp:413-434) with the zone filter, then rank_dense_targets_unified
+    // (:436-490, inwardWeight = 0): angular bins, per-bin order on (-deficit, cnt, cheb,
+    // dist2, U01) (a stable insertion sort), round robin over the bins from a random start.
+    // Lane k < 24 examines neighbour k; the kept ones keep their order (compacted index ci).
+    __device__ int select_targets(int l, bool low, int* T) {
         const int ix = gx_of(l), iy = gy_of(l);
-        int nb = -1;
+        int nb = -1, ddx = 0, ddy = 0, idx = 0;
         if (lane < 24) {
             const int kk = (lane < 12) ? lane : lane + 1;
             const int dy = kk / 5 - 2, dx = kk % 5 - 2;
@@ -706,33 +709,28 @@ struct ZoneState {
             keep = keep && ((same & m0 & lanemask_lt()) == 0);
         }
         const unsigned mk = __ballot_sync(0xffffffffu, keep);
-        if (keep) cand[__popc(mk & lanemask_lt())] = nb;
-        __syncwarp();
-        return __popc(mk);
-    }
-
-    // rank_dense_targets_unified (src/zone_pass.cpp:436-490), inwardWeight = 0: per-bin
-    // stable insertion sort on (-deficit, cnt, cheb, dist2, U01), then round robin
-    __device__ int rank_dense(int l, const int* cand, int m, bool low, int* T) {
+        const int m = __popc(mk);
         if (m == 0) return 0;
-        const int startBin = (int)rng.uint_in(1, 8) - 1;
-        rng.ensure(m);
-        int nb = -1, key2 = 0, idx = 0, ddx = 0, ddy = 0;
+        const int ci = __popc(mk & lanemask_lt());
+        // draws: uniform_int(1, 8) for the start bin (range 8: Lemire never rejects), then one
+        // U01 per target in compacted order
+        rng.ensure(m + 1);
+        const int startBin = (int)__umul64hi(rng.peek(0), 8ULL);
+        int key2 = 0;
         double dneg = 0.0, tie = 0.0;
-        if (lane < m) {
-            nb = cand[lane];
-            idx = step_index(gx_of(l), gy_of(l), gx_of(nb), gy_of(nb), ddx, ddy);
+        if (keep) {
+            idx = step_index(ix, iy, gx_of(nb), gy_of(nb), ddx, ddy);
             if (idx < 0) raise_error(A->st, kErrTableRange, zone);
             dneg = -smax(0.0, __dsub_rn(map_val(nb, low), (double)M.cnt[nb]));
             const int cheb = max(abs(ddx), abs(ddy)), d2 = ddx * ddx + ddy * ddy;
             key2 = (M.cnt[nb] << 8) | (cheb << 4) | d2;  // lexicographic (cnt, cheb, dist2)
-            tie = canon(rng.peek(lane));
+            tie = canon(rng.peek(1 + ci));
         }
-        rng.consume(m);
+        rng.consume(m + 1);
         // angular bin of the step (table held in lanes 0..24)
         const int tb = __shfl_sync(0xffffffffu, atanLane, idx < 0 ? 0 : idx);
-        const int bin = (lane < m) ? ((idx < 0) ? 0 : tb) : 8 + lane;
-        // rank within the bin: compare only with the other lanes of the same bin
+        const int bin = keep ? ((idx < 0) ? 0 : tb) : 8 + lane;
+        // rank within the bin: compare only with the other kept lanes of the same bin
         unsigned others = __match_any_sync(0xffffffffu, bin) & ~(1u << lane);
         int r = 0;
         while (__any_sync(0xffffffffu, others != 0u)) {
@@ -747,7 +745,7 @@ struct ZoneState {
                 else if (kj != key2) less = kj < key2;
                 else if (tj != tie) less = tj < tie;
                 else { less = false; eq = true; }
-                if (less || (eq && j < lane)) ++r;
+                if (less || (eq && j < lane)) ++r;  // lane order = compacted order
             }
         }
         // round robin over the bins from startBin: position = entries of rank < r in every
@@ -755,13 +753,13 @@ struct ZoneState {
         int pos = 0;
         for (int b = 0; b < 8; ++b) {
             const int cb = __popc(__ballot_sync(0xffffffffu, bin == b));
-            if (lane < m) {
+            if (keep) {
                 pos += min(cb, r);
                 const int rb = (b - startBin + 8) & 7, rq = (bin - startBin + 8) & 7;
                 if (rb < rq && cb > r) ++pos;
             }
         }
-        if (lane < m) T[pos] = nb;
+        if (keep) T[pos] = nb;
         __syncwarp();
         return m;
     }
@@ -769,7 +767,7 @@ struct ZoneState {
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589). Lane k holds
     // target k's map value and deficit; a move changes only the deficit of its own target, so
     // each round walks the targets whose deficit was positive at the start of the round.
-    __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int* recv, int& nrecv, int slotPre,
+    __device__ int spread(int s, const int* T, int nT, bool low, int needOut, int& recvReg, int& nrecv, int slotPre,
                           int preOff) {
         if (needOut <= 0 || nT == 0) return 0;
         const int srcLen = M.len[s];
@@ -793,7 +791,10 @@ struct ZoneState {
                 const int deficit = __shfl_sync(0xffffffffu, defj, kk);
                 const int t = __shfl_sync(0xffffffffu, tl, kk);
                 const int remaining = __popc(pm >> kk);
-                const int quota = max(1, (int)ceil(__ddiv_rn((double)needOut, (double)max(1, remaining))));
+                // ceil(needOut / remaining): integer division gives the same value as the
+                // reference's ceil of the double quotient for these magnitudes
+                const int rem1 = max(1, remaining);
+                const int quota = max(1, (needOut + rem1 - 1) / rem1);
                 const int nt = max(1, min(min(quota, deficit), min(needOut, srcLen - taken)));
                 if (t == s) {
                     if (lane == 0) raise_error(A->st, kErrTargetIsSource, zone);
@@ -801,7 +802,7 @@ struct ZoneState {
                     return moved;
                 }
                 if (!move_into(s, taken, nt, t, slotPre, preOff)) return moved;
-                push_recv(recv, nrecv, t);
+                push_recv(recvReg, nrecv, t);
                 if (lane == kk) defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
                 taken += nt;
                 moved += nt;
@@ -823,9 +824,8 @@ struct ZoneState {
 
     // one dense cell (src/zone_pass.cpp:734-753 calling :591-634)
     __device__ void dense_cell(int l) {
-        int* cand = M.small;
         int* T = M.small + 32;
-        int* recv = M.small + 64;
+        int recvReg = -1;
         const int ncc = M.cnt[l];
         if (ncc <= 0) return;
         const double hl = map_high(l);
@@ -849,15 +849,14 @@ struct ZoneState {
             const int need = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
             if (need <= 0) break;
             const bool low = (round == 0);
-            const int m = admissible(l, low, cand);
-            const int nT = rank_dense(l, cand, m, low, T);
-            moved += spread(l, T, nT, low, need, recv, nrecv, slotPre, moved);
+            const int nT = select_targets(l, low, T);
+            moved += spread(l, T, nT, low, need, recvReg, nrecv, slotPre, moved);
             if (failed || fatal) return;
         }
-        if (lane < nrecv) M.cflags[recv[lane]] |= (kCRecv | kCChanged);
+        if (lane < nrecv) M.cflags[recvReg] |= (kCRecv | kCChanged);
         if (lane == 0 && moved > 0) M.cflags[l] |= kCChanged;
         __syncwarp();
-        update_masks(l, recv, nrecv);
+        update_masks(l, recvReg, nrecv);
         movedDense += moved;
     }
 
@@ -958,8 +957,7 @@ struct ZoneState {
                 M.cflags[d] |= kCChanged;
             }
             __syncwarp();
-            int one = l;
-            update_masks(d, &one, 1);
+            update_masks(d, (lane == 0) ? l : -1, 1);
             movedSparse += nt;
             need -= nt;
             if (need <= 0) break;
