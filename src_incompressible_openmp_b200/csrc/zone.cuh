@@ -68,10 +68,9 @@ struct ZoneMem {
     double* nsm;       // (TX+2)(TY+2): smoothed occupancy; reused for dU2 at the end
     int* win;          // (TX+4)(TY+4): pass-input counts around the zone (-1 = outside)
     int* gstart;       // cell: start of its input segment in the cell index
-    int* cnt;          // cell: live count
     int* cnt0;         // cell: input count
     int* head;         // cell: list head (implicit: offset into the input segment)
-    int* len;          // cell
+    int* len;          // cell: list length = live count
     int* abase;        // cell: arena start of a materialised list
     int* cap;          // cell: arena capacity of a materialised list
     uint8_t* cflags;   // cell
@@ -88,7 +87,7 @@ struct ZoneMem {
         add(64 * 8, 8);
         add((size_t)winCap * 8, 8);
         add((size_t)winCap * 4, 4);
-        for (int k = 0; k < 7; ++k) add((size_t)maxCells * 4, 4);
+        for (int k = 0; k < 6; ++k) add((size_t)maxCells * 4, 4);
         add((size_t)maxCells, 1);
         add((size_t)maxCells * 2, 2);
         add((size_t)maxCells * 2, 2);
@@ -110,7 +109,6 @@ struct ZoneMem {
         nsm = (double*)take((size_t)winCap * 8, 8);
         win = (int*)take((size_t)winCap * 4, 4);
         gstart = (int*)take((size_t)maxCells * 4, 4);
-        cnt = (int*)take((size_t)maxCells * 4, 4);
         cnt0 = (int*)take((size_t)maxCells * 4, 4);
         head = (int*)take((size_t)maxCells * 4, 4);
         len = (int*)take((size_t)maxCells * 4, 4);
@@ -496,7 +494,7 @@ struct ZoneState {
     __device__ __forceinline__ int gy_of(int l) const { return ys + l % TY; }
 
     __device__ __forceinline__ int cnt_at(int ix, int iy) const {
-        if (in_zone(ix, iy)) return M.cnt[loc(ix, iy)];
+        if (in_zone(ix, iy)) return M.len[loc(ix, iy)];
         int wx = ix - (xs - 2), wy = iy - (ys - 2);
         if (wx < 0) wx += P().Nx;
         else if (wx >= TX + 4) wx -= P().Nx;
@@ -560,14 +558,14 @@ struct ZoneState {
 
     // ------------------------------------------------------------------ smoothing, maps
     __device__ void compute_nsm() {
-        zone_compute_nsm(M.nsm, M.win, M.cnt, xs, ys, TX, TY, P().Nx, P().Ny, P().perx, P().pery, lane);
+        zone_compute_nsm(M.nsm, M.win, M.len, xs, ys, TX, TY, P().Nx, P().Ny, P().perx, P().pery, lane);
     }
 
     // start of a map build: record which cells are bulk (cnt > 0)
     __device__ void mark_bulk() {
         for (int l = lane; l < nl; l += kWarp) {
             const uint8_t f = M.cflags[l];
-            M.cflags[l] = (uint8_t)((f & ~kCBulkBefore) | ((M.cnt[l] > 0) ? kCBulkBefore : 0));
+            M.cflags[l] = (uint8_t)((f & ~kCBulkBefore) | ((M.len[l] > 0) ? kCBulkBefore : 0));
         }
         __syncwarp();
     }
@@ -655,7 +653,6 @@ struct ZoneState {
         }
         if (lane == 0) {
             M.len[t] += nt;
-            M.cnt[t] += nt;
         }
         __syncwarp();
         return true;
@@ -699,7 +696,7 @@ struct ZoneState {
             int jy, jx;
             if (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy)) {
                 const int t = loc(jx, jy);
-                if ((double)M.cnt[t] < map_val(t, low)) nb = t;
+                if ((double)M.len[t] < map_val(t, low)) nb = t;
             }
         }
         bool keep = nb >= 0;
@@ -721,9 +718,9 @@ struct ZoneState {
         if (keep) {
             idx = step_index(ix, iy, gx_of(nb), gy_of(nb), ddx, ddy);
             if (idx < 0) raise_error(A->st, kErrTableRange, zone);
-            dneg = -smax(0.0, __dsub_rn(map_val(nb, low), (double)M.cnt[nb]));
+            dneg = -smax(0.0, __dsub_rn(map_val(nb, low), (double)M.len[nb]));
             const int cheb = max(abs(ddx), abs(ddy)), d2 = ddx * ddx + ddy * ddy;
-            key2 = (M.cnt[nb] << 8) | (cheb << 4) | d2;  // lexicographic (cnt, cheb, dist2)
+            key2 = (M.len[nb] << 8) | (cheb << 4) | d2;  // lexicographic (cnt, cheb, dist2)
             tie = canon(rng.peek(1 + ci));
         }
         rng.consume(m + 1);
@@ -777,7 +774,7 @@ struct ZoneState {
         if (lane < nT) {
             tl = T[lane];
             mv = map_val(tl, low);
-            defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
+            defj = max(0, (int)floor(__dsub_rn(mv, (double)M.len[tl])));
         }
         int taken = 0, moved = 0;
         bool stop = false;
@@ -803,7 +800,7 @@ struct ZoneState {
                 }
                 if (!move_into(s, taken, nt, t, slotPre, preOff)) return moved;
                 push_recv(recvReg, nrecv, t);
-                if (lane == kk) defj = max(0, (int)floor(__dsub_rn(mv, (double)M.cnt[tl])));
+                if (lane == kk) defj = max(0, (int)floor(__dsub_rn(mv, (double)M.len[tl])));
                 taken += nt;
                 moved += nt;
                 needOut -= nt;
@@ -816,7 +813,6 @@ struct ZoneState {
         if (moved > 0 && lane == 0) {
             M.head[s] += taken;
             M.len[s] -= taken;
-            M.cnt[s] = M.len[s];
         }
         __syncwarp();
         return moved;
@@ -826,7 +822,7 @@ struct ZoneState {
     __device__ void dense_cell(int l) {
         int* T = M.small + 32;
         int recvReg = -1;
-        const int ncc = M.cnt[l];
+        const int ncc = M.len[l];
         if (ncc <= 0) return;
         const double hl = map_high(l);
         if ((double)ncc <= hl) return;
@@ -846,7 +842,7 @@ struct ZoneState {
         // (one copy of the code for both rounds)
 #pragma unroll 1
         for (int round = 0; round < 2; ++round) {
-            const int need = max(0, (int)ceil(__dsub_rn((double)M.cnt[l], hl)));
+            const int need = max(0, (int)ceil(__dsub_rn((double)M.len[l], hl)));
             if (need <= 0) break;
             const bool low = (round == 0);
             const int nT = select_targets(l, low, T);
@@ -880,7 +876,7 @@ struct ZoneState {
     __device__ void sparse_cell(int l) {
         const DevParams& p = P();
         int* don = M.small + 96;
-        const int ncc = M.cnt[l];
+        const int ncc = M.len[l];
         if (ncc <= 0) return;
         if (M.len[l] == 0) return;
         const int ix = gx_of(l), iy = gy_of(l);
@@ -901,7 +897,7 @@ struct ZoneState {
         const int lowInt = p.lowThrBulkInt;
         int need = max(0, lowInt - ncc);
         if (need <= 0) return;
-        const bool isDonor = uniq && M.cnt[nb] > lowInt;
+        const bool isDonor = uniq && M.len[nb] > lowInt;
         const unsigned md = __ballot_sync(0xffffffffu, isDonor);
         const int nd = __popc(md);
         if (nd == 0) return;
@@ -942,7 +938,7 @@ struct ZoneState {
             const int d = don[k];
             const int ld = M.len[d];
             if (ld == 0) continue;
-            const int avail = M.cnt[d] - lowInt;
+            const int avail = M.len[d] - lowInt;
             if (avail <= 0) continue;
             const int nt = min(min(need, avail), ld);
             if (nt <= 0) continue;
@@ -952,7 +948,6 @@ struct ZoneState {
             if (lane == 0) {
                 M.head[d] += nt;
                 M.len[d] -= nt;
-                M.cnt[d] = M.len[d];
                 M.cflags[l] |= (kCRecv | kCChanged);
                 M.cflags[d] |= kCChanged;
             }
@@ -1035,7 +1030,6 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     for (int l = lane; l < S.nl; l += kWarp) {
         const int c = M.win[(l / S.TY + 2) * S.WY + (l % S.TY + 2)];
         M.cnt0[l] = c;
-        M.cnt[l] = c;
         M.len[l] = c;
         M.head[l] = 0;
         M.abase[l] = 0;
@@ -1048,7 +1042,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     for (int pass = 0; pass < p.maxPasses && !S.failed && !S.fatal; ++pass) {
         if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
-        const int nd = S.collect([&](int l) { return (double)M.cnt[l] > S.map_high(l); });
+        const int nd = S.collect([&](int l) { return (double)M.len[l] > S.map_high(l); });
         zone_shuffle_fast(M.list, nd, S.rng, lane);
         for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
     }
@@ -1058,7 +1052,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         // otherwise it is needed only if some cell is sparse (inward gradient, donor scores)
         if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
-        const int nlow = S.collect([&](int l) { return M.cnt[l] > 0 && (double)M.cnt[l] < S.map_low(l); });
+        const int nlow = S.collect([&](int l) { return M.len[l] > 0 && (double)M.len[l] < S.map_low(l); });
         if (!p.useLFF && nlow > 0) S.compute_nsm();
         zone_shuffle_fast(M.list, nlow, S.rng, lane);
         for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
