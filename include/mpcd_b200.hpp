@@ -13,6 +13,7 @@
 // the state resident on the device across steps instead (the fast path).
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -21,6 +22,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mpcd_c.h"
@@ -125,6 +127,49 @@ struct WallInfo {
     double dPxRight = 0.0;
     double dPyLeft = 0.0;
     double dPyRight = 0.0;
+};
+
+// reference include/types.h:113-123
+struct RunOutStep {
+    std::string inputTag;
+    std::string outputTag;
+    double pBotInst = 0.0;
+    double pTopInst = 0.0;
+    double pMeanInst = 0.0;
+    std::array<double, 6> redistribStats{};
+    std::array<double, 10> redistDiag{};
+    std::string layoutMode;
+    int nZonesExecuted = 0;
+};
+
+// reference include/zone_pass.h: the serial pass's result
+struct ZonePassMetrics {
+    double occStdBefore = 0.0;
+    double occStdAfter = 0.0;
+    double outBandBefore = 0.0;
+    double outBandAfter = 0.0;
+    int nDenseBefore = 0;
+    int nDenseAfter = 0;
+    int nSparseBefore = 0;
+    int nSparseAfter = 0;
+    int nEmptyActiveBefore = 0;
+    int nEmptyActiveAfter = 0;
+    int nParticlesMovedDense = 0;
+    int nParticlesMovedSparse = 0;
+    int nZonesExecuted = 0;
+    double corrRmsDU = 0.0;
+    double corrMaxDU = 0.0;
+    double momentumDeltaX = 0.0;
+    double momentumDeltaY = 0.0;
+    std::string layoutMode;
+};
+
+struct ZonePassResult {
+    State stateOut;
+    CellFields beforeFields;
+    CellFields afterFields;
+    ZonePassMetrics metrics;
+    std::vector<std::int32_t> zoneOwnerMap;
 };
 
 // reference include/zone_pass_openmp.h:12-33. Times are device seconds of the pass.
@@ -461,6 +506,90 @@ inline OpenMPPassResult run_zone_pass_sync_serial_base(const State& stateIn, con
     return run_zone_pass_openmp(stateIn, params, "base", rngSeedBase, 1);
 }
 
+namespace b200 {
+// Occupancy diagnostics of a count field (reference src/zone_pass.cpp:975-1047). The
+// threshold maps of those functions only matter for empty cells, which can be neither dense
+// nor sparse, so the bulk thresholds decide every cell.
+struct CountStats {
+    double occStd, outBand;
+    int nDense, nSparse, nEmpty;
+};
+inline CountStats count_stats(const std::vector<std::int32_t>& N, const Params& p) {
+    const double highThr = (p.highMode == "1+coef") ? p.gamma * (1.0 + p.coef) : p.gamma + p.gamma * p.coef;
+    double lowThr = (p.lowMode == "1+coef") ? p.gamma / (1.0 + p.coef) : p.gamma - p.gamma * p.coef;
+    if (std::isfinite(p.lowThrBulkOverride)) lowThr = p.lowThrBulkOverride;
+    CountStats s{0.0, 0.0, 0, 0, 0};
+    if (N.empty()) return s;
+    double sum = 0.0;
+    for (std::int32_t n : N) sum += static_cast<double>(n);
+    const double mean = sum / static_cast<double>(N.size());
+    double acc = 0.0;
+    int nOut = 0;
+    for (std::int32_t n : N) {
+        const double d = static_cast<double>(n) - mean;
+        acc += d * d;
+        const bool dense = static_cast<double>(n) > highThr;
+        const bool sparse = n > 0 && static_cast<double>(n) < lowThr;
+        s.nDense += dense;
+        s.nSparse += sparse;
+        s.nEmpty += (n == 0);
+        nOut += (dense || sparse);
+    }
+    s.occStd = std::sqrt(acc / static_cast<double>(N.size())) / std::max(p.gamma, 1e-30);
+    s.outBand = static_cast<double>(nOut) / static_cast<double>(N.size());
+    return s;
+}
+inline std::pair<double, double> total_momentum(const std::vector<double>& v, int n) {
+    double px = 0.0, py = 0.0;
+    for (int i = 0; i < n; ++i) {
+        px += v[2 * (std::size_t)i];
+        py += v[2 * (std::size_t)i + 1];
+    }
+    return {px, py};
+}
+}  // namespace b200
+
+// reference src/zone_pass.cpp:1096-1163: the zones one after another, in place
+inline ZonePassResult run_zone_pass(const State& stateIn, const Params& params, const std::string& layoutMode,
+                                    std::uint64_t rngSeedBase) {
+    mpcd_ctx* c = b200::context_for(params);
+    if (stateIn.x.size() != 2u * (std::size_t)params.n || stateIn.v.size() != 2u * (std::size_t)params.n)
+        throw std::runtime_error("run_zone_pass: unexpected state size");
+    const int mode = (layoutMode == "shifted") ? MPCD_LAYOUT_SHIFTED : MPCD_LAYOUT_BASE;
+    const double rhoTarget = params.gamma / ((params.Lx / (double)params.Nx) * (params.Ly / (double)params.Ny));
+    ZonePassResult out;
+    out.stateOut = stateIn;
+    b200::upload(c, stateIn.x, stateIn.v, params.n);
+    out.beforeFields = b200::make_fields(params);
+    mpcd_cellfields_c bv = b200::view(out.beforeFields);
+    b200::check(mpcd_cell_fields(c, rhoTarget, &bv));
+    mpcd_pass_metrics_c m;
+    b200::check(mpcd_zone_pass_serial(c, mode, rngSeedBase, &m));
+    b200::check(mpcd_get_state(c, out.stateOut.x.data(), out.stateOut.v.data()));
+    out.afterFields = b200::make_fields(params);
+    mpcd_cellfields_c av = b200::view(out.afterFields);
+    b200::check(mpcd_cell_fields(c, rhoTarget, &av));
+    out.zoneOwnerMap.assign(static_cast<std::size_t>(params.Nc), 0);
+    b200::check(mpcd_zone_owner_map(c, params.zoneSingleFullDomainMode ? MPCD_LAYOUT_SINGLE_FULL : mode, out.zoneOwnerMap.data()));
+    ZonePassMetrics& M = out.metrics;
+    M.layoutMode = layoutMode;
+    M.nZonesExecuted = m.nZones;
+    const auto b = b200::count_stats(out.beforeFields.N, params), a = b200::count_stats(out.afterFields.N, params);
+    M.occStdBefore = b.occStd; M.occStdAfter = a.occStd;
+    M.outBandBefore = b.outBand; M.outBandAfter = a.outBand;
+    M.nDenseBefore = b.nDense; M.nDenseAfter = a.nDense;
+    M.nSparseBefore = b.nSparse; M.nSparseAfter = a.nSparse;
+    M.nEmptyActiveBefore = b.nEmpty; M.nEmptyActiveAfter = a.nEmpty;
+    M.nParticlesMovedDense = m.nParticlesMovedDense;
+    M.nParticlesMovedSparse = m.nParticlesMovedSparse;
+    M.corrRmsDU = m.corrRmsDU;
+    M.corrMaxDU = m.corrMaxDU;
+    const auto p0 = b200::total_momentum(stateIn.v, params.n), p1 = b200::total_momentum(out.stateOut.v, params.n);
+    M.momentumDeltaX = p1.first - p0.first;
+    M.momentumDeltaY = p1.second - p0.second;
+    return out;
+}
+
 // reference src/liquid_closure.cpp:329-444
 inline LiquidClosureResult run_liquid_closure(const State& stateRef, const State& stateRed, const Params& params) {
     if (!params.useLiquidClosure) throw std::runtime_error("run_liquid_closure requires useLiquidClosure=true");
@@ -615,6 +744,26 @@ inline void write_cell_fields_bin(const std::string& filepath, const CellFields&
     };
     put(G.N);
     for (const auto* f : {&G.Ux, &G.Uy, &G.Px, &G.Py, &G.T, &G.rho, &G.Pkin, &G.Pvir, &G.P, &G.rhoTarget}) put(*f);
+}
+
+// reference src/params_io.cpp:139-151
+inline void write_runout_kv(const std::string& filepath, const RunOutStep& runout) {
+    std::ofstream fout(filepath);
+    if (!fout) throw std::runtime_error("Cannot open runout file for writing: " + filepath);
+    fout << "inputTag=" << runout.inputTag << '\n';
+    fout << "outputTag=" << runout.outputTag << '\n';
+    fout << "pBotInst=" << runout.pBotInst << '\n';
+    fout << "pTopInst=" << runout.pTopInst << '\n';
+    fout << "pMeanInst=" << runout.pMeanInst << '\n';
+    fout << "layoutMode=" << runout.layoutMode << '\n';
+    fout << "nZonesExecuted=" << runout.nZonesExecuted << '\n';
+}
+
+// reference src/zone_pass.cpp:1165-1181 (same layout as write_i32_grid_bin_lc)
+inline void write_i32_grid_bin(const std::string& filepath, int Nx, int Ny, const std::vector<std::int32_t>& data) {
+    if (data.size() != static_cast<std::size_t>(Nx) * static_cast<std::size_t>(Ny))
+        throw std::runtime_error("write_i32_grid_bin: unexpected data size");
+    b200::write_grid(filepath, Nx, Ny, data, "i32");
 }
 
 // reference src/liquid_closure.cpp:446-480

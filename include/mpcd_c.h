@@ -204,6 +204,12 @@ int mpcd_save_ref(mpcd_ctx* ctx);
 /* mpcd::run_zone_pass_openmp (reference src/zone_pass_openmp.cpp:176-182, snapshot
  * semantics of :34-172). mode: mpcd_layout_mode. metrics nullable. */
 int mpcd_zone_pass(mpcd_ctx* ctx, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics);
+/* mpcd::run_zone_pass (reference src/zone_pass.cpp:1096-1163): the zones one after another
+ * in id order, each on the state the previous ones left, in place. One warp runs them in
+ * sequence (the order is the semantics), so this is the slow pass; the validators and the
+ * non-OpenMP benchmark driver of the reference use it. metrics nullable (timeKernel: device
+ * seconds; nThreadsUsed: 1). */
+int mpcd_zone_pass_serial(mpcd_ctx* ctx, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics);
 /* mpcd::run_liquid_closure (reference src/liquid_closure.cpp:329-444) with stateRef = the
  * saved reference and stateRed = the current state; the current state becomes stateOut.
  * metrics and detail nullable. */

@@ -1168,6 +1168,58 @@ int oracle_zone_pass(const P* p, const double* xin, const double* vin, double* x
     return MPCD_OK;
 }
 
+/* run_zone_pass (src/zone_pass.cpp:1096-1163): the zones run one after another, each on the
+ * state the previous ones left (cell lists rebuilt from the current positions, ascending
+ * particle id), moving and correcting the particles of its rectangle in place. */
+int oracle_zone_pass_serial(const P* p, const double* xin, const double* vin, double* xout, double* vout, int mode,
+                            uint64_t seedBase, mpcd_pass_metrics_c* m) {
+    int rc = check_pass_params(p);
+    if (rc) return rc;
+    const int n = p->n, Nc = p->Nc;
+    int32_t* cid = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* cnt = (int32_t*)calloc((size_t)Nc, sizeof(int32_t));
+    int32_t* start = (int32_t*)calloc((size_t)Nc + 1, sizeof(int32_t));
+    int32_t* cur = (int32_t*)malloc(sizeof(int32_t) * (size_t)Nc);
+    int32_t* ids = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* owner = (int32_t*)malloc(sizeof(int32_t) * (size_t)Nc);
+    double* vsnap = (double*)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
+    rect* zones = NULL;
+    const int nz = build_layout(p, mode, &zones, owner);
+    memcpy(xout, xin, sizeof(double) * 2 * (size_t)n);
+    memcpy(vout, vin, sizeof(double) * 2 * (size_t)n);
+    int totD = 0, totS = 0, corrCount = 0;
+    double corrAcc = 0.0, corrMax = 0.0;
+    for (int iz = 0; iz < nz; ++iz) {
+        oracle_cell_ids(p, xout, cid);
+        memset(cnt, 0, sizeof(int32_t) * (size_t)Nc);
+        for (int i = 0; i < n; ++i) cnt[cid[i]]++;
+        for (int c = 0; c < Nc; ++c) start[c + 1] = start[c] + cnt[c];
+        memcpy(cur, start, sizeof(int32_t) * (size_t)Nc);
+        for (int i = 0; i < n; ++i) ids[cur[cid[i]]++] = i;
+        memcpy(vsnap, vout, sizeof(double) * 2 * (size_t)n);
+        int mD = 0, mS = 0;
+        double s4 = 0.0, s5 = 0.0;
+        zone_kernel(p, zones[iz], cnt, start, ids, vsnap, xout, vout, seedBase + 104729ULL * (uint64_t)(iz + 1), &mD, &mS,
+                    &s4, &s5);
+        totD += mD;
+        totS += mS;
+        if (s4 > 0.0) { corrAcc += s4 * s4; ++corrCount; }
+        corrMax = dmax(corrMax, s5);
+    }
+    if (m) {
+        memset(m, 0, sizeof *m);
+        m->nZones = nz;
+        m->nThreadsRequested = 1;
+        m->nThreadsUsed = 1;
+        m->nParticlesMovedDense = totD;
+        m->nParticlesMovedSparse = totS;
+        m->corrRmsDU = (corrCount > 0) ? sqrt(corrAcc / (double)corrCount) : 0.0;
+        m->corrMaxDU = corrMax;
+    }
+    free(cid); free(cnt); free(start); free(cur); free(ids); free(owner); free(vsnap); free(zones);
+    return MPCD_OK;
+}
+
 /* ============================================================== liquid closure */
 
 static double rho_target(const P* p) {

@@ -249,6 +249,29 @@ int ref_zone_pass(const mpcd_params_c* pc, const double* xin, const double* vin,
     REF_CATCH
 }
 
+// mpcd::run_zone_pass (src/zone_pass.cpp:1096-1163): zones one after another, in place
+int ref_zone_pass_serial(const mpcd_params_c* pc, const double* xin, const double* vin, double* xout, double* vout,
+                         int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* m) {
+    REF_TRY
+    const mpcd::Params p = to_params(pc);
+    mpcd::State s = make_state(p, xin, vin);
+    const auto r = mpcd::run_zone_pass(s, p, layout_name(mode), seed_base);
+    std::memcpy(xout, r.stateOut.x.data(), r.stateOut.x.size() * sizeof(double));
+    std::memcpy(vout, r.stateOut.v.data(), r.stateOut.v.size() * sizeof(double));
+    if (m) {
+        std::memset(m, 0, sizeof *m);
+        m->nZones = r.metrics.nZonesExecuted;
+        m->nThreadsRequested = 1;
+        m->nThreadsUsed = 1;
+        m->nParticlesMovedDense = r.metrics.nParticlesMovedDense;
+        m->nParticlesMovedSparse = r.metrics.nParticlesMovedSparse;
+        m->corrRmsDU = r.metrics.corrRmsDU;
+        m->corrMaxDU = r.metrics.corrMaxDU;
+    }
+    return 0;
+    REF_CATCH
+}
+
 int ref_liquid_closure(const mpcd_params_c* pc, const double* refx, const double* refv, const double* redx,
                        const double* redv, double* outx, double* outv, mpcd_closure_metrics_c* m,
                        mpcd_closure_detail_c* d) {

@@ -128,6 +128,14 @@ struct mpcd_ctx {
     double2* zoneCorr = nullptr;
     int* overflow = nullptr;
     int* nOverflow = nullptr;
+    // serial pass (allocated on first use): pass-input lists + live-list area, per-cell
+    // current list start and count, the area's top, per-cell corrections of a zone
+    int* slotsLive = nullptr;
+    int* liveCnt = nullptr;
+    int* liveStart = nullptr;
+    int* liveTop = nullptr;
+    double2* duScratch = nullptr;
+    int64_t liveCap = 0;
     int* zoneCost = nullptr;   // per zone: cost bucket
     int* zoneHist = nullptr;   // kCostBuckets
     int* zoneOrder = nullptr;  // launch order, heaviest first
@@ -656,6 +664,87 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     return MPCD_OK;
 }
 
+__global__ void k_live_init(const uint64_t* __restrict__ start, int Nc, int* __restrict__ cnt, int* __restrict__ st,
+                            int* __restrict__ top, int n) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < Nc) {
+        const int a = (int)(uint32_t)start[c];
+        st[c] = a;
+        cnt[c] = (int)(uint32_t)start[c + 1] - a;
+    }
+    if (c == 0) *top = n;
+}
+
+// run_zone_pass (src/zone_pass.cpp:1096-1163) on the current state, in place
+int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
+    if (!c->cidStdValid) {
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
+        c->cidStdValid = true;
+    }
+    int rc = ensure_std_index(c);
+    if (rc) return rc;
+    if (!c->slotsLive) {
+        // every zone appends at most the particles of its cells; overlapping layouts revisit
+        // some cells, so twice the particles (plus slack) bounds the live-list area
+        c->liveCap = 2LL * c->n + 1024;
+        if (c->n + c->liveCap >= (1LL << 31)) return set_err(MPCD_ERR_CAPACITY, "serial pass: too many particles");
+        CUDA_TRY(cudaMalloc(&c->slotsLive, sizeof(int) * (size_t)(c->n + c->liveCap)));
+        CUDA_TRY(cudaMalloc(&c->liveCnt, sizeof(int) * (size_t)c->Nc));
+        CUDA_TRY(cudaMalloc(&c->liveStart, sizeof(int) * (size_t)c->Nc));
+        CUDA_TRY(cudaMalloc(&c->liveTop, sizeof(int)));
+        CUDA_TRY(cudaMalloc(&c->duScratch, sizeof(double2) * (size_t)std::max(std::max(c->zMaxCells, c->ovMaxCells), 1)));
+    }
+    if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
+    if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
+    Layout& L = c->lay[mode];
+    k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
+        seedBase, L.nZones, c->seeds, nullptr, kSeedBase); ++c->launches;
+    if (c->n > 0)
+        CUDA_TRY(cudaMemcpyAsync(c->slotsLive, c->idxStd.slots, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
+    k_live_init<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->liveCnt, c->liveStart, c->liveTop,
+                                                               c->n); ++c->launches;
+    ZoneArgs A{};
+    A.P = c->P;
+    A.rects = L.rects;
+    A.owner = L.owner;
+    A.start = c->idxStd.start;
+    A.slots = c->slotsLive;
+    A.vin = c->vb[c->xv];
+    A.xout = c->xb[c->xv];
+    A.vout = c->vb[c->xv];
+    A.cid = c->cidStd;
+    A.seeds = c->seeds;
+    A.nZones = L.nZones;
+    A.maxCells = c->zMaxCells;
+    A.winCap = c->zWinCap;
+    A.arenaCap = c->zArenaCap;
+    A.overflow = c->overflow;
+    A.nOverflow = c->nOverflow;
+    A.zoneMoved = c->zoneMoved;
+    A.zoneCorr = c->zoneCorr;
+    A.order = nullptr;
+    A.st = c->st;
+    A.serial = 1;
+    A.slotsW = c->slotsLive;
+    A.liveCnt = c->liveCnt;
+    A.liveStart = c->liveStart;
+    A.liveTop = c->liveTop;
+    A.liveEnd = (int)(c->n + c->liveCap);
+    A.pid = c->pidb[c->pp];
+    A.duScratch = c->duScratch;
+    ZoneArgs B = A;
+    B.maxCells = c->ovMaxCells;
+    B.winCap = c->ovWinCap;
+    B.arenaCap = c->ovArenaCap;
+    k_zone_serial<<<1, 32, c->zSmem, c->stream>>>(A, B, c->ovMem); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
+    CUDA_TRY(cudaGetLastError());
+    c->idxStdValid = false;  // positions and velocities changed in place
+    c->cidStdValid = false;
+    c->srdCellsValid = false;
+    return MPCD_OK;
+}
+
 // closure on the current (red) state; permute: write particles in (cell, id) order into the
 // other buffers (next step's layout); vrep: repaired velocities wanted
 int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* pf = nullptr) {
@@ -729,6 +818,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
+                    c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -877,7 +967,8 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
             c->zSmem = ZoneMem::bytes(0, 0, 0);
         }
         if (c->zSmem > 48 * 1024 &&
-            cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess)
+            (cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
+             cudaFuncSetAttribute(k_zone_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess))
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
         c->ovWinCap = (maxTX + 4) * (maxTY + 4);
@@ -1140,6 +1231,35 @@ static void closure_metrics_from(mpcd_ctx* c, const double* r, mpcd_closure_metr
     m->momentumDeltaX = r[9] - r[7];
     m->momentumDeltaY = r[10] - r[8];
     m->nMaskedInterzoneCells = c->nMasked;
+}
+
+int mpcd_zone_pass_serial(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
+    if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass is restricted to no surface / no wetting / no reorientation");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (mode < 0 || mode > 2) mode = MPCD_LAYOUT_BASE;
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    CUDA_TRY(cudaEventRecord(a, c->stream));
+    int rc = run_zone_pass_serial(c, mode, seed_base);
+    CUDA_TRY(cudaEventRecord(b, c->stream));
+    if (rc == MPCD_OK) rc = check_device(c);
+    float ms = 0.f;
+    if (rc == MPCD_OK) cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (metrics) {
+        rc = pass_metrics_to_host(c, mode, metrics);
+        if (rc) return rc;
+        metrics->nThreadsUsed = 1;
+        metrics->timeKernel = ms * 1e-3;
+    }
+    return MPCD_OK;
 }
 
 int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail) {

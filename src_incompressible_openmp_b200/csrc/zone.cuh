@@ -59,6 +59,18 @@ struct ZoneArgs {
     double2* zoneCorr;        // (stats[4], stats[5]) per zone
     const int* order;         // launch order of the zones (heaviest first); nullptr = by id
     DevStatus* st;
+    // run_zone_pass (serial, in place): zones one after another on the live state. slots[]
+    // then holds the pass-input lists followed by an area where each zone appends the new
+    // lists (ascending particle id) of the cells it changed; liveStart/liveCnt point to the
+    // current list of every cell.
+    int serial;
+    int* slotsW;              // slots[], writable (the live-list area)
+    int* liveCnt;
+    int* liveStart;
+    int* liveTop;             // next free entry of the live-list area
+    int liveEnd;
+    const int* pid;           // particle id per slot
+    double2* duScratch;       // momentum correction per cell of the running zone
 };
 
 // Working set of one zone; carved from shared memory (fast path) or global memory.
@@ -960,8 +972,78 @@ struct ZoneState {
     }
 };
 
+// global cell of window position w (zone rectangle plus a 2-cell ring, wrapped)
+__device__ __forceinline__ int iy_ix_cell(const ZoneState& S, int w, const DevParams& p) {
+    int ix = S.xs - 2 + w / S.WY, iy = S.ys - 2 + w % S.WY;
+    if (p.perx) ix = wrap_index(ix, p.Nx);
+    if (p.pery) iy = wrap_index(iy, p.Ny);
+    return iy + p.Ny * ix;
+}
+
+// End of a zone of the serial pass: apply the deferred momentum corrections, then publish
+// the new list (ascending particle id) and count of every cell the zone changed.
+__device__ __forceinline__ void serial_finish(ZoneState& S, const ZoneArgs& A, const DevParams& p) {
+    ZoneMem& M = S.M;
+    const int lane = S.lane;
+    for (int l = lane; l < S.nl; l += kWarp) {
+        const double2 du = A.duScratch[l];
+        if (du.x != 0.0 || du.y != 0.0) {
+            const int n = M.len[l];
+            for (int j = 0; j < n; ++j) {
+                const uint32_t e = S.elem(l, j);
+                const int sl = A.slots[M.gstart[(int)(e >> kEntryShift)] + (int)(e & ((1u << kEntryShift) - 1))];
+                const double2 w = A.vin[sl];
+                A.vout[sl] = make_double2(__dadd_rn(w.x, du.x), __dadd_rn(w.y, du.y));
+            }
+        }
+    }
+    __syncwarp();
+    int top = *A.liveTop;
+    for (int b = 0; b < S.nl; b += kWarp) {
+        const int l = b + lane;
+        const bool ch = l < S.nl && (M.cflags[l] & kCChanged);
+        const int n = ch ? M.len[l] : 0;
+        int off = n;  // inclusive scan of the list lengths
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, off, kWarp - 1);
+        off -= n;
+        if (top + total > A.liveEnd) {
+            if (lane == 0) raise_error(A.st, kErrZoneCapacity, S.zone);
+            return;
+        }
+        if (ch) {
+            const int dst = top + off;
+            for (int j = 0; j < n; ++j) {
+                const uint32_t e = S.elem(l, j);
+                A.slotsW[dst + j] = A.slots[M.gstart[(int)(e >> kEntryShift)] + (int)(e & ((1u << kEntryShift) - 1))];
+            }
+            for (int i = dst + 1; i < dst + n; ++i) {  // insertion sort by particle id
+                const int v = A.slotsW[i];
+                const int pv = A.pid[v];
+                int j = i;
+                while (j > dst && A.pid[A.slotsW[j - 1]] > pv) {
+                    A.slotsW[j] = A.slotsW[j - 1];
+                    --j;
+                }
+                A.slotsW[j] = v;
+            }
+            const int gc = S.gy_of(l) + p.Ny * S.gx_of(l);
+            A.liveStart[gc] = dst;
+            A.liveCnt[gc] = n;
+        }
+        top += total;
+    }
+    __syncwarp();
+    if (lane == 0) *A.liveTop = top;
+    __syncwarp();
+}
+
 // ------------------------------------------------------------------ the zone body
 // Returns false if the zone must be re-run on the overflow path.
+template <bool kSerial>
 __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap) {
     ZoneState S;
     S.A = &A;
@@ -1003,7 +1085,11 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int w = w0 + lane + k * kWarp;
-            if (w < W) M.win[w] = ok[k] ? (int)((uint32_t)b[k] - (uint32_t)a[k]) : -1;
+            if (w < W) {
+                int cv = ok[k] ? (int)((uint32_t)b[k] - (uint32_t)a[k]) : -1;
+                if (kSerial && ok[k]) cv = A.liveCnt[iy_ix_cell(S, w, p)];
+                M.win[w] = cv;
+            }
         }
     }
     // zone cells: segment starts and ownership
@@ -1021,8 +1107,8 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         for (int k = 0; k < 4; ++k) {
             const int l = l0 + lane + k * kWarp;
             if (l < S.nl) {
-                M.gstart[l] = (int)(uint32_t)st[k];
-                M.cflags[l] = (own[k] == z + 1) ? kCOwned : 0;
+                M.gstart[l] = kSerial ? A.liveStart[S.gy_of(l) + p.Ny * S.gx_of(l)] : (int)(uint32_t)st[k];
+                M.cflags[l] = (kSerial || own[k] == z + 1) ? kCOwned : 0;
             }
         }
     }
@@ -1068,6 +1154,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         double d2 = 0.0;
         const uint8_t f = M.cflags[l];
         const int n = M.len[l];
+        if (kSerial) A.duScratch[l] = make_double2(0.0, 0.0);  // cells left unchanged get none
         if ((f & kCChanged) && n > 0) {
             double bx = 0.0, by = 0.0, axs = 0.0, ays = 0.0;
             const int n0 = M.cnt0[l], g0 = M.gstart[l];
@@ -1111,7 +1198,10 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
             bool doCorr = p.momCorr != 0;
             if (doCorr && (f & kCSkip)) doCorr = false;
             if (doCorr && (f & kCRecv) && !(f & kCBulkBulk)) doCorr = false;
-            if (doCorr && (ux != 0.0 || uy != 0.0)) {
+            if (kSerial) {
+                // in place: every cell's sums must read the velocities of the zone's start
+                A.duScratch[l] = (doCorr && (ux != 0.0 || uy != 0.0)) ? make_double2(ux, uy) : make_double2(0.0, 0.0);
+            } else if (doCorr && (ux != 0.0 || uy != 0.0)) {
                 for (int j = 0; j < n; ++j) {
                     const uint32_t e = S.elem(l, j);
                     const int lc = (int)(e >> kEntryShift);
@@ -1125,6 +1215,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         du2[l] = d2;
     }
     __syncwarp();
+    if (kSerial) serial_finish(S, A, p);
     // zone stats[4], stats[5] (src/zone_pass.cpp:911-922): the sum of positive dU2 in
     // ascending cell order and their maximum (zero entries change neither)
     double acc = 0.0, mx = 0.0;
@@ -1153,7 +1244,7 @@ __global__ void __launch_bounds__(32) k_zone_pass(ZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     if ((int)blockIdx.x >= A.nZones) return;
     const int z = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
-    if (!zone_body(A, z, smem, A.maxCells, A.winCap, A.arenaCap) && (threadIdx.x & 31) == 0)
+    if (!zone_body<false>(A, z, smem, A.maxCells, A.winCap, A.arenaCap) && (threadIdx.x & 31) == 0)
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
@@ -1199,9 +1290,25 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock) {
     const int nov = *A.nOverflow;
     for (int i = blockIdx.x; i < nov; i += gridDim.x)
-        if (!zone_body(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap) &&
+        if (!zone_body<false>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap) &&
             (threadIdx.x & 31) == 0)
             raise_error(A.st, kErrZoneCapacity, A.overflow[i]);
+}
+
+// run_zone_pass (src/zone_pass.cpp:1096-1163): one warp runs the zones in id order on the
+// live state; a zone that outgrows the shared-memory working set is re-run at once with the
+// global one (B's capacities), which is safe since a failed zone has published nothing.
+__global__ void __launch_bounds__(32) k_zone_serial(ZoneArgs A, ZoneArgs B, char* gmem) {
+    extern __shared__ __align__(16) char smem[];
+    for (int z = 0; z < A.nZones; ++z) {
+        bool ok = zone_body<true>(A, z, smem, A.maxCells, A.winCap, A.arenaCap);
+        if (!ok) ok = zone_body<true>(B, z, gmem, B.maxCells, B.winCap, B.arenaCap);
+        if (!ok) {
+            if ((threadIdx.x & 31) == 0) raise_error(A.st, kErrZoneCapacity, z);
+            return;
+        }
+        __syncwarp();
+    }
 }
 
 // Seeded MT19937-64 state of every zone: seed = seedBase + 104729 (iz + 1)

@@ -66,6 +66,7 @@ def lib():
         "mpcd_cell_fields": ([C.c_void_p, C.c_double, P(_abi.CellFieldsC)], C.c_int),
         "mpcd_save_ref": ([C.c_void_p], C.c_int),
         "mpcd_zone_pass": ([C.c_void_p, C.c_int32, C.c_uint64, P(_abi.PassMetricsC)], C.c_int),
+        "mpcd_zone_pass_serial": ([C.c_void_p, C.c_int32, C.c_uint64, P(_abi.PassMetricsC)], C.c_int),
         "mpcd_liquid_closure": ([C.c_void_p, P(_abi.ClosureMetricsC), P(_abi.ClosureDetailC)], C.c_int),
         "mpcd_zone_owner_map": ([C.c_void_p, C.c_int32, _ip], C.c_int),
         "mpcd_step": ([C.c_void_p, C.c_int64, C.c_int64, P(_abi.StepMetricsC)], C.c_int),
@@ -230,6 +231,13 @@ class Context:
     def zone_pass(self, mode, seed_base):
         m = _abi.PassMetricsC()
         _check(lib().mpcd_zone_pass(self.h, _abi.LAYOUT_MODES[mode] if isinstance(mode, str) else mode, seed_base, C.byref(m)))
+        return _abi.struct_to_dict(m)
+
+    def zone_pass_serial(self, mode, seed_base):
+        """mpcd_zone_pass_serial: zones one after another on the live state (in place)."""
+        m = _abi.PassMetricsC()
+        _check(lib().mpcd_zone_pass_serial(self.h, _abi.LAYOUT_MODES[mode] if isinstance(mode, str) else mode, seed_base,
+                                           C.byref(m)))
         return _abi.struct_to_dict(m)
 
     def liquid_closure(self, detail=False):

@@ -54,6 +54,8 @@ def closure_detail(n, Nc):
     return d, out
 
 
+_DPA = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
 class _Checker:
     prefix = ""
     threads_arg = False
@@ -133,6 +135,16 @@ class _Checker:
         self._chk(getattr(self.lib, self.prefix + "zone_pass")(
             C.byref(to_c(p)), np.ascontiguousarray(x), np.ascontiguousarray(v), xo, vo,
             _abi.LAYOUT_MODES[mode], seed_base, *self._t(), C.byref(m)))
+        return xo, vo, _abi.struct_to_dict(m)
+
+    def zone_pass_serial(self, p, x, v, mode, seed_base):
+        f = getattr(self.lib, self.prefix + "zone_pass_serial")
+        f.argtypes = [C.POINTER(_abi.ParamsC), _DPA, _DPA, _DPA, _DPA, C.c_int32, C.c_uint64, C.POINTER(_abi.PassMetricsC)]
+        f.restype = C.c_int
+        xo, vo = np.zeros_like(x), np.zeros_like(v)
+        m = _abi.PassMetricsC()
+        self._chk(f(C.byref(to_c(p)), np.ascontiguousarray(x), np.ascontiguousarray(v), xo, vo, _abi.LAYOUT_MODES[mode],
+                    seed_base, C.byref(m)))
         return xo, vo, _abi.struct_to_dict(m)
 
     def liquid_closure(self, p, refx, refv, redx, redv, detail=True):

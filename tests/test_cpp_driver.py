@@ -112,6 +112,9 @@ def test_driver_metrics_match_reference(runs, key):
         for k in rr:
             if k in SKIP_COLS:
                 continue
+            # below the reference's own bound on den (1e-20) num and num/den are rounding noise
+            if k in ("betaRepairOpt", "betaRepairNum") and float(rr["betaRepairDen"]) < 1e-20:
+                continue
             if k in INT_COLS:
                 assert rg[k] == rr[k], (key, rr["step"], k)
             else:

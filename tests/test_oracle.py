@@ -140,3 +140,21 @@ def test_oracle_multistep_matches_reference(oracle, reference):
         assert np.array_equal(xo, xr) and np.array_equal(vo, vr), s
         for k in ("occStd", "outBand", "meanKinetic", "meanUx", "Qx", "baseOccStd", "shiftedOutBand"):
             assert mo[k] == mr[k], (s, k)
+
+
+SERIAL_VARIANTS = ["default_40x30", "odd_tiles", "tile_not_dividing", "walls_all", "periodic_y", "lff_thresholds"]
+
+
+@pytest.mark.parametrize("name", SERIAL_VARIANTS)
+def test_oracle_serial_pass_matches_reference(oracle, reference, name):
+    """run_zone_pass (zones in sequence, in place): oracle restatement vs the reference."""
+    over, kind = {v[0]: (v[1], v[2]) for v in VARIANTS}[name]
+    p = poiseuille_params(40, 30, 10, **over)
+    x, v = uniform_state(p, 7) if kind == "uniform" else modulated_state(p, 7, mode=kind)
+    for mode, seed in (("base", 88172645463325252), ("shifted", 998244353)):
+        xo, vo, mo = oracle.zone_pass_serial(p, x, v, mode, seed)
+        xr, vr, mr = reference.zone_pass_serial(p, x, v, mode, seed)
+        assert np.array_equal(xo, xr) and np.array_equal(vo, vr), mode
+        for k in ("nZones", "nParticlesMovedDense", "nParticlesMovedSparse", "corrRmsDU", "corrMaxDU"):
+            assert mo[k] == mr[k], (mode, k)
+        x, v = xo, vo
