@@ -39,6 +39,8 @@ WORKLOADS = {
     "channel_2048x512_ppc10": dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10),
     # a smaller channel of the same physics, for profiler captures (state 47 MB)
     "channel_512x256_ppc10": dict(name="channel_512x256_ppc10", Nx=512, Ny=256, ppc=10),
+    # the precision-form domain at full size, here in the plain FP64 form (83.9 M particles)
+    "channel_4096x1024_ppc20": dict(name="channel_4096x1024_ppc20", Nx=4096, Ny=1024, ppc=20),
     # the reference's own benchmark case (50x50 cells, 25,000 particles)
     "channel_50x50_ppc10": dict(name="channel_50x50_ppc10", Nx=50, Ny=50, ppc=10),
     # batched ensemble: 256 independent channels, Nx ~ U[32,512], Ny ~ U[16,128],

@@ -7,6 +7,10 @@
 // writes <out_prefix>_metrics.csv (same columns), <out_prefix>_runout.kv (same keys) and the
 // snapshots of benchmark_dumpSteps (<out_prefix>_stepNNNN_{x,v,type,r0,cellfields}.bin).
 //
+// Resume: with the optional key benchmark_startStep = k, the input state is taken as the state
+// after step k (e.g. the step-k snapshot of an earlier run) and the run continues with steps
+// k+1 .. benchmark_nSteps, with the seeds, metrics rows and snapshot names of those steps.
+//
 // Unlike the reference driver, the state stays on the device for the whole run
 // (mpcd::b200::Session): the host only sees the metrics rows and the dumps. nthreads is
 // recorded but does not change the computation. Timing columns: timeStepTotal and the phase
@@ -34,6 +38,12 @@ std::string kv_string(const std::string& path, const char* key) {
     char buf[4096];
     if (mpcd_read_kv_string(path.c_str(), key, buf, (int)sizeof buf) != MPCD_OK)
         throw std::runtime_error(std::string("Missing benchmark key: ") + key);
+    return buf;
+}
+
+std::string kv_optional(const std::string& path, const char* key, const char* dflt) {
+    char buf[4096];
+    if (mpcd_read_kv_string(path.c_str(), key, buf, (int)sizeof buf) != MPCD_OK) return dflt;
     return buf;
 }
 
@@ -82,6 +92,8 @@ int main(int argc, char** argv) {
         const int nSteps = std::stoi(kv_string(params_path, "benchmark_nSteps"));
         const int metricsEvery = std::stoi(kv_string(params_path, "benchmark_metricsEvery"));
         const std::string dumpCsv = kv_string(params_path, "benchmark_dumpSteps");
+        const int startStep = std::stoi(kv_optional(params_path, "benchmark_startStep", "0"));
+        if (startStep < 0 || startStep > nSteps) throw std::runtime_error("benchmark_startStep out of range");
         const std::vector<int> dumpSteps = parse_steps(dumpCsv);
         auto isDump = [&](int s) { return std::binary_search(dumpSteps.begin(), dumpSteps.end(), s); };
         auto isMetrics = [&](int s) { return metricsEvery > 0 && (s % metricsEvery == 0 || s == nSteps); };
@@ -109,13 +121,13 @@ int main(int argc, char** argv) {
         mpcd::b200::Session S(params, state);
         double tLoop = 0.0, tDumps = 0.0;
         double devTotal = 0.0, devRef = 0.0, devBase = 0.0, devShift = 0.0, devClos = 0.0, devDiag = 0.0;
-        if (isDump(0)) {
+        if (startStep == 0 && isDump(0)) {
             const auto t0 = Clock::now();
             dump(out_prefix, 0, state, S.fields(rhoTarget), params.n, has_type, has_r0);
             tDumps += seconds(t0, Clock::now());
         }
         mpcd_step_metrics_c m{};
-        int step = 0;
+        int step = startStep;
         while (step < nSteps) {
             int stop = step + 1;
             while (stop < nSteps && !isMetrics(stop) && !isDump(stop)) ++stop;

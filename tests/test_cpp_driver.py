@@ -137,3 +137,26 @@ def test_driver_runout_keys(runs):
         assert G[k] == R[k], k
     for k in ("finalOccStd", "finalQx", "finalMeanKinetic"):
         assert abs(float(G[k]) - float(R[k])) <= 1e-5 * abs(float(R[k])) + 1e-12, k
+
+
+@pytest.mark.gpu
+def test_resume_from_snapshot(runs, tmp_path):
+    """benchmark_startStep: resuming from the step-3 snapshot reproduces the uninterrupted run."""
+    p, out = runs
+    import shutil
+    case = str(tmp_path / "resume")
+    os.makedirs(case)
+    src = os.path.dirname(os.path.dirname(out["ours"]))
+    with open(os.path.join(src, "case", "params.kv")) as f:
+        kv = f.read()
+    with open(os.path.join(case, "params.kv"), "w") as f:
+        f.write(kv + "benchmark_startStep=3\n")
+    for k in ("x", "v", "type", "r0"):
+        shutil.copy(f"{out['ours']}_step0003_{k}.bin", os.path.join(case, f"in_{k}.bin"))
+    prefix = os.path.join(case, "out")
+    run_driver(MPCD_BENCH, case, prefix)
+    x6, v6 = load_state(out["ours"], 6, p["n"])
+    xr, vr = load_state(prefix, 6, p["n"])
+    assert np.array_equal(xr, x6) and np.array_equal(vr, v6)
+    rows = read_csv(prefix + "_metrics.csv")
+    assert [r["step"] for r in rows] == ["4", "6"]
