@@ -143,6 +143,8 @@ struct mpcd_ctx {
     size_t ovPerBlock = 0;
     int ovBlocks = 2;
     int zMaxCells = 0, zWinCap = 0, zArenaCap = 0;
+    int collideTile = 0;       // velocities a collision block stages in shared memory
+    size_t collideSmem = 0;
     size_t zSmem = 0;
     int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0;
     double* passOut = nullptr;  // 4 doubles
@@ -554,8 +556,9 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         CUDA_TRY(cudaStreamWaitEvent(c->stream, c->wallsDone, 0));
         c->wallsPending = false;
     }
-    k_srd_collide<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc,
-                                                                 c->vb[c->xv], c->st, gs, c->signsBuf[1]); ++c->launches;
+    k_srd_collide<<<blocks_for(c->Nc, kCollideCells), kCollideThreads, c->collideSmem, c->stream>>>(
+        c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc, c->vb[c->xv], c->st, gs, c->signsBuf[1], c->collideTile);
+    ++c->launches;
     if (c->P.keepMeanFlow) {
         k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
@@ -948,6 +951,15 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     ALLOC(c->zoneOrder, (size_t)maxZones);
     ALLOC(c->nOverflow, 1);
     ALLOC(c->passOut, 8);
+    // collision tiles: room for 1.5x the mean particles per cell plus 8, per cell of a block
+    {
+        const double ppc = (double)n / (double)std::max(Nc, 1);
+        c->collideTile = std::max(256, std::min(8192, (int)(kCollideCells * (1.5 * ppc + 8.0))));
+        c->collideSmem = (size_t)c->collideTile * (sizeof(double2) + sizeof(int));
+        if (c->collideSmem > 48 * 1024 &&
+            cudaFuncSetAttribute(k_srd_collide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) != cudaSuccess)
+            return fail(set_err(MPCD_ERR_CUDA, "collision shared memory attribute"));
+    }
     // fast path: tiles of the base/shifted layouts in shared memory
     {
         const Layout& B = c->lay[0];

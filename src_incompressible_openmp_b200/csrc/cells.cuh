@@ -46,32 +46,26 @@ __global__ void __launch_bounds__(kSignThreads) k_srd_signs(uint64_t seed, int c
     }
 }
 
-// srd_collision_step (src/srd_collision.cpp:47-124) for one SRD cell per thread. start:
-// packed (segment start | rank among cells with >= 2 particles << 32).
-// seedDev (graph replay): the signs are sign or sign1 by the step's parity
-__global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
-                              const uint8_t* __restrict__ sign, int signCount, double2* __restrict__ v,
-                              DevStatus* st, const uint64_t* seedDev, const uint8_t* __restrict__ sign1) {
-    if (seedDev && seedDev[kSeedParity]) sign = sign1;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.Nc) return;
-    const uint64_t s0 = start[c];
-    const int a = (int)(uint32_t)s0, b = (int)(uint32_t)start[c + 1];
-    const int m = b - a;
-    if (m == 0) return;
+// srd_collision_step (src/srd_collision.cpp:47-124) on one SRD cell whose m velocities are
+// read by ld(j) and written by st(j, w), j in particle-id order: mean, a +-alpha rotation of
+// the relative velocities (sign from the cell's rank among cells with >= 2 particles) and the
+// thermostat rescaling. start0: packed (segment start | rank << 32). Returns false on error.
+template <typename Ld, typename St>
+__device__ __forceinline__ bool collide_cell(const DevParams& P, uint64_t start0, int m, const uint8_t* sign,
+                                             int signCount, DevStatus* st, Ld ld, St stv) {
     double sx = 0.0, sy = 0.0;
-    for (int j = a; j < b; ++j) {
-        const double2 w = v[slots[j]];
+    for (int j = 0; j < m; ++j) {
+        const double2 w = ld(j);
         sx = __dadd_rn(sx, w.x);
         sy = __dadd_rn(sy, w.y);
     }
     const double ux = __ddiv_rn(sx, (double)m), uy = __ddiv_rn(sy, (double)m);
     int rot = 0;
     if (m >= 2) {
-        const int r = (int)(s0 >> 32);
+        const int r = (int)(start0 >> 32);
         if (r >= signCount) {
             raise_error(st, kErrRngCapacity, r);
-            return;
+            return false;
         }
         rot = sign[r] ? 2 : 1;
     }
@@ -79,8 +73,8 @@ __global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, c
     double lam = 1.0;
     if (P.useThermostat) {
         double sr = 0.0;
-        for (int j = a; j < b; ++j) {
-            const double2 w = v[slots[j]];
+        for (int j = 0; j < m; ++j) {
+            const double2 w = ld(j);
             const double xr = __dsub_rn(w.x, ux), yr = __dsub_rn(w.y, uy);
             const double x2 = __dsub_rn(__dmul_rn(ct, xr), __dmul_rn(sn, yr));
             const double y2 = __dadd_rn(__dmul_rn(sn, xr), __dmul_rn(ct, yr));
@@ -88,9 +82,8 @@ __global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, c
         }
         if (m > 1 && sr > 0.0) lam = sqrt(__ddiv_rn(__dmul_rn((double)(2 * (m - 1)), P.kBT), sr));
     }
-    for (int j = a; j < b; ++j) {
-        const int s = slots[j];
-        const double2 w = v[s];
+    for (int j = 0; j < m; ++j) {
+        const double2 w = ld(j);
         const double xr = __dsub_rn(w.x, ux), yr = __dsub_rn(w.y, uy);
         double x2 = __dsub_rn(__dmul_rn(ct, xr), __dmul_rn(sn, yr));
         double y2 = __dadd_rn(__dmul_rn(sn, xr), __dmul_rn(ct, yr));
@@ -98,11 +91,58 @@ __global__ void k_srd_collide(DevParams P, const uint64_t* __restrict__ start, c
             x2 = __dmul_rn(x2, lam);
             y2 = __dmul_rn(y2, lam);
         }
-        v[s] = make_double2(__dadd_rn(ux, x2), __dadd_rn(uy, y2));
+        stv(j, make_double2(__dadd_rn(ux, x2), __dadd_rn(uy, y2)));
     }
+    return true;
 }
 
-// Output arrays of compute_cell_fields; any pointer may be null.
+// The collision over kCollideCells consecutive SRD cells per block. Their segments are
+// contiguous in slots[]: the velocities are gathered once into shared memory by the whole
+// block, each thread runs its cell there, and the block scatters them back. A block whose
+// segments exceed the tile works on global memory instead.
+constexpr int kCollideCells = 64;
+constexpr int kCollideThreads = 256;
+
+__global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, const uint64_t* __restrict__ start,
+                                                                 const int* __restrict__ slots,
+                                                                 const uint8_t* __restrict__ sign, int signCount,
+                                                                 double2* __restrict__ v, DevStatus* st,
+                                                                 const uint64_t* seedDev,
+                                                                 const uint8_t* __restrict__ sign1, int tileCap) {
+    extern __shared__ __align__(16) double2 tv[];
+    int* ts = reinterpret_cast<int*>(tv + tileCap);
+    if (seedDev && seedDev[kSeedParity]) sign = sign1;
+    const int c0 = blockIdx.x * kCollideCells;
+    const int nc = min(kCollideCells, P.Nc - c0);
+    const int A = (int)(uint32_t)start[c0], B = (int)(uint32_t)start[c0 + nc];
+    const int t = threadIdx.x;
+    if (B - A > tileCap) {
+        if (t < nc) {
+            const uint64_t s0 = start[c0 + t];
+            const int a = (int)(uint32_t)s0, m = (int)(uint32_t)start[c0 + t + 1] - a;
+            if (m > 0)
+                collide_cell(P, s0, m, sign, signCount, st, [&](int j) { return v[slots[a + j]]; },
+                             [&](int j, double2 w) { v[slots[a + j]] = w; });
+        }
+        return;
+    }
+    for (int i = t; i < B - A; i += blockDim.x) {
+        const int sl = slots[A + i];
+        ts[i] = sl;
+        tv[i] = v[sl];
+    }
+    __syncthreads();
+    if (t < nc) {
+        const uint64_t s0 = start[c0 + t];
+        const int a = (int)(uint32_t)s0 - A, m = (int)(uint32_t)start[c0 + t + 1] - A - a;
+        if (m > 0)
+            collide_cell(P, s0, m, sign, signCount, st, [&](int j) { return tv[a + j]; },
+                         [&](int j, double2 w) { tv[a + j] = w; });
+    }
+    __syncthreads();
+    for (int i = t; i < B - A; i += blockDim.x) v[ts[i]] = tv[i];
+}
+
 struct FieldsOut {
     int* N;
     double *Ux, *Uy, *Px, *Py, *T, *rho, *Pkin, *Pvir, *P, *rhoTarget;
