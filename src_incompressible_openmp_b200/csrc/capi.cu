@@ -142,11 +142,11 @@ struct mpcd_ctx {
     char* ovMem = nullptr;
     size_t ovPerBlock = 0;
     int ovBlocks = 2;
-    int zMaxCells = 0, zWinCap = 0, zArenaCap = 0;
+    int zMaxCells = 0, zWinCap = 0, zArenaCap = 0, zNsmCap = 0;
     int collideTile = 0;       // velocities a collision block stages in shared memory
     size_t collideSmem = 0;
     size_t zSmem = 0;
-    int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0;
+    int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0, ovNsmCap = 0;
     double* passOut = nullptr;  // 4 doubles
     // closure
     int* mask = nullptr;
@@ -640,6 +640,7 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     A.maxCells = c->zMaxCells;
     A.winCap = c->zWinCap;
     A.arenaCap = c->zArenaCap;
+    A.nsmCap = c->zNsmCap;
     A.overflow = c->overflow;
     A.nOverflow = c->nOverflow;
     A.zoneMoved = c->zoneMoved;
@@ -657,6 +658,7 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
+    B.nsmCap = c->ovNsmCap;
     k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock); ++c->launches;
     k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
     CUDA_TRY(cudaGetLastError());
@@ -721,6 +723,7 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     A.maxCells = c->zMaxCells;
     A.winCap = c->zWinCap;
     A.arenaCap = c->zArenaCap;
+    A.nsmCap = c->zNsmCap;
     A.overflow = c->overflow;
     A.nOverflow = c->nOverflow;
     A.zoneMoved = c->zoneMoved;
@@ -739,6 +742,7 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
+    B.nsmCap = c->ovNsmCap;
     k_zone_serial<<<1, 32, c->zSmem, c->stream>>>(A, B, c->ovMem); ++c->launches;
     k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
     CUDA_TRY(cudaGetLastError());
@@ -968,15 +972,17 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
         const int tx = std::max(B.maxTX, S.maxTX), ty = std::max(B.maxTY, S.maxTY);
         c->zMaxCells = std::max(1, area);
         c->zWinCap = (tx + 4) * (ty + 4);
+        c->zNsmCap = (tx + 2) * (ty + 2);
         const double g = std::max(1.0, params->gamma);
         // arena for the lists a zone materialises (receivers, donors): ~0.8 of the zone's
         // particles covers typical passes; a zone that runs out is re-run on the overflow path
         c->zArenaCap = ((int)std::ceil(0.8 * g * area) + 128 + 31) / 32 * 32;
-        c->zSmem = ZoneMem::bytes(c->zMaxCells, c->zWinCap, c->zArenaCap);
-        if (c->zSmem > 200 * 1024) {
-            // too large for the shared-memory path: every zone takes the overflow path
+        c->zSmem = ZoneMem<uint16_t>::bytes(c->zMaxCells, c->zWinCap, c->zArenaCap, c->zNsmCap);
+        if (c->zSmem > 200 * 1024 || c->zArenaCap > 65535 || c->zMaxCells > 65535) {
+            // too large for the shared-memory path (or its 16-bit offsets): every zone takes
+            // the overflow path
             c->zMaxCells = 0;
-            c->zSmem = ZoneMem::bytes(0, 0, 0);
+            c->zSmem = ZoneMem<uint16_t>::bytes(0, 0, 0, 0);
         }
         if (c->zSmem > 48 * 1024 &&
             (cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
@@ -984,10 +990,11 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
         c->ovWinCap = (maxTX + 4) * (maxTY + 4);
+        c->ovNsmCap = (maxTX + 2) * (maxTY + 2);
         // every materialised list fits in (particles of the zone + 4 per cell) entries after
         // compaction; bound the zone's particles by all particles
         c->ovArenaCap = (int)std::min<int64_t>((int64_t)n + 4LL * maxArea + 4096, (1LL << 31) - 1);
-        c->ovPerBlock = (ZoneMem::bytes(c->ovMaxCells, c->ovWinCap, c->ovArenaCap) + 255) / 256 * 256;
+        c->ovPerBlock = (ZoneMem<int>::bytes(c->ovMaxCells, c->ovWinCap, c->ovArenaCap, c->ovNsmCap) + 255) / 256 * 256;
         ALLOC(c->ovMem, c->ovPerBlock * (size_t)c->ovBlocks);
     }
     // closure

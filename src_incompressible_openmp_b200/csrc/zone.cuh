@@ -31,6 +31,8 @@
 // lane 0 are followed by __syncwarp() before any lane reads them.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace mpcd_dev {
@@ -52,7 +54,7 @@ struct ZoneArgs {
     int* cid;                 // standard-grid cell per slot; moved owned particles updated
     const uint64_t* seeds;    // seeded MT19937-64 state per zone (312 words each)
     int nZones;
-    int maxCells, winCap, arenaCap;  // capacities of the per-zone working set
+    int maxCells, winCap, arenaCap, nsmCap;  // capacities of the per-zone working set
     int* overflow;            // zones left to the overflow kernel
     int* nOverflow;
     int2* zoneMoved;          // (dense, sparse) per zone
@@ -73,42 +75,46 @@ struct ZoneArgs {
     double2* duScratch;       // momentum correction per cell of the running zone
 };
 
-// Working set of one zone; carved from shared memory (fast path) or global memory.
+// Working set of one zone; carved from shared memory (fast path, I = uint16_t: 16-bit
+// per-cell counts and arena offsets) or global memory (overflow path, I = int).
+template <typename I>
 struct ZoneMem {
+    using W = typename std::conditional<sizeof(I) == 2, int16_t, int>::type;
     uint64_t* mt;      // 312: MT19937-64 state
     uint64_t* carry;   // 64: untwisted words of the previous block still to be drawn
     double* nsm;       // (TX+2)(TY+2): smoothed occupancy; reused for dU2 at the end
-    int* win;          // (TX+4)(TY+4): pass-input counts around the zone (-1 = outside)
+    W* win;            // (TX+4)(TY+4): pass-input counts around the zone (-1 = outside)
     int* gstart;       // cell: start of its input segment in the cell index
-    int* cnt0;         // cell: input count
-    int* head;         // cell: list head (implicit: offset into the input segment)
-    int* len;          // cell: list length = live count
-    int* abase;        // cell: arena start of a materialised list
-    int* cap;          // cell: arena capacity of a materialised list
+    I* cnt0;           // cell: input count
+    I* head;           // cell: list head (implicit: offset into the input segment)
+    I* len;            // cell: list length = live count
+    I* abase;          // cell: arena start of a materialised list
+    I* cap;            // cell: arena capacity of a materialised list
     uint8_t* cflags;   // cell
     uint16_t* list;    // cell: dense / low cell order
     uint16_t* order;   // cell: arena order of materialised lists (compaction)
     uint32_t* arena;   // arenaCap
-    int* small;        // 128 ints: candidates, targets, receivers, donors
-    double* smallD;    // 16 doubles: donor scores
+    int* small;        // 64 ints: ranked targets, donors
+    double* smallD;    // 8 doubles: donor normals
 
-    __host__ __device__ static size_t bytes(int maxCells, int winCap, int arenaCap) {
+    __host__ __device__ static size_t bytes(int maxCells, int winCap, int arenaCap, int nsmCap) {
         size_t b = 0;
         auto add = [&](size_t n, size_t a) { b = (b + a - 1) / a * a + n; };
         add((size_t)kMtN * 8, 8);
         add(64 * 8, 8);
-        add((size_t)winCap * 8, 8);
-        add((size_t)winCap * 4, 4);
-        for (int k = 0; k < 6; ++k) add((size_t)maxCells * 4, 4);
+        add((size_t)nsmCap * 8, 8);
+        add((size_t)winCap * sizeof(W), sizeof(W));
+        add((size_t)maxCells * 4, 4);
+        for (int k = 0; k < 5; ++k) add((size_t)maxCells * sizeof(I), sizeof(I));
         add((size_t)maxCells, 1);
         add((size_t)maxCells * 2, 2);
         add((size_t)maxCells * 2, 2);
         add((size_t)arenaCap * 4, 4);
-        add(128 * 4, 4);
-        add(16 * 8, 8);
+        add(64 * 4, 4);
+        add(8 * 8, 8);
         return (b + 15) / 16 * 16;
     }
-    __device__ void carve(char* base, int maxCells, int winCap, int arenaCap) {
+    __device__ void carve(char* base, int maxCells, int winCap, int arenaCap, int nsmCap) {
         size_t b = 0;
         auto take = [&](size_t n, size_t a) {
             b = (b + a - 1) / a * a;
@@ -118,20 +124,20 @@ struct ZoneMem {
         };
         mt = (uint64_t*)take((size_t)kMtN * 8, 8);
         carry = (uint64_t*)take(64 * 8, 8);
-        nsm = (double*)take((size_t)winCap * 8, 8);
-        win = (int*)take((size_t)winCap * 4, 4);
+        nsm = (double*)take((size_t)nsmCap * 8, 8);
+        win = (W*)take((size_t)winCap * sizeof(W), sizeof(W));
         gstart = (int*)take((size_t)maxCells * 4, 4);
-        cnt0 = (int*)take((size_t)maxCells * 4, 4);
-        head = (int*)take((size_t)maxCells * 4, 4);
-        len = (int*)take((size_t)maxCells * 4, 4);
-        abase = (int*)take((size_t)maxCells * 4, 4);
-        cap = (int*)take((size_t)maxCells * 4, 4);
+        cnt0 = (I*)take((size_t)maxCells * sizeof(I), sizeof(I));
+        head = (I*)take((size_t)maxCells * sizeof(I), sizeof(I));
+        len = (I*)take((size_t)maxCells * sizeof(I), sizeof(I));
+        abase = (I*)take((size_t)maxCells * sizeof(I), sizeof(I));
+        cap = (I*)take((size_t)maxCells * sizeof(I), sizeof(I));
         cflags = (uint8_t*)take((size_t)maxCells, 1);
         list = (uint16_t*)take((size_t)maxCells * 2, 2);
         order = (uint16_t*)take((size_t)maxCells * 2, 2);
         arena = (uint32_t*)take((size_t)arenaCap * 4, 4);
-        small = (int*)take(128 * 4, 4);
-        smallD = (double*)take(16 * 8, 8);
+        small = (int*)take(64 * 4, 4);
+        smallD = (double*)take(8 * 8, 8);
     }
 };
 
@@ -374,7 +380,8 @@ struct ZoneNormal {
 
 // Repacks the materialised lists of a zone at the bottom of its arena, in arena order;
 // returns the new arena top. Out of line: it runs only when the arena is full.
-__device__ __noinline__ int zone_compact(uint8_t* cflags, int* abase, int* head, const int* len, int* cap,
+template <typename I>
+__device__ __noinline__ int zone_compact(uint8_t* cflags, I* abase, I* head, const I* len, I* cap,
                                          uint16_t* order, uint32_t* arena, int nl, int lane) {
     for (int l = lane; l < nl; l += kWarp) {
         int r = 0;
@@ -415,7 +422,8 @@ __device__ __noinline__ int zone_compact(uint8_t* cflags, int* abase, int* head,
 // smoothed occupancy on the zone plus a one-cell ring (src/zone_pass.cpp:296-319):
 // 3x3 binomial weights, renormalised over the in-domain neighbours. Out of line (called at
 // most twice per pass).
-__device__ __noinline__ void zone_compute_nsm(double* nsm, const int* win, const int* cnt, int xs, int ys, int TX,
+template <typename W, typename I>
+__device__ __noinline__ void zone_compute_nsm(double* nsm, const W* win, const I* cnt, int xs, int ys, int TX,
                                               int TY, int Nx, int Ny, int perx, int pery, int lane) {
     const int GX = TX + 2, GY = TY + 2, WY = TY + 4;
     for (int g = lane; g < GX * GY; g += kWarp) {
@@ -484,8 +492,9 @@ __device__ __forceinline__ void zone_normals(double* out, int cnt, ZoneMt& r, in
 }
 
 // Scalar (warp-uniform) state of one zone.
+template <typename I>
 struct ZoneState {
-    ZoneMem M;
+    ZoneMem<I> M;
     ZoneMt rng;
     const ZoneArgs* A;
     int lane, zone;
@@ -832,7 +841,7 @@ struct ZoneState {
 
     // one dense cell (src/zone_pass.cpp:734-753 calling :591-634)
     __device__ void dense_cell(int l) {
-        int* T = M.small + 32;
+        int* T = M.small;
         int recvReg = -1;
         const int ncc = M.len[l];
         if (ncc <= 0) return;
@@ -887,7 +896,7 @@ struct ZoneState {
     // one sparse cell (src/zone_pass.cpp:804-854)
     __device__ void sparse_cell(int l) {
         const DevParams& p = P();
-        int* don = M.small + 96;
+        int* don = M.small + 32;
         const int ncc = M.len[l];
         if (ncc <= 0) return;
         if (M.len[l] == 0) return;
@@ -973,7 +982,8 @@ struct ZoneState {
 };
 
 // global cell of window position w (zone rectangle plus a 2-cell ring, wrapped)
-__device__ __forceinline__ int iy_ix_cell(const ZoneState& S, int w, const DevParams& p) {
+template <typename I>
+__device__ __forceinline__ int iy_ix_cell(const ZoneState<I>& S, int w, const DevParams& p) {
     int ix = S.xs - 2 + w / S.WY, iy = S.ys - 2 + w % S.WY;
     if (p.perx) ix = wrap_index(ix, p.Nx);
     if (p.pery) iy = wrap_index(iy, p.Ny);
@@ -982,8 +992,9 @@ __device__ __forceinline__ int iy_ix_cell(const ZoneState& S, int w, const DevPa
 
 // End of a zone of the serial pass: apply the deferred momentum corrections, then publish
 // the new list (ascending particle id) and count of every cell the zone changed.
-__device__ __forceinline__ void serial_finish(ZoneState& S, const ZoneArgs& A, const DevParams& p) {
-    ZoneMem& M = S.M;
+template <typename I>
+__device__ __forceinline__ void serial_finish(ZoneState<I>& S, const ZoneArgs& A, const DevParams& p) {
+    ZoneMem<I>& M = S.M;
     const int lane = S.lane;
     for (int l = lane; l < S.nl; l += kWarp) {
         const double2 du = A.duScratch[l];
@@ -1043,9 +1054,9 @@ __device__ __forceinline__ void serial_finish(ZoneState& S, const ZoneArgs& A, c
 
 // ------------------------------------------------------------------ the zone body
 // Returns false if the zone must be re-run on the overflow path.
-template <bool kSerial>
-__device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap) {
-    ZoneState S;
+template <bool kSerial, typename I>
+__device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap, int nsmCap) {
+    ZoneState<I> S;
     S.A = &A;
     S.lane = threadIdx.x & 31;
     S.zone = z;
@@ -1062,11 +1073,13 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     S.dupNb5 = (p.perx && p.Nx < 5) || (p.pery && p.Ny < 5);
     S.dupNb3 = (p.perx && p.Nx < 3) || (p.pery && p.Ny < 3);
     const int W = (S.TX + 4) * S.WY;
-    if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > winCap || S.nl >= (1 << (32 - kEntryShift))) return false;
-    S.M.carve(mem, maxCells, winCap, arenaCap);
+    if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > nsmCap || S.nl >= (1 << (32 - kEntryShift))) return false;
+    S.M.carve(mem, maxCells, winCap, arenaCap, nsmCap);
+    constexpr bool kNarrow = sizeof(I) == 2;  // 16-bit counts: window counts <= 32767, zone total <= 65535
+    bool wide = false;
     S.arenaCap = arenaCap;
     S.arenaTop = 0;
-    ZoneMem& M = S.M;
+    ZoneMem<I>& M = S.M;
     // pass-input counts around the zone
     for (int w0 = 0; w0 < W; w0 += 4 * kWarp) {
         uint64_t a[4], b[4];
@@ -1088,6 +1101,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
             if (w < W) {
                 int cv = ok[k] ? (int)((uint32_t)b[k] - (uint32_t)a[k]) : -1;
                 if (kSerial && ok[k]) cv = A.liveCnt[iy_ix_cell(S, w, p)];
+                if (kNarrow && cv > 32767) wide = true;
                 M.win[w] = cv;
             }
         }
@@ -1113,13 +1127,19 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         }
     }
     __syncwarp();
+    int tot = 0;
     for (int l = lane; l < S.nl; l += kWarp) {
         const int c = M.win[(l / S.TY + 2) * S.WY + (l % S.TY + 2)];
+        tot += c;
         M.cnt0[l] = c;
         M.len[l] = c;
         M.head[l] = 0;
         M.abase[l] = 0;
         M.cap[l] = 0;
+    }
+    if (kNarrow) {  // counts too large for the 16-bit working set: the overflow path takes the zone
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        if (__any_sync(0xffffffffu, wide) || tot > 65535) return false;
     }
     __syncwarp();
     S.rng.init(M.mt, M.carry, A.seeds + (size_t)z * kMtN, lane);
@@ -1240,11 +1260,11 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     return true;
 }
 
-__global__ void __launch_bounds__(32) k_zone_pass(ZoneArgs A) {
+__global__ void __launch_bounds__(32, 20) k_zone_pass(ZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     if ((int)blockIdx.x >= A.nZones) return;
     const int z = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
-    if (!zone_body<false>(A, z, smem, A.maxCells, A.winCap, A.arenaCap) && (threadIdx.x & 31) == 0)
+    if (!zone_body<false, uint16_t>(A, z, smem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap) && (threadIdx.x & 31) == 0)
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
@@ -1290,7 +1310,8 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock) {
     const int nov = *A.nOverflow;
     for (int i = blockIdx.x; i < nov; i += gridDim.x)
-        if (!zone_body<false>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap) &&
+        if (!zone_body<false, int>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap,
+                                   A.nsmCap) &&
             (threadIdx.x & 31) == 0)
             raise_error(A.st, kErrZoneCapacity, A.overflow[i]);
 }
@@ -1301,8 +1322,8 @@ __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, si
 __global__ void __launch_bounds__(32) k_zone_serial(ZoneArgs A, ZoneArgs B, char* gmem) {
     extern __shared__ __align__(16) char smem[];
     for (int z = 0; z < A.nZones; ++z) {
-        bool ok = zone_body<true>(A, z, smem, A.maxCells, A.winCap, A.arenaCap);
-        if (!ok) ok = zone_body<true>(B, z, gmem, B.maxCells, B.winCap, B.arenaCap);
+        bool ok = zone_body<true, uint16_t>(A, z, smem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap);
+        if (!ok) ok = zone_body<true, int>(B, z, gmem, B.maxCells, B.winCap, B.arenaCap, B.nsmCap);
         if (!ok) {
             if ((threadIdx.x & 31) == 0) raise_error(A.st, kErrZoneCapacity, z);
             return;
