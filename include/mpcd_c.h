@@ -250,6 +250,52 @@ mpcd_ctx* mpcd_batch_member(mpcd_batch* batch, int index);
  * of the whole batch */
 int mpcd_batch_step(mpcd_batch* batch, int64_t step0, int64_t nsteps, double* device_seconds);
 
+/* ---------------------------------------------------------------- learned closure */
+/* A stencil MLP standing in for the liquid closure's per-cell velocity correction
+ * (reference src/liquid_closure.cpp:380-389 repair kick and :424-436 EOS kick, which the
+ * reference exposes as LiquidClosureResult::duRepairX/Y, duEOSX/Y and
+ * metrics.betaRepairApplied, include/liquid_closure.h:29-44). It has no counterpart in the
+ * reference.
+ *   features: 75 floats per cell, a 5x5 stencil (dy outer, dx inner, -2..2) of
+ *             N/gamma - 1 [0..24], Ux [25..49], Uy [50..74] of the red (post-redistribution)
+ *             cell fields; wrapped on periodic axes; outside a wall N term -1, U terms 0
+ *   target:   2 floats, beta_applied * duRepair + duEOS of the plain closure
+ *   network:  75 -> 64 -> 64 -> 2, GELU, BF16 weights with FP32 accumulation,
+ *             kick = output * scale
+ *   params:   MPCD_LEARNED_PARAMS floats: W1[64][75], b1[64], W2[64][64], b2[64], W3[2][64],
+ *             b3[2], scale */
+#define MPCD_LEARNED_FEATURES 75
+#define MPCD_LEARNED_OUTPUTS 2
+#define MPCD_LEARNED_PARAMS 9155
+int mpcd_learned_param_count(void);
+/* Glorot-uniform weights from seed, zero biases, scale 0 (the trainer sets it). */
+int mpcd_learned_init(uint64_t seed, float* params);
+/* Runs plain steps step0+1 .. step0+nsteps like mpcd_step and collects (features, target) of
+ * every stride-th cell after each step's closure (offset step % stride), at most capacity
+ * rows; *count = rows written. */
+int mpcd_learned_samples(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, int32_t stride, float* features,
+                         float* targets, int64_t capacity, int64_t* count);
+/* Adam training on device `device` (mini-batches of `batch` rows, shuffled per epoch from
+ * seed) of the mean squared error of output - target / scale; params in/out. If params' scale
+ * is not positive it is first set to the RMS of the targets. epoch_loss (nullable): the mean
+ * loss of each epoch. */
+int mpcd_learned_train(const float* features, const float* targets, int64_t rows, float* params, int32_t epochs,
+                       int32_t batch, float lr, uint64_t seed, int device, float* epoch_loss);
+/* Gradient (MPCD_LEARNED_PARAMS floats; the scale's entry 0) and loss of that error over all
+ * rows, as one batch. */
+int mpcd_learned_grad(const float* features, const float* targets, int64_t rows, const float* params, int device,
+                      float* grad, float* loss);
+/* The network's kick (output * scale) for feature rows: out has 2 floats per row. */
+int mpcd_learned_predict(const float* features, int64_t rows, const float* params, int device, float* out);
+/* Puts the network in the step's closure (params NULL: back to the plain closure). Each step
+ * then runs the learned kick, or the plain closure when the previous step's occupancy spread
+ * (occStd of the red state, as in the metrics row) exceeded occ_limit (occ_limit <= 0: never).
+ * The decision is made on the device, so graph replay keeps it. */
+int mpcd_learned_set(mpcd_ctx* ctx, const float* params, double occ_limit);
+/* Steps run with each closure since mpcd_learned_set, and the mode of the next step
+ * (1 learned, 0 plain). */
+int mpcd_learned_stats(mpcd_ctx* ctx, int64_t* plain_steps, int64_t* learned_steps, int32_t* next_mode);
+
 /* Page-locked host memory (for staging states); NULL on failure. */
 void* mpcd_host_alloc(size_t bytes);
 void mpcd_host_free(void* p);

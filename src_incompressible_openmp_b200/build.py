@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmpcd_b200.so")
 
 SOURCES = ["capi.cu", "io.cpp"]
-DEPS = ["common.cuh", "ddmath.cuh", "logtab.inc", "sort.cuh", "bc.cuh", "cells.cuh", "zone.cuh", "closure.cuh"]
+DEPS = sorted(f for f in os.listdir(CSRC)
+              if f.endswith((".cuh", ".inc", ".h")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

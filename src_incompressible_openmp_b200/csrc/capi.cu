@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -20,6 +21,7 @@
 #include "cells.cuh"
 #include "closure.cuh"
 #include "common.cuh"
+#include "learned.cuh"
 #include "sort.cuh"
 #include "zone.cuh"
 
@@ -136,6 +138,21 @@ struct mpcd_ctx {
     int* liveTop = nullptr;
     double2* duScratch = nullptr;
     int64_t liveCap = 0;
+    // learned closure (mpcd_learned_set): parameters, the per-step mode flag (1 learned,
+    // 0 plain) decided on the device from the previous step's occupancy spread, step counts
+    // per mode, the spread sums, the predicted kick, and the red fields the stencil reads
+    bool learnedOn = false;
+    bool sampling = false;     // red fields wanted (dataset collection)
+    double learnedLimit = 0.0;
+    float* lparams = nullptr;
+    int* lmode = nullptr;
+    long long* lcount = nullptr;
+    double* lsums = nullptr;
+    double* duLX = nullptr;
+    double* duLY = nullptr;
+    int* redN = nullptr;
+    double* redUx = nullptr;
+    double* redUy = nullptr;
     int* zoneCost = nullptr;   // per zone: cost bucket
     int* zoneHist = nullptr;   // kCostBuckets
     int* zoneOrder = nullptr;  // launch order, heaviest first
@@ -589,18 +606,21 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
     return MPCD_OK;
 }
 
-// reference fields of the current state + pdrive + EOS kick (depend on the reference only)
-int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr) {
+// reference fields of the current state + pdrive + EOS kick (depend on the reference only);
+// inStep: called from the step, where a learned step (device mode flag) skips them
+int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr, bool inStep = false) {
     int rc = ensure_std_index(c, pf);
     if (rc) return rc;
     FieldsOut o{};
     o.N = c->refNi; o.Ux = c->refUx; o.Uy = c->refUy; o.Px = c->refPx; o.Py = c->refPy; o.T = c->refT;
     o.rho = c->refRho; o.Pkin = c->refPkin; o.Pvir = c->refPvir; o.P = c->refP;
+    const int* skip = (inStep && c->learnedOn) ? c->lmode : nullptr;  // learned steps need no reference
     k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
-                                                                 c->P.rhoTarget, o); ++c->launches;
-    k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw); ++c->launches;
-    k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive); ++c->launches;
-    k_eos<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdrive, c->eosX, c->eosY); ++c->launches;
+                                                                 c->P.rhoTarget, o, skip); ++c->launches;
+    k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw, skip); ++c->launches;
+    k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive, skip);
+    ++c->launches;
+    k_eos<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdrive, c->eosX, c->eosY, skip); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 6);
     c->refValid = true;
@@ -753,13 +773,22 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
 }
 
 // closure on the current (red) state; permute: write particles in (cell, id) order into the
-// other buffers (next step's layout); vrep: repaired velocities wanted
+// other buffers (next step's layout), as the step does; vrep: repaired velocities wanted.
+// In the step, with a network set (mpcd_learned_set), the device mode flag picks the learned
+// or the plain kick per step.
 int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* pf = nullptr) {
     if (!c->refValid) return set_err(MPCD_ERR_STATE, "liquid closure needs a saved reference state (mpcd_save_ref)");
     int rc = ensure_std_index(c, pf);
     if (rc) return rc;
+    const bool learned = permute && c->learnedOn;
     RedFields rf{};
-    const bool flat = permute && !wantRep && !wantStats;  // the step's fast path
+    if (learned || c->sampling) {  // the stencil features read the red fields
+        rf.N = c->redN;
+        rf.Ux = c->redUx;
+        rf.Uy = c->redUy;
+    }
+    // the step's fast path; learned steps always take it (their closure has no diagnostics)
+    const bool flat = permute && (learned || (!wantRep && !wantStats));
     k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
                                                                    c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
                                                                    c->duRY, c->cols, flat ? c->cellOf : nullptr); ++c->launches;
@@ -767,18 +796,31 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     if (rc) return rc;
     mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
+    if (learned) {
+        k_learned_cells<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(c->P, c->redN, c->redUx, c->redUy, c->lparams,
+                                                                        c->duLX, c->duLY, c->lmode); ++c->launches;
+    }
     if (flat) {
-        k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX,
-                                                                   c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
-                                                                   c->pidb[np], c->xb[nx ^ 1], c->vb[nx ^ 1],
-                                                                   c->pidb[np ^ 1]); ++c->launches;
+        k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
+            c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
+            c->pidb[np], c->xb[nx ^ 1], c->vb[nx ^ 1], c->pidb[np ^ 1], learned ? c->lmode : nullptr, c->duLX,
+            c->duLY); ++c->launches;
     } else
     k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
         c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
         c->pidb[np], permute ? c->xb[nx ^ 1] : nullptr, permute ? c->vb[nx ^ 1] : nullptr,
         permute ? c->pidb[np ^ 1] : nullptr, wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr); ++c->launches;
     CUDA_TRY(cudaGetLastError());
-    if (wantStats) {
+    if (learned) {
+        // the next step's mode, from this step's occupancy spread (the red counts)
+        k_count_cols<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->P.highThr, c->P.lowThrBulk,
+                                                                    c->cols); ++c->launches;
+        rc = reduce_cols(c, c->cols, c->Nc, 3, 0u, c->lsums);
+        if (rc) return rc;
+        k_learned_decide<<<1, 1, 0, c->stream>>>(c->lsums, c->Nc, c->pc.gamma, c->learnedLimit, c->lmode, c->lcount);
+        ++c->launches;
+        if (wantStats) CUDA_TRY(cudaMemsetAsync(c->red + 2, 0, sizeof(double) * kKickCols, c->stream));
+    } else if (wantStats) {
         // sum, max, sum, sum, max, sum, sum, sum, sum
         rc = reduce_cols(c, c->cols, c->Nc, kKickCols, (1u << 1) | (1u << 4), c->red + 2);
         if (rc) return rc;
@@ -826,6 +868,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
                     c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
+                    c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->redN, c->redUx, c->redUy,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -1383,7 +1426,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     c->idxStdValid = false;
     rc = run_collide(c, 433494437ULL + 10007ULL * s, pf, step);
     if (rc) return rc;
-    rc = run_save_ref(c, pf);
+    rc = run_save_ref(c, pf, true);
     if (rc) return rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
     rc = run_zone_pass(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s, pf);
@@ -1889,6 +1932,293 @@ int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device
         const int rc = check_device(c);
         if (rc) return rc;
     }
+    return MPCD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- learned closure
+static void drop_graphs(mpcd_ctx* c) {
+    for (auto& g : c->gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+static int ensure_learned_buffers(mpcd_ctx* c) {
+    if (c->lparams) return MPCD_OK;
+    int rc;
+    if ((rc = dalloc(&c->lparams, kParams)) || (rc = dalloc(&c->lmode, 1)) || (rc = dalloc(&c->lcount, 2)) ||
+        (rc = dalloc(&c->lsums, 3)) || (rc = dalloc(&c->duLX, (size_t)c->Nc)) || (rc = dalloc(&c->duLY, (size_t)c->Nc)) ||
+        (rc = dalloc(&c->redN, (size_t)c->Nc)) || (rc = dalloc(&c->redUx, (size_t)c->Nc)) ||
+        (rc = dalloc(&c->redUy, (size_t)c->Nc)))
+        return rc;
+    return MPCD_OK;
+}
+
+static int step_flags_ok(const mpcd_ctx* c) {
+    if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution || !c->pc.useLiquidClosure)
+        return set_err(MPCD_ERR_INVALID_ARG, "the benchmark step needs useIncompressibleRedistribution, useZoneRedistribution and useLiquidClosure");
+    if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
+    return MPCD_OK;
+}
+
+// Context-free device work of the trainer: a device, a stream and its buffers, freed on exit.
+struct LearnedDev {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> bufs;
+    template <typename T>
+    int alloc(T** p, size_t count) {
+        const int rc = dalloc(p, count);
+        if (rc == MPCD_OK) bufs.push_back((void*)*p);
+        return rc;
+    }
+    int open(int dev) {
+        device = dev;
+        CUDA_TRY(cudaSetDevice(dev));
+        CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        return MPCD_OK;
+    }
+    ~LearnedDev() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : bufs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static int learned_rows_ok(const float* X, const float* Y, int64_t rows, const float* params) {
+    if (!X || !params || rows < 1 || rows > (int64_t)INT32_MAX / kFeat)
+        return set_err(MPCD_ERR_INVALID_ARG, "null argument or rows out of range");
+    (void)Y;
+    return MPCD_OK;
+}
+
+extern "C" {
+
+static_assert(kParams == MPCD_LEARNED_PARAMS && kFeat == MPCD_LEARNED_FEATURES && kOut == MPCD_LEARNED_OUTPUTS,
+              "C-ABI network layout");
+
+int mpcd_learned_param_count(void) { return kParams; }
+
+int mpcd_learned_init(uint64_t seed, float* params) {
+    if (!params) return set_err(MPCD_ERR_INVALID_ARG, "null params");
+    uint64_t st = seed;
+    auto next = [&st]() {  // splitmix64
+        uint64_t z = (st += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    };
+    auto fill = [&](int off, int fanOut, int fanIn) {  // Glorot uniform
+        const double b = std::sqrt(6.0 / (double)(fanIn + fanOut));
+        for (int i = 0; i < fanOut * fanIn; ++i) {
+            const double u = (double)(next() >> 11) * 0x1.0p-53;
+            params[off + i] = (float)((2.0 * u - 1.0) * b);
+        }
+    };
+    for (int i = 0; i < kParams; ++i) params[i] = 0.0f;
+    fill(kOffW1, kHid, kFeat);
+    fill(kOffW2, kHid, kHid);
+    fill(kOffW3, kOut, kHid);
+    return MPCD_OK;  // biases 0; the output scale 0 = set by the trainer
+}
+
+int mpcd_learned_set(mpcd_ctx* c, const float* params, double occ_limit) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // captured steps hold the previous closure
+    if (!params) {
+        c->learnedOn = false;
+        return MPCD_OK;
+    }
+    if (!(params[kOffScale] > 0.0f)) return set_err(MPCD_ERR_INVALID_ARG, "the network's output scale is not set (train it first)");
+    int rc = ensure_learned_buffers(c);
+    if (rc) return rc;
+    const int one = 1;
+    CUDA_TRY(cudaMemcpy(c->lparams, params, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(c->lmode, &one, sizeof one, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(c->lcount, 0, sizeof(long long) * 2));
+    c->learnedLimit = occ_limit;
+    c->learnedOn = true;
+    return MPCD_OK;
+}
+
+int mpcd_learned_stats(mpcd_ctx* c, int64_t* plain_steps, int64_t* learned_steps, int32_t* next_mode) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    long long n[2] = {0, 0};
+    int mode = 0;
+    if (c->lcount) {
+        CUDA_TRY(cudaSetDevice(c->device));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        CUDA_TRY(cudaMemcpy(n, c->lcount, sizeof n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(&mode, c->lmode, sizeof mode, cudaMemcpyDeviceToHost));
+    }
+    if (plain_steps) *plain_steps = n[0];
+    if (learned_steps) *learned_steps = n[1];
+    if (next_mode) *next_mode = c->learnedOn ? mode : 0;
+    return MPCD_OK;
+}
+
+int mpcd_learned_samples(mpcd_ctx* c, int64_t step0, int64_t nsteps, int32_t stride, float* features, float* targets,
+                         int64_t capacity, int64_t* count) {
+    if (!c || !features || !targets || !count) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (nsteps < 0 || stride < 1 || capacity < 0) return set_err(MPCD_ERR_INVALID_ARG, "nsteps, stride or capacity out of range");
+    if (c->learnedOn) return set_err(MPCD_ERR_STATE, "samples come from the plain closure: unset the network first");
+    int rc = step_flags_ok(c);
+    if (rc) return rc;
+    *count = 0;
+    CUDA_TRY(cudaSetDevice(c->device));
+    rc = ensure_learned_buffers(c);
+    if (rc) return rc;
+    const int perStep = (c->Nc + stride - 1) / stride;
+    const int64_t total = std::min<int64_t>(capacity, (int64_t)perStep * nsteps);
+    float *dX = nullptr, *dY = nullptr;
+    if ((rc = dalloc(&dX, (size_t)std::max<int64_t>(total, 1) * kFeat))) return rc;
+    if ((rc = dalloc(&dY, (size_t)std::max<int64_t>(total, 1) * kOut))) {
+        cudaFree(dX);
+        return rc;
+    }
+    int64_t got = 0;
+    c->sampling = true;
+    for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) {
+        const int64_t s = step0 + k;
+        rc = step_once(c, s, false);
+        if (rc || got >= total) continue;
+        const int offset = (int)(s % stride);
+        int cnt = (c->Nc - offset + stride - 1) / stride;
+        cnt = (int)std::min<int64_t>(cnt, total - got);
+        if (cnt <= 0) continue;
+        k_learned_samples<<<blocks_for(cnt), kThreads, 0, c->stream>>>(c->P, c->redN, c->redUx, c->redUy, c->duRX, c->duRY,
+                                                                       c->eosX, c->eosY, c->red, stride, offset, cnt,
+                                                                       dX + got * kFeat, dY + got * kOut);
+        ++c->launches;
+        if (cudaGetLastError() != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "k_learned_samples launch");
+        got += cnt;
+    }
+    c->sampling = false;
+    drop_graphs(c);  // graphs captured while sampling write the red fields; recapture without
+    if (rc == MPCD_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "samples");
+    if (rc == MPCD_OK && got > 0) {
+        if (cudaMemcpy(features, dX, sizeof(float) * kFeat * got, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(targets, dY, sizeof(float) * kOut * got, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = set_err(MPCD_ERR_CUDA, "samples copy");
+    }
+    cudaFree(dX);
+    cudaFree(dY);
+    if (rc) return rc;
+    *count = got;
+    return check_device(c);
+}
+
+int mpcd_learned_predict(const float* features, int64_t rows, const float* params, int device, float* out) {
+    int rc = learned_rows_ok(features, nullptr, rows, params);
+    if (rc) return rc;
+    if (!out) return set_err(MPCD_ERR_INVALID_ARG, "null output");
+    LearnedDev D;
+    float *dX, *dP, *dO;
+    if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dP, kParams)) ||
+        (rc = D.alloc(&dO, (size_t)rows * kOut)))
+        return rc;
+    CUDA_TRY(cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, D.stream));
+    k_mlp_rows<<<(unsigned)((rows + 127) / 128), 128, 0, D.stream>>>(dX, (int)rows, dP, dO);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, dO, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, D.stream));
+    CUDA_TRY(cudaStreamSynchronize(D.stream));
+    return MPCD_OK;
+}
+
+int mpcd_learned_grad(const float* features, const float* targets, int64_t rows, const float* params, int device,
+                      float* grad, float* loss) {
+    int rc = learned_rows_ok(features, targets, rows, params);
+    if (rc) return rc;
+    if (!targets || !grad || !loss) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (!(params[kOffScale] > 0.0f)) return set_err(MPCD_ERR_INVALID_ARG, "the network's output scale is not set");
+    LearnedDev D;
+    float *dX, *dY, *dP, *dG, *dL;
+    int* dI;
+    if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dY, (size_t)rows * kOut)) ||
+        (rc = D.alloc(&dP, kParams)) || (rc = D.alloc(&dG, kParams)) || (rc = D.alloc(&dL, 1)) ||
+        (rc = D.alloc(&dI, (size_t)rows)))
+        return rc;
+    std::vector<int> idx((size_t)rows);
+    for (int64_t i = 0; i < rows; ++i) idx[(size_t)i] = (int)i;
+    CUDA_TRY(cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dY, targets, sizeof(float) * kOut * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dI, idx.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemsetAsync(dG, 0, sizeof(float) * kParams, D.stream));
+    CUDA_TRY(cudaMemsetAsync(dL, 0, sizeof(float), D.stream));
+    k_mlp_grad<<<(unsigned)((rows + kMlpTile - 1) / kMlpTile), kMlpThreads, 0, D.stream>>>(
+        dX, dY, dI, (int)rows, (int)rows, 1.0f / params[kOffScale], dP, dG, dL);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(grad, dG, sizeof(float) * kParams, cudaMemcpyDeviceToHost, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(loss, dL, sizeof(float), cudaMemcpyDeviceToHost, D.stream));
+    CUDA_TRY(cudaStreamSynchronize(D.stream));
+    return MPCD_OK;
+}
+
+int mpcd_learned_train(const float* features, const float* targets, int64_t rows, float* params, int32_t epochs,
+                       int32_t batch, float lr, uint64_t seed, int device, float* epoch_loss) {
+    int rc = learned_rows_ok(features, targets, rows, params);
+    if (rc) return rc;
+    if (!targets) return set_err(MPCD_ERR_INVALID_ARG, "null targets");
+    if (epochs < 0 || batch < 1 || !(lr > 0.0f)) return set_err(MPCD_ERR_INVALID_ARG, "epochs, batch or lr out of range");
+    if (!(params[kOffScale] > 0.0f)) {  // the output scale: RMS of the targets
+        double ss = 0.0;
+        for (int64_t i = 0; i < rows * kOut; ++i) ss += (double)targets[i] * (double)targets[i];
+        const double rms = std::sqrt(ss / (double)(rows * kOut));
+        params[kOffScale] = (float)(rms > 0.0 ? rms : 1.0);
+    }
+    LearnedDev D;
+    float *dX, *dY, *dP, *dG, *dM, *dV, *dL;
+    int* dI;
+    const int64_t nb = (rows + batch - 1) / batch;
+    if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dY, (size_t)rows * kOut)) ||
+        (rc = D.alloc(&dP, kParams)) || (rc = D.alloc(&dG, kParams)) || (rc = D.alloc(&dM, kParams)) ||
+        (rc = D.alloc(&dV, kParams)) || (rc = D.alloc(&dL, (size_t)nb)) || (rc = D.alloc(&dI, (size_t)rows)))
+        return rc;
+    CUDA_TRY(cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dY, targets, sizeof(float) * kOut * rows, cudaMemcpyHostToDevice, D.stream));
+    CUDA_TRY(cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, D.stream));
+    for (float* b : {dG, dM, dV}) CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(float) * kParams, D.stream));
+    const float yinv = 1.0f / params[kOffScale];
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    std::vector<int> idx((size_t)rows);
+    std::vector<float> lossB((size_t)nb);
+    std::mt19937_64 rng(seed);
+    int64_t t = 0;
+    for (int e = 0; e < epochs; ++e) {
+        for (int64_t i = 0; i < rows; ++i) idx[(size_t)i] = (int)i;
+        for (int64_t i = rows - 1; i > 0; --i) std::swap(idx[(size_t)i], idx[(size_t)(rng() % (uint64_t)(i + 1))]);
+        CUDA_TRY(cudaStreamSynchronize(D.stream));  // idx is re-filled on the host
+        CUDA_TRY(cudaMemcpyAsync(dI, idx.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, D.stream));
+        CUDA_TRY(cudaMemsetAsync(dL, 0, sizeof(float) * nb, D.stream));
+        for (int64_t b = 0; b < nb; ++b) {
+            const int64_t r0 = b * batch;
+            const int n = (int)std::min<int64_t>(batch, rows - r0);
+            ++t;
+            k_mlp_grad<<<(unsigned)((n + kMlpTile - 1) / kMlpTile), kMlpThreads, 0, D.stream>>>(dX, dY, dI + r0, n, n, yinv,
+                                                                                               dP, dG, dL + b);
+            k_adam<<<(kTrained + 255) / 256, 256, 0, D.stream>>>(dP, dG, dM, dV, kTrained, lr, b1, b2, eps,
+                                                                 1.0f - (float)std::pow((double)b1, (double)t),
+                                                                 1.0f - (float)std::pow((double)b2, (double)t));
+        }
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(lossB.data(), dL, sizeof(float) * nb, cudaMemcpyDeviceToHost, D.stream));
+        CUDA_TRY(cudaStreamSynchronize(D.stream));
+        if (epoch_loss) {
+            double sum = 0.0;
+            for (int64_t b = 0; b < nb; ++b) sum += (double)lossB[(size_t)b] * (double)std::min<int64_t>(batch, rows - b * batch);
+            epoch_loss[e] = (float)(sum / (double)rows);
+        }
+    }
+    CUDA_TRY(cudaMemcpyAsync(params, dP, sizeof(float) * kTrained, cudaMemcpyDeviceToHost, D.stream));
+    CUDA_TRY(cudaStreamSynchronize(D.stream));
     return MPCD_OK;
 }
 

@@ -150,7 +150,8 @@ struct FieldsOut {
 
 // compute_cell_fields (src/common_grid.cpp:32-100), one cell per thread.
 __global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, const int* __restrict__ slots,
-                              const double2* __restrict__ v, double rhoTarget, FieldsOut o) {
+                              const double2* __restrict__ v, double rhoTarget, FieldsOut o, const int* skip = nullptr) {
+    if (skip && *skip) return;  // a learned-closure step needs no reference fields
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= Pm.Nc) return;
     const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];

@@ -31,14 +31,19 @@ __device__ __forceinline__ double cross_smooth(const double* raw, int ix, int iy
     return __ddiv_rn(acc, (double)cnt);
 }
 
-__global__ void k_pdrive(DevParams P, const double* __restrict__ pkin, const double* __restrict__ pvir, double* __restrict__ raw) {
+// skip (nullable): a device flag; when set, the step runs the learned closure and these
+// kernels of the plain one do nothing
+__global__ void k_pdrive(DevParams P, const double* __restrict__ pkin, const double* __restrict__ pvir, double* __restrict__ raw,
+                         const int* skip) {
+    if (skip && *skip) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     raw[c] = __dadd_rn(pkin[c], pvir[c]);
 }
 
 __global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, const int* __restrict__ mask, int anyMask,
-                               double* __restrict__ pdrive) {
+                               double* __restrict__ pdrive, const int* skip) {
+    if (skip && *skip) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     double v = raw[c];
@@ -50,7 +55,9 @@ __global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, cons
     pdrive[c] = v;
 }
 
-__global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __restrict__ eosX, double* __restrict__ eosY) {
+__global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __restrict__ eosX, double* __restrict__ eosY,
+                      const int* skip) {
+    if (skip && *skip) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const int ix = c / P.Ny, iy = c - ix * P.Ny;
@@ -232,16 +239,21 @@ __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, 
                             const double* __restrict__ duRY, const double* __restrict__ eosX,
                             const double* __restrict__ eosY, const double2* __restrict__ x,
                             const double2* __restrict__ v, const int* __restrict__ pid, double2* __restrict__ xo,
-                            double2* __restrict__ vo, int* __restrict__ pido) {
+                            double2* __restrict__ vo, int* __restrict__ pido, const int* learned,
+                            const double* __restrict__ duLX, const double* __restrict__ duLY) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
-    const double beta = beta_applied(P, numden[0], numden[1]);
     const int c = cellOf[j];
     const int s = slots[j];
     const double2 w = v[s];
-    const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
-    const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
-    vo[j] = make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c]));
+    if (learned && *learned) {  // the learned closure's kick
+        vo[j] = make_double2(__dadd_rn(w.x, duLX[c]), __dadd_rn(w.y, duLY[c]));
+    } else {
+        const double beta = beta_applied(P, numden[0], numden[1]);
+        const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
+        const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
+        vo[j] = make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c]));
+    }
     xo[j] = x[s];
     pido[j] = pid[s];
 }

@@ -28,6 +28,7 @@ LIB_PATH = os.path.join(HERE, "libmpcd_b200.so")
 _lib = None
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_fp = C.POINTER(C.c_float)
 
 
 class MpcdError(RuntimeError):
@@ -82,6 +83,16 @@ def lib():
         "mpcd_batch_step": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
         "mpcd_cell_fields_static": ([P(_abi.ParamsC), C.c_void_p, C.c_void_p, C.c_int64, C.c_double,
                                      P(_abi.CellFieldsC), C.c_void_p], C.c_int),
+        "mpcd_learned_param_count": ([], C.c_int),
+        "mpcd_learned_init": ([C.c_uint64, _fp], C.c_int),
+        "mpcd_learned_samples": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int32, _fp, _fp, C.c_int64, P(C.c_int64)],
+                                 C.c_int),
+        "mpcd_learned_train": ([_fp, _fp, C.c_int64, _fp, C.c_int32, C.c_int32, C.c_float, C.c_uint64, C.c_int, _fp],
+                               C.c_int),
+        "mpcd_learned_grad": ([_fp, _fp, C.c_int64, _fp, C.c_int, _fp, _fp], C.c_int),
+        "mpcd_learned_predict": ([_fp, C.c_int64, _fp, C.c_int, _fp], C.c_int),
+        "mpcd_learned_set": ([C.c_void_p, _fp, C.c_double], C.c_int),
+        "mpcd_learned_stats": ([C.c_void_p, P(C.c_int64), P(C.c_int64), P(C.c_int32)], C.c_int),
         "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
         "mpcd_host_free": ([C.c_void_p], None),
     }
@@ -293,6 +304,91 @@ class Context:
         m = _abi.StepMetricsC() if metrics else None
         _check(lib().mpcd_step(self.h, step0, nsteps, C.byref(m) if m is not None else None))
         return _abi.struct_to_dict(m) if metrics else None
+
+    def learned_samples(self, step0, nsteps, stride, capacity=None):
+        """mpcd_learned_samples: runs plain steps and returns (features [rows, 75], targets
+        [rows, 2]) of every stride-th cell after each step's closure."""
+        if capacity is None:
+            capacity = nsteps * ((self.params["Nc"] + stride - 1) // stride)
+        X = np.empty((max(capacity, 1), LEARNED_FEATURES), np.float32)
+        Y = np.empty((max(capacity, 1), LEARNED_OUTPUTS), np.float32)
+        n = C.c_int64()
+        _check(lib().mpcd_learned_samples(self.h, step0, nsteps, stride, _f32p(X), _f32p(Y), capacity, C.byref(n)))
+        return X[:n.value].copy(), Y[:n.value].copy()
+
+    def learned_set(self, params, occ_limit=0.0):
+        """mpcd_learned_set: the network in the step's closure (None: the plain closure), with
+        the plain closure as the fallback of steps after one whose occStd exceeded occ_limit."""
+        if params is None:
+            _check(lib().mpcd_learned_set(self.h, None, 0.0))
+            return
+        p = _params32(params)
+        _check(lib().mpcd_learned_set(self.h, _f32p(p), float(occ_limit)))
+
+    def learned_stats(self):
+        """(plain steps, learned steps, next step's mode) since learned_set."""
+        a, b, m = C.c_int64(), C.c_int64(), C.c_int32()
+        _check(lib().mpcd_learned_stats(self.h, C.byref(a), C.byref(b), C.byref(m)))
+        return a.value, b.value, m.value
+
+
+LEARNED_FEATURES, LEARNED_OUTPUTS, LEARNED_PARAMS = 75, 2, 9155
+
+
+def _f32p(a):
+    return a.ctypes.data_as(_fp)
+
+
+def _params32(params):
+    p = np.ascontiguousarray(params, np.float32)
+    if p.shape != (LEARNED_PARAMS,):
+        raise ValueError(f"network parameters: {LEARNED_PARAMS} floats expected, got {p.shape}")
+    return p
+
+
+def _rows32(X, cols):
+    X = np.ascontiguousarray(X, np.float32)
+    if X.ndim != 2 or X.shape[1] != cols:
+        raise ValueError(f"rows of {cols} floats expected, got {X.shape}")
+    return X
+
+
+def learned_init(seed):
+    """mpcd_learned_init: Glorot-uniform weights, zero biases, unset output scale."""
+    p = np.empty(LEARNED_PARAMS, np.float32)
+    _check(lib().mpcd_learned_init(seed, _f32p(p)))
+    return p
+
+
+def learned_train(X, Y, params, epochs, batch=256, lr=1e-3, seed=0, device=0):
+    """mpcd_learned_train: Adam on the device; returns (trained params, mean loss per epoch)."""
+    X, Y = _rows32(X, LEARNED_FEATURES), _rows32(Y, LEARNED_OUTPUTS)
+    if len(X) != len(Y):
+        raise ValueError("features and targets differ in rows")
+    p = _params32(params).copy()
+    losses = np.zeros(max(epochs, 1), np.float32)
+    _check(lib().mpcd_learned_train(_f32p(X), _f32p(Y), len(X), _f32p(p), epochs, batch, lr, seed, device,
+                                    _f32p(losses)))
+    return p, losses[:epochs]
+
+
+def learned_grad(X, Y, params, device=0):
+    """mpcd_learned_grad: (gradient, loss) of the mean squared error over all rows."""
+    X, Y = _rows32(X, LEARNED_FEATURES), _rows32(Y, LEARNED_OUTPUTS)
+    p = _params32(params)
+    g = np.empty(LEARNED_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    _check(lib().mpcd_learned_grad(_f32p(X), _f32p(Y), len(X), _f32p(p), device, _f32p(g), _f32p(loss)))
+    return g, float(loss[0])
+
+
+def learned_predict(X, params, device=0):
+    """mpcd_learned_predict: the network's kick for feature rows, [rows, 2]."""
+    X = _rows32(X, LEARNED_FEATURES)
+    p = _params32(params)
+    out = np.empty((len(X), LEARNED_OUTPUTS), np.float32)
+    _check(lib().mpcd_learned_predict(_f32p(X), len(X), _f32p(p), device, _f32p(out)))
+    return out
 
 
 class _Member(Context):
