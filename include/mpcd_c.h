@@ -260,7 +260,8 @@ int mpcd_batch_step(mpcd_batch* batch, int64_t step0, int64_t nsteps, double* de
  *             N/gamma - 1 [0..24], Ux [25..49], Uy [50..74] of the red (post-redistribution)
  *             cell fields; wrapped on periodic axes; outside a wall N term -1, U terms 0
  *   target:   2 floats, beta_applied * duRepair + duEOS of the plain closure
- *   network:  75 -> 64 -> 64 -> 2, GELU, BF16 weights with FP32 accumulation,
+ *   network:  75 -> 64 -> 64 -> 2, GELU (tanh form), BF16 weights, BF16 operands of the
+ *             two 64-wide layers (tcgen05 tensor cores), FP32 accumulation and output layer,
  *             kick = output * scale
  *   params:   MPCD_LEARNED_PARAMS floats: W1[64][75], b1[64], W2[64][64], b2[64], W3[2][64],
  *             b3[2], scale */

@@ -10,9 +10,13 @@ this file restates the library's own definition of it, in float64:
   features  75 per cell: a 5x5 stencil (dy outer, dx inner, offsets -2..2) of N/gamma - 1,
             Ux, Uy of the red cell fields; wrapped on periodic axes; a stencil cell beyond a
             wall gives N term -1 and U terms 0. Cell index c = iy + Ny * ix.
-  network   75 -> 64 -> 64 -> 2, GELU (erf form), weights and biases rounded to BF16
-            (round to nearest even), kick = output * scale
-  loss      mean over rows and both outputs of (output - target / scale)^2
+  network   z1 = W1 bf(x) + b1, a1 = gelu(z1), z2 = W2 bf(a1) + b2, a2 = gelu(z2),
+            output = W3 a2 + b3, kick = output * scale; GELU in the tanh form of Hendrycks
+            and Gimpel, z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))) / 2; every weight
+            and bias rounded to BF16 (bf: round to nearest even); the operands of the two
+            64-wide layers (x, a1) are BF16 too, a2 is not
+  loss      mean over rows and both outputs of (output - target / scale)^2; gradients pass
+            straight through the roundings
   Adam      m = b1 m + (1 - b1) g; v = b2 v + (1 - b2) g^2;
             p -= lr * (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps)
 
@@ -20,7 +24,6 @@ Parameter layout (one float32 array): W1[64][75], b1[64], W2[64][64], b2[64], W3
 b3[2], scale.
 """
 import numpy as np
-from scipy.special import erf
 
 FEAT, HID, OUT = 75, 64, 2
 OFF_W1 = 0
@@ -51,20 +54,24 @@ def unpack(params):
     return W1, b1, W2, b2, W3, b3, float(np.float32(params[OFF_SCALE]))
 
 
+_C = np.sqrt(2.0 / np.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(_C * (z + 0.044715 * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(_C * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _C * (1.0 + 3 * 0.044715 * z * z)
 
 
 def forward(X, params):
     """Network outputs (before the scale) and the intermediates."""
     W1, b1, W2, b2, W3, b3, _ = unpack(params)
-    X = np.asarray(X, np.float64)
+    X = bf16(np.asarray(X, np.float32))
     z1 = X @ W1.T + b1
-    a1 = gelu(z1)
+    a1 = bf16(gelu(z1).astype(np.float32))
     z2 = a1 @ W2.T + b2
     a2 = gelu(z2)
     out = a2 @ W3.T + b3

@@ -144,15 +144,14 @@ struct mpcd_ctx {
     bool learnedOn = false;
     bool sampling = false;     // red fields wanted (dataset collection)
     double learnedLimit = 0.0;
+    int tcGrid = 0;            // CTAs of the tensor-core inference kernel
     float* lparams = nullptr;
     int* lmode = nullptr;
     long long* lcount = nullptr;
     double* lsums = nullptr;
     double* duLX = nullptr;
     double* duLY = nullptr;
-    int* redN = nullptr;
-    double* redUx = nullptr;
-    double* redUy = nullptr;
+    float4* redFeat = nullptr;  // per cell of the red state: (N/gamma - 1, Ux, Uy, 0)
     int* zoneCost = nullptr;   // per zone: cost bucket
     int* zoneHist = nullptr;   // kCostBuckets
     int* zoneOrder = nullptr;  // launch order, heaviest first
@@ -206,6 +205,7 @@ const char* dev_error_text(int code) {
         case kErrCellId: return "cell id outside [0, Nc)";
         case kErrTargetIsSource: return "a dense cell targeted itself (periodic axis shorter than 3 cells)";
         case kErrRngCapacity: return "collision sign stream shorter than the number of cells with >= 2 particles";
+        case kErrTensorWait: return "a tensor-core MMA of the learned closure did not complete within the wait limit";
         default: return "device error";
     }
 }
@@ -783,9 +783,7 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     const bool learned = permute && c->learnedOn;
     RedFields rf{};
     if (learned || c->sampling) {  // the stencil features read the red fields
-        rf.N = c->redN;
-        rf.Ux = c->redUx;
-        rf.Uy = c->redUy;
+        rf.feat = c->redFeat;
     }
     // the step's fast path; learned steps always take it (their closure has no diagnostics)
     const bool flat = permute && (learned || (!wantRep && !wantStats));
@@ -797,8 +795,9 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
     if (learned) {
-        k_learned_cells<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(c->P, c->redN, c->redUx, c->redUy, c->lparams,
-                                                                        c->duLX, c->duLY, c->lmode); ++c->launches;
+        k_mlp_tc<false><<<c->tcGrid, kTcThreads, kTcSmem, c->stream>>>(c->P, c->redFeat, nullptr, 0,
+                                                                        c->lparams, c->duLX, c->duLY, nullptr, c->lmode,
+                                                                        c->st); ++c->launches;
     }
     if (flat) {
         k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
@@ -868,7 +867,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
                     c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
-                    c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->redN, c->redUx, c->redUy,
+                    c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->redFeat,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -1946,13 +1945,25 @@ static void drop_graphs(mpcd_ctx* c) {
         }
 }
 
+// the tensor-core kernels' shared memory opt-in and their persistent grid: tiles of 128 rows,
+// at most 4 CTAs per SM
+static int tc_setup(int device, int rows, int* grid) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int tiles = (rows + kTcRows - 1) / kTcRows;
+    *grid = std::max(1, std::min(tiles, 4 * sms));
+    return MPCD_OK;
+}
+
 static int ensure_learned_buffers(mpcd_ctx* c) {
     if (c->lparams) return MPCD_OK;
-    int rc;
+    int rc = tc_setup(c->device, c->Nc, &c->tcGrid);
+    if (rc) return rc;
     if ((rc = dalloc(&c->lparams, kParams)) || (rc = dalloc(&c->lmode, 1)) || (rc = dalloc(&c->lcount, 2)) ||
         (rc = dalloc(&c->lsums, 3)) || (rc = dalloc(&c->duLX, (size_t)c->Nc)) || (rc = dalloc(&c->duLY, (size_t)c->Nc)) ||
-        (rc = dalloc(&c->redN, (size_t)c->Nc)) || (rc = dalloc(&c->redUx, (size_t)c->Nc)) ||
-        (rc = dalloc(&c->redUy, (size_t)c->Nc)))
+        (rc = dalloc(&c->redFeat, (size_t)c->Nc)))
         return rc;
     return MPCD_OK;
 }
@@ -2092,7 +2103,7 @@ int mpcd_learned_samples(mpcd_ctx* c, int64_t step0, int64_t nsteps, int32_t str
         int cnt = (c->Nc - offset + stride - 1) / stride;
         cnt = (int)std::min<int64_t>(cnt, total - got);
         if (cnt <= 0) continue;
-        k_learned_samples<<<blocks_for(cnt), kThreads, 0, c->stream>>>(c->P, c->redN, c->redUx, c->redUy, c->duRX, c->duRY,
+        k_learned_samples<<<blocks_for(cnt), kThreads, 0, c->stream>>>(c->P, c->redFeat, c->duRX, c->duRY,
                                                                        c->eosX, c->eosY, c->red, stride, offset, cnt,
                                                                        dX + got * kFeat, dY + got * kOut);
         ++c->launches;
@@ -2120,15 +2131,23 @@ int mpcd_learned_predict(const float* features, int64_t rows, const float* param
     if (!out) return set_err(MPCD_ERR_INVALID_ARG, "null output");
     LearnedDev D;
     float *dX, *dP, *dO;
+    DevStatus* dS;
+    int grid = 0;
     if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dP, kParams)) ||
-        (rc = D.alloc(&dO, (size_t)rows * kOut)))
+        (rc = D.alloc(&dO, (size_t)rows * kOut)) || (rc = D.alloc(&dS, 1)) || (rc = tc_setup(device, (int)rows, &grid)))
         return rc;
     CUDA_TRY(cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * rows, cudaMemcpyHostToDevice, D.stream));
     CUDA_TRY(cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, D.stream));
-    k_mlp_rows<<<(unsigned)((rows + 127) / 128), 128, 0, D.stream>>>(dX, (int)rows, dP, dO);
+    CUDA_TRY(cudaMemsetAsync(dS, 0, sizeof(DevStatus), D.stream));
+    DevParams P{};
+    k_mlp_tc<true><<<grid, kTcThreads, kTcSmem, D.stream>>>(P, nullptr, dX, (int)rows, dP, nullptr,
+                                                            nullptr, dO, nullptr, dS);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, dO, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, D.stream));
+    DevStatus hs{};
+    CUDA_TRY(cudaMemcpyAsync(&hs, dS, sizeof hs, cudaMemcpyDeviceToHost, D.stream));
     CUDA_TRY(cudaStreamSynchronize(D.stream));
+    if (hs.code) return set_err(MPCD_ERR_DEVICE, std::string(dev_error_text(hs.code)) + " (detail " + std::to_string(hs.detail) + ")");
     return MPCD_OK;
 }
 

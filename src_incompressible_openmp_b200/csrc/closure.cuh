@@ -81,6 +81,7 @@ __global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __rest
 struct RedFields {
     int* N;
     double *Px, *Py, *Ux, *Uy;
+    float4* feat;  // (N/gamma - 1, Ux, Uy, 0) as FP32: the learned closure's stencil input
 };
 __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
                                 const double2* __restrict__ v, const double* __restrict__ refPx,
@@ -115,6 +116,7 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
     if (red.Py) red.Py[c] = py;
     if (red.Ux) red.Ux[c] = ux;
     if (red.Uy) red.Uy[c] = uy;
+    if (red.feat) red.feat[c] = make_float4((float)__dsub_rn(__ddiv_rn((double)m, P.gamma), 1.0), (float)ux, (float)uy, 0.0f);
 }
 
 // ---------------------------------------------------------------- fixed-order reductions

@@ -27,7 +27,8 @@ enum DevError : int {
     kErrEventCapacity = 8,      // more wall events than the event buffer holds
     kErrCellId = 9,             // a caller-given cell id outside [0, Nc)
     kErrTargetIsSource = 10,    // a dense cell targeting itself (periodic axis shorter than 3)
-    kErrRngCapacity = 11        // the collision sign stream was shorter than needed
+    kErrRngCapacity = 11,       // the collision sign stream was shorter than needed
+    kErrTensorWait = 12         // a tensor-core MMA did not complete within the wait limit
 };
 
 struct DevStatus {

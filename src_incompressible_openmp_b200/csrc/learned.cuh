@@ -6,13 +6,16 @@
 //                  the walls)
 //   target (2)   : the plain closure's kick, beta_applied * duRepair + duEOS
 //                  (reference src/liquid_closure.cpp:380-389, :424-436), in velocity units
-//   network      : 75 -> 64 -> 64 -> 2, GELU, weights rounded to BF16, FP32 accumulation;
-//                  kick = output * scale
+//   network      : 75 -> 64 -> 64 -> 2, GELU (tanh form); kick = output * scale
+//                  z1 = W1 bf(x) + b1, a1 = gelu(z1); z2 = W2 bf(a1) + b2, a2 = gelu(z2);
+//                  output = W3 a2 + b3, with every weight and bias rounded to BF16 (bf) and
+//                  FP32 accumulation: the operands of the two 64-wide layers are BF16 (they
+//                  run on the tensor cores), the 64 -> 2 output layer takes a2 in FP32
 //
 // Parameters live in one float array: W1[64][75], b1[64], W2[64][64], b2[64], W3[2][64], b3[2],
 // scale. Training (k_mlp_grad + k_adam) keeps FP32 master weights and fits output = target /
-// scale; every forward pass, in training and in the step, uses the weights' BF16 roundings.
-// The scale is not trained (the trainer sets it to the targets' RMS).
+// scale (gradients pass straight through the BF16 roundings). The scale is not trained (the
+// trainer sets it to the targets' RMS).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -28,60 +31,42 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kHid * kFeat, kOffW2 = kOffB1 + kHid
               kTrained = kOffScale, kParams = kOffScale + 1;  // 9154 trained + the output scale
 
 __device__ __forceinline__ float bf16r(float w) { return __bfloat162float(__float2bfloat16_rn(w)); }
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in the tanh form of Hendrycks and Gimpel, written as z * sigmoid(2u) with
+// u = sqrt(2/pi) (z + 0.044715 z^3) (0.5 (1 + tanh u) = sigmoid(2u))
+constexpr float kGeluC2 = 1.5957691216057308f;  // 2 sqrt(2/pi)
+constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu_sig(float z) {
+    return __fdividef(1.0f, 1.0f + __expf(-kGeluC2 * fmaf(kGeluA * z, z * z, z)));
+}
+__device__ __forceinline__ float gelu(float z) { return z * gelu_sig(z); }
 __device__ __forceinline__ float gelu_d(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    const float s = gelu_sig(z);
+    return fmaf(z * s * (1.0f - s), kGeluC2 * fmaf(3.0f * kGeluA, z * z, 1.0f), s);
 }
 
-// the stencil features of cell c
-__device__ __forceinline__ void cell_features(const DevParams& P, const int* __restrict__ N, const double* __restrict__ Ux,
-                                              const double* __restrict__ Uy, int c, float* f) {
+// the stencil features of cell c from the per-cell (N/gamma - 1, Ux, Uy, 0) array
+__device__ __forceinline__ void cell_features(const DevParams& P, const float4* __restrict__ feat, int c, float* f) {
     const int ix = c / P.Ny, iy = c - ix * P.Ny;
-    int k = 0;
-    for (int dy = -2; dy <= 2; ++dy)
-        for (int dx = -2; dx <= 2; ++dx, ++k) {
-            int jx = ix + dx, jy = iy + dy;
-            bool in = true;
-            if (P.perx) jx = wrap_index(jx, P.Nx);
-            else in = in && jx >= 0 && jx < P.Nx;
-            if (P.pery) jy = wrap_index(jy, P.Ny);
-            else in = in && jy >= 0 && jy < P.Ny;
-            float n = 0.0f, ux = 0.0f, uy = 0.0f;
-            if (in) {
-                const int q = jy + P.Ny * jx;
-                n = (float)__dsub_rn(__ddiv_rn((double)N[q], P.gamma), 1.0);
-                ux = (float)Ux[q];
-                uy = (float)Uy[q];
-            } else {
-                n = -1.0f;
-            }
-            f[k] = n;
-            f[25 + k] = ux;
-            f[50 + k] = uy;
+    int col[5], row[5];  // start of column jx (or -1 outside a wall), row jy (or -1)
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        int jx = ix + d - 2, jy = iy + d - 2;
+        if (P.perx) jx = wrap_index(jx, P.Nx);
+        col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
+        if (P.pery) jy = wrap_index(jy, P.Ny);
+        row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
+    }
+#pragma unroll
+    for (int dy = 0; dy < 5; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 5; ++dx) {
+            const int k = 5 * dy + dx;
+            float4 q = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+            if (col[dx] >= 0 && row[dy] >= 0) q = __ldg(feat + col[dx] + row[dy]);
+            f[k] = q.x;
+            f[25 + k] = q.y;
+            f[50 + k] = q.z;
         }
-}
-
-// the network on one feature row (weights: BF16 in shared memory)
-__device__ __forceinline__ void mlp_forward(const __nv_bfloat16* __restrict__ sw, const float* f, float& o0, float& o1) {
-    float h1[kHid];
-#pragma unroll 4
-    for (int j = 0; j < kHid; ++j) {
-        float z = __bfloat162float(sw[kOffB1 + j]);
-#pragma unroll
-        for (int k = 0; k < kFeat; ++k) z = fmaf(__bfloat162float(sw[kOffW1 + j * kFeat + k]), f[k], z);
-        h1[j] = gelu(z);
-    }
-    o0 = __bfloat162float(sw[kOffB3]);
-    o1 = __bfloat162float(sw[kOffB3 + 1]);
-#pragma unroll 4
-    for (int j = 0; j < kHid; ++j) {
-        float z = __bfloat162float(sw[kOffB2 + j]);
-#pragma unroll
-        for (int k = 0; k < kHid; ++k) z = fmaf(__bfloat162float(sw[kOffW2 + j * kHid + k]), h1[k], z);
-        const float a = gelu(z);
-        o0 = fmaf(__bfloat162float(sw[kOffW3 + j]), a, o0);
-        o1 = fmaf(__bfloat162float(sw[kOffW3 + kHid + j]), a, o1);
-    }
 }
 
 __device__ __forceinline__ void stage_weights(const float* __restrict__ params, __nv_bfloat16* sw) {
@@ -89,8 +74,7 @@ __device__ __forceinline__ void stage_weights(const float* __restrict__ params, 
 }
 
 // features and targets of every stride-th cell from offset (dataset collection)
-__global__ void k_learned_samples(DevParams P, const int* __restrict__ N, const double* __restrict__ Ux,
-                                  const double* __restrict__ Uy, const double* __restrict__ duRX,
+__global__ void k_learned_samples(DevParams P, const float4* __restrict__ feat, const double* __restrict__ duRX,
                                   const double* __restrict__ duRY, const double* __restrict__ eosX,
                                   const double* __restrict__ eosY, const double* __restrict__ red, int stride, int offset,
                                   int count, float* __restrict__ X, float* __restrict__ Y) {
@@ -98,7 +82,7 @@ __global__ void k_learned_samples(DevParams P, const int* __restrict__ N, const 
     if (s >= count) return;
     const int c = offset + s * stride;
     if (c >= P.Nc) return;
-    cell_features(P, N, Ux, Uy, c, X + (size_t)s * kFeat);
+    cell_features(P, feat, c, X + (size_t)s * kFeat);
     const double beta = beta_applied(P, red[0], red[1]);
     Y[2 * (size_t)s] = (float)__dadd_rn(__dmul_rn(beta, duRX[c]), eosX[c]);
     Y[2 * (size_t)s + 1] = (float)__dadd_rn(__dmul_rn(beta, duRY[c]), eosY[c]);
@@ -122,7 +106,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restric
     stage_weights(params, sw);
     for (int i = t; i < kMlpTile * kFeat; i += blockDim.x) {
         const int r = i / kFeat, k = i - r * kFeat;
-        x[r][k] = (r < nr) ? X[(size_t)idx[r0 + r] * kFeat + k] : 0.0f;
+        x[r][k] = (r < nr) ? bf16r(X[(size_t)idx[r0 + r] * kFeat + k]) : 0.0f;
     }
     __syncthreads();
     for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
@@ -130,7 +114,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restric
         float z = __bfloat162float(sw[kOffB1 + j]);
         for (int k = 0; k < kFeat; ++k) z = fmaf(__bfloat162float(sw[kOffW1 + j * kFeat + k]), x[r][k], z);
         z1[r][j] = z;
-        a1[r][j] = gelu(z);
+        a1[r][j] = bf16r(gelu(z));
     }
     __syncthreads();
     for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
@@ -222,42 +206,273 @@ __global__ void k_adam(float* __restrict__ params, float* __restrict__ grad, flo
     grad[i] = 0.0f;
 }
 
-// The learned kick of every cell of the red state, one thread per cell with the BF16-rounded
-// weights in shared memory.
-__global__ void __launch_bounds__(128) k_learned_cells(DevParams P, const int* __restrict__ N, const double* __restrict__ Ux,
-                                                       const double* __restrict__ Uy, const float* __restrict__ params,
-                                                       double* __restrict__ duX, double* __restrict__ duY,
-                                                       const int* __restrict__ mode) {
-    if (mode && *mode == 0) return;  // this step runs the plain closure
-    __shared__ __nv_bfloat16 sw[kTrained];
-    stage_weights(params, sw);
-    __syncthreads();
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.Nc) return;
-    float f[kFeat];
-    cell_features(P, N, Ux, Uy, c, f);
-    float o0, o1;
-    mlp_forward(sw, f, o0, o1);
-    const float scale = params[kOffScale];
-    duX[c] = (double)(o0 * scale);
-    duY[c] = (double)(o1 * scale);
+// ---------------------------------------------------------------- tensor-core inference
+// One CTA of 128 threads runs tiles of 128 rows (cells, or feature rows): thread t owns row t,
+// which is TMEM lane t of the accumulators. Per tile:
+//   1. every thread writes its row's 80 layer-1 operands to shared memory as BF16: the 75
+//      features point-major (operand column 3p + ch holds channel ch of stencil point p, so a
+//      point's three values are written together), a constant 1 that carries b1, 4 zeros;
+//   2. one thread issues 5 tcgen05.mma (M=128, N=64, K=16) into TMEM columns [0, 64);
+//   3. every thread loads its 64 accumulators (tcgen05.ld), applies GELU and writes a1 as BF16;
+//   4. one thread issues 4 tcgen05.mma into TMEM columns [64, 128);
+//   5. every thread loads z2, adds b2, applies GELU and runs the 64 -> 2 layer in FP32.
+// Operands use the canonical K-major layout without swizzle: 8x8 core matrices (8 rows of
+// 16 bytes, stored contiguously), adjacent along K at 128 bytes (LBO), 8-row groups at
+// K * 16 bytes (SBO).
+constexpr int kTcRows = 128, kTcThreads = 128, kTcK1 = 80;
+constexpr uint32_t kTcOffA = 0;                                  // [128][80] bf16
+constexpr uint32_t kTcOffH = kTcOffA + kTcRows * kTcK1 * 2;       // [128][64] bf16
+constexpr uint32_t kTcOffW1 = kTcOffH + kTcRows * kHid * 2;       // [64][80] bf16 (b1 in column 75)
+constexpr uint32_t kTcOffW2 = kTcOffW1 + kHid * kTcK1 * 2;        // [64][64] bf16
+constexpr uint32_t kTcOffB2 = kTcOffW2 + kHid * kHid * 2;         // [64] f32
+constexpr uint32_t kTcOffW3 = kTcOffB2 + kHid * 4;                // [2][64] f32
+constexpr uint32_t kTcOffB3 = kTcOffW3 + kOut * kHid * 4;         // b3[2], scale, pad: f32
+constexpr uint32_t kTcOffBar = kTcOffB3 + 16;                     // mbarrier (8 bytes)
+constexpr uint32_t kTcOffTmem = kTcOffBar + 8;                    // TMEM base address
+constexpr uint32_t kTcSmem = kTcOffTmem + 8;
+constexpr uint32_t kTcTmemCols = 128;
+constexpr int kTcSpinLimit = 1 << 22;
+// Shared memory bounds the CTAs per SM to 4, so their TMEM (4 x 128 columns) always fits.
+static_assert(5 * (kTcSmem + 1024) > 228 * 1024, "more than 4 CTAs per SM would oversubscribe TMEM");
+
+// instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+// both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kHid >> 3) << 17) |
+                              ((uint32_t)(kTcRows >> 4) << 24);
+
+__host__ __device__ constexpr uint32_t kmajor_offset(int r, int k, int K) {
+    return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
-// The network on feature rows (inference check): out[r] = output * scale.
-__global__ void __launch_bounds__(128) k_mlp_rows(const float* __restrict__ X, int rows, const float* __restrict__ params,
-                                                  float* __restrict__ out) {
-    __shared__ __nv_bfloat16 sw[kTrained];
-    stage_weights(params, sw);
+// shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1 (bit 46), no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool tc_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait for the barrier phase; false when the limit ran out
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    for (int i = 0; i < kTcSpinLimit; ++i)
+        if (tc_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive FP32 accumulator columns of this thread's lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+}
+// completes the loads; the registers are tied to it so no use is scheduled earlier
+__device__ __forceinline__ void tc_ld_wait16(uint32_t* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]) :: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Inference on tiles of 128 rows. kRows: rows of X (count rows), out[2 r] = kick; else the
+// cells of the red state, features gathered from feat, kick written to duX, duY (and
+// nothing when *mode == 0: the step runs the plain closure).
+template <bool kRows>
+__global__ void __launch_bounds__(kTcThreads, 4)
+    k_mlp_tc(DevParams P, const float4* __restrict__ feat, const float* __restrict__ X, int rows, const float* __restrict__ params, double* __restrict__ duX,
+             double* __restrict__ duY, float* __restrict__ out, const int* __restrict__ mode, DevStatus* st) {
+    if (!kRows && mode && *mode == 0) return;
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t bar = sbase + kTcOffBar;
+    float* sB2 = reinterpret_cast<float*>(sm + kTcOffB2);
+    float* sW3 = reinterpret_cast<float*>(sm + kTcOffW3);
+    float* sB3 = reinterpret_cast<float*>(sm + kTcOffB3);
+    // weights once per CTA (W1's columns in the point-major operand order)
+    for (int i = t; i < kHid * kTcK1; i += kTcThreads) {
+        const int n = i / kTcK1, k = i - n * kTcK1;
+        const int pk = (k % 3) * 25 + k / 3;  // parameter column of operand column k
+        const float w = k < kFeat ? params[kOffW1 + n * kFeat + pk] : (k == kFeat ? params[kOffB1 + n] : 0.0f);
+        *reinterpret_cast<__nv_bfloat16*>(sm + kTcOffW1 + kmajor_offset(n, k, kTcK1)) = __float2bfloat16_rn(w);
+    }
+    for (int i = t; i < kHid * kHid; i += kTcThreads) {
+        const int n = i / kHid, k = i - n * kHid;
+        *reinterpret_cast<__nv_bfloat16*>(sm + kTcOffW2 + kmajor_offset(n, k, kHid)) =
+            __float2bfloat16_rn(params[kOffW2 + i]);
+    }
+    if (t < kHid) sB2[t] = bf16r(params[kOffB2 + t]);
+    for (int i = t; i < kOut * kHid; i += kTcThreads) sW3[i] = bf16r(params[kOffW3 + i]);
+    if (t < kOut) sB3[t] = bf16r(params[kOffB3 + t]);
+    if (t == 0) {
+        sB3[2] = params[kOffScale];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kTcOffTmem),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_smem_async();
+    tc_fence_before();
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    float f[kFeat];
-    for (int k = 0; k < kFeat; ++k) f[k] = X[(size_t)r * kFeat + k];
-    float o0, o1;
-    mlp_forward(sw, f, o0, o1);
-    const float scale = params[kOffScale];
-    out[2 * (size_t)r] = o0 * scale;
-    out[2 * (size_t)r + 1] = o1 * scale;
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTcOffTmem);
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 TMEM lanes
+    const float scale = sB3[2];
+    const int total = kRows ? rows : P.Nc;
+    const int tiles = (total + kTcRows - 1) / kTcRows;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int r = tile * kTcRows + t;
+        const bool live = r < total;
+        // 1. layer-1 operands of row t
+        {
+            int col[5], row[5];  // stencil columns / rows of the cell (-1 beyond a wall)
+            if (!kRows && live) {
+                const int ix = r / P.Ny, iy = r - ix * P.Ny;
+#pragma unroll
+                for (int d = 0; d < 5; ++d) {
+                    int jx = ix + d - 2, jy = iy + d - 2;
+                    if (P.perx) jx = wrap_index(jx, P.Nx);
+                    col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
+                    if (P.pery) jy = wrap_index(jy, P.Ny);
+                    row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
+                }
+            }
+            // operand column k: stencil point k / 3, channel k % 3
+            auto operand = [&](int k) -> float {
+                if (k >= kFeat) return k == kFeat ? 1.0f : 0.0f;
+                if (!live) return 0.0f;
+                const int pnt = k / 3, ch = k - 3 * pnt;
+                if (kRows) return X[(size_t)r * kFeat + ch * 25 + pnt];
+                const int dy = pnt / 5, dx = pnt - 5 * dy;
+                if (col[dx] < 0 || row[dy] < 0) return ch == 0 ? -1.0f : 0.0f;
+                const float* q = reinterpret_cast<const float*>(feat + col[dx] + row[dy]);
+                return __ldg(q + ch);
+            };
+#pragma unroll
+            for (int j = 0; j < kTcK1 / 8; ++j) {
+                uint32_t w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) w[q] = pack_bf16(operand(8 * j + 2 * q), operand(8 * j + 2 * q + 1));
+                *reinterpret_cast<uint4*>(sm + kTcOffA + kmajor_offset(t, 8 * j, kTcK1)) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+        tc_fence_smem_async();
+        tc_fence_before();
+        __syncthreads();
+        // 2. layer 1 on the tensor cores
+        if (t == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < kTcK1 / 16; ++ks)
+                tc_mma(tmem, tc_desc(sbase + kTcOffA + ks * 256, 128, kTcK1 * 16),
+                       tc_desc(sbase + kTcOffW1 + ks * 256, 128, kTcK1 * 16), ks > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        ok = tc_wait(bar, phase);
+        phase ^= 1;
+        if (__syncthreads_and(ok) == 0) {
+            if (t == 0) raise_error(st, kErrTensorWait, tile);
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        // 3. a1 = gelu(z1) as BF16 operands of layer 2
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16];
+            tc_ld16(lane_base + 16 * h, z);
+            tc_ld_wait16(z);
+            uint32_t w[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) w[q] = pack_bf16(gelu(__uint_as_float(z[2 * q])), gelu(__uint_as_float(z[2 * q + 1])));
+            *reinterpret_cast<uint4*>(sm + kTcOffH + kmajor_offset(t, 16 * h, kHid)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(sm + kTcOffH + kmajor_offset(t, 16 * h + 8, kHid)) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        tc_fence_smem_async();
+        tc_fence_before();
+        __syncthreads();
+        // 4. layer 2 on the tensor cores
+        if (t == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < kHid / 16; ++ks)
+                tc_mma(tmem + kHid, tc_desc(sbase + kTcOffH + ks * 256, 128, kHid * 16),
+                       tc_desc(sbase + kTcOffW2 + ks * 256, 128, kHid * 16), ks > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        ok = tc_wait(bar, phase);
+        phase ^= 1;
+        if (__syncthreads_and(ok) == 0) {
+            if (t == 0) raise_error(st, kErrTensorWait, tile);
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        // 5. output layer in FP32
+        float o0 = sB3[0], o1 = sB3[1];
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16];
+            tc_ld16(lane_base + kHid + 16 * h, z);
+            tc_ld_wait16(z);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int j = 16 * h + q;
+                const float a = gelu(__uint_as_float(z[q]) + sB2[j]);
+                o0 = fmaf(sW3[j], a, o0);
+                o1 = fmaf(sW3[kHid + j], a, o1);
+            }
+        }
+        tc_fence_before();  // the next tile's MMAs overwrite these columns after the barrier
+        if (live) {
+            if (kRows) {
+                out[2 * (size_t)r] = o0 * scale;
+                out[2 * (size_t)r + 1] = o1 * scale;
+            } else {
+                duX[r] = (double)(o0 * scale);
+                duY[r] = (double)(o1 * scale);
+            }
+        }
+    }
+    if (!ok) {  // an MMA did not complete in time: give it one more bounded wait before freeing TMEM
+        tc_wait(bar, phase ^ 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+    }
 }
 
 // Mode of the next step from the occupancy spread of this step's red state: learned (1) while

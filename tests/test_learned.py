@@ -3,8 +3,11 @@ dataset collection against the step it samples, and the closure mode switch of t
 
 CPU tests pin the oracle itself (finite differences, an independent stencil loop, BF16
 rounding against torch). GPU tests call the library through the C-ABI:
-- mpcd_learned_predict and mpcd_learned_grad against the oracle: FP32 accumulation over BF16
-  weights, so outputs within 1e-5 relative and gradients within 1e-4 of the largest entry;
+- mpcd_learned_predict (the tcgen05 tensor-core kernel) and mpcd_learned_grad against the
+  oracle: FP32 accumulation in another order than the oracle's float64 one can move a1 across a
+  BF16 rounding boundary (one BF16 ulp, 2^-8 relative, in one of 64 hidden values), so outputs
+  agree within 1e-3 of the largest output and to 1e-5 for all but a few rows; gradients within
+  1e-4 of the largest entry;
 - mpcd_learned_train (one full-batch Adam step) against the oracle's Adam update;
 - mpcd_learned_samples: the centre features and targets against the state the step leaves
   (the plain kick is uniform per cell, so the cell mean velocity after the step is the red mean
@@ -46,8 +49,8 @@ def test_oracle_bf16_matches_torch():
 
 
 def test_oracle_gradient_finite_differences():
-    """The oracle's backward pass against central differences of its own loss, taken in the
-    BF16-rounded weights (the gradient flows straight through the rounding)."""
+    """The oracle's backward pass against central differences of its loss with the roundings
+    held fixed (weights and a1 at their BF16 values): the straight-through gradient."""
     X, Y, p = _rand_case(7, 3)
     loss, g = MO.loss_grad(X, Y, p)
     W = MO.unpack(p)
@@ -57,10 +60,15 @@ def test_oracle_gradient_finite_differences():
         (MO.OFF_W3, MO.OFF_B3))] + [np.arange(MO.OFF_B3, MO.OFF_SCALE)])
     flat = np.concatenate([W[0].ravel(), W[1], W[2].ravel(), W[3], W[4].ravel(), W[5]])
 
+    Xr = MO.bf16(X)
+    a1_fixed = MO.forward(X, p)[1][2]
+    z1_0 = Xr @ W[0].T + W[1]
+
     def loss_of(q):
         W1 = q[MO.OFF_W1:MO.OFF_B1].reshape(MO.HID, MO.FEAT)
-        z1 = X.astype(np.float64) @ W1.T + q[MO.OFF_B1:MO.OFF_W2]
-        a1 = MO.gelu(z1)
+        z1 = Xr @ W1.T + q[MO.OFF_B1:MO.OFF_W2]
+        # a1 rounded at the base point, moved by its first-order change (straight through)
+        a1 = a1_fixed + (MO.gelu(z1) - MO.gelu(z1_0))
         a2 = MO.gelu(a1 @ q[MO.OFF_W2:MO.OFF_B2].reshape(MO.HID, MO.HID).T + q[MO.OFF_B2:MO.OFF_W3])
         out = a2 @ q[MO.OFF_W3:MO.OFF_B3].reshape(MO.OUT, MO.HID).T + q[MO.OFF_B3:MO.OFF_SCALE]
         e = out - Y.astype(np.float64) / W[6]
@@ -122,10 +130,13 @@ def _native():
 @pytest.mark.gpu
 def test_predict_matches_oracle():
     native = _native()
-    X, _, p = _rand_case(333, 11)
+    X, _, p = _rand_case(1000, 11)  # 7 full tiles of 128 rows and a partial one
     got = native.learned_predict(X, p)
     want = MO.predict(X, p)
-    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
+    top = np.max(np.abs(want))
+    err = np.max(np.abs(got - want), axis=1)
+    assert np.max(err) <= 1e-3 * top
+    assert np.count_nonzero(err > 1e-5 * top) <= 10
 
 
 @pytest.mark.gpu
@@ -236,6 +247,39 @@ def test_zero_network_is_the_step_without_kick():
         xp, vp = ctx.get_state()
     assert np.array_equal(xl, xp)
     assert np.array_equal(vl, vp)
+
+
+@pytest.mark.gpu
+def test_learned_kick_matches_oracle():
+    """A learned step = the step without closure kick, then every particle of cell c kicked by
+    the network's output on the stencil of the red fields (the tensor-core kernel in the step)."""
+    native = _native()
+    p = poiseuille_params(48, 24, 10)
+    x, v = uniform_state(p, 15)
+    net = native.learned_init(8)
+    net[MO.OFF_B1:MO.OFF_W2] = np.random.default_rng(2).standard_normal(MO.HID) * 0.2
+    net[MO.OFF_SCALE] = 1e-2
+    with native.Context(p) as ctx:
+        ctx.set_state(x, v)
+        ctx.learned_set(net)
+        ctx.step(0, 1)
+        xl, vl = ctx.get_state()
+    with native.Context(p) as ctx:
+        ctx.set_state(x, v)
+        _phases_without_closure(ctx, 1)
+        xr, vr = ctx.get_state()
+    assert np.array_equal(xl, xr)
+    N, Ux, Uy = _cells(p, xr, vr)
+    F = MO.features(N, Ux, Uy, p["Nx"], p["Ny"], True, False, p["gamma"])
+    want = MO.predict(F.astype(np.float32), net)
+    a_x, a_y = p["Lx"] / p["Nx"], p["Ly"] / p["Ny"]
+    c = (np.floor(xr[1::2] / a_y).astype(int).clip(0, p["Ny"] - 1) +
+         p["Ny"] * np.floor(xr[0::2] / a_x).astype(int).clip(0, p["Nx"] - 1))
+    kick = (vl - vr).reshape(-1, 2)
+    top = np.max(np.abs(want))
+    err = np.abs(kick - want[c]).max(axis=1)
+    assert np.max(err) <= 1e-3 * top + 1e-12
+    assert np.count_nonzero(err > 1e-5 * top + 1e-12) <= 0.01 * len(err)
 
 
 @pytest.mark.gpu
