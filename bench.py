@@ -286,21 +286,10 @@ def run_ours(args):
 
 
 def ensemble_params(W):
-    """Parameters and initial states of the batched ensemble (seeded)."""
-    import numpy as np
+    """Parameters and initial state seeds of the batched ensemble."""
+    from src_incompressible_openmp_b200.cases import ensemble_family
 
-    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
-
-    rng = np.random.default_rng(W["seed"])
-    out = []
-    for r in range(W["replicas"]):
-        Nx = int(rng.integers(32, 513))
-        Ny = int(rng.integers(16, 129))
-        ppc = int(rng.integers(5, 21))
-        force = float(10.0 ** rng.uniform(-4.0, -2.0))
-        p = poiseuille_params(Nx, Ny, ppc, bodyForceX=force)
-        out.append((p, 1000 + r))
-    return out
+    return ensemble_family(W["replicas"], W["seed"])
 
 
 def run_ensemble(args):

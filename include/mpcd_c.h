@@ -293,6 +293,9 @@ int mpcd_learned_predict(const float* features, int64_t rows, const float* param
  * (occStd of the red state, as in the metrics row) exceeded occ_limit (occ_limit <= 0: never).
  * The decision is made on the device, so graph replay keeps it. */
 int mpcd_learned_set(mpcd_ctx* ctx, const float* params, double occ_limit);
+/* bulk_only (default 1): cells whose 5x5 stencil crosses a wall get no learned kick (the
+ * network's inputs there are partly wall padding); 0: every cell gets the network's kick. */
+int mpcd_learned_options(mpcd_ctx* ctx, int32_t bulk_only);
 /* Steps run with each closure since mpcd_learned_set, and the mode of the next step
  * (1 learned, 0 plain). */
 int mpcd_learned_stats(mpcd_ctx* ctx, int64_t* plain_steps, int64_t* learned_steps, int32_t* next_mode);

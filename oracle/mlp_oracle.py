@@ -8,8 +8,11 @@ duEOSX/Y, include/liquid_closure.h:29-44) by a stencil MLP. The reference has no
 this file restates the library's own definition of it, in float64:
 
   features  75 per cell: a 5x5 stencil (dy outer, dx inner, offsets -2..2) of N/gamma - 1,
-            Ux, Uy of the red cell fields; wrapped on periodic axes; a stencil cell beyond a
-            wall gives N term -1 and U terms 0. Cell index c = iy + Ny * ix.
+            Ux - <Ux>, Uy - <Uy> of the red cell fields, <.> the mean over the stencil points
+            inside the walls; wrapped on periodic axes; a stencil point beyond a wall gives
+            N term -1 and velocity terms 0. Cell index c = iy + Ny * ix.
+  kick      the network's kick per cell, zero in cells whose stencil crosses a wall (bulk
+            only), less sum_c N_c kick_c / n (momentum conserving)
   network   z1 = W1 bf(x) + b1, a1 = gelu(z1), z2 = W2 bf(a1) + b2, a2 = gelu(z2),
             output = W3 a2 + b3, kick = output * scale; GELU in the tanh form of Hendrycks
             and Gimpel, z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))) / 2; every weight
@@ -121,6 +124,7 @@ def features(N, Ux, Uy, Nx, Ny, perx, pery, gamma):
     Uy = np.asarray(Uy, np.float64).reshape(Nx, Ny)
     ix, iy = np.meshgrid(np.arange(Nx), np.arange(Ny), indexing="ij")
     F = np.zeros((Nx, Ny, FEAT))
+    ins = np.zeros((Nx, Ny, 25), bool)
     k = 0
     for dy in range(-2, 3):
         for dx in range(-2, 3):
@@ -138,8 +142,30 @@ def features(N, Ux, Uy, Nx, Ny, perx, pery, gamma):
             F[..., k] = np.where(inside, N[qx, qy] / gamma - 1.0, -1.0)
             F[..., 25 + k] = np.where(inside, Ux[qx, qy], 0.0)
             F[..., 50 + k] = np.where(inside, Uy[qx, qy], 0.0)
+            ins[..., k] = inside
             k += 1
+    cnt = ins.sum(-1, keepdims=True)
+    for ch in (1, 2):
+        U = F[..., 25 * ch:25 * ch + 25]
+        F[..., 25 * ch:25 * ch + 25] = np.where(ins, U - U.sum(-1, keepdims=True) / cnt, 0.0)
     return F.reshape(Nx * Ny, FEAT)
+
+
+def bulk_mask(Nx, Ny, perx, pery):
+    """Cells whose 5x5 stencil stays inside the walls (c = iy + Ny * ix)."""
+    ix, iy = np.meshgrid(np.arange(Nx), np.arange(Ny), indexing="ij")
+    m = np.ones((Nx, Ny), bool)
+    if not perx:
+        m &= (ix >= 2) & (ix < Nx - 2)
+    if not pery:
+        m &= (iy >= 2) & (iy < Ny - 2)
+    return m.reshape(-1)
+
+
+def conserving(kick, N):
+    """The kick per cell less its particle mean: kick - sum_c N_c kick_c / sum_c N_c."""
+    N = np.asarray(N, np.float64)
+    return kick - (N[:, None] * kick).sum(0) / N.sum()
 
 
 def init(seed):

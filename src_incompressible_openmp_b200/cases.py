@@ -71,6 +71,21 @@ WORKLOADS = {
 }
 
 
+def ensemble_family(count, seed):
+    """Independent Poiseuille channels of uneven size, density and forcing, seeded: Nx uniform in
+    [32, 512], Ny in [16, 128], particles per cell in [5, 20], bodyForceX log-uniform in
+    [1e-4, 1e-2]; replica r's initial state seed is 1000 + r. Returns [(params, state_seed)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(count):
+        Nx = int(rng.integers(32, 513))
+        Ny = int(rng.integers(16, 129))
+        ppc = int(rng.integers(5, 21))
+        force = float(10.0 ** rng.uniform(-4.0, -2.0))
+        out.append((poiseuille_params(Nx, Ny, ppc, bodyForceX=force), 1000 + r))
+    return out
+
+
 def to_c(p):
     """Parameter dict -> include/mpcd_c.h mpcd_params_c."""
     c = _abi.ParamsC()

@@ -144,6 +144,7 @@ struct mpcd_ctx {
     bool learnedOn = false;
     bool sampling = false;     // red fields wanted (dataset collection)
     double learnedLimit = 0.0;
+    int learnedBulkOnly = 1;   // no learned kick in cells whose stencil crosses a wall
     int tcGrid = 0;            // CTAs of the tensor-core inference kernel
     float* lparams = nullptr;
     int* lmode = nullptr;
@@ -151,6 +152,7 @@ struct mpcd_ctx {
     double* lsums = nullptr;
     double* duLX = nullptr;
     double* duLY = nullptr;
+    unsigned long long* duLSum = nullptr;  // sum over cells of N du (x, y), int64 at 2^-32
     float4* redFeat = nullptr;  // per cell of the red state: (N/gamma - 1, Ux, Uy, 0)
     int* zoneCost = nullptr;   // per zone: cost bucket
     int* zoneHist = nullptr;   // kCostBuckets
@@ -795,15 +797,17 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
     if (learned) {
+        CUDA_TRY(cudaMemsetAsync(c->duLSum, 0, 2 * sizeof(unsigned long long), c->stream));
         k_mlp_tc<false><<<c->tcGrid, kTcThreads, kTcSmem, c->stream>>>(c->P, c->redFeat, nullptr, 0,
                                                                         c->lparams, c->duLX, c->duLY, nullptr, c->lmode,
-                                                                        c->st); ++c->launches;
+                                                                        c->duLSum, c->learnedBulkOnly, c->st);
+        ++c->launches;
     }
     if (flat) {
         k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
             c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
             c->pidb[np], c->xb[nx ^ 1], c->vb[nx ^ 1], c->pidb[np ^ 1], learned ? c->lmode : nullptr, c->duLX,
-            c->duLY); ++c->launches;
+            c->duLY, reinterpret_cast<const long long*>(c->duLSum)); ++c->launches;
     } else
     k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
         c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
@@ -867,7 +871,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
                     c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
-                    c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->redFeat,
+                    c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->duLSum, c->redFeat,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
                     c->duRY, c->cols, c->partial, c->red, c->fieldTmp, c->fieldTmpN, c->vrep, c->cellOf, c->st};
@@ -1963,7 +1967,7 @@ static int ensure_learned_buffers(mpcd_ctx* c) {
     if (rc) return rc;
     if ((rc = dalloc(&c->lparams, kParams)) || (rc = dalloc(&c->lmode, 1)) || (rc = dalloc(&c->lcount, 2)) ||
         (rc = dalloc(&c->lsums, 3)) || (rc = dalloc(&c->duLX, (size_t)c->Nc)) || (rc = dalloc(&c->duLY, (size_t)c->Nc)) ||
-        (rc = dalloc(&c->redFeat, (size_t)c->Nc)))
+        (rc = dalloc(&c->redFeat, (size_t)c->Nc)) || (rc = dalloc(&c->duLSum, 2)))
         return rc;
     return MPCD_OK;
 }
@@ -2058,6 +2062,15 @@ int mpcd_learned_set(mpcd_ctx* c, const float* params, double occ_limit) {
     return MPCD_OK;
 }
 
+int mpcd_learned_options(mpcd_ctx* c, int32_t bulk_only) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->learnedBulkOnly = bulk_only != 0;
+    return MPCD_OK;
+}
+
 int mpcd_learned_stats(mpcd_ctx* c, int64_t* plain_steps, int64_t* learned_steps, int32_t* next_mode) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     long long n[2] = {0, 0};
@@ -2141,7 +2154,7 @@ int mpcd_learned_predict(const float* features, int64_t rows, const float* param
     CUDA_TRY(cudaMemsetAsync(dS, 0, sizeof(DevStatus), D.stream));
     DevParams P{};
     k_mlp_tc<true><<<grid, kTcThreads, kTcSmem, D.stream>>>(P, nullptr, dX, (int)rows, dP, nullptr,
-                                                            nullptr, dO, nullptr, dS);
+                                                            nullptr, dO, nullptr, nullptr, 0, dS);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, dO, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, D.stream));
     DevStatus hs{};

@@ -81,7 +81,7 @@ __global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __rest
 struct RedFields {
     int* N;
     double *Px, *Py, *Ux, *Uy;
-    float4* feat;  // (N/gamma - 1, Ux, Uy, 0) as FP32: the learned closure's stencil input
+    float4* feat;  // (N/gamma - 1, Ux, Uy, N) as FP32: the learned closure's stencil input
 };
 __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
                                 const double2* __restrict__ v, const double* __restrict__ refPx,
@@ -116,7 +116,7 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
     if (red.Py) red.Py[c] = py;
     if (red.Ux) red.Ux[c] = ux;
     if (red.Uy) red.Uy[c] = uy;
-    if (red.feat) red.feat[c] = make_float4((float)__dsub_rn(__ddiv_rn((double)m, P.gamma), 1.0), (float)ux, (float)uy, 0.0f);
+    if (red.feat) red.feat[c] = make_float4((float)__dsub_rn(__ddiv_rn((double)m, P.gamma), 1.0), (float)ux, (float)uy, (float)m);
 }
 
 // ---------------------------------------------------------------- fixed-order reductions
@@ -242,14 +242,19 @@ __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, 
                             const double* __restrict__ eosY, const double2* __restrict__ x,
                             const double2* __restrict__ v, const int* __restrict__ pid, double2* __restrict__ xo,
                             double2* __restrict__ vo, int* __restrict__ pido, const int* learned,
-                            const double* __restrict__ duLX, const double* __restrict__ duLY) {
+                            const double* __restrict__ duLX, const double* __restrict__ duLY,
+                            const long long* __restrict__ duLSum) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const int c = cellOf[j];
     const int s = slots[j];
     const double2 w = v[s];
-    if (learned && *learned) {  // the learned closure's kick
-        vo[j] = make_double2(__dadd_rn(w.x, duLX[c]), __dadd_rn(w.y, duLY[c]));
+    if (learned && *learned) {
+        // the learned closure's kick less its particle mean (sum over cells of N du, int64 at
+        // 2^-32), so that it leaves the total momentum unchanged
+        const double mx = __ddiv_rn((double)duLSum[0] * 0x1p-32, (double)P.n);
+        const double my = __ddiv_rn((double)duLSum[1] * 0x1p-32, (double)P.n);
+        vo[j] = make_double2(__dadd_rn(w.x, __dsub_rn(duLX[c], mx)), __dadd_rn(w.y, __dsub_rn(duLY[c], my)));
     } else {
         const double beta = beta_applied(P, numden[0], numden[1]);
         const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);

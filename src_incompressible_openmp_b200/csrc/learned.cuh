@@ -1,9 +1,13 @@
 // Learned closure: a stencil MLP that predicts the liquid closure's per-cell velocity
 // correction from the red (post-redistribution) occupancy and mean-velocity fields.
 //
-//   features (75): a 5x5 stencil around the cell of N/gamma - 1, Ux, Uy of the red state
-//                  (channel-major, dy outer, dx inner; wrapped on periodic axes, zero outside
-//                  the walls)
+//   features (75): a 5x5 stencil around the cell of N/gamma - 1, Ux - <Ux>, Uy - <Uy> of the
+//                  red state, <.> the mean over the stencil's cells inside the walls
+//                  (channel-major, dy outer, dx inner; wrapped on periodic axes; a point
+//                  beyond a wall gives N term -1 and velocity terms 0). Velocities relative to
+//                  the stencil mean make the network blind to a uniform flow, as the closure is.
+//   kick         : the network's output per cell less its particle mean (sum of N du over the
+//                  cells / n), so the learned kick conserves momentum
 //   target (2)   : the plain closure's kick, beta_applied * duRepair + duEOS
 //                  (reference src/liquid_closure.cpp:380-389, :424-436), in velocity units
 //   network      : 75 -> 64 -> 64 -> 2, GELU (tanh form); kick = output * scale
@@ -44,29 +48,55 @@ __device__ __forceinline__ float gelu_d(float z) {
     return fmaf(z * s * (1.0f - s), kGeluC2 * fmaf(3.0f * kGeluA, z * z, 1.0f), s);
 }
 
-// the stencil features of cell c from the per-cell (N/gamma - 1, Ux, Uy, 0) array
-__device__ __forceinline__ void cell_features(const DevParams& P, const float4* __restrict__ feat, int c, float* f) {
+// Stencil of cell c: start of each column jx (-1 beyond a wall) and each row jy (-1), and the
+// mean velocity over the points inside the walls.
+struct Stencil {
+    int col[5], row[5];
+    float mx, my;
+};
+
+__device__ __forceinline__ Stencil stencil_of(const DevParams& P, const float4* __restrict__ feat, int c) {
+    Stencil S;
     const int ix = c / P.Ny, iy = c - ix * P.Ny;
-    int col[5], row[5];  // start of column jx (or -1 outside a wall), row jy (or -1)
 #pragma unroll
     for (int d = 0; d < 5; ++d) {
         int jx = ix + d - 2, jy = iy + d - 2;
         if (P.perx) jx = wrap_index(jx, P.Nx);
-        col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
+        S.col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
         if (P.pery) jy = wrap_index(jy, P.Ny);
-        row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
+        S.row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
     }
+    float sx = 0.0f, sy = 0.0f;
+    int cnt = 0;
 #pragma unroll
     for (int dy = 0; dy < 5; ++dy)
 #pragma unroll
-        for (int dx = 0; dx < 5; ++dx) {
-            const int k = 5 * dy + dx;
-            float4 q = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
-            if (col[dx] >= 0 && row[dy] >= 0) q = __ldg(feat + col[dx] + row[dy]);
-            f[k] = q.x;
-            f[25 + k] = q.y;
-            f[50 + k] = q.z;
-        }
+        for (int dx = 0; dx < 5; ++dx)
+            if (S.col[dx] >= 0 && S.row[dy] >= 0) {
+                const float4 q = __ldg(feat + S.col[dx] + S.row[dy]);
+                sx += q.y;
+                sy += q.z;
+                ++cnt;
+            }
+    S.mx = sx / (float)cnt;  // the cell itself is always inside
+    S.my = sy / (float)cnt;
+    return S;
+}
+
+// channel ch (0 N, 1 Ux, 2 Uy) of stencil point pnt (5 dy + dx)
+__device__ __forceinline__ float stencil_value(const Stencil& S, const float4* __restrict__ feat, int pnt, int ch) {
+    const int dy = pnt / 5, dx = pnt - 5 * dy;
+    if (S.col[dx] < 0 || S.row[dy] < 0) return ch == 0 ? -1.0f : 0.0f;
+    const float* q = reinterpret_cast<const float*>(feat + S.col[dx] + S.row[dy]);
+    const float val = __ldg(q + ch);
+    return ch == 0 ? val : val - (ch == 1 ? S.mx : S.my);
+}
+
+// the stencil features of cell c (channel-major)
+__device__ __forceinline__ void cell_features(const DevParams& P, const float4* __restrict__ feat, int c, float* f) {
+    const Stencil S = stencil_of(P, feat, c);
+    for (int ch = 0; ch < 3; ++ch)
+        for (int k = 0; k < 25; ++k) f[25 * ch + k] = stencil_value(S, feat, k, ch);
 }
 
 __device__ __forceinline__ void stage_weights(const float* __restrict__ params, __nv_bfloat16* sw) {
@@ -304,7 +334,8 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 template <bool kRows>
 __global__ void __launch_bounds__(kTcThreads, 4)
     k_mlp_tc(DevParams P, const float4* __restrict__ feat, const float* __restrict__ X, int rows, const float* __restrict__ params, double* __restrict__ duX,
-             double* __restrict__ duY, float* __restrict__ out, const int* __restrict__ mode, DevStatus* st) {
+             double* __restrict__ duY, float* __restrict__ out, const int* __restrict__ mode,
+             unsigned long long* __restrict__ duSum, int bulkOnly, DevStatus* st) {
     if (!kRows && mode && *mode == 0) return;
     extern __shared__ __align__(128) unsigned char sm[];
     const int t = threadIdx.x, warp = t >> 5;
@@ -353,30 +384,17 @@ __global__ void __launch_bounds__(kTcThreads, 4)
     for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const int r = tile * kTcRows + t;
         const bool live = r < total;
+        Stencil S{};
         // 1. layer-1 operands of row t
         {
-            int col[5], row[5];  // stencil columns / rows of the cell (-1 beyond a wall)
-            if (!kRows && live) {
-                const int ix = r / P.Ny, iy = r - ix * P.Ny;
-#pragma unroll
-                for (int d = 0; d < 5; ++d) {
-                    int jx = ix + d - 2, jy = iy + d - 2;
-                    if (P.perx) jx = wrap_index(jx, P.Nx);
-                    col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
-                    if (P.pery) jy = wrap_index(jy, P.Ny);
-                    row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
-                }
-            }
+            if (!kRows && live) S = stencil_of(P, feat, r);
             // operand column k: stencil point k / 3, channel k % 3
             auto operand = [&](int k) -> float {
                 if (k >= kFeat) return k == kFeat ? 1.0f : 0.0f;
                 if (!live) return 0.0f;
                 const int pnt = k / 3, ch = k - 3 * pnt;
                 if (kRows) return X[(size_t)r * kFeat + ch * 25 + pnt];
-                const int dy = pnt / 5, dx = pnt - 5 * dy;
-                if (col[dx] < 0 || row[dy] < 0) return ch == 0 ? -1.0f : 0.0f;
-                const float* q = reinterpret_cast<const float*>(feat + col[dx] + row[dy]);
-                return __ldg(q + ch);
+                return stencil_value(S, feat, pnt, ch);
             };
 #pragma unroll
             for (int j = 0; j < kTcK1 / 8; ++j) {
@@ -454,6 +472,12 @@ __global__ void __launch_bounds__(kTcThreads, 4)
             }
         }
         tc_fence_before();  // the next tile's MMAs overwrite these columns after the barrier
+        if (!kRows && bulkOnly) {  // no learned kick where the stencil crosses a wall
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < 5; ++d) inside = inside && S.col[d] >= 0 && S.row[d] >= 0;
+            if (!inside) o0 = o1 = 0.0f;
+        }
         if (live) {
             if (kRows) {
                 out[2 * (size_t)r] = o0 * scale;
@@ -461,6 +485,23 @@ __global__ void __launch_bounds__(kTcThreads, 4)
             } else {
                 duX[r] = (double)(o0 * scale);
                 duY[r] = (double)(o1 * scale);
+            }
+        }
+        if (!kRows) {  // sum of N du over the cells, int64 at 2^-32 (exact and order-free)
+            long long qx = 0, qy = 0;
+            if (live) {
+                const double nc = (double)__ldg(reinterpret_cast<const float*>(feat + r) + 3);
+                qx = __double2ll_rn(nc * (double)(o0 * scale) * 0x1p32);
+                qy = __double2ll_rn(nc * (double)(o1 * scale) * 0x1p32);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                qx += __shfl_xor_sync(0xffffffffu, qx, o);
+                qy += __shfl_xor_sync(0xffffffffu, qy, o);
+            }
+            if ((t & 31) == 0 && (qx != 0 || qy != 0)) {
+                atomicAdd(duSum, (unsigned long long)qx);
+                atomicAdd(duSum + 1, (unsigned long long)qy);
             }
         }
     }

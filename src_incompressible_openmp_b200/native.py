@@ -93,6 +93,7 @@ def lib():
         "mpcd_learned_predict": ([_fp, C.c_int64, _fp, C.c_int, _fp], C.c_int),
         "mpcd_learned_set": ([C.c_void_p, _fp, C.c_double], C.c_int),
         "mpcd_learned_stats": ([C.c_void_p, P(C.c_int64), P(C.c_int64), P(C.c_int32)], C.c_int),
+        "mpcd_learned_options": ([C.c_void_p, C.c_int32], C.c_int),
         "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
         "mpcd_host_free": ([C.c_void_p], None),
     }
@@ -324,6 +325,10 @@ class Context:
             return
         p = _params32(params)
         _check(lib().mpcd_learned_set(self.h, _f32p(p), float(occ_limit)))
+
+    def learned_options(self, bulk_only=True):
+        """mpcd_learned_options: bulk_only -> no learned kick where the stencil crosses a wall."""
+        _check(lib().mpcd_learned_options(self.h, 1 if bulk_only else 0))
 
     def learned_stats(self):
         """(plain steps, learned steps, next step's mode) since learned_set."""

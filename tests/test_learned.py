@@ -12,7 +12,9 @@ rounding against torch). GPU tests call the library through the C-ABI:
 - mpcd_learned_samples: the centre features and targets against the state the step leaves
   (the plain kick is uniform per cell, so the cell mean velocity after the step is the red mean
   plus the target), and every feature against the oracle's stencil of those fields;
-- mpcd_learned_set: a zero network gives exactly the step without a closure kick; the device
+- mpcd_learned_set: a zero network gives exactly the step without a closure kick; a learned
+  step kicks every particle by the oracle's momentum-conserving kick of its cell (none where
+  the stencil crosses a wall); the device
   mode flag follows the occupancy limit, eagerly and under graph replay alike.
 """
 import os
@@ -93,7 +95,7 @@ def test_oracle_stencil_against_loop():
         F = MO.features(N, Ux, Uy, Nx, Ny, perx, pery, gamma)
         for c in (0, 5, 13, Nx * Ny - 1):
             ix, iy = divmod(c, Ny)
-            k = 0
+            pts = []
             for dy in range(-2, 3):
                 for dx in range(-2, 3):
                     jx, jy = ix + dx, iy + dy
@@ -106,10 +108,12 @@ def test_oracle_stencil_against_loop():
                         jy %= Ny
                     elif not 0 <= jy < Ny:
                         ok = False
-                    q = jy + Ny * jx
-                    want = (N[q] / gamma - 1, Ux[q], Uy[q]) if ok else (-1.0, 0.0, 0.0)
-                    assert (F[c, k], F[c, 25 + k], F[c, 50 + k]) == want, (perx, pery, c, k)
-                    k += 1
+                    pts.append(jy + Ny * jx if ok else None)
+            inside = [q for q in pts if q is not None]
+            mx, my = sum(Ux[q] for q in inside) / len(inside), sum(Uy[q] for q in inside) / len(inside)
+            for k, q in enumerate(pts):
+                want = (N[q] / gamma - 1, Ux[q] - mx, Uy[q] - my) if q is not None else (-1.0, 0.0, 0.0)
+                assert np.allclose((F[c, k], F[c, 25 + k], F[c, 50 + k]), want, rtol=0, atol=1e-14), (perx, pery, c, k)
 
 
 def test_param_layout_matches_header():
@@ -211,10 +215,9 @@ def test_samples_match_the_step():
     X, Y = X[p["Nc"]:], Y[p["Nc"]:]  # the last step's rows, every cell in order
     N, Ux, Uy = _cells(p, xs, vs)
     assert np.array_equal(X[:, 12], (N / p["gamma"] - 1).astype(np.float32))
-    red_ux, red_uy = Ux - Y[:, 0], Uy - Y[:, 1]
-    assert np.max(np.abs(X[:, 37] - red_ux)) <= 1e-6 and np.max(np.abs(X[:, 62] - red_uy)) <= 1e-6
+    red_ux, red_uy = Ux - Y[:, 0], Uy - Y[:, 1]  # the plain kick is uniform per cell
     F = MO.features(N, red_ux, red_uy, p["Nx"], p["Ny"], True, False, p["gamma"])  # channel: periodic x, walls in y
-    assert np.max(np.abs(X - F)) <= 1e-6
+    assert np.max(np.abs(X - F)) <= 2e-6
     assert np.max(np.abs(Y)) > 0
 
 
@@ -271,11 +274,14 @@ def test_learned_kick_matches_oracle():
     assert np.array_equal(xl, xr)
     N, Ux, Uy = _cells(p, xr, vr)
     F = MO.features(N, Ux, Uy, p["Nx"], p["Ny"], True, False, p["gamma"])
-    want = MO.predict(F.astype(np.float32), net)
+    bulk = MO.bulk_mask(p["Nx"], p["Ny"], True, False)
+    want = MO.conserving(MO.predict(F.astype(np.float32), net) * bulk[:, None], N)
     a_x, a_y = p["Lx"] / p["Nx"], p["Ly"] / p["Ny"]
     c = (np.floor(xr[1::2] / a_y).astype(int).clip(0, p["Ny"] - 1) +
          p["Ny"] * np.floor(xr[0::2] / a_x).astype(int).clip(0, p["Nx"] - 1))
     kick = (vl - vr).reshape(-1, 2)
+    # momentum: only the int64 rounding of each cell's N du (2^-33 at most) survives
+    assert np.all(np.abs(kick.sum(0)) <= p["Nc"] * 2.0 ** -33 + 1e-10)
     top = np.max(np.abs(want))
     err = np.abs(kick - want[c]).max(axis=1)
     assert np.max(err) <= 1e-3 * top + 1e-12
@@ -323,3 +329,26 @@ def test_graph_replay_matches_eager_with_network():
             res.append((ctx.get_state(), ctx.learned_stats()))
     assert res[0][1] == res[1][1]
     assert np.array_equal(res[0][0][0], res[1][0][0]) and np.array_equal(res[0][0][1], res[1][0][1])
+
+
+@pytest.mark.gpu
+def test_network_gain_over_no_kick():
+    """What the trained network gains over the method without it. The network is trained on
+    samples of 12 channels of the ensemble family and scored on 2 held-out channels: its kick
+    must explain a share of the plain closure's kick (no kick explains none). In deployment on
+    an unseen channel it must keep the plain closure's statistics (kinetic energy, occupancy
+    spread) and take every step itself."""
+    from src_incompressible_openmp_b200 import learned as L
+    X, Y = L.collect(runs=12, seed=21, warmup=40, steps=10, stride=3)
+    net, losses = L.train(X, Y, epochs=4)
+    assert losses[-1] < losses[0]
+    Xh, Yh = L.collect(runs=2, seed=99, warmup=40, steps=5, stride=3)
+    fvu = L.unexplained(net, Xh, Yh)
+    assert fvu < 0.85, fvu
+    assert L.unexplained(L.zero_network(), Xh, Yh) == pytest.approx(1.0)
+    p = poiseuille_params(128, 64, 10)
+    plain = L.deploy(p, None, 300)
+    lrn = L.deploy(p, net, 300)
+    assert lrn["closure_steps"] == (0, 300, 1)
+    assert abs(lrn["meanKinetic"] / plain["meanKinetic"] - 1) < 0.02
+    assert abs(lrn["occStd"] / plain["occStd"] - 1) < 0.05
