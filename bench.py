@@ -161,10 +161,11 @@ def whole_job_value(world, n_per_rank, steps, t_max):
     return world * n_per_rank * steps / t_max
 
 
-def config_dict(p, world):
+def config_dict(p, world, closure="plain"):
     return {
         "workload": WORKLOAD["name"], "Nx": p["Nx"], "Ny": p["Ny"], "particles_per_cell": WORKLOAD["ppc"],
-        "n_particles": p["n"], "n_cells": p["Nc"], "form": "plain_f64", "dt": p["dt"],
+        "n_particles": p["n"], "n_cells": p["Nc"], "form": "plain_f64" if closure == "plain" else "learned_closure_f64",
+        "dt": p["dt"],
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "l2_policy": f"state ({36 * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
     }
@@ -209,10 +210,20 @@ def run_ours(args):
     world, rank, local, dist, torch = dist_setup(args.gpus)
     p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
     x, v = uniform_state(p, 1 + rank)
+    learned = None
+    if args.closure == "learned":
+        learned = learned_network(args, local)
     ctx = native.Context(p, device=local)
     ctx.set_state(x, v)
     W, K = args.warmup, args.steps
-    ctx.step(0, W)
+    if learned is not None:
+        # fallback limit: 1.2 x the plain closure's occupancy spread, taken from a plain step
+        occ_plain = ctx.step(0, 1, metrics=True)["occStd"]
+        ctx.learned_set(learned["params"], 1.2 * occ_plain)
+        learned["occ_limit"] = 1.2 * occ_plain
+        ctx.step(1, W - 1)
+    else:
+        ctx.step(0, W)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -246,6 +257,7 @@ def run_ours(args):
     te = reduce_max(time.perf_counter() - t0, dist, torch)
     hx.close()
     hv.close()
+    ctx_stats = ctx.learned_stats()
     e2e = {"value": whole_job_value(world, p["n"], KE, te), "unit": UNIT, "h2d_bytes_per_step": 32 * p["n"],
            "d2h_bytes_per_step": 32 * p["n"], "steps": KE,
            "note": "per step: state upload from pinned host memory, one step, state download (C-ABI)"}
@@ -265,7 +277,7 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": 1e3 * t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": DATA, "config": config_dict(p, world),
+        "dtype": "f64", "data": DATA, "config": config_dict(p, world, args.closure),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": measured_traffic(dom),
                      "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
@@ -278,11 +290,34 @@ def run_ours(args):
         "gpu_launches": int((l1 - l0) * world),
         "clocks": clocks,
     }
+    if learned is not None:
+        plain_steps, learned_steps, _ = ctx_stats
+        line["learned_closure"] = {k: learned[k] for k in learned if k != "params"}
+        line["learned_closure"].update({"steps_plain": plain_steps, "steps_learned": learned_steps})
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(p, x, v)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def learned_network(args, device):
+    """The learned closure's network: loaded from --network, or collected and trained here on
+    the ensemble family (the plain closure's kicks in 200 seeded channels, up to 2 M cells, with
+    their mirror images; Adam on the GPU)."""
+    import numpy as np
+
+    from src_incompressible_openmp_b200 import learned as L
+
+    if args.network:
+        return {"params": np.load(args.network), "source": args.network}
+    t0 = time.perf_counter()
+    X, Y = L.collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=2_000_000, device=device)
+    t1 = time.perf_counter()
+    net, losses = L.train(X, Y, epochs=6, device=device)
+    t2 = time.perf_counter()
+    return {"params": net, "source": "trained in this run", "train_samples": int(len(X)),
+            "collect_s": t1 - t0, "train_s": t2 - t1, "final_loss": float(losses[-1])}
 
 
 def ensemble_params(W):
@@ -395,6 +430,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel_2048x512_ppc10")
+    ap.add_argument("--closure", choices=["plain", "learned"], default="plain",
+                    help="learned: the stencil-MLP closure with the plain closure as fallback")
+    ap.add_argument("--network", default=None, help="learned closure parameters (.npy); default: train here")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]

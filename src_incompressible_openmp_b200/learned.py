@@ -20,13 +20,13 @@ from . import native
 from .cases import ensemble_family, uniform_state
 
 
-def collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=None, log=None):
+def collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=None, log=None, device=0):
     """Samples from `runs` channels of the ensemble family: each runs `warmup` plain steps, then
     `steps` steps whose closure is sampled at every stride-th cell. Returns (X, Y) float32."""
     Xs, Ys, total = [], [], 0
     for r, (p, s) in enumerate(ensemble_family(runs, seed)):
         x, v = uniform_state(p, s)
-        with native.Context(p) as ctx:
+        with native.Context(p, device) as ctx:
             ctx.set_state(x, v)
             ctx.step(0, warmup)
             X, Y = ctx.learned_samples(warmup, steps, stride)
@@ -74,12 +74,12 @@ def mirrored(X, Y):
     return np.concatenate(outX), np.concatenate(outY)
 
 
-def train(X, Y, epochs=6, batch=512, lr=1e-3, seed=3, init_seed=1, mirror=True):
+def train(X, Y, epochs=6, batch=512, lr=1e-3, seed=3, init_seed=1, mirror=True, device=0):
     """Adam on the device from Glorot weights, on the samples and (mirror) their reflections;
     returns (params, mean loss per epoch)."""
     if mirror:
         X, Y = mirrored(X, Y)
-    return native.learned_train(X, Y, native.learned_init(init_seed), epochs, batch, lr, seed)
+    return native.learned_train(X, Y, native.learned_init(init_seed), epochs, batch, lr, seed, device)
 
 
 def unexplained(params, X, Y):
@@ -135,6 +135,27 @@ def profile_error(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+def time_case(Nx, Ny, ppc, steps, params=None):
+    """Device ms per step of the plain and the learned closure on one channel (an untrained
+    Glorot network when params is None: the cost does not depend on the weights)."""
+    from .cases import poiseuille_params
+    p = poiseuille_params(Nx, Ny, ppc)
+    x, v = uniform_state(p, 1)
+    if params is None:
+        params = native.learned_init(1)
+        params[-1] = 0.07
+    out = {}
+    with native.Context(p) as ctx:
+        ctx.set_state(x, v)
+        ctx.step(0, 3)
+        out["plain_ms"] = 1e3 * ctx.step_timed(3, steps) / steps
+        ctx.learned_set(params)
+        ctx.step(3 + steps, 3)
+        out["learned_ms"] = 1e3 * ctx.step_timed(6 + steps, steps) / steps
+        out["closure_steps"] = ctx.learned_stats()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--runs", type=int, default=200)
@@ -142,7 +163,12 @@ def main():
     ap.add_argument("--stride", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--out", default="net.npy")
+    ap.add_argument("--time-case", type=int, nargs=4, metavar=("NX", "NY", "PPC", "STEPS"),
+                    help="only time plain and learned steps on one channel")
     a = ap.parse_args()
+    if a.time_case:
+        print(time_case(*a.time_case))
+        return
     t0 = time.time()
     X, Y = collect(a.runs, stride=a.stride, capacity=a.samples, log=print)
     t1 = time.time()
