@@ -60,6 +60,17 @@ PHASE_BYTES = {
     "ref_fields": (20, 96),     # read slot 4, v 16 | 10 field arrays + start
     "closure_cells": (20, 64),
 }
+# the same for the FP32 precision form: 20 B of state per particle (cell 4, FP32 offset 8,
+# FP32 velocity 8) instead of 32
+PHASE_BYTES_F32 = {
+    "stream_bc": (48, 0),       # read cell, offset, v 20 B; write 20 B; write 2 cell ids 8 B
+    "zone_pass": (44, 8),       # read slot 4, state 20; write state 20 | counts 8 per cell
+    "kick_resort": (52, 32),    # read slot 4, state 20, pid 4; write state, pid 24 | 32 per cell
+    "collide": (20, 16),        # read slot 4, v 8; write v 8 | segment starts 16 per cell
+    "cell_index": (32, 24),
+    "ref_fields": (12, 96),     # read slot 4, v 8 | 10 field arrays + start
+    "closure_cells": (12, 64),
+}
 LAUNCHES_PER_STEP = {"zone_pass": 2, "cell_index": 4}
 
 
@@ -161,13 +172,16 @@ def whole_job_value(world, n_per_rank, steps, t_max):
     return world * n_per_rank * steps / t_max
 
 
-def config_dict(p, world, closure="plain"):
+def config_dict(p, world, closure="plain", form="f64"):
+    state_bytes = 36 if form == "f64" else 24
     return {
         "workload": WORKLOAD["name"], "Nx": p["Nx"], "Ny": p["Ny"], "particles_per_cell": WORKLOAD["ppc"],
-        "n_particles": p["n"], "n_cells": p["Nc"], "form": "plain_f64" if closure == "plain" else "learned_closure_f64",
+        "n_particles": p["n"], "n_cells": p["Nc"],
+        "form": ("plain_" if closure == "plain" else "learned_closure_") + form,
+        "state": "FP64 x, v" if form == "f64" else "int32 cell, FP32 offset in cell, FP32 v (FP64 arithmetic)",
         "dt": p["dt"],
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        "l2_policy": f"state ({36 * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
+        "l2_policy": f"state ({state_bytes * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
     }
 
 
@@ -191,12 +205,12 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def measured_traffic(kernel):
+def measured_traffic(kernel, form="f64"):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             d = json.load(f)
         e = d.get(kernel)
-        if e and e.get("workload") == WORKLOAD["name"]:
+        if e and e.get("workload") == WORKLOAD["name"] and e.get("form", "f64") == form:
             return float(e["bytes_per_launch"])
     except (OSError, ValueError):
         pass
@@ -213,7 +227,7 @@ def run_ours(args):
     learned = None
     if args.closure == "learned":
         learned = learned_network(args, local)
-    ctx = native.Context(p, device=local)
+    ctx = native.Context(p, device=local, form=args.form)
     ctx.set_state(x, v)
     W, K = args.warmup, args.steps
     if learned is not None:
@@ -268,23 +282,25 @@ def run_ours(args):
         return
     # roofline of the dominant kernel
     peak, peak_src = measured_peaks()
-    dom = max((k for k in phases if k in PHASE_BYTES), key=lambda k: phases[k])
+    table = PHASE_BYTES if args.form == "f64" else PHASE_BYTES_F32
+    dom = max((k for k in phases if k in table), key=lambda k: phases[k])
     per_launch_s = phases[dom] / (KP * LAUNCHES_PER_STEP.get(dom, 1))
-    bp, bc = PHASE_BYTES[dom]
+    bp, bc = table[dom]
     alg = bp * p["n"] + bc * p["Nc"]
     achieved = alg / per_launch_s / 1e9
-    step_bytes = 256 * p["n"] + 128 * p["Nc"]
+    bp_step = 256 if args.form == "f64" else 160  # 4 state sweeps, read + write
+    step_bytes = bp_step * p["n"] + 128 * p["Nc"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": 1e3 * t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": DATA, "config": config_dict(p, world, args.closure),
+        "dtype": args.form, "data": DATA, "config": config_dict(p, world, args.closure, args.form),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": measured_traffic(dom),
+                     "frac": achieved / peak, "traffic": measured_traffic(dom, args.form),
                      "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
                      "avg_launch_ms": 1e3 * per_launch_s},
         "step_hbm": {"algorithmic_bytes_per_step": step_bytes,
                      "achieved_GBps": step_bytes * K / t_max / 1e9 * world,
-                     "note": "256 B per particle + 128 B per cell per step"},
+                     "note": f"{bp_step} B per particle + 128 B per cell per step"},
         "phases_ms_per_step": {k: 1e3 * t / KP for k, t in phases.items()},
         "e2e": e2e,
         "gpu_launches": int((l1 - l0) * world),
@@ -433,6 +449,8 @@ def main():
     ap.add_argument("--closure", choices=["plain", "learned"], default="plain",
                     help="learned: the stencil-MLP closure with the plain closure as fallback")
     ap.add_argument("--network", default=None, help="learned closure parameters (.npy); default: train here")
+    ap.add_argument("--form", choices=["f64", "f32"], default="f64",
+                    help="f32: the FP32 precision form (FP32 cell-relative positions and velocities)")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]

@@ -153,6 +153,15 @@ const char* mpcd_io_last_error(void);
 /* Allocates device buffers for params->n particles and params->Nc cells on `device`.
  * Validates params (reference src/zone_pass.cpp:1100-1105, src/liquid_closure.cpp:332). */
 int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out);
+/* State forms of a context. MPCD_FORM_F64, the plain form: FP64 positions and velocities,
+ * results bit-exact or within 1e-12 of the reference. MPCD_FORM_F32, the precision form: per
+ * particle the standard-grid cell (int32), the position inside that cell as FP32 offsets and
+ * FP32 velocities (20 bytes of state instead of 32); arithmetic in FP64 registers, results
+ * rounded to FP32 on every store. An FP32 context runs the whole step (mpcd_step,
+ * mpcd_step_timed, mpcd_step_profile, mpcd_step_metrics, the learned closure) and state I/O in
+ * FP64 particle-id order; the phase functions return MPCD_ERR_INVALID_ARG. */
+enum mpcd_state_form { MPCD_FORM_F64 = 0, MPCD_FORM_F32 = 1 };
+int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, mpcd_ctx** out);
 int mpcd_ctx_destroy(mpcd_ctx* ctx);
 /* The stream every kernel of this context runs on (a cudaStream_t). */
 void* mpcd_ctx_stream(mpcd_ctx* ctx);

@@ -244,17 +244,16 @@ __global__ void k_srd_shift(DevParams P, uint64_t seed, double* out, const uint6
 }
 
 // Streams (optional), replays the sweeps, and computes the cell ids the next phases need.
-// x, v: slot-ordered state. cidStd: cell on the standard grid; cidSrd (optional): SRD cell.
-template <bool kInfo>
-__global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, double2* __restrict__ v,
-                            const int* __restrict__ pid, int* __restrict__ cidStd, int* __restrict__ cidSrd,
-                            BcWork W, DevStatus* st) {
+// S: slot-ordered state. cidStd: cell on the standard grid; cidSrd (optional): SRD cell.
+template <bool kInfo, class V>
+__global__ void k_stream_bc(DevParams P, int doStream, V S, const int* __restrict__ pid, int* __restrict__ cidStd,
+                            int* __restrict__ cidSrd, BcWork W, DevStatus* st) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[kWallDoubles];
     for (int k = 0; k < kWallDoubles; ++k) acc[k] = 0.0;
     int nhit[4] = {0, 0, 0, 0};
     if (s < P.n) {
-        double2 xs = x[s], vs = v[s];
+        double2 xs = S.pos(s, P), vs = S.vel(s);
         if (doStream) {
             vs.x = __dadd_rn(vs.x, __dmul_rn(P.bodyForceX, P.dt));
             vs.y = __dadd_rn(vs.y, __dmul_rn(P.g, P.dt));
@@ -270,7 +269,7 @@ __global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, 
         if (!ok) {
             raise_error(st, err, s);
         } else if (tx + ty == 0 && !late) {
-            v[s] = vs;
+            S.set_vel(s, vs);
             for (int k = 0; k < kWallDoubles; ++k) acc[k] = a2[k];
             for (int k = 0; k < 4; ++k) nhit[k] = h2[k];
         } else {
@@ -292,8 +291,9 @@ __global__ void k_stream_bc(DevParams P, int doStream, double2* __restrict__ x, 
                 raise_error(st, kErrEventCapacity, e);
             }
         }
-        x[s] = xs;
-        if (cidStd) cidStd[s] = cell_of(xs.x, xs.y, P);
+        const int cs = cell_of(xs.x, xs.y, P);
+        S.set_pos(s, xs, cs, P);
+        if (cidStd) cidStd[s] = cs;
         if (cidSrd) cidSrd[s] = srd_cell(xs.x, xs.y, W.srdShift[0], W.srdShift[1], P);
     }
     if (!kInfo) return;
@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(kNormThreads) k_wall_normals(uint64_t seed, co
 
 // Thermal particles: replay with their pairs; write the final velocity and the WallInfo
 // contribution at the slot of their first pair.
-__global__ void k_wall_apply(DevParams P, double2* __restrict__ v, BcWork W, DevStatus* st) {
+template <class V>
+__global__ void k_wall_apply(DevParams P, V S, BcWork W, DevStatus* st) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int ne = min(*W.nEvents, W.eventCap);
     if (e >= ne) return;
@@ -409,7 +410,7 @@ __global__ void k_wall_apply(DevParams P, double2* __restrict__ v, BcWork W, Dev
         raise_error(st, err, ev.slot);
         return;
     }
-    v[ev.slot] = make_double2(vx, vy);
+    S.set_vel(ev.slot, make_double2(vx, vy));
     const int npairs = tx + ty;
     for (int k = 0; k < kWallDoubles; ++k) {
         W.contrib[(size_t)first * kWallDoubles + k] = acc[k];

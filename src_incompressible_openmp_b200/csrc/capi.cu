@@ -78,9 +78,13 @@ struct mpcd_ctx {
     mpcd_params_c pc{};
     DevParams P{};
     int n = 0, Nc = 0;
-    // state
+    // state: the plain form keeps xb, vb; the FP32 precision form (f32) keeps offb, cellb, v32b
+    bool f32 = false;
     double2* xb[2] = {nullptr, nullptr};
     double2* vb[2] = {nullptr, nullptr};
+    float2* offb[2] = {nullptr, nullptr};
+    int* cellb[2] = {nullptr, nullptr};
+    float2* v32b[2] = {nullptr, nullptr};
     int* pidb[2] = {nullptr, nullptr};
     int xv = 0, pp = 0;
     int* cidStd = nullptr;
@@ -218,6 +222,32 @@ void mark(mpcd_ctx* c, Prof* p, int label) {
     p->label[p->n] = label;
     cudaEventRecord(p->ev[p->n++], c->stream);
 }
+
+// The state views of ping-pong buffer k, and a launch site written once for both forms:
+// WITH_VIEW(k, ...) runs its body with S, the view of buffer k; WITH_VIEWS(k, k2, ...) also
+// binds T, the view of buffer k2.
+inline View64 view64(const mpcd_ctx* c, int k) { return View64{c->xb[k], c->vb[k]}; }
+inline View32 view32(const mpcd_ctx* c, int k) { return View32{c->offb[k], c->cellb[k], c->v32b[k]}; }
+#define WITH_VIEW(k, ...)                          \
+    do {                                           \
+        if (c->f32) {                              \
+            const View32 S = view32(c, (k));       \
+            __VA_ARGS__;                           \
+        } else {                                   \
+            const View64 S = view64(c, (k));       \
+            __VA_ARGS__;                           \
+        }                                          \
+    } while (0)
+#define WITH_VIEWS(k, k2, ...)                                        \
+    do {                                                              \
+        if (c->f32) {                                                 \
+            const View32 S = view32(c, (k)), T = view32(c, (k2));     \
+            __VA_ARGS__;                                              \
+        } else {                                                      \
+            const View64 S = view64(c, (k)), T = view64(c, (k2));     \
+            __VA_ARGS__;                                              \
+        }                                                             \
+    } while (0)
 
 int check_device(mpcd_ctx* c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -372,6 +402,14 @@ DevParams make_dev_params(const mpcd_params_c& p) {
     d.betaRepair = p.betaRepair; d.betaEOS = p.betaEOS; d.Kvirial = p.Kvirial;
     d.smoothBlend = p.smoothPdriveInterzoneBlend;
     d.rhoTarget = p.gamma / ((p.Lx / (double)p.Nx) * (p.Ly / (double)p.Ny));
+    // the largest FP32 offset strictly below a cell width (FP32 form positions)
+    auto below = [](double w) {
+        float f = (float)w;
+        while ((double)f >= w) f = std::nextafter(f, 0.0f);
+        return f;
+    };
+    d.offMaxX = below(d.dx);
+    d.offMaxY = below(d.dy);
     // rotation constants (reference src/srd_collision.cpp:93-94 evaluates cos/sin of theta)
     const double th[3] = {0.0, p.alpha * 1.0, p.alpha * -1.0};
     for (int k = 0; k < 3; ++k) {
@@ -426,15 +464,17 @@ __global__ void k_set_step(long long* step, long long value) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *step = value;
 }
 
-__global__ void k_std_cells(DevParams P, const double2* __restrict__ x, int* __restrict__ cid) {
+template <class V>
+__global__ void k_std_cells(DevParams P, V S, int* __restrict__ cid) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < P.n) cid[s] = cell_of(x[s].x, x[s].y, P);
+    if (s < P.n) cid[s] = S.std_cell(s, P);
 }
 
 int ensure_std_index(mpcd_ctx* c, Prof* pf = nullptr) {
     if (c->idxStdValid) return MPCD_OK;
     if (!c->cidStdValid) {
-        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
+        WITH_VIEW(c->xv, k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, S, c->cidStd));
+        ++c->launches;
         c->cidStdValid = true;
     }
     const int rc = build_index(c, c->cidStd, c->idxStd, pf, 5);
@@ -456,6 +496,25 @@ __global__ void k_gather_by_pid(const double2* __restrict__ x, const double2* __
     const int p = pid[s];
     if (xo) xo[p] = x[s];
     if (vo) vo[p] = v[s];
+}
+
+// FP32 form, state I/O: positions and velocities in particle-id order, widened to FP64
+__global__ void k_f32_by_pid(DevParams P, View32 S, const int* __restrict__ pid, int n, double2* __restrict__ xo,
+                             double2* __restrict__ vo) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int p = pid[s];
+    if (xo) xo[p] = S.pos(s, P);
+    if (vo) vo[p] = S.vel(s);
+}
+
+// FP32 form, state I/O: FP64 positions and velocities (slot s = particle id s) into the view
+__global__ void k_f32_from(DevParams P, const double2* __restrict__ x, const double2* __restrict__ v, int n, View32 S) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double2 X = x[s];
+    S.set_pos(s, X, cell_of(X.x, X.y, P), P);
+    S.set_vel(s, v[s]);
 }
 
 __global__ void k_int_by_pid(const int* __restrict__ a, const int* __restrict__ pid, int n, int* __restrict__ out) {
@@ -489,11 +548,13 @@ __global__ void k_srd_cells(DevParams P, const double2* __restrict__ x, const do
     if (s < P.n) cid[s] = srd_cell(x[s].x, x[s].y, shift[0], shift[1], P);
 }
 
-__global__ void k_sub_mean(double2* __restrict__ v, int n, const double* __restrict__ sums) {
+template <class V>
+__global__ void k_sub_mean(V S, int n, const double* __restrict__ sums) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const double mx = __ddiv_rn(sums[1], (double)n), my = __ddiv_rn(sums[2], (double)n);
-    v[s] = make_double2(__dsub_rn(v[s].x, mx), __dsub_rn(v[s].y, my));
+    const double2 w = S.vel(s);
+    S.set_vel(s, make_double2(__dsub_rn(w.x, mx), __dsub_rn(w.y, my)));
 }
 
 int reduce_cols(mpcd_ctx* c, const double* cols, int64_t rows, int K, unsigned maxMask, double* out) {
@@ -517,11 +578,11 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     CUDA_TRY(cudaMemsetAsync(W.nEvents, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaMemsetAsync(W.ints, 0, sizeof(int) * 4, c->stream));
     if (wantInfo)
-        k_stream_bc<true><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv],
-                                                                   c->pidb[c->pp], cidStd, cidSrd, W, c->st);
+        WITH_VIEW(c->xv, k_stream_bc<true><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, S, c->pidb[c->pp],
+                                                                                   cidStd, cidSrd, W, c->st));
     else
-        k_stream_bc<false><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, c->xb[c->xv], c->vb[c->xv],
-                                                                    c->pidb[c->pp], cidStd, cidSrd, W, c->st);
+        WITH_VIEW(c->xv, k_stream_bc<false><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, S, c->pidb[c->pp],
+                                                                                    cidStd, cidSrd, W, c->st));
     ++c->launches;
     mark(c, pf, 0);
     cudaStream_t ws = c->stream;
@@ -537,7 +598,7 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     if (rc) return rc;
     k_wall_normals<<<1, kNormThreads, 0, ws>>>(seed, W.wordPrefix + c->nwords, W.normalCap, W.normals, c->st,
                                                c->graphMode ? c->stepSeeds : nullptr); ++c->launches;
-    k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, ws>>>(c->P, c->vb[c->xv], W, c->st); ++c->launches;
+    WITH_VIEW(c->xv, k_wall_apply<<<blocks_for(W.eventCap), kThreads, 0, ws>>>(c->P, S, W, c->st)); ++c->launches;
     if (wantInfo)
         k_wall_reduce<<<1, 32, 0, ws>>>(W.blockPartial, c->bcBlocks, W.contrib, W.wordPrefix + c->nwords, W.normalCap, c->wallOut); ++c->launches;
     CUDA_TRY(cudaGetLastError());
@@ -575,14 +636,15 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         CUDA_TRY(cudaStreamWaitEvent(c->stream, c->wallsDone, 0));
         c->wallsPending = false;
     }
-    k_srd_collide<<<blocks_for(c->Nc, kCollideCells), kCollideThreads, c->collideSmem, c->stream>>>(
-        c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc, c->vb[c->xv], c->st, gs, c->signsBuf[1], c->collideTile);
+    WITH_VIEW(c->xv, k_srd_collide<<<blocks_for(c->Nc, kCollideCells), kCollideThreads, c->collideSmem, c->stream>>>(
+                         c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc, S, c->st, gs, c->signsBuf[1],
+                         c->collideTile));
     ++c->launches;
     if (c->P.keepMeanFlow) {
-        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
+        WITH_VIEW(c->xv, k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->cols)); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
         if (rc) return rc;
-        k_sub_mean<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->red + 8); ++c->launches;
+        WITH_VIEW(c->xv, k_sub_mean<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->red + 8)); ++c->launches;
     }
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 4);
@@ -617,8 +679,9 @@ int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr, bool inStep = false) {
     o.N = c->refNi; o.Ux = c->refUx; o.Uy = c->refUy; o.Px = c->refPx; o.Py = c->refPy; o.T = c->refT;
     o.rho = c->refRho; o.Pkin = c->refPkin; o.Pvir = c->refPvir; o.P = c->refP;
     const int* skip = (inStep && c->learnedOn) ? c->lmode : nullptr;  // learned steps need no reference
-    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
-                                                                 c->P.rhoTarget, o, skip); ++c->launches;
+    WITH_VIEW(c->xv, k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, S,
+                                                                                  c->P.rhoTarget, o, skip));
+    ++c->launches;
     k_pdrive<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->refPkin, c->refPvir, c->pdRaw, skip); ++c->launches;
     k_pdrive_blend<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->pdRaw, c->mask, c->nMasked > 0, c->pdrive, skip);
     ++c->launches;
@@ -631,7 +694,7 @@ int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr, bool inStep = false) {
 
 int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) {
     if (!c->cidStdValid) {
-        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
+        WITH_VIEW(c->xv, k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, S, c->cidStd)); ++c->launches;
         c->cidStdValid = true;
     }
     int rc = ensure_std_index(c, pf);
@@ -645,17 +708,28 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     mark(c, pf, 7);
     CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
     // out of place: outputs start as a copy of the inputs; zones write what they change
-    CUDA_TRY(cudaMemcpyAsync(c->xb[c->xv ^ 1], c->xb[c->xv], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->vb[c->xv ^ 1], c->vb[c->xv], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
+    const size_t nn = (size_t)c->n;
+    const int xi = c->xv, xo = c->xv ^ 1;
+    if (c->f32) {
+        CUDA_TRY(cudaMemcpyAsync(c->offb[xo], c->offb[xi], sizeof(float2) * nn, cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(c->cellb[xo], c->cellb[xi], sizeof(int) * nn, cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(c->v32b[xo], c->v32b[xi], sizeof(float2) * nn, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(c->xb[xo], c->xb[xi], sizeof(double2) * nn, cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(c->vb[xo], c->vb[xi], sizeof(double2) * nn, cudaMemcpyDeviceToDevice, c->stream));
+    }
     ZoneArgs A{};
     A.P = c->P;
     A.rects = L.rects;
     A.owner = L.owner;
     A.start = c->idxStd.start;
     A.slots = c->idxStd.slots;
-    A.vin = c->vb[c->xv];
-    A.xout = c->xb[c->xv ^ 1];
-    A.vout = c->vb[c->xv ^ 1];
+    A.vin = c->vb[xi];
+    A.xout = c->xb[xo];
+    A.vout = c->vb[xo];
+    A.f32 = c->f32 ? 1 : 0;
+    A.in32 = view32(c, xi);
+    A.out32 = view32(c, xo);
     A.cid = c->cidStd;
     A.seeds = c->seeds;
     A.nZones = L.nZones;
@@ -673,7 +747,11 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
                                                                    c->zoneHist); ++c->launches;
     k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
     A.order = c->zoneOrder;
-    k_zone_pass<<<L.nZones, 32, c->zSmem, c->stream>>>(A); ++c->launches;
+    if (c->f32)
+        k_zone_pass<true><<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+    else
+        k_zone_pass<false><<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+    ++c->launches;
     CUDA_TRY(cudaGetLastError());
     ZoneArgs B = A;
     B.order = nullptr;
@@ -681,7 +759,11 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
     B.nsmCap = c->ovNsmCap;
-    k_zone_overflow<<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock); ++c->launches;
+    if (c->f32)
+        k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
+    else
+        k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
+    ++c->launches;
     k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 8);
@@ -705,7 +787,7 @@ __global__ void k_live_init(const uint64_t* __restrict__ start, int Nc, int* __r
 // run_zone_pass (src/zone_pass.cpp:1096-1163) on the current state, in place
 int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     if (!c->cidStdValid) {
-        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->cidStd); ++c->launches;
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view64(c, c->xv), c->cidStd); ++c->launches;
         c->cidStdValid = true;
     }
     int rc = ensure_std_index(c);
@@ -789,9 +871,10 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     }
     // the step's fast path; learned steps always take it (their closure has no diagnostics)
     const bool flat = permute && (learned || (!wantRep && !wantStats));
-    k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv],
-                                                                   c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
-                                                                   c->duRY, c->cols, flat ? c->cellOf : nullptr); ++c->launches;
+    WITH_VIEW(c->xv, k_closure_cells<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
+                         c->P, c->idxStd.start, c->idxStd.slots, S, c->refPx, c->refPy, c->refUx, c->refUy, rf, c->duRX,
+                         c->duRY, c->cols, flat ? c->cellOf : nullptr));
+    ++c->launches;
     rc = reduce_cols(c, c->cols, c->Nc, 2, 0u, c->red);
     if (rc) return rc;
     mark(c, pf, 9);
@@ -804,15 +887,18 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
         ++c->launches;
     }
     if (flat) {
-        k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
-            c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
-            c->pidb[np], c->xb[nx ^ 1], c->vb[nx ^ 1], c->pidb[np ^ 1], learned ? c->lmode : nullptr, c->duLX,
-            c->duLY, reinterpret_cast<const long long*>(c->duLSum)); ++c->launches;
-    } else
-    k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
-        c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, c->xb[nx], c->vb[nx],
-        c->pidb[np], permute ? c->xb[nx ^ 1] : nullptr, permute ? c->vb[nx ^ 1] : nullptr,
-        permute ? c->pidb[np ^ 1] : nullptr, wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr); ++c->launches;
+        WITH_VIEWS(nx, nx ^ 1, k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
+                                   c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, S,
+                                   c->pidb[np], T, c->pidb[np ^ 1], learned ? c->lmode : nullptr, c->duLX, c->duLY,
+                                   reinterpret_cast<const long long*>(c->duLSum)));
+        ++c->launches;
+    } else {
+        WITH_VIEWS(nx, nx ^ 1, k_kick<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(
+                                   c->P, c->idxStd.start, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, S,
+                                   c->pidb[np], permute ? 1 : 0, T, permute ? c->pidb[np ^ 1] : nullptr,
+                                   wantRep ? c->vrep : nullptr, wantStats ? c->cols : nullptr));
+        ++c->launches;
+    }
     CUDA_TRY(cudaGetLastError());
     if (learned) {
         // the next step's mode, from this step's occupancy spread (the red counts)
@@ -863,7 +949,8 @@ int mpcd_device_available(void) {
 int mpcd_ctx_destroy(mpcd_ctx* c) {
     if (!c) return MPCD_OK;
     cudaSetDevice(c->device);
-    void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd,
+    void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->offb[0], c->offb[1], c->cellb[0], c->cellb[1],
+                    c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd,
                     c->idxStd.count, c->idxStd.packed, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
                     c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
@@ -901,6 +988,11 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
 }
 
 int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
+    return mpcd_ctx_create_form(params, device, MPCD_FORM_F64, out);
+}
+
+int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, mpcd_ctx** out) {
+    if (form != MPCD_FORM_F64 && form != MPCD_FORM_F32) return set_err(MPCD_ERR_INVALID_ARG, "unknown state form");
     if (!params || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     int rc = validate(*params);
@@ -927,9 +1019,16 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
     const int n = c->n, Nc = c->Nc;
 #define ALLOC(p, cnt) \
     if ((rc = dalloc(&(p), (cnt)))) return fail(rc)
+    c->f32 = form == MPCD_FORM_F32;
     for (int k = 0; k < 2; ++k) {
-        ALLOC(c->xb[k], (size_t)n);
-        ALLOC(c->vb[k], (size_t)n);
+        if (c->f32) {
+            ALLOC(c->offb[k], (size_t)n);
+            ALLOC(c->cellb[k], (size_t)n);
+            ALLOC(c->v32b[k], (size_t)n);
+        } else {
+            ALLOC(c->xb[k], (size_t)n);
+            ALLOC(c->vb[k], (size_t)n);
+        }
         ALLOC(c->pidb[k], (size_t)n);
     }
     ALLOC(c->cidStd, (size_t)n);
@@ -1007,7 +1106,10 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
         c->collideTile = std::max(256, std::min(8192, (int)(kCollideCells * (1.5 * ppc + 8.0))));
         c->collideSmem = (size_t)c->collideTile * (sizeof(double2) + sizeof(int));
         if (c->collideSmem > 48 * 1024 &&
-            cudaFuncSetAttribute(k_srd_collide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) != cudaSuccess)
+            (cudaFuncSetAttribute(k_srd_collide<View64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) !=
+                 cudaSuccess ||
+             cudaFuncSetAttribute(k_srd_collide<View32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) !=
+                 cudaSuccess))
             return fail(set_err(MPCD_ERR_CUDA, "collision shared memory attribute"));
     }
     // fast path: tiles of the base/shifted layouts in shared memory
@@ -1031,7 +1133,8 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
             c->zSmem = ZoneMem<uint16_t>::bytes(0, 0, 0, 0);
         }
         if (c->zSmem > 48 * 1024 &&
-            (cudaFuncSetAttribute(k_zone_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
+            (cudaFuncSetAttribute(k_zone_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
+             cudaFuncSetAttribute(k_zone_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
              cudaFuncSetAttribute(k_zone_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess))
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
@@ -1083,7 +1186,23 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
     CUDA_TRY(cudaSetDevice(c->device));
     c->xv = 0;
     c->pp = 0;
-    if (n > 0) {
+    if (n > 0 && c->f32) {
+        // staged through FP64 scratch, then split into cell, FP32 offset and FP32 velocity
+        double2 *tx = nullptr, *tv = nullptr;
+        int rc = dalloc(&tx, (size_t)n);
+        if (!rc) rc = dalloc(&tv, (size_t)n);
+        if (!rc && (cudaMemcpyAsync(tx, x, sizeof(double2) * (size_t)n, kind, c->stream) != cudaSuccess ||
+                    cudaMemcpyAsync(tv, v, sizeof(double2) * (size_t)n, kind, c->stream) != cudaSuccess))
+            rc = set_err(MPCD_ERR_CUDA, "state upload");
+        if (!rc) {
+            k_f32_from<<<blocks_for(n), kThreads, 0, c->stream>>>(c->P, tx, tv, (int)n, view32(c, 0)); ++c->launches;
+            k_iota<<<blocks_for(n), kThreads, 0, c->stream>>>(c->pidb[0], (int)n); ++c->launches;
+            if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "state conversion");
+        }
+        cudaFree(tx);
+        cudaFree(tv);
+        if (rc) return rc;
+    } else if (n > 0) {
         CUDA_TRY(cudaMemcpyAsync(c->xb[0], x, sizeof(double2) * (size_t)n, kind, c->stream));
         CUDA_TRY(cudaMemcpyAsync(c->vb[0], v, sizeof(double2) * (size_t)n, kind, c->stream));
         k_iota<<<blocks_for(n), kThreads, 0, c->stream>>>(c->pidb[0], (int)n); ++c->launches;
@@ -1104,11 +1223,28 @@ static int get_state_impl(mpcd_ctx* c, double* x, double* v, bool toHost) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
     if (c->n == 0) return MPCD_OK;
+    const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (c->f32) {
+        double2 *tx = nullptr, *tv = nullptr;
+        int rc = dalloc(&tx, (size_t)c->n);
+        if (!rc) rc = dalloc(&tv, (size_t)c->n);
+        if (!rc) {
+            k_f32_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view32(c, c->xv), c->pidb[c->pp], c->n, tx, tv);
+            ++c->launches;
+            if ((x && cudaMemcpyAsync(x, tx, sizeof(double2) * (size_t)c->n, k, c->stream) != cudaSuccess) ||
+                (v && cudaMemcpyAsync(v, tv, sizeof(double2) * (size_t)c->n, k, c->stream) != cudaSuccess) ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess)
+                rc = set_err(MPCD_ERR_CUDA, "state download");
+        }
+        cudaFree(tx);
+        cudaFree(tv);
+        if (rc) return rc;
+        return check_device(c);
+    }
     double2* tx = c->xb[c->xv ^ 1];
     double2* tv = c->vb[c->xv ^ 1];
     k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv); ++c->launches;
     CUDA_TRY(cudaGetLastError());
-    const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (x) CUDA_TRY(cudaMemcpyAsync(x, tx, sizeof(double2) * (size_t)c->n, k, c->stream));
     if (v) CUDA_TRY(cudaMemcpyAsync(v, tv, sizeof(double2) * (size_t)c->n, k, c->stream));
     return check_device(c);
@@ -1119,6 +1255,7 @@ int mpcd_get_state_device(mpcd_ctx* c, double* x, double* v) { return get_state_
 
 int mpcd_stream(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->vb[c->xv]); ++c->launches;
     CUDA_TRY(cudaGetLastError());
@@ -1128,6 +1265,7 @@ int mpcd_stream(mpcd_ctx* c) {
 
 int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_bc(c, false, seed, nullptr, nullptr, info != nullptr);
     if (rc) return rc;
@@ -1148,6 +1286,7 @@ int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
 
 int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift, nullptr); ++c->launches;
     k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd); ++c->launches;
@@ -1163,6 +1302,7 @@ int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
 
 int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->srdCellsValid) return set_err(MPCD_ERR_STATE, "no SRD cell ids: call mpcd_srd_shift_cells first");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_collide(c, seed);
@@ -1172,6 +1312,7 @@ int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
 
 int mpcd_srd_collide_cells(mpcd_ctx* c, const int32_t* cid, uint64_t seed) {
     if (!c || !cid) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     if (c->n > 0) {
         int* tmp = c->idxSrd.pos;
@@ -1207,11 +1348,12 @@ static FieldsOut tmp_fields(mpcd_ctx* c) {
 
 int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
     if (!c || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = ensure_std_index(c);
     if (rc) return rc;
     const FieldsOut o = tmp_fields(c);
-    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], rho_target, o); ++c->launches;
+    k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, view64(c, c->xv), rho_target, o); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     rc = fields_to_host(c, o, out);
     if (rc) return rc;
@@ -1220,6 +1362,7 @@ int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
 
 int mpcd_save_ref(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_save_ref(c);
     if (rc) return rc;
@@ -1243,6 +1386,7 @@ static int pass_metrics_to_host(mpcd_ctx* c, int mode, mpcd_pass_metrics_c* m) {
 
 int mpcd_zone_pass(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
@@ -1300,6 +1444,7 @@ static void closure_metrics_from(mpcd_ctx* c, const double* r, mpcd_closure_metr
 
 int mpcd_zone_pass_serial(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
@@ -1329,6 +1474,7 @@ int mpcd_zone_pass_serial(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pa
 
 int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useLiquidClosure) return set_err(MPCD_ERR_INVALID_ARG, "run_liquid_closure requires useLiquidClosure=true");
     CUDA_TRY(cudaSetDevice(c->device));
     const bool wantRep = detail && (detail->repairedV || detail->repairedX || detail->repairedFields.N ||
@@ -1339,7 +1485,7 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
         rc = ensure_std_index(c);
         if (rc) return rc;
         const FieldsOut o = tmp_fields(c);
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, view64(c, c->xv), c->P.rhoTarget, o); ++c->launches;
         rc = fields_to_host(c, o, &detail->redFields);
         if (rc) return rc;
         CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1388,12 +1534,12 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
                 if (detail->repairedV) CUDA_TRY(cudaMemcpyAsync(detail->repairedV, c->vb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
                 CUDA_TRY(cudaStreamSynchronize(c->stream));
             }
-            k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vrep, c->P.rhoTarget, o); ++c->launches;
+            k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, View64{nullptr, c->vrep}, c->P.rhoTarget, o); ++c->launches;
             rc = fields_to_host(c, o, &detail->repairedFields);
             if (rc) return rc;
             CUDA_TRY(cudaStreamSynchronize(c->stream));
         }
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
+        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, view64(c, c->xv), c->P.rhoTarget, o); ++c->launches;
         rc = fields_to_host(c, o, &detail->outFields);
         if (rc) return rc;
         rc = check_device(c);
@@ -1460,13 +1606,15 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
         if (rc) return rc;
         rc = reduce_cols(c, c->pdrive, c->Nc, 1, 0u, c->red + 17);
         if (rc) return rc;
-        k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->vb[c->xv], c->n, c->cols); ++c->launches;
+        WITH_VIEW(c->xv, k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->cols)); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 26);
         if (rc) return rc;
         FieldsOut o{};
         o.Ux = c->fieldTmp;
         o.Uy = c->fieldTmp + c->Nc;
-        k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots, c->vb[c->xv], c->P.rhoTarget, o); ++c->launches;
+        WITH_VIEW(c->xv, k_cell_fields<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->P, c->idxStd.start, c->idxStd.slots,
+                                                                                      S, c->P.rhoTarget, o));
+        ++c->launches;
         rc = reduce_cols(c, c->fieldTmp, c->Nc, 1, 0u, c->red + 29);
         if (rc) return rc;
         rc = reduce_cols(c, c->fieldTmp + c->Nc, c->Nc, 1, 0u, c->red + 30);

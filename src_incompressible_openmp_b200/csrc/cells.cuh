@@ -103,10 +103,11 @@ __device__ __forceinline__ bool collide_cell(const DevParams& P, uint64_t start0
 constexpr int kCollideCells = 64;
 constexpr int kCollideThreads = 256;
 
+template <class V>
 __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, const uint64_t* __restrict__ start,
                                                                  const int* __restrict__ slots,
                                                                  const uint8_t* __restrict__ sign, int signCount,
-                                                                 double2* __restrict__ v, DevStatus* st,
+                                                                 V S, DevStatus* st,
                                                                  const uint64_t* seedDev,
                                                                  const uint8_t* __restrict__ sign1, int tileCap) {
     extern __shared__ __align__(16) double2 tv[];
@@ -121,15 +122,15 @@ __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, co
             const uint64_t s0 = start[c0 + t];
             const int a = (int)(uint32_t)s0, m = (int)(uint32_t)start[c0 + t + 1] - a;
             if (m > 0)
-                collide_cell(P, s0, m, sign, signCount, st, [&](int j) { return v[slots[a + j]]; },
-                             [&](int j, double2 w) { v[slots[a + j]] = w; });
+                collide_cell(P, s0, m, sign, signCount, st, [&](int j) { return S.vel(slots[a + j]); },
+                             [&](int j, double2 w) { S.set_vel(slots[a + j], w); });
         }
         return;
     }
     for (int i = t; i < B - A; i += blockDim.x) {
         const int sl = slots[A + i];
         ts[i] = sl;
-        tv[i] = v[sl];
+        tv[i] = S.vel(sl);
     }
     __syncthreads();
     if (t < nc) {
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, co
                          [&](int j, double2 w) { tv[a + j] = w; });
     }
     __syncthreads();
-    for (int i = t; i < B - A; i += blockDim.x) v[ts[i]] = tv[i];
+    for (int i = t; i < B - A; i += blockDim.x) S.set_vel(ts[i], tv[i]);
 }
 
 struct FieldsOut {
@@ -149,8 +150,9 @@ struct FieldsOut {
 };
 
 // compute_cell_fields (src/common_grid.cpp:32-100), one cell per thread.
-__global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, const int* __restrict__ slots,
-                              const double2* __restrict__ v, double rhoTarget, FieldsOut o, const int* skip = nullptr) {
+template <class V>
+__global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, const int* __restrict__ slots, V S,
+                              double rhoTarget, FieldsOut o, const int* skip = nullptr) {
     if (skip && *skip) return;  // a learned-closure step needs no reference fields
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= Pm.Nc) return;
@@ -158,7 +160,7 @@ __global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, 
     const int m = b - a;
     double px = 0.0, py = 0.0;
     for (int j = a; j < b; ++j) {
-        const double2 w = v[slots[j]];
+        const double2 w = S.vel(slots[j]);
         px = __dadd_rn(px, w.x);
         py = __dadd_rn(py, w.y);
     }
@@ -173,7 +175,7 @@ __global__ void k_cell_fields(DevParams Pm, const uint64_t* __restrict__ start, 
     if (dof > 0 && (o.T || o.Pkin || o.P)) {
         double s2 = 0.0;
         for (int j = a; j < b; ++j) {
-            const double2 w = v[slots[j]];
+            const double2 w = S.vel(slots[j]);
             const double ax = __dsub_rn(w.x, ux), ay = __dsub_rn(w.y, uy);
             s2 = __dadd_rn(s2, __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
         }

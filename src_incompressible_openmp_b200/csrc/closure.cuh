@@ -83,8 +83,9 @@ struct RedFields {
     double *Px, *Py, *Ux, *Uy;
     float4* feat;  // (N/gamma - 1, Ux, Uy, N) as FP32: the learned closure's stencil input
 };
-__global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
-                                const double2* __restrict__ v, const double* __restrict__ refPx,
+template <class V>
+__global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots, V S,
+                                const double* __restrict__ refPx,
                                 const double* __restrict__ refPy, const double* __restrict__ refUx,
                                 const double* __restrict__ refUy, RedFields red, double* __restrict__ duRX,
                                 double* __restrict__ duRY, double* __restrict__ cols, int* __restrict__ cellOf) {
@@ -94,7 +95,7 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
     const int m = b - a;
     double px = 0.0, py = 0.0;
     for (int j = a; j < b; ++j) {
-        const double2 w = v[slots[j]];
+        const double2 w = S.vel(slots[j]);
         px = __dadd_rn(px, w.x);
         py = __dadd_rn(py, w.y);
         if (cellOf) cellOf[j] = c;
@@ -186,11 +187,12 @@ __device__ __forceinline__ double beta_applied(const DevParams& P, double num, d
 // sum kn_rep^2, max kn_rep, hypot(beta*duR), sum kn_eos^2, max kn_eos, sum vin.x, sum vin.y,
 // sum vout.x - not used (momentum delta from vout sums) -> see column list in k_kick.
 constexpr int kKickCols = 9;
+// S: the red state (kicked in place unless permute); T: the next step's layout (permute)
+template <class V>
 __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const int* __restrict__ slots,
                        const double* __restrict__ numden, const double* __restrict__ duRX,
                        const double* __restrict__ duRY, const double* __restrict__ eosX,
-                       const double* __restrict__ eosY, const double2* __restrict__ x, double2* __restrict__ v,
-                       const int* __restrict__ pid, double2* __restrict__ xo, double2* __restrict__ vo,
+                       const double* __restrict__ eosY, V S, const int* __restrict__ pid, int permute, V T,
                        int* __restrict__ pido, double2* __restrict__ vrep, double* __restrict__ stats) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
@@ -201,16 +203,16 @@ __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const in
     double sinx = 0.0, siny = 0.0, soutx = 0.0, souty = 0.0;
     for (int j = a; j < b; ++j) {
         const int s = slots[j];
-        const double2 w = v[s];
+        const double2 w = S.vel(s);
         const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
         const double2 o = make_double2(__dadd_rn(r.x, ex), __dadd_rn(r.y, ey));
         if (vrep) vrep[s] = r;
-        if (vo) {
-            xo[j] = x[s];
-            vo[j] = o;
+        if (permute) {
+            T.copy_pos(j, S, s);
+            T.set_vel(j, o);
             pido[j] = pid[s];
         } else {
-            v[s] = o;
+            S.set_vel(s, o);
         }
         sinx = __dadd_rn(sinx, w.x);
         siny = __dadd_rn(siny, w.y);
@@ -236,32 +238,32 @@ __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const in
 
 // The two kicks for one index position j (flat, coalesced), writing the particle at
 // position j of the next step's layout: (cell, particle id) order.
+template <class V>
 __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, const int* __restrict__ slots,
                             const double* __restrict__ numden, const double* __restrict__ duRX,
                             const double* __restrict__ duRY, const double* __restrict__ eosX,
-                            const double* __restrict__ eosY, const double2* __restrict__ x,
-                            const double2* __restrict__ v, const int* __restrict__ pid, double2* __restrict__ xo,
-                            double2* __restrict__ vo, int* __restrict__ pido, const int* learned,
+                            const double* __restrict__ eosY, V S, const int* __restrict__ pid, V T,
+                            int* __restrict__ pido, const int* learned,
                             const double* __restrict__ duLX, const double* __restrict__ duLY,
                             const long long* __restrict__ duLSum) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const int c = cellOf[j];
     const int s = slots[j];
-    const double2 w = v[s];
+    const double2 w = S.vel(s);
     if (learned && *learned) {
         // the learned closure's kick less its particle mean (sum over cells of N du, int64 at
         // 2^-32), so that it leaves the total momentum unchanged
         const double mx = __ddiv_rn((double)duLSum[0] * 0x1p-32, (double)P.n);
         const double my = __ddiv_rn((double)duLSum[1] * 0x1p-32, (double)P.n);
-        vo[j] = make_double2(__dadd_rn(w.x, __dsub_rn(duLX[c], mx)), __dadd_rn(w.y, __dsub_rn(duLY[c], my)));
+        T.set_vel(j, make_double2(__dadd_rn(w.x, __dsub_rn(duLX[c], mx)), __dadd_rn(w.y, __dsub_rn(duLY[c], my))));
     } else {
         const double beta = beta_applied(P, numden[0], numden[1]);
         const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
         const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
-        vo[j] = make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c]));
+        T.set_vel(j, make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c])));
     }
-    xo[j] = x[s];
+    T.copy_pos(j, S, s);
     pido[j] = pid[s];
 }
 
@@ -272,10 +274,11 @@ __global__ void k_iota(int* __restrict__ a, int n) {
 }
 
 // per-particle sums for the step metrics: 0.5|v|^2, vx, vy (slot order; fixed reduction)
-__global__ void k_particle_cols(const double2* __restrict__ v, int n, double* __restrict__ cols) {
+template <class V>
+__global__ void k_particle_cols(V S, int n, double* __restrict__ cols) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double2 w = v[i];
+    const double2 w = S.vel(i);
     cols[3 * (size_t)i] = __dmul_rn(0.5, __dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y)));
     cols[3 * (size_t)i + 1] = w.x;
     cols[3 * (size_t)i + 2] = w.y;

@@ -61,6 +61,8 @@ struct DevParams {
     // (ddx+2) + 5*(ddy+2) -> angular bin of atan2(ddy, ddx) and hypot(ddx, ddy)
     int atanBin[25];
     double hypotTab[25];
+    // FP32 precision form: the largest FP32 offsets strictly inside a cell (x, y)
+    float offMaxX, offMaxY;
 };
 
 // Device-side seed table of one step (CUDA-graph replay: the step number lives on the
@@ -101,6 +103,62 @@ __device__ __forceinline__ int cell_of(double x, double y, const DevParams& P) {
     if (iy >= P.Ny) iy = P.Ny - 1;
     return iy + P.Ny * ix;
 }
+
+// ------------------------------------------------------------------ particle state views
+// The step's kernels read and write the slot-ordered particle state through a view.
+// View64, the plain form: FP64 positions and velocities (the reference's arithmetic, bit for
+// bit). View32, the FP32 precision form: per slot the standard-grid cell (int32), the
+// position inside that cell as FP32 offsets from the cell's lower corner, and FP32
+// velocities (8 + 4 + 8 bytes instead of 32). Loads widen to FP64 and all arithmetic stays
+// FP64; stores round to FP32 (positions relative to the cell, so to 2^-24 of a cell width).
+struct View64 {
+    double2* x;
+    double2* v;
+    static constexpr bool kF32 = false;
+    __device__ __forceinline__ double2 pos(int s, const DevParams&) const { return x[s]; }
+    // c: the standard-grid cell of X (cell_of), kept by the FP32 form
+    __device__ __forceinline__ void set_pos(int s, double2 X, int, const DevParams&) const { x[s] = X; }
+    __device__ __forceinline__ int std_cell(int s, const DevParams& P) const;
+    __device__ __forceinline__ double2 vel(int s) const { return v[s]; }
+    __device__ __forceinline__ void set_vel(int s, double2 V) const { v[s] = V; }
+    // position of slot s of src into slot j (a permutation keeps the stored bits)
+    __device__ __forceinline__ void copy_pos(int j, const View64& src, int s) const { x[j] = src.x[s]; }
+};
+
+struct View32 {
+    float2* off;
+    int* cell;
+    float2* v;
+    static constexpr bool kF32 = true;
+    __device__ __forceinline__ double2 pos(int s, const DevParams& P) const {
+        const int c = cell[s];
+        const int ix = c / P.Ny, iy = c - ix * P.Ny;
+        const float2 o = off[s];
+        return make_double2(__dadd_rn(__dmul_rn((double)ix, P.dx), (double)o.x),
+                            __dadd_rn(__dmul_rn((double)iy, P.dy), (double)o.y));
+    }
+    __device__ __forceinline__ void set_pos(int s, double2 X, int c, const DevParams& P) const {
+        const int ix = c / P.Ny, iy = c - ix * P.Ny;
+        const float ox = __double2float_rn(__dsub_rn(X.x, __dmul_rn((double)ix, P.dx)));
+        const float oy = __double2float_rn(__dsub_rn(X.y, __dmul_rn((double)iy, P.dy)));
+        off[s] = make_float2(fminf(fmaxf(ox, 0.0f), P.offMaxX), fminf(fmaxf(oy, 0.0f), P.offMaxY));
+        cell[s] = c;
+    }
+    __device__ __forceinline__ int std_cell(int s, const DevParams&) const { return cell[s]; }
+    __device__ __forceinline__ double2 vel(int s) const {
+        const float2 w = v[s];
+        return make_double2((double)w.x, (double)w.y);
+    }
+    __device__ __forceinline__ void set_vel(int s, double2 V) const {
+        v[s] = make_float2(__double2float_rn(V.x), __double2float_rn(V.y));
+    }
+    __device__ __forceinline__ void copy_pos(int j, const View32& src, int s) const {
+        off[j] = src.off[s];
+        cell[j] = src.cell[s];
+    }
+};
+
+__device__ __forceinline__ int View64::std_cell(int s, const DevParams& P) const { return cell_of(x[s].x, x[s].y, P); }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;

@@ -73,7 +73,22 @@ struct ZoneArgs {
     int liveEnd;
     const int* pid;           // particle id per slot
     double2* duScratch;       // momentum correction per cell of the running zone
+    // FP32 precision form (f32 != 0): the pass input and output states are these views and
+    // vin, xout, vout are unused
+    int f32;
+    View32 in32, out32;
 };
+
+// pass input / output velocities of slot s (kF32: the FP32 views, instantiated separately)
+template <bool kF32>
+__device__ __forceinline__ double2 zone_vin(const ZoneArgs& A, int s) { return kF32 ? A.in32.vel(s) : A.vin[s]; }
+template <bool kF32>
+__device__ __forceinline__ void zone_vout(const ZoneArgs& A, int s, double2 w) {
+    if (kF32)
+        A.out32.set_vel(s, w);
+    else
+        A.vout[s] = w;
+}
 
 // Working set of one zone; carved from shared memory (fast path, I = uint16_t: 16-bit
 // per-cell counts and arena offsets) or global memory (overflow path, I = int).
@@ -492,7 +507,7 @@ __device__ __forceinline__ void zone_normals(double* out, int cnt, ZoneMt& r, in
 }
 
 // Scalar (warp-uniform) state of one zone.
-template <typename I>
+template <typename I, bool kF32 = false>
 struct ZoneState {
     ZoneMem<I> M;
     ZoneMt rng;
@@ -664,8 +679,12 @@ struct ZoneState {
                 const int lc = (int)(e >> kEntryShift);
                 if (M.cflags[lc] & kCOwned) {
                     const int sl = (w < kWarp) ? pre : A->slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
-                    A->xout[sl] = make_double2(px, py);
-                    A->cid[sl] = cell_of(px, py, p);
+                    const int cc = cell_of(px, py, p);
+                    if (kF32)
+                        A->out32.set_pos(sl, make_double2(px, py), cc, p);
+                    else
+                        A->xout[sl] = make_double2(px, py);
+                    A->cid[sl] = cc;
                 }
                 M.arena[dst + q] = e;
             }
@@ -982,8 +1001,8 @@ struct ZoneState {
 };
 
 // global cell of window position w (zone rectangle plus a 2-cell ring, wrapped)
-template <typename I>
-__device__ __forceinline__ int iy_ix_cell(const ZoneState<I>& S, int w, const DevParams& p) {
+template <typename I, bool kF32>
+__device__ __forceinline__ int iy_ix_cell(const ZoneState<I, kF32>& S, int w, const DevParams& p) {
     int ix = S.xs - 2 + w / S.WY, iy = S.ys - 2 + w % S.WY;
     if (p.perx) ix = wrap_index(ix, p.Nx);
     if (p.pery) iy = wrap_index(iy, p.Ny);
@@ -992,8 +1011,8 @@ __device__ __forceinline__ int iy_ix_cell(const ZoneState<I>& S, int w, const De
 
 // End of a zone of the serial pass: apply the deferred momentum corrections, then publish
 // the new list (ascending particle id) and count of every cell the zone changed.
-template <typename I>
-__device__ __forceinline__ void serial_finish(ZoneState<I>& S, const ZoneArgs& A, const DevParams& p) {
+template <typename I, bool kF32>
+__device__ __forceinline__ void serial_finish(ZoneState<I, kF32>& S, const ZoneArgs& A, const DevParams& p) {
     ZoneMem<I>& M = S.M;
     const int lane = S.lane;
     for (int l = lane; l < S.nl; l += kWarp) {
@@ -1003,8 +1022,8 @@ __device__ __forceinline__ void serial_finish(ZoneState<I>& S, const ZoneArgs& A
             for (int j = 0; j < n; ++j) {
                 const uint32_t e = S.elem(l, j);
                 const int sl = A.slots[M.gstart[(int)(e >> kEntryShift)] + (int)(e & ((1u << kEntryShift) - 1))];
-                const double2 w = A.vin[sl];
-                A.vout[sl] = make_double2(__dadd_rn(w.x, du.x), __dadd_rn(w.y, du.y));
+                const double2 w = zone_vin<false>(A, sl);
+                zone_vout<false>(A, sl, make_double2(__dadd_rn(w.x, du.x), __dadd_rn(w.y, du.y)));
             }
         }
     }
@@ -1054,9 +1073,9 @@ __device__ __forceinline__ void serial_finish(ZoneState<I>& S, const ZoneArgs& A
 
 // ------------------------------------------------------------------ the zone body
 // Returns false if the zone must be re-run on the overflow path.
-template <bool kSerial, typename I>
+template <bool kSerial, typename I, bool kF32 = false>
 __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap, int nsmCap) {
-    ZoneState<I> S;
+    ZoneState<I, kF32> S;
     S.A = &A;
     S.lane = threadIdx.x & 31;
     S.zone = z;
@@ -1184,7 +1203,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
 #pragma unroll
                 for (int u = 0; u < 8; ++u) sl[u] = (j0 + u < n0) ? A.slots[g0 + j0 + u] : 0;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n0) ? A.vin[sl[u]] : make_double2(0.0, 0.0);
+                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n0) ? zone_vin<kF32>(A, sl[u]) : make_double2(0.0, 0.0);
 #pragma unroll
                 for (int u = 0; u < 8; ++u)
                     if (j0 + u < n0) {
@@ -1204,7 +1223,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n) ? A.vin[sl[u]] : make_double2(0.0, 0.0);
+                for (int u = 0; u < 8; ++u) w[u] = (j0 + u < n) ? zone_vin<kF32>(A, sl[u]) : make_double2(0.0, 0.0);
 #pragma unroll
                 for (int u = 0; u < 8; ++u)
                     if (j0 + u < n) {
@@ -1227,8 +1246,8 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
                     const int lc = (int)(e >> kEntryShift);
                     if (!(M.cflags[lc] & kCOwned)) continue;
                     const int sl = A.slots[M.gstart[lc] + (int)(e & ((1u << kEntryShift) - 1))];
-                    const double2 w = A.vin[sl];
-                    A.vout[sl] = make_double2(__dadd_rn(w.x, ux), __dadd_rn(w.y, uy));
+                    const double2 w = zone_vin<kF32>(A, sl);
+                    zone_vout<kF32>(A, sl, make_double2(__dadd_rn(w.x, ux), __dadd_rn(w.y, uy)));
                 }
             }
         }
@@ -1260,11 +1279,13 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     return true;
 }
 
+// kF32: the FP32 precision form's state (A.in32, A.out32)
+template <bool kF32>
 __global__ void __launch_bounds__(32, 20) k_zone_pass(ZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     if ((int)blockIdx.x >= A.nZones) return;
     const int z = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
-    if (!zone_body<false, uint16_t>(A, z, smem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap) && (threadIdx.x & 31) == 0)
+    if (!zone_body<false, uint16_t, kF32>(A, z, smem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap) && (threadIdx.x & 31) == 0)
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
@@ -1307,10 +1328,11 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 
 // zones that did not fit the shared-memory working set, re-run from their seed with a
 // global-memory working set per block (deterministic: identical decisions and writes)
+template <bool kF32>
 __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock) {
     const int nov = *A.nOverflow;
     for (int i = blockIdx.x; i < nov; i += gridDim.x)
-        if (!zone_body<false, int>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap,
+        if (!zone_body<false, int, kF32>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap,
                                    A.nsmCap) &&
             (threadIdx.x & 31) == 0)
             raise_error(A.st, kErrZoneCapacity, A.overflow[i]);

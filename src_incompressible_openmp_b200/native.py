@@ -53,6 +53,7 @@ def lib():
         "mpcd_read_params_kv": ([C.c_char_p, P(_abi.ParamsC)], C.c_int),
         "mpcd_read_kv_string": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_int], C.c_int),
         "mpcd_ctx_create": ([P(_abi.ParamsC), C.c_int, P(C.c_void_p)], C.c_int),
+        "mpcd_ctx_create_form": ([P(_abi.ParamsC), C.c_int, C.c_int32, P(C.c_void_p)], C.c_int),
         "mpcd_ctx_destroy": ([C.c_void_p], C.c_int),
         "mpcd_ctx_stream": ([C.c_void_p], C.c_void_p),
         "mpcd_set_state": ([C.c_void_p, _dp, _dp, C.c_int64], C.c_int),
@@ -160,16 +161,21 @@ def cell_fields_static(params, x_ptr, v_ptr, n, rho_target, out_ptrs, stream=0):
                                          C.byref(s), C.c_void_p(stream)))
 
 
-class Context:
-    """A device-resident MPCD state for one parameter set (one GPU)."""
+FORMS = {"f64": 0, "f32": 1}  # mpcd_state_form
 
-    def __init__(self, params, device=0):
+
+class Context:
+    """A device-resident MPCD state for one parameter set (one GPU). form "f64" is the plain
+    form; "f32" the FP32 precision form (whole steps and state I/O only)."""
+
+    def __init__(self, params, device=0, form="f64"):
         self.params = dict(params)
         self.n = int(params["n"])
         self.Nc = int(params["Nc"])
+        self.form = form
         self._pc = to_c(params)
         h = C.c_void_p()
-        _check(lib().mpcd_ctx_create(C.byref(self._pc), device, C.byref(h)))
+        _check(lib().mpcd_ctx_create_form(C.byref(self._pc), device, FORMS[form], C.byref(h)))
         self.h = h
 
     def close(self):
