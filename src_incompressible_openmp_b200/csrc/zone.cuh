@@ -110,7 +110,7 @@ struct ZoneMem {
     uint16_t* order;   // cell: arena order of materialised lists (compaction)
     uint32_t* arena;   // arenaCap
     int* small;        // 64 ints: ranked targets, donors
-    double* smallD;    // 8 doubles: donor normals
+    double* smallD;    // 24 doubles: donor normals, their polar components and radii
 
     __host__ __device__ static size_t bytes(int maxCells, int winCap, int arenaCap, int nsmCap) {
         size_t b = 0;
@@ -126,7 +126,7 @@ struct ZoneMem {
         add((size_t)maxCells * 2, 2);
         add((size_t)arenaCap * 4, 4);
         add(64 * 4, 4);
-        add(8 * 8, 8);
+        add(24 * 8, 8);
         return (b + 15) / 16 * 16;
     }
     __device__ void carve(char* base, int maxCells, int winCap, int arenaCap, int nsmCap) {
@@ -152,7 +152,7 @@ struct ZoneMem {
         order = (uint16_t*)take((size_t)maxCells * 2, 2);
         arena = (uint32_t*)take((size_t)arenaCap * 4, 4);
         small = (int*)take(64 * 4, 4);
-        smallD = (double*)take(8 * 8, 8);
+        smallD = (double*)take(24 * 8, 8);
     }
 };
 
@@ -479,8 +479,11 @@ __device__ __noinline__ double zone_hypot(double a, double b) { return mpcd_dd::
 
 // cnt deviates of one fresh normal_distribution (polar method: pairs of uniforms in stream
 // order until r2 is in (0, 1]; each accepted pair gives y*m, then the cached x*m) into out[].
-// Lane c examines candidate pair c of the batch; the accepted ones are ranked by ballot.
-__device__ __forceinline__ void zone_normals(double* out, int cnt, ZoneMt& r, int lane) {
+// Lane c examines candidate pair c of the batch; the accepted ones are ranked by ballot. The
+// polar scale m uses the CUDA log (a few ulp from the correctly rounded one); comp and rad
+// keep each deviate's polar component and r2, so that the exact deviate can be rebuilt as
+// comp * polar_scale(r2).
+__device__ __forceinline__ void zone_normals_fast(double* out, double* comp, double* rad, int cnt, ZoneMt& r, int lane) {
     int got = 0;
     while (got < cnt) {
         r.ensure(2 * kWarp);
@@ -495,10 +498,16 @@ __device__ __forceinline__ void zone_normals(double* out, int cnt, ZoneMt& r, in
         int last = kWarp - 1;
         if (__popc(am) >= need) last = __ffs(__ballot_sync(0xffffffffu, acc && rank == need - 1)) - 1;
         if (acc && rank < need) {
-            const double mult = polar_scale(r2);
+            const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
             const int k0 = got + 2 * rank;
             out[k0] = __dmul_rn(y, mult);
-            if (k0 + 1 < cnt) out[k0 + 1] = __dmul_rn(x, mult);
+            comp[k0] = y;
+            rad[k0] = r2;
+            if (k0 + 1 < cnt) {
+                out[k0 + 1] = __dmul_rn(x, mult);
+                comp[k0 + 1] = x;
+                rad[k0 + 1] = r2;
+            }
         }
         r.consume(2 * (last + 1));
         got += 2 * used;
@@ -514,6 +523,9 @@ struct ZoneState {
     const ZoneArgs* A;
     int lane, zone;
     int xs, xe, ys, ye, TX, TY, nl, WY;
+    // l / TY as (l * tyMagic) >> 32, tyMagic = ceil(2^32 / TY) (2^32 for TY = 1): exact for
+    // l * TY < 2^32, which the 16-bit working set guarantees (l, TY < 2^16); the int path divides
+    unsigned long long tyMagic;
     int arenaTop, arenaCap;
     int movedDense, movedSparse;
     int atanLane;   // lane k < 25 holds the angular bin of step k (DevParams::atanBin)
@@ -526,8 +538,11 @@ struct ZoneState {
     __device__ __forceinline__ const DevParams& P() const { return A->P; }
     __device__ __forceinline__ bool in_zone(int ix, int iy) const { return ix >= xs && ix < xe && iy >= ys && iy < ye; }
     __device__ __forceinline__ int loc(int ix, int iy) const { return (ix - xs) * TY + (iy - ys); }
-    __device__ __forceinline__ int gx_of(int l) const { return xs + l / TY; }
-    __device__ __forceinline__ int gy_of(int l) const { return ys + l % TY; }
+    __device__ __forceinline__ int lx_of(int l) const {
+        return (sizeof(I) == 2) ? (int)(((unsigned long long)(unsigned)l * tyMagic) >> 32) : l / TY;
+    }
+    __device__ __forceinline__ int gx_of(int l) const { return xs + lx_of(l); }
+    __device__ __forceinline__ int gy_of(int l) const { return ys + (l - lx_of(l) * TY); }
 
     __device__ __forceinline__ int cnt_at(int ix, int iy) const {
         if (in_zone(ix, iy)) return M.len[loc(ix, iy)];
@@ -946,24 +961,39 @@ struct ZoneState {
         double gx, gy;
         inward(l, gx, gy);
         zone_shuffle_fast(don, nd, rng, lane);
-        const double ndir = zone_hypot(gx, gy);
-        // one N(0,1) per donor in shuffled order, then scores in parallel (lane k = donor k)
+        // one N(0,1) per donor in shuffled order, then scores in parallel (lane k = donor k).
+        // The scores only rank the donors: they are computed first with the CUDA hypot and
+        // log, and again with the correctly rounded ones (the reference's values) only if two
+        // scores lie closer than those functions' few-ulp differences could move them.
         double* nrm = M.smallD;
-        zone_normals(nrm, nd, rng, lane);
+        zone_normals_fast(nrm, M.smallD + 8, M.smallD + 16, nd, rng, lane);
         int dk = -1, idx = 0, ddx = 0, ddy = 0;
         if (lane < nd) {
             dk = don[lane];
             idx = step_index(ix, iy, gx_of(dk), gy_of(dk), ddx, ddy);
         }
         const double hs = __shfl_sync(0xffffffffu, hypLane, idx < 0 ? 0 : idx);
-        double sc = 0.0;
-        if (lane < nd) {
+        const double nsmd = (lane < nd) ? M.nsm[nsm_index(gx_of(dk), gy_of(dk))] : 0.0;
+        auto score = [&](double ndir, double nv) {
             const double nstep = (idx >= 0) ? hs : 0.0;
             double align = 0.0;
             if (ndir >= 1e-14 && nstep >= 1e-14)
                 align = __ddiv_rn(__dadd_rn(__dmul_rn((double)ddx, gx), __dmul_rn((double)ddy, gy)), __dmul_rn(ndir, nstep));
-            const double noise = __dmul_rn(1e-9, nrm[lane]);
-            sc = __dadd_rn(__dadd_rn(__dmul_rn(100.0, align), M.nsm[nsm_index(gx_of(dk), gy_of(dk))]), noise);
+            const double noise = __dmul_rn(1e-9, nv);
+            return __dadd_rn(__dadd_rn(__dmul_rn(100.0, align), nsmd), noise);
+        };
+        const double ndirF = hypot(gx, gy);
+        double sc = (lane < nd) ? score(ndirF, nrm[lane]) : 0.0;
+        // the fast and exact scores differ by under 2e-13 (1 + |score|): distinct ranks are
+        // certain when every gap exceeds 1e-12 (1 + |score|) and the norm is clear of 1e-14
+        bool sure = !(ndirF > 0.5e-14 && ndirF < 2e-14);
+        for (int j = 0; j < nd; ++j) {
+            const double sj = __shfl_sync(0xffffffffu, sc, j);
+            if (lane < nd && j != lane && fabs(sj - sc) <= 1e-12 * (1.0 + fabs(sc))) sure = false;
+        }
+        if (!__all_sync(0xffffffffu, sure)) {
+            const double ndir = zone_hypot(gx, gy);
+            if (lane < nd) sc = score(ndir, __dmul_rn(M.smallD[8 + lane], polar_scale(M.smallD[16 + lane])));
         }
         // descending, ties in shuffled order (std::sort of <= 16 elements is an insertion sort)
         int rk = 0;
@@ -1087,12 +1117,15 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     const int4 R = A.rects[z];
     S.xs = R.x; S.xe = R.y; S.ys = R.z; S.ye = R.w;
     S.TX = S.xe - S.xs; S.TY = S.ye - S.ys; S.nl = S.TX * S.TY; S.WY = S.TY + 4;
+    S.tyMagic = (S.TY > 0) ? ((1ULL << 32) + (unsigned long long)S.TY - 1ULL) / (unsigned long long)S.TY : 0ULL;
     S.atanLane = (lane < 25) ? p.atanBin[lane] : 0;
     S.hypLane = (lane < 25) ? p.hypotTab[lane] : 0.0;
     S.dupNb5 = (p.perx && p.Nx < 5) || (p.pery && p.Ny < 5);
     S.dupNb3 = (p.perx && p.Nx < 3) || (p.pery && p.Ny < 3);
     const int W = (S.TX + 4) * S.WY;
-    if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > nsmCap || S.nl >= (1 << (32 - kEntryShift))) return false;
+    if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > nsmCap || S.nl >= (1 << (32 - kEntryShift)) ||
+        (sizeof(I) == 2 && S.nl > 65535))
+        return false;
     S.M.carve(mem, maxCells, winCap, arenaCap, nsmCap);
     constexpr bool kNarrow = sizeof(I) == 2;  // 16-bit counts: window counts <= 32767, zone total <= 65535
     bool wide = false;
