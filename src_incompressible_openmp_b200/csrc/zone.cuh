@@ -530,6 +530,7 @@ struct ZoneState {
     int movedDense, movedSparse;
     int atanLane;   // lane k < 25 holds the angular bin of step k (DevParams::atanBin)
     double hypLane; // lane k < 25 holds the length of step k (DevParams::hypotTab)
+    bool nbDirect;  // no wrapped neighbour (|offset| <= 2) of a zone cell lies in the zone
     bool dupNb5;    // a periodic axis shorter than 5 cells: range-2 neighbours can coincide
     bool dupNb3;    // a periodic axis shorter than 3 cells: 8-neighbours can coincide
     bool failed;   // capacity exhausted: the zone is handed to the overflow path
@@ -749,7 +750,7 @@ struct ZoneState {
             const int kk = (lane < 12) ? lane : lane + 1;
             const int dy = kk / 5 - 2, dx = kk % 5 - 2;
             int jy, jx;
-            if (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy)) {
+            if (nbDirect ? in_zone(jx = ix + dx, jy = iy + dy) : (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy))) {
                 const int t = loc(jx, jy);
                 if ((double)M.len[t] < map_val(t, low)) nb = t;
             }
@@ -940,7 +941,8 @@ struct ZoneState {
             const int kk = (lane < 4) ? lane : lane + 1;
             const int dy = kk / 3 - 1, dx = kk % 3 - 1;
             int jy, jx;
-            if (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy)) nb = loc(jx, jy);
+            if (nbDirect ? in_zone(jx = ix + dx, jy = iy + dy) : (shift_index(iy, ix, dy, dx, jy, jx) && in_zone(jx, jy)))
+                nb = loc(jx, jy);
         }
         const unsigned m0 = __ballot_sync(0xffffffffu, nb >= 0);
         if (m0 == 0) return;
@@ -1121,6 +1123,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     S.atanLane = (lane < 25) ? p.atanBin[lane] : 0;
     S.hypLane = (lane < 25) ? p.hypotTab[lane] : 0.0;
     S.dupNb5 = (p.perx && p.Nx < 5) || (p.pery && p.Ny < 5);
+    S.nbDirect = (!p.perx || S.TX < p.Nx - 2) && (!p.pery || S.TY < p.Ny - 2);
     S.dupNb3 = (p.perx && p.Nx < 3) || (p.pery && p.Ny < 3);
     const int W = (S.TX + 4) * S.WY;
     if (S.nl > maxCells || W > winCap || (S.TX + 2) * (S.TY + 2) > nsmCap || S.nl >= (1 << (32 - kEntryShift)) ||
