@@ -158,6 +158,8 @@ struct mpcd_ctx {
     double* duLY = nullptr;
     unsigned long long* duLSum = nullptr;  // sum over cells of N du (x, y), int64 at 2^-32
     float4* redFeat = nullptr;  // per cell of the red state: (N/gamma - 1, Ux, Uy, 0)
+    ZoneArgs zA{};             // the zone pass in progress (zone_pass_prep .. zone_pass_finish)
+    int zMode = 0;
     int* zoneCost = nullptr;   // per zone: cost bucket
     int* zoneHist = nullptr;   // kCostBuckets
     int* zoneOrder = nullptr;  // launch order, heaviest first
@@ -692,7 +694,10 @@ int run_save_ref(mpcd_ctx* c, Prof* pf = nullptr, bool inStep = false) {
     return MPCD_OK;
 }
 
-int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) {
+// The snapshot pass in three parts, so that a batch can run the middle one for all its
+// replicas in one launch: prep (index, seeds, output copies, launch order; fills c->zA),
+// the zone kernel, and finish (overflow zones, metrics, state flags).
+int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) {
     if (!c->cidStdValid) {
         WITH_VIEW(c->xv, k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, S, c->cidStd)); ++c->launches;
         c->cidStdValid = true;
@@ -747,12 +752,26 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
                                                                    c->zoneHist); ++c->launches;
     k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
     A.order = c->zoneOrder;
+    CUDA_TRY(cudaGetLastError());
+    c->zA = A;
+    c->zMode = mode;
+    return MPCD_OK;
+}
+
+int zone_pass_kernel(mpcd_ctx* c) {
+    const ZoneArgs& A = c->zA;
     if (c->f32)
-        k_zone_pass<true><<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+        k_zone_pass<true><<<A.nZones, 32, c->zSmem, c->stream>>>(A);
     else
-        k_zone_pass<false><<<L.nZones, 32, c->zSmem, c->stream>>>(A);
+        k_zone_pass<false><<<A.nZones, 32, c->zSmem, c->stream>>>(A);
     ++c->launches;
     CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
+    const ZoneArgs& A = c->zA;
+    const int mode = c->zMode;
     ZoneArgs B = A;
     B.order = nullptr;
     B.maxCells = c->ovMaxCells;
@@ -764,13 +783,20 @@ int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) 
     else
         k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
     ++c->launches;
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, A.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 8);
     c->xv ^= 1;
     c->idxStdValid = false;  // cid was updated for moved particles; positions changed
     c->srdCellsValid = false;
     return MPCD_OK;
+}
+
+int run_zone_pass(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr) {
+    int rc = zone_pass_prep(c, mode, seedBase, pf);
+    if (!rc) rc = zone_pass_kernel(c);
+    if (!rc) rc = zone_pass_finish(c, pf);
+    return rc;
 }
 
 __global__ void k_live_init(const uint64_t* __restrict__ start, int Nc, int* __restrict__ cnt, int* __restrict__ st,
@@ -1558,7 +1584,11 @@ static int count_metrics(mpcd_ctx* c, double* dst /* device: 3 doubles */) {
 
 // One iteration of the profiled benchmark loop (reference
 // src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:241-279) with its seeds.
-static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr) {
+// The step in three parts around its two zone kernels: head (stream, walls, collision,
+// reference fields, base-pass prep), mid (base-pass finish, shifted-pass prep), tail
+// (shifted-pass finish, closure and re-sort). step_once runs them with each replica's own
+// zone kernels; a batch runs the zone kernels of all its replicas in one launch.
+static int step_head(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     const uint64_t s = (uint64_t)step;
     int rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
@@ -1578,7 +1608,12 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     rc = run_save_ref(c, pf, true);
     if (rc) return rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
-    rc = run_zone_pass(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s, pf);
+    return zone_pass_prep(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s, pf);
+}
+
+static int step_mid(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
+    const uint64_t s = (uint64_t)step;
+    int rc = zone_pass_finish(c, pf);
     if (rc) return rc;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
@@ -1588,7 +1623,11 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
         if (rc) return rc;
         CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
     }
-    rc = run_zone_pass(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s, pf);
+    return zone_pass_prep(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s, pf);
+}
+
+static int step_tail(mpcd_ctx* c, bool metrics, Prof* pf) {
+    int rc = zone_pass_finish(c, pf);
     if (rc) return rc;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[4], c->stream));
@@ -1623,6 +1662,15 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
     }
     if (c->graphMode) CUDA_TRY(cudaStreamWaitEvent(c->stream, c->sideDone, 0));  // join the sign prefetch
     return MPCD_OK;
+}
+
+static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr) {
+    int rc = step_head(c, step, metrics, pf);
+    if (!rc) rc = zone_pass_kernel(c);
+    if (!rc) rc = step_mid(c, step, metrics, pf);
+    if (!rc) rc = zone_pass_kernel(c);
+    if (!rc) rc = step_tail(c, metrics, pf);
+    return rc;
 }
 
 // A step replayed from a CUDA graph. The graph of each entry parity of the ping-pong
@@ -1990,9 +2038,133 @@ struct mpcd_batch {
     int device = 0;
     std::vector<mpcd_ctx*> members;
     cudaStream_t stream = nullptr;  // timing and the fork/join of the members' streams
-    cudaEvent_t start = nullptr, stop = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr, fork = nullptr;
     std::vector<cudaEvent_t> done;
+    // the zone kernels of all replicas as one launch per pass: arguments and zone-count prefix
+    // sums per (buffer parity, pass), staged in page-locked memory (constant per slot, so a
+    // captured copy replays correctly) and copied to the device before the launch
+    ZoneArgs* hArgs = nullptr;
+    int* hOffs = nullptr;
+    ZoneArgs* dArgs = nullptr;
+    int* dOffs = nullptr;
+    size_t zSmem = 0;
+    // whole batched steps replayed from CUDA graphs, one per buffer parity of the replicas
+    bool useGraphs = true;
+    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<mpcd_ctx::HostFlags> gpost[4];
+    std::vector<int64_t> gkernels[4];
+    long long** dStepPtrs = nullptr;  // each replica's device step counter
 };
+
+__global__ void k_set_steps(long long** steps, int n, long long value) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) *steps[i] = value;
+}
+
+// the zone kernels of pass `pass` (0 base, 1 shifted) of every replica in one launch; each
+// replica's zone_pass_prep has filled its zA
+static int batch_zone_kernel(mpcd_batch* b, int pass) {
+    const int n = (int)b->members.size();
+    const int slot = (b->members[0]->xv & 1) * 2 + pass;
+    ZoneArgs* h = b->hArgs + (size_t)slot * n;
+    int* ho = b->hOffs + (size_t)slot * (n + 1);
+    ho[0] = 0;
+    for (int r = 0; r < n; ++r) {
+        h[r] = b->members[r]->zA;
+        ho[r + 1] = ho[r] + h[r].nZones;
+    }
+    ZoneArgs* d = b->dArgs + (size_t)slot * n;
+    int* dof = b->dOffs + (size_t)slot * (n + 1);
+    CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(ZoneArgs) * n, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaMemcpyAsync(dof, ho, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+    if (ho[n] > 0) {
+        k_zone_pass_batch<false><<<ho[n], 32, b->zSmem, b->stream>>>(d, dof, n);
+        ++b->members[0]->launches;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+// one batched step: each replica's parts on its own streams, the zone kernels of all
+// replicas as one launch per pass on the batch stream (fork/join by events)
+static int batch_step_body(mpcd_batch* b, int64_t step) {
+    const int n = (int)b->members.size();
+    int rc;
+    for (int part = 0; part < 3; ++part) {
+        CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+        for (int r = 0; r < n; ++r) {
+            mpcd_ctx* c = b->members[r];
+            CUDA_TRY(cudaStreamWaitEvent(c->stream, b->fork, 0));
+            rc = part == 0 ? step_head(c, step, false, nullptr) : part == 1 ? step_mid(c, step, false, nullptr)
+                                                                         : step_tail(c, false, nullptr);
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(b->done[r], c->stream));
+            CUDA_TRY(cudaStreamWaitEvent(b->stream, b->done[r], 0));
+        }
+        if (part < 2) {
+            rc = batch_zone_kernel(b, part);
+            if (rc) return rc;
+        }
+    }
+    return MPCD_OK;
+}
+
+// a batched step replayed from the graph of the replicas' buffer parity (captured on first
+// use); every replica's sign stream must have been prefetched by the step before
+static int batch_graph_step(mpcd_batch* b, int64_t step) {
+    const int n = (int)b->members.size();
+    mpcd_ctx* c0 = b->members[0];
+    const int key = c0->xv * 2 + c0->pp;
+    if (!b->gexec[key]) {
+        std::vector<int64_t> l0(n);
+        for (int r = 0; r < n; ++r) l0[r] = b->members[r]->launches;
+        CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        for (mpcd_ctx* c : b->members) c->graphMode = true;
+        const int rc = batch_step_body(b, step);
+        for (mpcd_ctx* c : b->members) c->graphMode = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc != MPCD_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != MPCD_OK ? rc : set_err(MPCD_ERR_CUDA, std::string("batch step capture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&b->gexec[key], g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            b->gexec[key] = nullptr;
+            cudaGetLastError();
+            return set_err(MPCD_ERR_CUDA, std::string("batch step graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        b->gpost[key].resize(n);
+        b->gkernels[key].resize(n);
+        for (int r = 0; r < n; ++r) {
+            mpcd_ctx* c = b->members[r];
+            b->gkernels[key][r] = c->launches - l0[r];
+            c->launches = l0[r];
+            b->gpost[key][r] = {c->xv, c->pp, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
+        }
+    }
+    for (int r = 0; r < n; ++r) {
+        mpcd_ctx* c = b->members[r];
+        const mpcd_ctx::HostFlags& f = b->gpost[key][r];
+        c->xv = f.xv;
+        c->pp = f.pp;
+        c->cidStdValid = f.cidStdValid;
+        c->srdCellsValid = f.srdCellsValid;
+        c->idxStdValid = f.idxStdValid;
+        c->refValid = f.refValid;
+        CUDA_TRY(cudaStreamWaitEvent(b->stream, c->signsReady[step & 1], 0));
+    }
+    k_set_steps<<<(n + 255) / 256, 256, 0, b->stream>>>(b->dStepPtrs, n, (long long)(step - 1));
+    CUDA_TRY(cudaGraphLaunch(b->gexec[key], b->stream));
+    for (int r = 0; r < n; ++r) {
+        mpcd_ctx* c = b->members[r];
+        c->launches += b->gkernels[key][r];
+        c->signsStep[(step + 1) & 1] = step + 1;
+    }
+    return MPCD_OK;
+}
 
 extern "C" {
 
@@ -2005,6 +2177,15 @@ int mpcd_ctx_set_graphs(mpcd_ctx* c, int enable) {
 int mpcd_batch_destroy(mpcd_batch* b) {
     if (!b) return MPCD_OK;
     cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& g : b->gexec)
+        if (g) cudaGraphExecDestroy(g);
+    if (b->hArgs) cudaFreeHost(b->hArgs);
+    if (b->hOffs) cudaFreeHost(b->hOffs);
+    if (b->dArgs) cudaFree(b->dArgs);
+    if (b->dOffs) cudaFree(b->dOffs);
+    if (b->dStepPtrs) cudaFree(b->dStepPtrs);
+    if (b->fork) cudaEventDestroy(b->fork);
     for (mpcd_ctx* c : b->members) mpcd_ctx_destroy(c);
     for (cudaEvent_t e : b->done)
         if (e) cudaEventDestroy(e);
@@ -2031,10 +2212,34 @@ int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_b
         b->members.push_back(c);
     }
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->start) != cudaSuccess || cudaEventCreate(&b->stop) != cudaSuccess) {
+        cudaEventCreate(&b->start) != cudaSuccess || cudaEventCreate(&b->stop) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         mpcd_batch_destroy(b);
         return set_err(MPCD_ERR_CUDA, "batch stream");
+    }
+    {
+        // staging of the batched zone kernels (4 slots: buffer parity x pass), the shared
+        // memory of the largest working set plus the arguments, the step counters
+        const size_t nslots = 4;
+        std::vector<long long*> steps((size_t)count);
+        for (int r = 0; r < count; ++r) {
+            b->zSmem = std::max(b->zSmem, b->members[r]->zSmem + (size_t)kZoneArgsSmem);
+            steps[(size_t)r] = b->members[r]->dStep;
+        }
+        if (cudaMallocHost((void**)&b->hArgs, sizeof(ZoneArgs) * count * nslots) != cudaSuccess ||
+            cudaMallocHost((void**)&b->hOffs, sizeof(int) * (count + 1) * nslots) != cudaSuccess ||
+            cudaMalloc((void**)&b->dArgs, sizeof(ZoneArgs) * count * nslots) != cudaSuccess ||
+            cudaMalloc((void**)&b->dOffs, sizeof(int) * (count + 1) * nslots) != cudaSuccess ||
+            cudaMalloc((void**)&b->dStepPtrs, sizeof(long long*) * count) != cudaSuccess ||
+            cudaMemcpy(b->dStepPtrs, steps.data(), sizeof(long long*) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+            (b->zSmem > 48 * 1024 &&
+             cudaFuncSetAttribute(k_zone_pass_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->zSmem) !=
+                 cudaSuccess)) {
+            cudaGetLastError();
+            mpcd_batch_destroy(b);
+            return set_err(MPCD_ERR_CUDA, "batch zone-pass staging");
+        }
     }
     b->done.assign((size_t)count, nullptr);
     for (auto& e : b->done)
@@ -2063,11 +2268,16 @@ int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device
     CUDA_TRY(cudaSetDevice(b->device));
     CUDA_TRY(cudaEventRecord(b->start, b->stream));
     for (mpcd_ctx* c : b->members) CUDA_TRY(cudaStreamWaitEvent(c->stream, b->start, 0));
-    for (int64_t k = 1; k <= nsteps; ++k)
-        for (mpcd_ctx* c : b->members) {
-            const int rc = run_steps(c, step0 + k - 1, 1, false);
-            if (rc) return rc;
-        }
+    for (int64_t k = 1; k <= nsteps; ++k) {
+        const int64_t s = step0 + k;
+        // the graph needs every replica's sign stream prefetched and one common buffer parity
+        bool graph = b->useGraphs;
+        for (mpcd_ctx* c : b->members)
+            graph = graph && c->useGraphs && c->signsStep[s & 1] == s && c->xv == b->members[0]->xv &&
+                    c->pp == b->members[0]->pp;
+        const int rc = graph ? batch_graph_step(b, s) : batch_step_body(b, s);
+        if (rc) return rc;
+    }
     for (size_t i = 0; i < b->members.size(); ++i) {
         mpcd_ctx* c = b->members[i];
         CUDA_TRY(cudaEventRecord(b->done[i], c->stream));

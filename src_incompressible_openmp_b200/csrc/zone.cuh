@@ -1325,6 +1325,35 @@ __global__ void __launch_bounds__(32, 20) k_zone_pass(ZoneArgs A) {
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
+// The zone pass of several replicas in one launch. Block b runs the zone at launch position
+// b - offs[r] of replica r, offs being the prefix sums of the replicas' zone counts; the
+// replica's arguments are copied into shared memory ahead of the zone's working set.
+constexpr int kZoneArgsSmem = (int)((sizeof(ZoneArgs) + 15) / 16 * 16);
+template <bool kF32>
+__global__ void __launch_bounds__(32, 20) k_zone_pass_batch(const ZoneArgs* __restrict__ args, const int* __restrict__ offs,
+                                                            int nRep) {
+    extern __shared__ __align__(16) char smem[];
+    const int b = (int)blockIdx.x;
+    if (nRep <= 0 || b >= offs[nRep]) return;
+    int lo = 0, hi = nRep - 1;  // the replica r with offs[r] <= b < offs[r + 1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offs[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    static_assert(sizeof(ZoneArgs) % 8 == 0, "ZoneArgs is copied in 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(args + lo);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(smem);
+    for (int i = (int)threadIdx.x; i < (int)(sizeof(ZoneArgs) / 8); i += 32) dst[i] = src[i];
+    __syncwarp();
+    const ZoneArgs& A = *reinterpret_cast<const ZoneArgs*>(smem);
+    const int local = b - offs[lo];
+    const int z = A.order ? A.order[local] : local;
+    if (!zone_body<false, uint16_t, kF32>(A, z, smem + kZoneArgsSmem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap) &&
+        (threadIdx.x & 31) == 0)
+        A.overflow[atomicAdd(A.nOverflow, 1)] = z;
+}
+
 // Launch order of the zones, heaviest first, so that the last wave of blocks holds the
 // cheapest zones. The cost estimate is the number of particles above the bulk high threshold
 // in the zone's cells (the dense-phase work); ties keep no particular order, which is fine:

@@ -46,15 +46,19 @@ def test_batch_equals_replicas_alone(oracle):
         alone.append(outs)
     for (xa, va), (xb, vb) in zip(*alone):  # graph replay = eager steps, bit for bit
         assert np.array_equal(xa, xb) and np.array_equal(va, vb)
-    with native.Batch([c[0] for c in cases]) as B:
-        for i, (p, x, v) in enumerate(cases):
-            B.member(i).set_state(x, v)
-        t = B.step(0, 2)
-        t += B.step(2, nsteps - 2)
-        assert t > 0.0
-        for i in range(len(cases)):
-            xg, vg = B.member(i).get_state()
-            assert np.array_equal(xg, alone[0][i][0]) and np.array_equal(vg, alone[0][i][1]), i
+    # batched steps (the zone kernels of all replicas in one launch per pass), replayed from
+    # the batch's graph after the first step, or eager when a member has graphs off
+    for graphs in (True, False):
+        with native.Batch([c[0] for c in cases]) as B:
+            for i, (p, x, v) in enumerate(cases):
+                B.member(i).set_state(x, v)
+                B.member(i).set_graphs(graphs)
+            t = B.step(0, 2)
+            t += B.step(2, nsteps - 2)
+            assert t > 0.0
+            for i in range(len(cases)):
+                xg, vg = B.member(i).get_state()
+                assert np.array_equal(xg, alone[0][i][0]) and np.array_equal(vg, alone[0][i][1]), (graphs, i)
     # the first replica against the oracle (free run: one-ulp thermal draws may propagate)
     p, x, v = cases[0]
     xo, vo = x, v
