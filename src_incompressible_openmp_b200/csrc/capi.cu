@@ -435,6 +435,11 @@ int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out, cudaStre
              uint64_t* sums = nullptr) {
     if (!s) s = c->stream;
     if (!sums) sums = c->blockSums;
+    if (n <= kSmallScan) {
+        k_scan_small<<<1, kScanThreads, 0, s>>>(in, (int)n, out); ++c->launches;
+        CUDA_TRY(cudaGetLastError());
+        return MPCD_OK;
+    }
     const int nb = (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile);
     if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
     k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, sums); ++c->launches;
@@ -444,14 +449,19 @@ int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out, cudaStre
     return MPCD_OK;
 }
 
+// I.count is all zero between builds (set at creation, cleared again by the scan's read)
 int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, int label = -1) {
-    CUDA_TRY(cudaMemsetAsync(I.count, 0, sizeof(int) * (size_t)c->Nc, c->stream));
     if (c->n > 0) {
         k_histogram<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
         ++c->launches;
     }
-    k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed); ++c->launches;
-    int rc = scan_u64(c, I.packed, c->Nc, I.start);
+    int rc = MPCD_OK;
+    if (c->Nc <= kSmallScan) {
+        k_scan_counts_small<<<1, kScanThreads, 0, c->stream>>>(I.count, c->Nc, I.start); ++c->launches;
+    } else {
+        k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed); ++c->launches;
+        rc = scan_u64(c, I.packed, c->Nc, I.start);
+    }
     if (rc) return rc;
     if (c->n > 0) {
         k_scatter<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, I.pos, c->n, I.start, I.slots); ++c->launches;
@@ -464,6 +474,27 @@ int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, i
 
 __global__ void k_set_step(long long* step, long long value) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *step = value;
+}
+
+// the wall bitmaps and counters of a boundary sweep, cleared in one launch
+__global__ void k_walls_clear(BcWork W, int nwords) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nwords) {
+        W.bitsX[i] = 0u;
+        W.bitsY[i] = 0u;
+    }
+    if (i < 4) W.ints[i] = 0;
+    if (i == 0) *W.nEvents = 0;
+}
+
+// the particle state of slots [0, n) from S to T, in one launch
+template <class V>
+__global__ void k_copy_state(V S, V T, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        T.copy_pos(i, S, i);
+        T.set_vel(i, S.vel(i));
+    }
 }
 
 template <class V>
@@ -575,10 +606,7 @@ int reduce_cols(mpcd_ctx* c, const double* cols, int64_t rows, int K, unsigned m
 int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, bool wantInfo, Prof* pf = nullptr,
            bool overlap = false) {
     BcWork& W = c->W;
-    CUDA_TRY(cudaMemsetAsync(W.bitsX, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
-    CUDA_TRY(cudaMemsetAsync(W.bitsY, 0, sizeof(uint32_t) * (size_t)c->nwords, c->stream));
-    CUDA_TRY(cudaMemsetAsync(W.nEvents, 0, sizeof(int), c->stream));
-    CUDA_TRY(cudaMemsetAsync(W.ints, 0, sizeof(int) * 4, c->stream));
+    k_walls_clear<<<blocks_for(c->nwords), kThreads, 0, c->stream>>>(W, c->nwords); ++c->launches;
     if (wantInfo)
         WITH_VIEW(c->xv, k_stream_bc<true><<<c->bcBlocks, kThreads, 0, c->stream>>>(c->P, doStream ? 1 : 0, S, c->pidb[c->pp],
                                                                                    cidStd, cidSrd, W, c->st));
@@ -711,17 +739,11 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
         seedBase, L.nZones, c->seeds, c->graphMode ? c->stepSeeds : nullptr,
         mode == MPCD_LAYOUT_SHIFTED ? kSeedShifted : kSeedBase); ++c->launches;
     mark(c, pf, 7);
-    CUDA_TRY(cudaMemsetAsync(c->nOverflow, 0, sizeof(int), c->stream));
     // out of place: outputs start as a copy of the inputs; zones write what they change
-    const size_t nn = (size_t)c->n;
     const int xi = c->xv, xo = c->xv ^ 1;
-    if (c->f32) {
-        CUDA_TRY(cudaMemcpyAsync(c->offb[xo], c->offb[xi], sizeof(float2) * nn, cudaMemcpyDeviceToDevice, c->stream));
-        CUDA_TRY(cudaMemcpyAsync(c->cellb[xo], c->cellb[xi], sizeof(int) * nn, cudaMemcpyDeviceToDevice, c->stream));
-        CUDA_TRY(cudaMemcpyAsync(c->v32b[xo], c->v32b[xi], sizeof(float2) * nn, cudaMemcpyDeviceToDevice, c->stream));
-    } else {
-        CUDA_TRY(cudaMemcpyAsync(c->xb[xo], c->xb[xi], sizeof(double2) * nn, cudaMemcpyDeviceToDevice, c->stream));
-        CUDA_TRY(cudaMemcpyAsync(c->vb[xo], c->vb[xi], sizeof(double2) * nn, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->n > 0) {
+        WITH_VIEWS(xi, xo, k_copy_state<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, T, c->n));
+        ++c->launches;
     }
     ZoneArgs A{};
     A.P = c->P;
@@ -747,7 +769,6 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
     A.zoneMoved = c->zoneMoved;
     A.zoneCorr = c->zoneCorr;
     A.st = c->st;
-    CUDA_TRY(cudaMemsetAsync(c->zoneHist, 0, sizeof(int) * kCostBuckets, c->stream));
     k_zone_cost<<<blocks_for(L.nZones), kThreads, 0, c->stream>>>(c->P, L.rects, c->idxStd.start, L.nZones, c->zoneCost,
                                                                    c->zoneHist); ++c->launches;
     k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
@@ -783,7 +804,7 @@ int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
     else
         k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
     ++c->launches;
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, A.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, A.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0), c->nOverflow); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 8);
     c->xv ^= 1;
@@ -874,7 +895,7 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     B.arenaCap = c->ovArenaCap;
     B.nsmCap = c->ovNsmCap;
     k_zone_serial<<<1, 32, c->zSmem, c->stream>>>(A, B, c->ovMem); ++c->launches;
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0)); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0), c->nOverflow); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     c->idxStdValid = false;  // positions and velocities changed in place
     c->cidStdValid = false;
@@ -943,7 +964,9 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     if (permute) {
         c->xv ^= 1;
         c->pp ^= 1;
-        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
+        if (!flat) {  // the flat kick has already made the slots the identity
+            k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
+        }
         CUDA_TRY(cudaGetLastError());
         mark(c, pf, 10);
         // the standard index stays valid (same cells, identity slots); per-slot cell ids and
@@ -1061,6 +1084,8 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     ALLOC(c->cidSrd, (size_t)n);
     for (CellIndex* I : {&c->idxStd, &c->idxSrd}) {
         ALLOC(I->count, (size_t)Nc);
+        if (cudaMemset(I->count, 0, sizeof(int) * (size_t)std::max(Nc, 1)) != cudaSuccess)
+            return fail(set_err(MPCD_ERR_CUDA, "index counts"));
         ALLOC(I->packed, (size_t)Nc);
         ALLOC(I->start, (size_t)Nc + 1);
         ALLOC(I->pos, (size_t)n);
@@ -1123,8 +1148,10 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     ALLOC(c->overflow, (size_t)maxZones);
     ALLOC(c->zoneCost, (size_t)maxZones);
     ALLOC(c->zoneHist, (size_t)kCostBuckets);
+    if (cudaMemset(c->zoneHist, 0, sizeof(int) * kCostBuckets) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "zone histogram"));
     ALLOC(c->zoneOrder, (size_t)maxZones);
     ALLOC(c->nOverflow, 1);
+    if (cudaMemset(c->nOverflow, 0, sizeof(int)) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "overflow counter"));
     ALLOC(c->passOut, 8);
     // collision tiles: room for 1.5x the mean particles per cell plus 8, per cell of a block
     {

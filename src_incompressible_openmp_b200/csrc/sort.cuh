@@ -67,15 +67,61 @@ __global__ void k_scan_apply(const uint64_t* __restrict__ in, int64_t n, const u
     if (base + kScanItems >= n && base < n) out[n] = ex;  // the thread holding the last element
 }
 
+// Arrays of at most kSmallScan entries are scanned by one block in one launch (a step of a
+// small replica launches many short kernels, so their number counts).
+constexpr int kSmallScan = 65536;
+
+// one block: out[i] = exclusive prefix of in, out[n] = total (n <= kSmallScan)
+__global__ void __launch_bounds__(kScanThreads) k_scan_small(const uint64_t* __restrict__ in, int n,
+                                                              uint64_t* __restrict__ out) {
+    __shared__ uint64_t sh[32];
+    const int per = (n + kScanThreads - 1) / kScanThreads;
+    const int a = min(n, (int)threadIdx.x * per), b = min(n, a + per);
+    uint64_t sum = 0;
+    for (int i = a; i < b; ++i) sum += in[i];
+    uint64_t tot;
+    uint64_t ex = block_exclusive_scan(sum, sh, &tot);
+    for (int i = a; i < b; ++i) {
+        const uint64_t v = in[i];
+        out[i] = ex;
+        ex += v;
+    }
+    if (threadIdx.x == 0) out[n] = tot;
+}
+
 // ------------------------------------------------------------------ cell index
 // pack (count, count >= 2) so one scan yields both the segment starts and the rank of each
-// cell among cells holding at least two particles (the SRD sign stream index).
-__global__ void k_pack_counts(const int* __restrict__ count, int Nc, uint64_t* __restrict__ packed) {
+// cell among cells holding at least two particles (the SRD sign stream index). Each count is
+// cleared once read, ready for the next build's histogram.
+__global__ void k_pack_counts(int* __restrict__ count, int Nc, uint64_t* __restrict__ packed) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < Nc) {
         const int k = count[c];
+        count[c] = 0;
         packed[c] = (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
     }
+}
+
+// one block: the packed counts' exclusive scan into start (Nc <= kSmallScan), clearing the counts
+__global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restrict__ count, int Nc,
+                                                                     uint64_t* __restrict__ start) {
+    __shared__ uint64_t sh[32];
+    const int per = (Nc + kScanThreads - 1) / kScanThreads;
+    const int a = min(Nc, (int)threadIdx.x * per), b = min(Nc, a + per);
+    uint64_t sum = 0;
+    for (int i = a; i < b; ++i) {
+        const int k = count[i];
+        sum += (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+    }
+    uint64_t tot;
+    uint64_t ex = block_exclusive_scan(sum, sh, &tot);
+    for (int i = a; i < b; ++i) {
+        const int k = count[i];
+        count[i] = 0;
+        start[i] = ex;
+        ex += (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+    }
+    if (threadIdx.x == 0) start[Nc] = tot;
 }
 
 // pos[s] = arrival order of slot s within its cell (any order; fixed later by k_cell_sort).

@@ -1388,6 +1388,7 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
         }
     }
     __syncthreads();
+    for (int b = threadIdx.x; b < kCostBuckets; b += blockDim.x) hist[b] = 0;  // ready for the next pass
     for (int z = threadIdx.x; z < nZones; z += blockDim.x) order[atomicAdd(&off[cost[z]], 1)] = z;
 }
 
@@ -1443,8 +1444,11 @@ __global__ void __launch_bounds__(kSeedZonesPerBlock * 2) k_zone_seeds(uint64_t 
 }
 
 // pass metrics: integer sums and a fixed-order reduction of the per-zone correction stats
+// (also clears the overflow-zone counter for the next pass, which starts after this kernel)
 __global__ void k_zone_metrics(const int2* __restrict__ moved, const double2* __restrict__ corr, int nZones,
-                               double* __restrict__ out /* movedDense, movedSparse, corrRms, corrMax */) {
+                               double* __restrict__ out /* movedDense, movedSparse, corrRms, corrMax */,
+                               int* __restrict__ nOverflow) {
+    if (threadIdx.x == 0 && nOverflow) *nOverflow = 0;
     __shared__ double sa[256], sm[256];
     __shared__ long long sd[256], ss[256];
     __shared__ int sc[256];
