@@ -230,8 +230,12 @@ __device__ __forceinline__ int srd_cell(double x, double y, double sx, double sy
 
 // The two shift draws U(-a0/2, a0/2) of srd_cell_id_with_random_shift: outputs 0 and 1 of
 // mt19937_64(seed), which need seeded words 0, 1, 2, 156, 157 only. One thread.
-__global__ void k_srd_shift(DevParams P, uint64_t seed, double* out, const uint64_t* seedDev) {
+// stepCounter (graph replay): first begin the step on the device (step_begin), then draw its
+// shift from the device seed table
+__global__ void k_srd_shift(DevParams P, uint64_t seed, double* out, const uint64_t* seedDev,
+                            long long* stepCounter = nullptr, uint64_t* stepSeeds = nullptr) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (stepCounter) step_begin(stepCounter, stepSeeds);
     if (seedDev) seed = seedDev[kSeedSrdShift];
     uint64_t w[kMtM + 2];
     w[0] = seed;

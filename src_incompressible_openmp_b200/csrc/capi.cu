@@ -113,7 +113,7 @@ struct mpcd_ctx {
     cudaEvent_t bcDone = nullptr, wallsDone = nullptr;
     bool wallsPending = false;
     // CUDA-graph replay of the plain step: the step number and its seeds live on the device
-    // (k_step_begin); one graph per entry parity of the ping-pong buffers
+    // (step_begin, in k_srd_shift); one graph per entry parity of the ping-pong buffers
     bool graphMode = false;            // true while a step is being captured
     bool useGraphs = true;
     long long* dStep = nullptr;        // device: number of the last step begun
@@ -134,6 +134,7 @@ struct mpcd_ctx {
     double2* zoneCorr = nullptr;
     int* overflow = nullptr;
     int* nOverflow = nullptr;
+    int* ovDone = nullptr;       // overflow blocks finished (the last computes the pass metrics)
     // serial pass (allocated on first use): pass-input lists + live-list area, per-cell
     // current list start and count, the area's top, per-cell corrections of a zone
     int* slotsLive = nullptr;
@@ -799,12 +800,12 @@ int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
     B.nsmCap = c->ovNsmCap;
+    double* mout = c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0);
     if (c->f32)
-        k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
+        k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock, c->ovDone, mout);
     else
-        k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock);
+        k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock, c->ovDone, mout);
     ++c->launches;
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, A.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0), c->nOverflow); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 8);
     c->xv ^= 1;
@@ -964,9 +965,7 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     if (permute) {
         c->xv ^= 1;
         c->pp ^= 1;
-        if (!flat) {  // the flat kick has already made the slots the identity
-            k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
-        }
+        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
         CUDA_TRY(cudaGetLastError());
         mark(c, pf, 10);
         // the standard index stays valid (same cells, identity slots); per-slot cell ids and
@@ -1004,7 +1003,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
-                    c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow,
+                    c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow, c->ovDone,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
                     c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
                     c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->duLSum, c->redFeat,
@@ -1151,6 +1150,8 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     if (cudaMemset(c->zoneHist, 0, sizeof(int) * kCostBuckets) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "zone histogram"));
     ALLOC(c->zoneOrder, (size_t)maxZones);
     ALLOC(c->nOverflow, 1);
+    ALLOC(c->ovDone, 1);
+    if (cudaMemset(c->ovDone, 0, sizeof(int)) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "overflow block counter"));
     if (cudaMemset(c->nOverflow, 0, sizeof(int)) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "overflow counter"));
     ALLOC(c->passOut, 8);
     // collision tiles: room for 1.5x the mean particles per cell plus 8, per cell of a block
@@ -1620,11 +1621,9 @@ static int step_head(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     int rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
     mark(c, pf, -1);
-    if (c->graphMode) {
-        k_step_begin<<<1, 1, 0, c->stream>>>(c->dStep, c->stepSeeds); ++c->launches;
-    }
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift,
-                                        c->graphMode ? c->stepSeeds : nullptr); ++c->launches;
+                                        c->graphMode ? c->stepSeeds : nullptr, c->graphMode ? c->dStep : nullptr,
+                                        c->stepSeeds); ++c->launches;
     rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
     if (rc) return rc;
     c->cidStdValid = true;
@@ -1702,7 +1701,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
 
 // A step replayed from a CUDA graph. The graph of each entry parity of the ping-pong
 // buffers is captured from step_once on first use; the step number and seeds come from the
-// device (k_step_begin increments *dStep), so one graph serves every step. Needs the step's
+// device (step_begin, run by the step's k_srd_shift, increments *dStep), so one graph serves every step. Needs the step's
 // sign stream prefetched by the step before (signsStep), like the eager path's fast case.
 static int graph_step(mpcd_ctx* c, int64_t step) {
     const int key = c->xv * 2 + c->pp;

@@ -238,10 +238,8 @@ __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const in
 
 // The two kicks for one index position j (flat, coalesced), writing the particle at
 // position j of the next step's layout: (cell, particle id) order.
-// slots: the index order of the red state; entry j is set to j once read (the next step's
-// layout is that order, so its index is the identity)
 template <class V>
-__global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, int* __restrict__ slots,
+__global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, const int* __restrict__ slots,
                             const double* __restrict__ numden, const double* __restrict__ duRX,
                             const double* __restrict__ duRY, const double* __restrict__ eosX,
                             const double* __restrict__ eosY, V S, const int* __restrict__ pid, V T,
@@ -252,7 +250,6 @@ __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, 
     if (j >= n) return;
     const int c = cellOf[j];
     const int s = slots[j];
-    slots[j] = j;
     const double2 w = S.vel(s);
     if (learned && *learned) {
         // the learned closure's kick less its particle mean (sum over cells of N du, int64 at

@@ -71,8 +71,7 @@ struct DevParams {
 enum StepSeed { kSeedBc = 0, kSeedSrdShift, kSeedSignsNext, kSeedBase, kSeedShifted, kSeedParity, kSeedNextParity,
                 kStepSeeds };
 
-__global__ void k_step_begin(long long* __restrict__ step, uint64_t* __restrict__ seeds) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void step_begin(long long* __restrict__ step, uint64_t* __restrict__ seeds) {
     const long long s = *step + 1;
     *step = s;
     const uint64_t u = (uint64_t)s;

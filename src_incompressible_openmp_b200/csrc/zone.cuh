@@ -1394,14 +1394,33 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 
 // zones that did not fit the shared-memory working set, re-run from their seed with a
 // global-memory working set per block (deterministic: identical decisions and writes)
+// The last of its blocks to finish then computes the pass metrics (zone_metrics_warp) and
+// resets the overflow and block counters for the next pass.
+__device__ void zone_metrics_warp(const int2* __restrict__ moved, const double2* __restrict__ corr, int nZones,
+                                  double* __restrict__ out);
 template <bool kF32>
-__global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock) {
+__global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock, int* blocksDone,
+                                                      double* metricsOut) {
     const int nov = *A.nOverflow;
     for (int i = blockIdx.x; i < nov; i += gridDim.x)
         if (!zone_body<false, int, kF32>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap,
                                    A.nsmCap) &&
             (threadIdx.x & 31) == 0)
             raise_error(A.st, kErrZoneCapacity, A.overflow[i]);
+    __syncwarp();
+    int last = 0;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(blocksDone, 1) == (int)gridDim.x - 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    zone_metrics_warp(A.zoneMoved, A.zoneCorr, A.nZones, metricsOut);
+    if (threadIdx.x == 0) {
+        *blocksDone = 0;
+        *A.nOverflow = 0;
+    }
 }
 
 // run_zone_pass (src/zone_pass.cpp:1096-1163): one warp runs the zones in id order on the
@@ -1441,6 +1460,39 @@ __global__ void __launch_bounds__(kSeedZonesPerBlock * 2) k_zone_seeds(uint64_t 
     __syncthreads();
     const int nz = min(kSeedZonesPerBlock, nZones - z0);
     for (int i = t; i < nz * kMtN; i += blockDim.x) out[(size_t)z0 * kMtN + i] = st[i / kMtN][i % kMtN];
+}
+
+// pass metrics as in k_zone_metrics, by one warp (fixed order: lane stride, then a shuffle tree)
+__device__ void zone_metrics_warp(const int2* __restrict__ moved, const double2* __restrict__ corr, int nZones,
+                                  double* __restrict__ out) {
+    const int t = threadIdx.x & 31;
+    double acc = 0.0, mx = 0.0;
+    long long d = 0, s = 0;
+    int c = 0;
+    for (int z = t; z < nZones; z += 32) {
+        const double2 q = __ldcg(corr + z);
+        const int2 m = __ldcg(moved + z);
+        if (q.x > 0.0) {
+            acc = __dadd_rn(acc, __dmul_rn(q.x, q.x));
+            ++c;
+        }
+        mx = smax(mx, q.y);
+        d += m.x;
+        s += m.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        acc = __dadd_rn(acc, __shfl_down_sync(0xffffffffu, acc, o));
+        mx = smax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        d += __shfl_down_sync(0xffffffffu, d, o);
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if (t == 0) {
+        out[0] = (double)d;
+        out[1] = (double)s;
+        out[2] = (c > 0) ? sqrt(__ddiv_rn(acc, (double)c)) : 0.0;
+        out[3] = mx;
+    }
 }
 
 // pass metrics: integer sums and a fixed-order reduction of the per-zone correction stats
