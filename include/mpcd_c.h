@@ -244,6 +244,12 @@ int mpcd_step_profile(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* phas
 /* Step replay from CUDA graphs (default on): after the first step, plain steps without a
  * metrics row are replayed from a captured graph with device-side seeds. 0 turns it off. */
 int mpcd_ctx_set_graphs(mpcd_ctx* ctx, int enable);
+/* Tile shape of the SRD collision (cells x threads per block: 0 = 32x128, 1 = 64x256,
+ * 2 = 128x256, 3 = 256x512). A context times the four on its own state at its first eager
+ * collision and keeps the fastest (the autotuner). shape >= 0 sets one instead; -1 leaves it.
+ * *in_use (nullable): the shape in use, -1 before the first collision. Every shape gives the
+ * same results. */
+int mpcd_ctx_collide_shape(mpcd_ctx* ctx, int32_t shape, int32_t* in_use);
 
 /* ---------------------------------------------------------------- batched replicas */
 /* Independent replicas (reference: one run of the benchmark driver per replica), each with

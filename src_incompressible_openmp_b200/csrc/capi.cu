@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <random>
 #include <string>
@@ -168,8 +169,8 @@ struct mpcd_ctx {
     size_t ovPerBlock = 0;
     int ovBlocks = 2;
     int zMaxCells = 0, zWinCap = 0, zArenaCap = 0, zNsmCap = 0;
-    int collideTile = 0;       // velocities a collision block stages in shared memory
-    size_t collideSmem = 0;
+    int collideShape = -1;     // index into kCollideShape; -1: autotune at the next eager collision
+    int collideTiles[kCollideShapes] = {0, 0, 0, 0};
     size_t zSmem = 0;
     int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0, ovNsmCap = 0;
     double* passOut = nullptr;  // 4 doubles
@@ -251,6 +252,23 @@ inline View32 view32(const mpcd_ctx* c, int k) { return View32{c->offb[k], c->ce
             __VA_ARGS__;                                              \
         }                                                             \
     } while (0)
+
+// A kernel's dynamic shared-memory limit belongs to the function (per device) and so to every
+// context of the process: raise it to what one context needs, never below another's need.
+bool raise_smem(const void* fn, size_t need, int device) {
+    if (need <= 48 * 1024) return true;
+    static std::mutex m;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    std::lock_guard<std::mutex> g(m);
+    size_t& cur = done[{fn, device}];
+    if (need <= cur) return true;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cur = need;
+    return true;
+}
 
 int check_device(mpcd_ctx* c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -641,6 +659,67 @@ int run_bc(mpcd_ctx* c, bool doStream, uint64_t seed, int* cidStd, int* cidSrd, 
     return MPCD_OK;
 }
 
+// the collision with tile shape k on ping-pong buffer `buf`
+static int launch_collide(mpcd_ctx* c, int k, int buf, const uint8_t* signs, const uint64_t* gs, cudaStream_t s) {
+    const int tile = c->collideTiles[k];
+    const size_t smem = (size_t)tile * (sizeof(double2) + sizeof(int));
+#define MPCD_COLLIDE(K)                                                                                      \
+    case K:                                                                                                  \
+        WITH_VIEW(buf, (k_srd_collide<std::remove_const_t<decltype(S)>, kCollideShape[K].cells, kCollideShape[K].threads>          \
+                        <<<blocks_for(c->Nc, kCollideShape[K].cells), kCollideShape[K].threads, smem, s>>>(  \
+                            c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc, S, c->st, gs, c->signsBuf[1], \
+                            tile)));                                                                         \
+        break;
+    switch (k) {
+        MPCD_COLLIDE(0)
+        MPCD_COLLIDE(1)
+        MPCD_COLLIDE(2)
+        MPCD_COLLIDE(3)
+        default: return set_err(MPCD_ERR_INVALID_ARG, "collision tile shape out of range");
+    }
+#undef MPCD_COLLIDE
+    ++c->launches;
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+// Autotuner of the collision tile shape: every candidate runs three times on a scratch copy of
+// the velocities (the spare ping-pong buffer) and the fastest is kept for the context.
+static int tune_collide(mpcd_ctx* c, const uint8_t* signs) {
+    const int spare = c->xv ^ 1;
+    if (c->n > 0) {
+        WITH_VIEWS(c->xv, spare, k_copy_state<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, T, c->n));
+        ++c->launches;
+    }
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = 0.f;
+    int pick = 1;
+    for (int k = 0; k < kCollideShapes; ++k) {
+        int rc = launch_collide(c, k, spare, signs, nullptr, c->stream);  // warm-up
+        if (!rc) CUDA_TRY(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < 3 && !rc; ++r) rc = launch_collide(c, k, spare, signs, nullptr, c->stream);
+        if (rc) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
+        CUDA_TRY(cudaEventRecord(e1, c->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (k == 0 || ms < best) {
+            best = ms;
+            pick = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->collideShape = pick;
+    return check_device(c);
+}
+
 // step < 0: phase API (sign stream generated here, synchronously); otherwise the stream of
 // that step from the double buffer (generated ahead on the side stream when possible)
 int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -1) {
@@ -667,10 +746,12 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         CUDA_TRY(cudaStreamWaitEvent(c->stream, c->wallsDone, 0));
         c->wallsPending = false;
     }
-    WITH_VIEW(c->xv, k_srd_collide<<<blocks_for(c->Nc, kCollideCells), kCollideThreads, c->collideSmem, c->stream>>>(
-                         c->P, c->idxSrd.start, c->idxSrd.slots, signs, c->Nc, S, c->st, gs, c->signsBuf[1],
-                         c->collideTile));
-    ++c->launches;
+    if (c->collideShape < 0 && !c->graphMode) {
+        rc = tune_collide(c, signs);
+        if (rc) return rc;
+    }
+    rc = launch_collide(c, c->collideShape < 0 ? 1 : c->collideShape, c->xv, signs, gs, c->stream);
+    if (rc) return rc;
     if (c->P.keepMeanFlow) {
         WITH_VIEW(c->xv, k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->cols)); ++c->launches;
         rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->red + 8);
@@ -1157,14 +1238,24 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     // collision tiles: room for 1.5x the mean particles per cell plus 8, per cell of a block
     {
         const double ppc = (double)n / (double)std::max(Nc, 1);
-        c->collideTile = std::max(256, std::min(8192, (int)(kCollideCells * (1.5 * ppc + 8.0))));
-        c->collideSmem = (size_t)c->collideTile * (sizeof(double2) + sizeof(int));
-        if (c->collideSmem > 48 * 1024 &&
-            (cudaFuncSetAttribute(k_srd_collide<View64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) !=
-                 cudaSuccess ||
-             cudaFuncSetAttribute(k_srd_collide<View32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->collideSmem) !=
-                 cudaSuccess))
-            return fail(set_err(MPCD_ERR_CUDA, "collision shared memory attribute"));
+        bool ok = true;
+#define MPCD_COLLIDE_ATTR(K)                                                                                          \
+    {                                                                                                                 \
+        const int cells = kCollideShape[K].cells;                                                                     \
+        c->collideTiles[K] = std::max(256, std::min(8192, (int)(cells * (1.5 * ppc + 8.0))));                         \
+        const size_t sm = (size_t)c->collideTiles[K] * (sizeof(double2) + sizeof(int));                               \
+        ok = ok &&                                                                                                    \
+             raise_smem((const void*)k_srd_collide<View64, kCollideShape[K].cells, kCollideShape[K].threads>, sm,      \
+                        device) &&                                                                                    \
+             raise_smem((const void*)k_srd_collide<View32, kCollideShape[K].cells, kCollideShape[K].threads>, sm,      \
+                        device);                                                                                      \
+    }
+        MPCD_COLLIDE_ATTR(0)
+        MPCD_COLLIDE_ATTR(1)
+        MPCD_COLLIDE_ATTR(2)
+        MPCD_COLLIDE_ATTR(3)
+#undef MPCD_COLLIDE_ATTR
+        if (!ok) return fail(set_err(MPCD_ERR_CUDA, "collision shared memory attribute"));
     }
     // fast path: tiles of the base/shifted layouts in shared memory
     {
@@ -1186,10 +1277,9 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
             c->zMaxCells = 0;
             c->zSmem = ZoneMem<uint16_t>::bytes(0, 0, 0, 0);
         }
-        if (c->zSmem > 48 * 1024 &&
-            (cudaFuncSetAttribute(k_zone_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
-             cudaFuncSetAttribute(k_zone_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess ||
-             cudaFuncSetAttribute(k_zone_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->zSmem) != cudaSuccess))
+        if (!raise_smem((const void*)k_zone_pass<false>, c->zSmem, device) ||
+            !raise_smem((const void*)k_zone_pass<true>, c->zSmem, device) ||
+            !raise_smem((const void*)k_zone_serial, c->zSmem, device))
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
         c->ovWinCap = (maxTX + 4) * (maxTY + 4);
@@ -2194,6 +2284,23 @@ static int batch_graph_step(mpcd_batch* b, int64_t step) {
 
 extern "C" {
 
+int mpcd_ctx_collide_shape(mpcd_ctx* c, int32_t shape, int32_t* in_use) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (shape < -1 || shape >= kCollideShapes) return set_err(MPCD_ERR_INVALID_ARG, "collision tile shape out of range");
+    if (shape >= 0) {
+        CUDA_TRY(cudaSetDevice(c->device));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (auto& g : c->gexec)  // captured steps hold the previous shape
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        c->collideShape = shape;
+    }
+    if (in_use) *in_use = c->collideShape;
+    return MPCD_OK;
+}
+
 int mpcd_ctx_set_graphs(mpcd_ctx* c, int enable) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     c->useGraphs = enable != 0;
@@ -2259,9 +2366,7 @@ int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_b
             cudaMalloc((void**)&b->dOffs, sizeof(int) * (count + 1) * nslots) != cudaSuccess ||
             cudaMalloc((void**)&b->dStepPtrs, sizeof(long long*) * count) != cudaSuccess ||
             cudaMemcpy(b->dStepPtrs, steps.data(), sizeof(long long*) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
-            (b->zSmem > 48 * 1024 &&
-             cudaFuncSetAttribute(k_zone_pass_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->zSmem) !=
-                 cudaSuccess)) {
+            !raise_smem((const void*)k_zone_pass_batch<false>, b->zSmem, device)) {
             cudaGetLastError();
             mpcd_batch_destroy(b);
             return set_err(MPCD_ERR_CUDA, "batch zone-pass staging");

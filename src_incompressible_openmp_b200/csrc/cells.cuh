@@ -99,11 +99,17 @@ __device__ __forceinline__ bool collide_cell(const DevParams& P, uint64_t start0
 // The collision over kCollideCells consecutive SRD cells per block. Their segments are
 // contiguous in slots[]: the velocities are gathered once into shared memory by the whole
 // block, each thread runs its cell there, and the block scatters them back. A block whose
-// segments exceed the tile works on global memory instead.
-constexpr int kCollideCells = 64;
-constexpr int kCollideThreads = 256;
+// segments exceed the tile works on global memory instead. The tile shape (cells and threads
+// per block) is a template argument; the context's autotuner picks one of kCollideShapes by
+// timing them on its own state. Every shape gives the same result: a cell's collision does
+// not depend on the tiling.
+struct CollideShape {
+    int cells, threads;
+};
+constexpr int kCollideShapes = 4;
+constexpr CollideShape kCollideShape[kCollideShapes] = {{32, 128}, {64, 256}, {128, 256}, {256, 512}};
 
-template <class V>
+template <class V, int kCollideCells, int kCollideThreads>
 __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, const uint64_t* __restrict__ start,
                                                                  const int* __restrict__ slots,
                                                                  const uint8_t* __restrict__ sign, int signCount,

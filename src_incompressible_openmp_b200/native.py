@@ -77,6 +77,7 @@ def lib():
         "mpcd_step_profile": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double), C.c_int], C.c_int),
         "mpcd_launch_count": ([C.c_void_p], C.c_int64),
         "mpcd_ctx_set_graphs": ([C.c_void_p, C.c_int], C.c_int),
+        "mpcd_ctx_collide_shape": ([C.c_void_p, C.c_int32, P(C.c_int32)], C.c_int),
         "mpcd_batch_create": ([P(_abi.ParamsC), C.c_int, C.c_int, P(C.c_void_p)], C.c_int),
         "mpcd_batch_destroy": ([C.c_void_p], C.c_int),
         "mpcd_batch_size": ([C.c_void_p], C.c_int),
@@ -302,6 +303,13 @@ class Context:
 
     def launch_count(self):
         return int(lib().mpcd_launch_count(self.h))
+
+    def collide_shape(self, shape=-1):
+        """mpcd_ctx_collide_shape: set the collision tile shape (0..3) or, with -1, only query;
+        returns the shape in use (-1 before the autotuner has run)."""
+        r = C.c_int32()
+        _check(lib().mpcd_ctx_collide_shape(self.h, shape, C.byref(r)))
+        return r.value
 
     def set_graphs(self, enable):
         """Step replay from CUDA graphs (on by default)."""
