@@ -170,6 +170,8 @@ struct mpcd_ctx {
     int ovBlocks = 2;
     int zMaxCells = 0, zWinCap = 0, zArenaCap = 0, zNsmCap = 0;
     int collideShape = -1;     // index into kCollideShape; -1: autotune at the next eager collision
+                               // that finds the slots in (cell, id) order
+    bool slotsSorted = false;  // slots in (cell, id) order: false after a state upload until a step
     int collideTiles[kCollideShapes] = {0, 0, 0, 0};
     size_t zSmem = 0;
     int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0, ovNsmCap = 0;
@@ -683,39 +685,42 @@ static int launch_collide(mpcd_ctx* c, int k, int buf, const uint8_t* signs, con
     return MPCD_OK;
 }
 
-// Autotuner of the collision tile shape: every candidate runs three times on a scratch copy of
-// the velocities (the spare ping-pong buffer) and the fastest is kept for the context.
+// Autotuner of the collision tile shape: on a scratch copy of the velocities (the spare
+// ping-pong buffer) every candidate runs once to warm up, then the candidates run in turn for
+// three rounds, and the shape with the fastest single run is kept for the context. Running the
+// rounds in turn keeps clock ramps at the start of a run from favouring the later candidates.
 static int tune_collide(mpcd_ctx* c, const uint8_t* signs) {
     const int spare = c->xv ^ 1;
     if (c->n > 0) {
         WITH_VIEWS(c->xv, spare, k_copy_state<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, T, c->n));
         ++c->launches;
     }
-    cudaEvent_t e0, e1;
-    CUDA_TRY(cudaEventCreate(&e0));
-    CUDA_TRY(cudaEventCreate(&e1));
-    float best = 0.f;
-    int pick = 1;
-    for (int k = 0; k < kCollideShapes; ++k) {
-        int rc = launch_collide(c, k, spare, signs, nullptr, c->stream);  // warm-up
-        if (!rc) CUDA_TRY(cudaEventRecord(e0, c->stream));
-        for (int r = 0; r < 3 && !rc; ++r) rc = launch_collide(c, k, spare, signs, nullptr, c->stream);
-        if (rc) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return rc;
-        }
-        CUDA_TRY(cudaEventRecord(e1, c->stream));
-        CUDA_TRY(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-        if (k == 0 || ms < best) {
-            best = ms;
-            pick = k;
-        }
+    constexpr int kRounds = 3;
+    cudaEvent_t ev[kRounds * kCollideShapes + 1];
+    for (auto& e : ev) e = nullptr;
+    int rc = MPCD_OK;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "tuning events");
+    for (int k = 0; k < kCollideShapes && !rc; ++k) rc = launch_collide(c, k, spare, signs, nullptr, c->stream);
+    if (!rc && cudaEventRecord(ev[0], c->stream) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "tuning event");
+    for (int i = 0; i < kRounds * kCollideShapes && !rc; ++i) {
+        rc = launch_collide(c, i % kCollideShapes, spare, signs, nullptr, c->stream);
+        if (!rc && cudaEventRecord(ev[i + 1], c->stream) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "tuning event");
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    float best[kCollideShapes];
+    for (float& b : best) b = 1e30f;
+    if (!rc && cudaEventSynchronize(ev[kRounds * kCollideShapes]) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "tuning");
+    for (int i = 0; i < kRounds * kCollideShapes && !rc; ++i) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) != cudaSuccess) rc = set_err(MPCD_ERR_CUDA, "tuning time");
+        best[i % kCollideShapes] = std::min(best[i % kCollideShapes], ms);
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc) return rc;
+    int pick = 0;
+    for (int k = 1; k < kCollideShapes; ++k)
+        if (best[k] < best[pick]) pick = k;
     c->collideShape = pick;
     return check_device(c);
 }
@@ -746,7 +751,9 @@ int run_collide(mpcd_ctx* c, uint64_t seed, Prof* pf = nullptr, int64_t step = -
         CUDA_TRY(cudaStreamWaitEvent(c->stream, c->wallsDone, 0));
         c->wallsPending = false;
     }
-    if (c->collideShape < 0 && !c->graphMode) {
+    // Tuned only on cell-sorted slots: an uploaded state is in particle-id order, whose scattered
+    // gathers favour other tile shapes than the sorted layout every later step has.
+    if (c->collideShape < 0 && !c->graphMode && c->slotsSorted) {
         rc = tune_collide(c, signs);
         if (rc) return rc;
     }
@@ -1046,6 +1053,7 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     if (permute) {
         c->xv ^= 1;
         c->pp ^= 1;
+        c->slotsSorted = true;
         k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->idxStd.slots, c->n); ++c->launches;
         CUDA_TRY(cudaGetLastError());
         mark(c, pf, 10);
@@ -1330,6 +1338,7 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
     CUDA_TRY(cudaSetDevice(c->device));
     c->xv = 0;
     c->pp = 0;
+    c->slotsSorted = false;
     if (n > 0 && c->f32) {
         // staged through FP64 scratch, then split into cell, FP32 offset and FP32 velocity
         double2 *tx = nullptr, *tv = nullptr;
@@ -1836,14 +1845,15 @@ static int graph_step(mpcd_ctx* c, int64_t step) {
     return MPCD_OK;
 }
 
-// steps step0+1 .. step0+nsteps; the metrics step (if any) and steps whose sign stream was
-// not prefetched run eagerly, the others from graphs
+// steps step0+1 .. step0+nsteps; the metrics step (if any), steps whose sign stream was
+// not prefetched and steps before the collision tile shape is tuned run eagerly, the others
+// from graphs
 static int run_steps(mpcd_ctx* c, int64_t step0, int64_t nsteps, bool metricsLast) {
     for (int64_t k = 1; k <= nsteps; ++k) {
         const int64_t s = step0 + k;
         const bool m = metricsLast && k == nsteps;
         int rc;
-        if (c->useGraphs && !m && c->signsStep[s & 1] == s)
+        if (c->useGraphs && !m && c->signsStep[s & 1] == s && c->collideShape >= 0)
             rc = graph_step(c, s);
         else
             rc = step_once(c, s, m);
@@ -2401,11 +2411,12 @@ int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device
     for (mpcd_ctx* c : b->members) CUDA_TRY(cudaStreamWaitEvent(c->stream, b->start, 0));
     for (int64_t k = 1; k <= nsteps; ++k) {
         const int64_t s = step0 + k;
-        // the graph needs every replica's sign stream prefetched and one common buffer parity
+        // the graph needs every replica's sign stream prefetched, one common buffer parity and
+        // every replica's collision tile shape tuned
         bool graph = b->useGraphs;
         for (mpcd_ctx* c : b->members)
             graph = graph && c->useGraphs && c->signsStep[s & 1] == s && c->xv == b->members[0]->xv &&
-                    c->pp == b->members[0]->pp;
+                    c->pp == b->members[0]->pp && c->collideShape >= 0;
         const int rc = graph ? batch_graph_step(b, s) : batch_step_body(b, s);
         if (rc) return rc;
     }

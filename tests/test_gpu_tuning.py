@@ -1,5 +1,7 @@
-"""The collision's tile-shape autotuner: the shape it picks is one of the four, and every shape
-gives the same state, bit for bit (a cell's collision does not depend on the tiling)."""
+"""The collision's tile-shape autotuner: the shape it picks is one of the four, it waits for
+cell-sorted slots (an uploaded state is in particle-id order until the first step re-sorts it),
+and every shape gives the same state, bit for bit (a cell's collision does not depend on the
+tiling)."""
 import numpy as np
 import pytest
 
@@ -23,7 +25,9 @@ def test_every_collision_shape_gives_the_same_state():
     with native.Context(p) as ctx:
         ctx.set_state(x, v)
         assert ctx.collide_shape() == -1
-        ctx.step(0, 3)
+        ctx.step(0, 1)
+        assert ctx.collide_shape() == -1  # the first step sorts the uploaded slots
+        ctx.step(1, 2)
         assert 0 <= ctx.collide_shape() < 4  # picked by timing
         out.append(ctx.get_state())
     for shape in range(4):
