@@ -90,6 +90,8 @@ struct mpcd_ctx {
     int xv = 0, pp = 0;
     int* cidStd = nullptr;
     int* cidSrd = nullptr;
+    uint64_t* sortKeys = nullptr;  // n: (particle id, slot) keys of the index being built
+    int rankCells = 1;             // cells per block of k_cell_rank
     bool cidStdValid = false;
     bool srdCellsValid = false;
     CellIndex idxStd, idxSrd;
@@ -473,7 +475,7 @@ int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out, cudaStre
 // I.count is all zero between builds (set at creation, cleared again by the scan's read)
 int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, int label = -1) {
     if (c->n > 0) {
-        k_histogram<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
+        k_histogram<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
         ++c->launches;
     }
     int rc = MPCD_OK;
@@ -485,8 +487,10 @@ int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, i
     }
     if (rc) return rc;
     if (c->n > 0) {
-        k_scatter<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cid, I.pos, c->n, I.start, I.slots); ++c->launches;
-        k_cell_sort<<<blocks_for(c->Nc, 128), 128, 0, c->stream>>>(I.start, c->Nc, c->pidb[c->pp], I.slots); ++c->launches;
+        k_scatter_keys<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(
+            cid, I.pos, c->pidb[c->pp], c->n, I.start, c->sortKeys); ++c->launches;
+        k_cell_rank<<<blocks_for(c->Nc, c->rankCells), kRankThreads, 0, c->stream>>>(I.start, c->Nc, c->rankCells,
+                                                                                    c->sortKeys, I.slots); ++c->launches;
     }
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, label);
@@ -1087,7 +1091,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     if (!c) return MPCD_OK;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->offb[0], c->offb[1], c->cellb[0], c->cellb[1],
-                    c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd,
+                    c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd, c->sortKeys,
                     c->idxStd.count, c->idxStd.packed, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
                     c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
@@ -1170,6 +1174,8 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     }
     ALLOC(c->cidStd, (size_t)n);
     ALLOC(c->cidSrd, (size_t)n);
+    ALLOC(c->sortKeys, (size_t)n);
+    c->rankCells = rank_cells_per_block(n, Nc);
     for (CellIndex* I : {&c->idxStd, &c->idxSrd}) {
         ALLOC(I->count, (size_t)Nc);
         if (cudaMemset(I->count, 0, sizeof(int) * (size_t)std::max(Nc, 1)) != cudaSuccess)

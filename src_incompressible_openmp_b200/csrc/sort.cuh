@@ -6,8 +6,9 @@
 // per-cell FP64 sum on the device run in exactly that order, so sums are bit-identical.
 //
 // Build: warp-aggregated histogram with atomics (one atomic per run of equal cell ids in a
-// warp), exclusive scan of the counts, scatter of slots, then an insertion sort of each
-// cell's short segment by particle id.
+// warp), exclusive scan of the counts, scatter of (particle id, slot) keys into the cells'
+// segments, then a rank sort of each tile of cells in shared memory: an entry's place in its
+// cell is the number of the cell's keys below its own.
 #pragma once
 
 #include "common.cuh"
@@ -124,91 +125,130 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restr
     if (threadIdx.x == 0) start[Nc] = tot;
 }
 
-// pos[s] = arrival order of slot s within its cell (any order; fixed later by k_cell_sort).
+// pos[s] = arrival order of slot s within its cell (any order; fixed by k_cell_rank).
 // One atomic per run of equal cell ids among consecutive lanes: after the end-of-step
-// re-sort, slots are ordered by cell, so a warp's lanes form a few long runs.
+// re-sort, slots are ordered by cell, so a warp's lanes form a few long runs. Each warp
+// covers kIndexItems runs of 32 consecutive slots, whose atomics are in flight together.
+constexpr int kIndexItems = 4;
+
 __global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict__ count, int* __restrict__ pos) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const int c = (s < n) ? cid[s] : -1;
-    const int prev = __shfl_up_sync(0xffffffffu, c, 1);
-    const bool headOfRun = (lane == 0) || (prev != c);
-    const unsigned heads = __ballot_sync(0xffffffffu, headOfRun);
-    // run start = highest head lane <= lane; run end = next head lane
-    const unsigned upTo = heads & (0xffffffffu >> (31 - lane));
-    const int runStart = 31 - __clz(upTo);
-    const unsigned after = heads & ~(0xffffffffu >> (31 - lane));
-    const int runEnd = after ? (__ffs(after) - 1) : 32;
-    int base = 0;
-    if (headOfRun && c >= 0) base = atomicAdd(&count[c], runEnd - runStart);
-    base = __shfl_sync(0xffffffffu, base, runStart);
-    if (s < n) pos[s] = base + (lane - runStart);
+    const int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
+    int c[kIndexItems], got[kIndexItems], runStart[kIndexItems];
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) c[k] = (base + 32 * k < n) ? cid[base + 32 * k] : -1;
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) {
+        const int prev = __shfl_up_sync(0xffffffffu, c[k], 1);
+        const bool headOfRun = (lane == 0) || (prev != c[k]);
+        const unsigned heads = __ballot_sync(0xffffffffu, headOfRun);
+        // run start = highest head lane <= lane; run end = next head lane
+        runStart[k] = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+        const unsigned after = heads & ~(0xffffffffu >> (31 - lane));
+        const int runEnd = after ? (__ffs(after) - 1) : 32;
+        got[k] = (headOfRun && c[k] >= 0) ? atomicAdd(&count[c[k]], runEnd - runStart[k]) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) {
+        const int b = __shfl_sync(0xffffffffu, got[k], runStart[k]);
+        if (base + 32 * k < n) pos[base + 32 * k] = b + (lane - runStart[k]);
+    }
 }
 
-__global__ void k_scatter(const int* __restrict__ cid, const int* __restrict__ pos, int n,
-                          const uint64_t* __restrict__ start, int* __restrict__ slots) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < n) slots[(uint32_t)start[cid[s]] + pos[s]] = s;
+// keys[start[cid[s]] + pos[s]] = (pid[s] << 32) | s: each cell's segment holds its
+// particles' keys in arrival order (same slot coverage as k_histogram)
+__global__ void k_scatter_keys(const int* __restrict__ cid, const int* __restrict__ pos, const int* __restrict__ pid,
+                               int n, const uint64_t* __restrict__ start, uint64_t* __restrict__ keys) {
+    const int lane = threadIdx.x & 31;
+    const int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
+    int c[kIndexItems], p[kIndexItems], q[kIndexItems];
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) {
+        const int s = base + 32 * k;
+        c[k] = s < n ? cid[s] : 0;
+        p[k] = s < n ? pos[s] : 0;
+        q[k] = s < n ? pid[s] : 0;
+    }
+    uint32_t at[kIndexItems];
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) at[k] = (uint32_t)start[c[k]];
+#pragma unroll
+    for (int k = 0; k < kIndexItems; ++k) {
+        const int s = base + 32 * k;
+        if (s < n) keys[at[k] + p[k]] = ((uint64_t)(uint32_t)q[k] << 32) | (uint32_t)s;
+    }
 }
 
-// Bitonic sort of 16 or 32 keys held in registers (fully unrolled, no local memory).
-template <int N>
-__device__ __forceinline__ void bitonic_regs(uint64_t (&k)[N]) {
-#pragma unroll
-    for (int size = 2; size <= N; size <<= 1)
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const bool up = ((i & size) == 0);
-                    const uint64_t a = k[i], b = k[j];
-                    const bool sw = up ? (a > b) : (a < b);
-                    k[i] = sw ? b : a;
-                    k[j] = sw ? a : b;
-                }
+constexpr int kRankThreads = 128;
+constexpr int kRankCap = 2048;  // keys of one shared-memory tile (24 KB with their segment words)
+
+// cells per block of k_cell_rank: a power of two giving about 1,280 keys per block at the
+// mean occupancy (so a tile rarely needs splitting)
+inline int rank_cells_per_block(int64_t n, int Nc) {
+    const double mean = Nc > 0 ? (double)n / (double)Nc : 1.0;
+    int cells = 1;
+    while (cells < 4096 && (double)(2 * cells) * mean <= 1280.0) cells *= 2;
+    return cells;
+}
+
+__device__ __forceinline__ int seg_lo(uint64_t s) { return (int)(uint32_t)s; }
+
+// slots[start[c] + rank] = slot of the key of that rank among cell c's keys (pid, then slot:
+// ascending particle id). A block takes cellsPerBlock consecutive cells, stages their keys in
+// shared memory (splitting the run of cells where it exceeds kRankCap keys) and ranks each key
+// against its own cell's keys. A cell above kRankCap keys on its own is ranked from global memory.
+__global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __restrict__ start, int Nc,
+                                                            int cellsPerBlock, const uint64_t* __restrict__ keys,
+                                                            int* __restrict__ slots) {
+    __shared__ uint64_t key[kRankCap];
+    __shared__ uint32_t seg[kRankCap];  // per key: its cell's segment [a, b) in the tile, a | b << 16
+    const int t = threadIdx.x;
+    const int c0 = (int)min((int64_t)blockIdx.x * cellsPerBlock, (int64_t)Nc);
+    const int c1 = min(Nc, c0 + cellsPerBlock);
+    int cs = c0;
+    while (cs < c1) {  // block-uniform
+        const int A = seg_lo(start[cs]);
+        int ce = c1;
+        if (seg_lo(start[c1]) - A > kRankCap) {
+            int lo = cs, hi = c1 - 1;  // the last ce with start[ce] - A <= kRankCap
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (seg_lo(start[mid]) - A <= kRankCap)
+                    lo = mid;
+                else
+                    hi = mid - 1;
             }
-}
-
-template <int N>
-__device__ __forceinline__ void sort_segment_regs(int a, int m, const int* __restrict__ pid, int* __restrict__ slots) {
-    uint64_t k[N];
-    int sl[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) sl[i] = (i < m) ? slots[a + i] : 0;
-#pragma unroll
-    for (int i = 0; i < N; ++i) k[i] = (i < m) ? (((uint64_t)(uint32_t)pid[sl[i]] << 32) | (uint32_t)sl[i]) : ~0ULL;
-    bitonic_regs<N>(k);
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-        if (i < m) slots[a + i] = (int)(uint32_t)k[i];
-}
-
-// sort each cell's slots by particle id (segments are short: ~ particles per cell)
-__global__ void k_cell_sort(const uint64_t* __restrict__ start, int Nc, const int* __restrict__ pid,
-                            int* __restrict__ slots) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= Nc) return;
-    const int a = (int)(uint32_t)start[c], b = (int)(uint32_t)start[c + 1];
-    const int m = b - a;
-    if (m <= 1) return;
-    if (m <= 16) {
-        sort_segment_regs<16>(a, m, pid, slots);
-    } else if (m <= 32) {
-        sort_segment_regs<32>(a, m, pid, slots);
-    } else {
-        // long segment: insertion sort in place in global memory
-        for (int i = a + 1; i < b; ++i) {
-            const int v = slots[i];
-            const int pv = pid[v];
-            int j = i;
-            while (j > a && pid[slots[j - 1]] > pv) {
-                slots[j] = slots[j - 1];
-                --j;
-            }
-            slots[j] = v;
+            ce = lo;
         }
+        if (ce == cs) {
+            const int b = seg_lo(start[cs + 1]);
+            for (int i = A + t; i < b; i += kRankThreads) {
+                const uint64_t k = keys[i];
+                int r = 0;
+                for (int j = A; j < b; ++j) r += keys[j] < k;
+                slots[A + r] = (int)(uint32_t)k;
+            }
+            ++cs;
+            continue;
+        }
+        const int m = seg_lo(start[ce]) - A;
+#pragma unroll 4
+        for (int i = t; i < m; i += kRankThreads) key[i] = keys[A + i];
+        for (int c = cs + t; c < ce; c += kRankThreads) {
+            const int a = seg_lo(start[c]) - A, b = seg_lo(start[c + 1]) - A;
+            for (int j = a; j < b; ++j) seg[j] = (uint32_t)a | ((uint32_t)b << 16);
+        }
+        __syncthreads();
+        for (int i = t; i < m; i += kRankThreads) {
+            const uint32_t sg = seg[i];
+            const int a = (int)(sg & 0xffffu), b = (int)(sg >> 16);
+            const uint64_t k = key[i];
+            int r = 0;
+            for (int j = a; j < b; ++j) r += key[j] < k;
+            slots[A + a + r] = (int)(uint32_t)k;
+        }
+        __syncthreads();
+        cs = ce;
     }
 }
 
