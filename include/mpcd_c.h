@@ -232,6 +232,17 @@ int mpcd_zone_owner_map(mpcd_ctx* ctx, int32_t mode, int32_t* owner_out);
  * with its per-step seed schedule. If `last` is given, fills the metrics row of the last
  * step (costs extra device reductions and one synchronisation). */
 int mpcd_step(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* last);
+/* Independent jobs through one context, with host buffers: job j (0 <= j < njobs) loads the
+ * state (x_in[j], v_in[j]), runs steps step0 + j*nsteps + 1 .. step0 + (j+1)*nsteps and stores
+ * the resulting state in (x_out[j], v_out[j]), with the results of mpcd_set_state + mpcd_step
+ * + mpcd_get_state per job. The upload of job j+1's input and the download of job j-1's result
+ * run on two copy streams while job j steps (asynchronously when the host buffers are
+ * page-locked). x_out[j] / v_out[j] may be x_in[j] / v_in[j]; no other output may alias an
+ * input. Layouts as mpcd_set_state. The device status is checked after the last job: an error
+ * of any job is returned then, and the outputs of that job and the jobs after it are
+ * unspecified. No counterpart in the reference: its state lives in host memory. */
+int mpcd_run_jobs(mpcd_ctx* ctx, int64_t njobs, const double* const* x_in, const double* const* v_in,
+                  int64_t step0, int64_t nsteps, double* const* x_out, double* const* v_out);
 /* Device-side metrics row of the current state after a step (see mpcd_step). */
 int mpcd_step_metrics(mpcd_ctx* ctx, mpcd_step_metrics_c* out);
 /* mpcd_step without metrics, timed with CUDA events recorded on the context's stream

@@ -48,8 +48,7 @@ inline int blocks_for(int64_t n, int t = kThreads) { return (int)std::max<int64_
 
 struct CellIndex {
     int* count = nullptr;      // Nc
-    uint64_t* packed = nullptr;// Nc   (count | (count >= 2) << 32)
-    uint64_t* start = nullptr; // Nc + 1 (exclusive scan of packed)
+    uint64_t* start = nullptr; // Nc + 1: exclusive scan of (count, count >= 2) packed in a u64
     int* pos = nullptr;        // n
     int* slots = nullptr;      // n
 };
@@ -88,6 +87,10 @@ struct mpcd_ctx {
     float2* v32b[2] = {nullptr, nullptr};
     int* pidb[2] = {nullptr, nullptr};
     int xv = 0, pp = 0;
+    // Position buffers are addressed as [k ^ xflip] for view index k: the zone passes update
+    // positions in place and velocities out of place, so each pass flips xv and xflip together
+    // (the positions stay in their buffer); a whole step leaves xflip as it found it.
+    int xflip = 0;
     int* cidStd = nullptr;
     int* cidSrd = nullptr;
     uint64_t* sortKeys = nullptr;  // n: (particle id, slot) keys of the index being built
@@ -122,14 +125,21 @@ struct mpcd_ctx {
     long long* dStep = nullptr;        // device: number of the last step begun
     uint64_t* stepSeeds = nullptr;     // device: kStepSeeds
     cudaEvent_t sideDone = nullptr;    // the captured step joins its sign prefetch
-    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-    int64_t gkernels[4] = {0, 0, 0, 0};
+    cudaGraphExec_t gexec[8] = {};  // by (xv, pp, xflip) at step entry
+    int64_t gkernels[8] = {};
     struct HostFlags {
-        int xv, pp;
+        int xv, pp, xflip;
         bool cidStdValid, srdCellsValid, idxStdValid, refValid;
-    } gpost[4];
+    } gpost[8];
     cudaEvent_t signsReady[2] = {nullptr, nullptr};
     cudaEvent_t collDone = nullptr;
+    // mpcd_run_jobs: double-buffered device staging of job inputs and results (x then v,
+    // 2n double2 each) and the streams that copy them to and from the host
+    double2* jobIn[2] = {nullptr, nullptr};
+    double2* jobOut[2] = {nullptr, nullptr};
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t upDone[2] = {nullptr, nullptr}, inFree[2] = {nullptr, nullptr};
+    cudaEvent_t outReady[2] = {nullptr, nullptr}, downDone[2] = {nullptr, nullptr};
     // zones
     Layout lay[3];  // base, shifted, single_full
     uint64_t* seeds = nullptr;
@@ -234,8 +244,13 @@ void mark(mpcd_ctx* c, Prof* p, int label) {
 // The state views of ping-pong buffer k, and a launch site written once for both forms:
 // WITH_VIEW(k, ...) runs its body with S, the view of buffer k; WITH_VIEWS(k, k2, ...) also
 // binds T, the view of buffer k2.
-inline View64 view64(const mpcd_ctx* c, int k) { return View64{c->xb[k], c->vb[k]}; }
-inline View32 view32(const mpcd_ctx* c, int k) { return View32{c->offb[k], c->cellb[k], c->v32b[k]}; }
+inline View64 view64(const mpcd_ctx* c, int k) { return View64{c->xb[k ^ c->xflip], c->vb[k]}; }
+inline View32 view32(const mpcd_ctx* c, int k) {
+    return View32{c->offb[k ^ c->xflip], c->cellb[k ^ c->xflip], c->v32b[k]};
+}
+// positions of the current state, and the other position buffer (free as scratch)
+inline double2* cur_x(const mpcd_ctx* c) { return c->xb[c->xv ^ c->xflip]; }
+inline double2* spare_x(const mpcd_ctx* c) { return c->xb[c->xv ^ c->xflip ^ 1]; }
 #define WITH_VIEW(k, ...)                          \
     do {                                           \
         if (c->f32) {                              \
@@ -478,14 +493,15 @@ int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, i
         k_histogram<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
         ++c->launches;
     }
-    int rc = MPCD_OK;
     if (c->Nc <= kSmallScan) {
         k_scan_counts_small<<<1, kScanThreads, 0, c->stream>>>(I.count, c->Nc, I.start); ++c->launches;
     } else {
-        k_pack_counts<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(I.count, c->Nc, I.packed); ++c->launches;
-        rc = scan_u64(c, I.packed, c->Nc, I.start);
+        const int nb = (c->Nc + kScanTile - 1) / kScanTile;
+        if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
+        k_count_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(I.count, c->Nc, c->blockSums); ++c->launches;
+        k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb); ++c->launches;
+        k_count_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(I.count, c->Nc, c->blockSums, I.start); ++c->launches;
     }
-    if (rc) return rc;
     if (c->n > 0) {
         k_scatter_keys<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(
             cid, I.pos, c->pidb[c->pp], c->n, I.start, c->sortKeys); ++c->launches;
@@ -520,6 +536,13 @@ __global__ void k_copy_state(V S, V T, int n) {
         T.copy_pos(i, S, i);
         T.set_vel(i, S.vel(i));
     }
+}
+
+// the velocities of slots [0, n) from S to T
+template <class V>
+__global__ void k_copy_vel(V S, V T, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) T.set_vel(i, S.vel(i));
 }
 
 template <class V>
@@ -832,10 +855,11 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
         seedBase, L.nZones, c->seeds, c->graphMode ? c->stepSeeds : nullptr,
         mode == MPCD_LAYOUT_SHIFTED ? kSeedShifted : kSeedBase); ++c->launches;
     mark(c, pf, 7);
-    // out of place: outputs start as a copy of the inputs; zones write what they change
+    // velocities out of place (output starts as a copy of the input; zones write what they
+    // change), positions in place (the zone kernel never reads them)
     const int xi = c->xv, xo = c->xv ^ 1;
     if (c->n > 0) {
-        WITH_VIEWS(xi, xo, k_copy_state<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, T, c->n));
+        WITH_VIEWS(xi, xo, k_copy_vel<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, T, c->n));
         ++c->launches;
     }
     ZoneArgs A{};
@@ -845,11 +869,11 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
     A.start = c->idxStd.start;
     A.slots = c->idxStd.slots;
     A.vin = c->vb[xi];
-    A.xout = c->xb[xo];
+    A.xout = cur_x(c);
     A.vout = c->vb[xo];
     A.f32 = c->f32 ? 1 : 0;
     A.in32 = view32(c, xi);
-    A.out32 = view32(c, xo);
+    A.out32 = View32{c->offb[xi ^ c->xflip], c->cellb[xi ^ c->xflip], c->v32b[xo]};
     A.cid = c->cidStd;
     A.seeds = c->seeds;
     A.nZones = L.nZones;
@@ -901,6 +925,7 @@ int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, 8);
     c->xv ^= 1;
+    c->xflip ^= 1;
     c->idxStdValid = false;  // cid was updated for moved particles; positions changed
     c->srdCellsValid = false;
     return MPCD_OK;
@@ -959,7 +984,7 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     A.start = c->idxStd.start;
     A.slots = c->slotsLive;
     A.vin = c->vb[c->xv];
-    A.xout = c->xb[c->xv];
+    A.xout = cur_x(c);
     A.vout = c->vb[c->xv];
     A.cid = c->cidStd;
     A.seeds = c->seeds;
@@ -1092,8 +1117,8 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     cudaSetDevice(c->device);
     void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->offb[0], c->offb[1], c->cellb[0], c->cellb[1],
                     c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd, c->sortKeys,
-                    c->idxStd.count, c->idxStd.packed, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
-                    c->idxSrd.count, c->idxSrd.packed, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
+                    c->idxStd.count, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
+                    c->idxSrd.count, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow, c->ovDone,
@@ -1113,8 +1138,16 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
         if (e) cudaEventDestroy(e);
     if (c->side) cudaStreamSynchronize(c->side);
     if (c->walls) cudaStreamSynchronize(c->walls);
-    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone, c->sideDone})
+    for (cudaStream_t q : {c->up, c->down})
+        if (q) cudaStreamSynchronize(q);
+    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone, c->sideDone,
+                          c->upDone[0], c->upDone[1], c->inFree[0], c->inFree[1], c->outReady[0], c->outReady[1],
+                          c->downDone[0], c->downDone[1]})
         if (e) cudaEventDestroy(e);
+    for (double2* b : {c->jobIn[0], c->jobIn[1], c->jobOut[0], c->jobOut[1]})
+        if (b) cudaFree(b);
+    for (cudaStream_t q : {c->up, c->down})
+        if (q) cudaStreamDestroy(q);
     for (auto& g : c->gexec)
         if (g) cudaGraphExecDestroy(g);
     if (c->side) cudaStreamDestroy(c->side);
@@ -1180,7 +1213,6 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
         ALLOC(I->count, (size_t)Nc);
         if (cudaMemset(I->count, 0, sizeof(int) * (size_t)std::max(Nc, 1)) != cudaSuccess)
             return fail(set_err(MPCD_ERR_CUDA, "index counts"));
-        ALLOC(I->packed, (size_t)Nc);
         ALLOC(I->start, (size_t)Nc + 1);
         ALLOC(I->pos, (size_t)n);
         ALLOC(I->slots, (size_t)n);
@@ -1344,6 +1376,7 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
     CUDA_TRY(cudaSetDevice(c->device));
     c->xv = 0;
     c->pp = 0;
+    c->xflip = 0;
     c->slotsSorted = false;
     if (n > 0 && c->f32) {
         // staged through FP64 scratch, then split into cell, FP32 offset and FP32 velocity
@@ -1400,9 +1433,9 @@ static int get_state_impl(mpcd_ctx* c, double* x, double* v, bool toHost) {
         if (rc) return rc;
         return check_device(c);
     }
-    double2* tx = c->xb[c->xv ^ 1];
+    double2* tx = spare_x(c);
     double2* tv = c->vb[c->xv ^ 1];
-    k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv); ++c->launches;
+    k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cur_x(c), c->vb[c->xv], c->pidb[c->pp], c->n, tx, tv); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     if (x) CUDA_TRY(cudaMemcpyAsync(x, tx, sizeof(double2) * (size_t)c->n, k, c->stream));
     if (v) CUDA_TRY(cudaMemcpyAsync(v, tv, sizeof(double2) * (size_t)c->n, k, c->stream));
@@ -1416,7 +1449,7 @@ int mpcd_stream(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
-    k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->vb[c->xv]); ++c->launches;
+    k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, cur_x(c), c->vb[c->xv]); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     invalidate_positions(c);
     return check_device(c);
@@ -1448,7 +1481,7 @@ int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
     if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift, nullptr); ++c->launches;
-    k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, c->xb[c->xv], c->W.srdShift, c->cidSrd); ++c->launches;
+    k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, cur_x(c), c->W.srdShift, c->cidSrd); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     c->srdCellsValid = true;
     if (cid_out && c->n > 0) {
@@ -1687,9 +1720,9 @@ int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closu
         if (wantRep) {
             // repaired state: positions unchanged, velocities = vrep
             if (detail->repairedX || detail->repairedV) {
-                k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->xb[c->xv], c->vrep, c->pidb[c->pp], c->n,
-                                                                              c->xb[c->xv ^ 1], c->vb[c->xv ^ 1]); ++c->launches;
-                if (detail->repairedX) CUDA_TRY(cudaMemcpyAsync(detail->repairedX, c->xb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+                k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cur_x(c), c->vrep, c->pidb[c->pp], c->n,
+                                                                              spare_x(c), c->vb[c->xv ^ 1]); ++c->launches;
+                if (detail->repairedX) CUDA_TRY(cudaMemcpyAsync(detail->repairedX, spare_x(c), sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
                 if (detail->repairedV) CUDA_TRY(cudaMemcpyAsync(detail->repairedV, c->vb[c->xv ^ 1], sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
                 CUDA_TRY(cudaStreamSynchronize(c->stream));
             }
@@ -1809,7 +1842,7 @@ static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr
 // device (step_begin, run by the step's k_srd_shift, increments *dStep), so one graph serves every step. Needs the step's
 // sign stream prefetched by the step before (signsStep), like the eager path's fast case.
 static int graph_step(mpcd_ctx* c, int64_t step) {
-    const int key = c->xv * 2 + c->pp;
+    const int key = (c->xv * 2 + c->pp) * 2 + c->xflip;
     if (!c->gexec[key]) {
         const int64_t l0 = c->launches;
         CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1832,11 +1865,13 @@ static int graph_step(mpcd_ctx* c, int64_t step) {
         }
         c->gkernels[key] = c->launches - l0;
         c->launches = l0;
-        c->gpost[key] = {c->xv, c->pp, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
+        c->gpost[key] = {c->xv, c->pp, c->xflip, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
     } else {
         const auto& f = c->gpost[key];  // host-side state after the step, as step_once leaves it
         c->xv = f.xv;
         c->pp = f.pp;
+        c->xflip = f.xflip;
+        c->slotsSorted = true;
         c->cidStdValid = f.cidStdValid;
         c->srdCellsValid = f.srdCellsValid;
         c->idxStdValid = f.idxStdValid;
@@ -1935,6 +1970,110 @@ int mpcd_step(mpcd_ctx* c, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* l
         c->last = M;
     }
     return MPCD_OK;
+}
+
+// the state from device buffers (x, v: n double2 each, particle-id order), enqueued on the
+// context's stream without a host synchronisation
+static int load_state_async(mpcd_ctx* c, const double2* x, const double2* v) {
+    c->xv = 0;
+    c->pp = 0;
+    c->xflip = 0;
+    c->slotsSorted = false;
+    if (c->n > 0) {
+        if (c->f32) {
+            k_f32_from<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, x, v, c->n, view32(c, 0)); ++c->launches;
+        } else {
+            CUDA_TRY(cudaMemcpyAsync(c->xb[0], x, sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
+            CUDA_TRY(cudaMemcpyAsync(c->vb[0], v, sizeof(double2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        k_iota<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->pidb[0], c->n); ++c->launches;
+    }
+    invalidate_positions(c);
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+// the state into device buffers in particle-id order, enqueued on the context's stream
+static int store_state_async(mpcd_ctx* c, double2* x, double2* v) {
+    if (c->n == 0) return MPCD_OK;
+    if (c->f32) {
+        k_f32_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view32(c, c->xv), c->pidb[c->pp], c->n, x, v);
+    } else {
+        k_gather_by_pid<<<blocks_for(c->n), kThreads, 0, c->stream>>>(cur_x(c), c->vb[c->xv], c->pidb[c->pp], c->n, x, v);
+    }
+    ++c->launches;
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
+static int ensure_job_buffers(mpcd_ctx* c) {
+    if (c->up) return MPCD_OK;
+    for (int b = 0; b < 2; ++b) {
+        int rc = dalloc(&c->jobIn[b], 2 * (size_t)c->n);
+        if (!rc) rc = dalloc(&c->jobOut[b], 2 * (size_t)c->n);
+        if (rc) return rc;
+        for (cudaEvent_t* e : {&c->upDone[b], &c->inFree[b], &c->outReady[b], &c->downDone[b]})
+            CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->down, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking));
+    return MPCD_OK;
+}
+
+int mpcd_run_jobs(mpcd_ctx* c, int64_t njobs, const double* const* x_in, const double* const* v_in, int64_t step0,
+                  int64_t nsteps, double* const* x_out, double* const* v_out) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (njobs < 0 || nsteps < 0) return set_err(MPCD_ERR_INVALID_ARG, "njobs and nsteps must be >= 0");
+    if (njobs == 0) return MPCD_OK;
+    if (!x_in || !v_in || !x_out || !v_out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    for (int64_t j = 0; j < njobs; ++j)
+        if (!x_in[j] || !v_in[j] || !x_out[j] || !v_out[j]) return set_err(MPCD_ERR_INVALID_ARG, "null job buffer");
+    if (nsteps > 0 &&
+        (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution || !c->pc.useLiquidClosure))
+        return set_err(MPCD_ERR_INVALID_ARG, "the benchmark step needs useIncompressibleRedistribution, useZoneRedistribution and useLiquidClosure");
+    if (nsteps > 0 && (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled ||
+                       c->pc.useInterfaceVelocityReorientation))
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = ensure_job_buffers(c);
+    if (rc) return rc;
+    const size_t bytes = sizeof(double2) * (size_t)c->n;
+    // job j's input into jobIn[j & 1], once the load of job j-2 has read that buffer
+    auto upload = [&](int64_t j) -> int {
+        const int b = (int)(j & 1);
+        CUDA_TRY(cudaStreamWaitEvent(c->up, c->inFree[b], 0));
+        CUDA_TRY(cudaMemcpyAsync(c->jobIn[b], x_in[j], bytes, cudaMemcpyHostToDevice, c->up));
+        CUDA_TRY(cudaMemcpyAsync(c->jobIn[b] + c->n, v_in[j], bytes, cudaMemcpyHostToDevice, c->up));
+        CUDA_TRY(cudaEventRecord(c->upDone[b], c->up));
+        return MPCD_OK;
+    };
+    // events not yet recorded count as complete in waits
+    for (int64_t j = 0; j < njobs && !rc; ++j) {
+        const int b = (int)(j & 1);
+        if (j == 0) rc = upload(0);
+        if (rc) break;
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->upDone[b], 0));
+        rc = load_state_async(c, c->jobIn[b], c->jobIn[b] + c->n);
+        if (rc) break;
+        CUDA_TRY(cudaEventRecord(c->inFree[b], c->stream));
+        if (j + 1 < njobs) rc = upload(j + 1);  // overlaps this job's steps
+        if (!rc) rc = run_steps(c, step0 + j * nsteps, nsteps, false);
+        if (rc) break;
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->downDone[b], 0));  // job j-2's result has left
+        rc = store_state_async(c, c->jobOut[b], c->jobOut[b] + c->n);
+        if (rc) break;
+        CUDA_TRY(cudaEventRecord(c->outReady[b], c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->down, c->outReady[b], 0));
+        CUDA_TRY(cudaMemcpyAsync(x_out[j], c->jobOut[b], bytes, cudaMemcpyDeviceToHost, c->down));
+        CUDA_TRY(cudaMemcpyAsync(v_out[j], c->jobOut[b] + c->n, bytes, cudaMemcpyDeviceToHost, c->down));
+        CUDA_TRY(cudaEventRecord(c->downDone[b], c->down));
+        // no host synchronisation per job: a status read would queue behind this job's
+        // download on the copy engine; the device status is checked once at the end
+    }
+    const cudaError_t e1 = cudaStreamSynchronize(c->up), e2 = cudaStreamSynchronize(c->down);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return set_err(MPCD_ERR_CUDA, "job copies");
+    return check_device(c);
 }
 
 int mpcd_step_metrics(mpcd_ctx* c, mpcd_step_metrics_c* out) {
@@ -2182,9 +2321,9 @@ struct mpcd_batch {
     size_t zSmem = 0;
     // whole batched steps replayed from CUDA graphs, one per buffer parity of the replicas
     bool useGraphs = true;
-    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-    std::vector<mpcd_ctx::HostFlags> gpost[4];
-    std::vector<int64_t> gkernels[4];
+    cudaGraphExec_t gexec[8] = {};  // by (xv, pp, xflip) of the replicas at step entry
+    std::vector<mpcd_ctx::HostFlags> gpost[8];
+    std::vector<int64_t> gkernels[8];
     long long** dStepPtrs = nullptr;  // each replica's device step counter
 };
 
@@ -2246,7 +2385,7 @@ static int batch_step_body(mpcd_batch* b, int64_t step) {
 static int batch_graph_step(mpcd_batch* b, int64_t step) {
     const int n = (int)b->members.size();
     mpcd_ctx* c0 = b->members[0];
-    const int key = c0->xv * 2 + c0->pp;
+    const int key = (c0->xv * 2 + c0->pp) * 2 + c0->xflip;
     if (!b->gexec[key]) {
         std::vector<int64_t> l0(n);
         for (int r = 0; r < n; ++r) l0[r] = b->members[r]->launches;
@@ -2274,7 +2413,7 @@ static int batch_graph_step(mpcd_batch* b, int64_t step) {
             mpcd_ctx* c = b->members[r];
             b->gkernels[key][r] = c->launches - l0[r];
             c->launches = l0[r];
-            b->gpost[key][r] = {c->xv, c->pp, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
+            b->gpost[key][r] = {c->xv, c->pp, c->xflip, c->cidStdValid, c->srdCellsValid, c->idxStdValid, c->refValid};
         }
     }
     for (int r = 0; r < n; ++r) {
@@ -2282,6 +2421,8 @@ static int batch_graph_step(mpcd_batch* b, int64_t step) {
         const mpcd_ctx::HostFlags& f = b->gpost[key][r];
         c->xv = f.xv;
         c->pp = f.pp;
+        c->xflip = f.xflip;
+        c->slotsSorted = true;
         c->cidStdValid = f.cidStdValid;
         c->srdCellsValid = f.srdCellsValid;
         c->idxStdValid = f.idxStdValid;
@@ -2422,7 +2563,7 @@ int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device
         bool graph = b->useGraphs;
         for (mpcd_ctx* c : b->members)
             graph = graph && c->useGraphs && c->signsStep[s & 1] == s && c->xv == b->members[0]->xv &&
-                    c->pp == b->members[0]->pp && c->collideShape >= 0;
+                    c->pp == b->members[0]->pp && c->xflip == b->members[0]->xflip && c->collideShape >= 0;
         const int rc = graph ? batch_graph_step(b, s) : batch_step_body(b, s);
         if (rc) return rc;
     }

@@ -91,16 +91,47 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_small(const uint64_t* __r
 }
 
 // ------------------------------------------------------------------ cell index
-// pack (count, count >= 2) so one scan yields both the segment starts and the rank of each
-// cell among cells holding at least two particles (the SRD sign stream index). Each count is
-// cleared once read, ready for the next build's histogram.
-__global__ void k_pack_counts(int* __restrict__ count, int Nc, uint64_t* __restrict__ packed) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < Nc) {
-        const int k = count[c];
-        count[c] = 0;
-        packed[c] = (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+// A cell's count is scanned packed as (count, count >= 2), so one scan yields both the segment
+// starts and the rank of each cell among cells holding at least two particles (the SRD sign
+// stream index). Each count is cleared once read, ready for the next build's histogram.
+__device__ __forceinline__ uint64_t pack_count(int k) { return (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32); }
+
+// k_scan_reduce over the packed counts
+__global__ void k_count_scan_reduce(const int* __restrict__ count, int64_t n, uint64_t* __restrict__ blockSums) {
+    __shared__ uint64_t sh[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
+        if (i < n) s += pack_count(count[i]);
     }
+    uint64_t tot;
+    block_exclusive_scan(s, sh, &tot);
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = tot;
+}
+
+// k_scan_apply over the packed counts, clearing them
+__global__ void k_count_scan_apply(int* __restrict__ count, int64_t n, const uint64_t* __restrict__ blockSums,
+                                   uint64_t* __restrict__ out) {
+    __shared__ uint64_t sh[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint64_t v[kScanItems];
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = 0ULL;
+        if (base + k < n) {
+            v[k] = pack_count(count[base + k]);
+            count[base + k] = 0;
+        }
+        s += v[k];
+    }
+    uint64_t tot;
+    uint64_t ex = block_exclusive_scan(s, sh, &tot) + blockSums[blockIdx.x];
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (base + kScanItems >= n && base < n) out[n] = ex;  // the thread holding the last element
 }
 
 // one block: the packed counts' exclusive scan into start (Nc <= kSmallScan), clearing the counts
@@ -111,8 +142,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restr
     const int a = min(Nc, (int)threadIdx.x * per), b = min(Nc, a + per);
     uint64_t sum = 0;
     for (int i = a; i < b; ++i) {
-        const int k = count[i];
-        sum += (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+        sum += pack_count(count[i]);
     }
     uint64_t tot;
     uint64_t ex = block_exclusive_scan(sum, sh, &tot);
@@ -120,7 +150,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restr
         const int k = count[i];
         count[i] = 0;
         start[i] = ex;
-        ex += (uint64_t)(uint32_t)k | ((uint64_t)(k >= 2) << 32);
+        ex += pack_count(k);
     }
     if (threadIdx.x == 0) start[Nc] = tot;
 }

@@ -73,6 +73,8 @@ def lib():
         "mpcd_zone_owner_map": ([C.c_void_p, C.c_int32, _ip], C.c_int),
         "mpcd_step": ([C.c_void_p, C.c_int64, C.c_int64, P(_abi.StepMetricsC)], C.c_int),
         "mpcd_step_metrics": ([C.c_void_p, P(_abi.StepMetricsC)], C.c_int),
+        "mpcd_run_jobs": ([C.c_void_p, C.c_int64, P(C.c_void_p), P(C.c_void_p), C.c_int64, C.c_int64,
+                           P(C.c_void_p), P(C.c_void_p)], C.c_int),
         "mpcd_step_timed": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double)], C.c_int),
         "mpcd_step_profile": ([C.c_void_p, C.c_int64, C.c_int64, P(C.c_double), C.c_int], C.c_int),
         "mpcd_launch_count": ([C.c_void_p], C.c_int64),
@@ -208,6 +210,26 @@ class Context:
         v = np.empty(2 * self.n) if v is None else v
         _check(lib().mpcd_get_state(self.h, x, v))
         return x, v
+
+    def run_jobs(self, xs, vs, step0, nsteps, xo=None, vo=None):
+        """Independent jobs with host buffers (mpcd_run_jobs): job j loads (xs[j], vs[j]), runs
+        steps step0 + j*nsteps + 1 .. step0 + (j+1)*nsteps and stores its result in (xo[j], vo[j])
+        (new arrays when not given); the copies of neighbouring jobs overlap each job's steps.
+        Returns (xo, vo)."""
+        k = len(xs)
+        if len(vs) != k:
+            raise ValueError("xs and vs differ in length")
+        for a in list(xs) + list(vs):
+            if a.dtype != np.float64 or a.size != 2 * self.n or not a.flags.c_contiguous:
+                raise ValueError("job buffers must be contiguous float64 arrays of 2n values")
+        xo = [np.empty(2 * self.n) for _ in range(k)] if xo is None else xo
+        vo = [np.empty(2 * self.n) for _ in range(k)] if vo is None else vo
+        for a in list(xo) + list(vo):
+            if a.dtype != np.float64 or a.size != 2 * self.n or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError("job outputs must be writeable contiguous float64 arrays of 2n values")
+        ptrs = lambda arrs: (C.c_void_p * max(k, 1))(*[a.ctypes.data for a in arrs])
+        _check(lib().mpcd_run_jobs(self.h, k, ptrs(xs), ptrs(vs), step0, nsteps, ptrs(xo), ptrs(vo)))
+        return xo, vo
 
     def set_state_device(self, x_ptr, v_ptr):
         _check(lib().mpcd_set_state_device(self.h, C.c_void_p(x_ptr), C.c_void_p(v_ptr), self.n))
