@@ -256,10 +256,11 @@ int mpcd_step_profile(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, double* phas
  * metrics row are replayed from a captured graph with device-side seeds. 0 turns it off. */
 int mpcd_ctx_set_graphs(mpcd_ctx* ctx, int enable);
 /* Tile shape of the SRD collision (cells x threads per block: 0 = 32x128, 1 = 64x256,
- * 2 = 128x256, 3 = 256x512). A context times the four on its own state at its first eager
- * collision and keeps the fastest (the autotuner). shape >= 0 sets one instead; -1 leaves it.
- * *in_use (nullable): the shape in use, -1 before the first collision. Every shape gives the
- * same results. */
+ * 2 = 128x256, 3 = 256x512, 4 = 16x128, 5 = 32x256, 6 = 16x64). A context times them all on
+ * its own state at its first eager collision on cell-sorted slots and keeps the fastest (the
+ * autotuner). shape >= 0 sets one instead; -1 leaves it. *in_use (nullable): the shape in use,
+ * -1 before the autotuner has run. Every shape gives the same results. */
+#define MPCD_COLLIDE_SHAPES 7
 int mpcd_ctx_collide_shape(mpcd_ctx* ctx, int32_t shape, int32_t* in_use);
 
 /* ---------------------------------------------------------------- batched replicas */

@@ -184,7 +184,7 @@ struct mpcd_ctx {
     int collideShape = -1;     // index into kCollideShape; -1: autotune at the next eager collision
                                // that finds the slots in (cell, id) order
     bool slotsSorted = false;  // slots in (cell, id) order: false after a state upload until a step
-    int collideTiles[kCollideShapes] = {0, 0, 0, 0};
+    int collideTiles[kCollideShapes] = {};
     size_t zSmem = 0;
     int ovMaxCells = 0, ovWinCap = 0, ovArenaCap = 0, ovNsmCap = 0;
     double* passOut = nullptr;  // 4 doubles
@@ -704,6 +704,9 @@ static int launch_collide(mpcd_ctx* c, int k, int buf, const uint8_t* signs, con
         MPCD_COLLIDE(1)
         MPCD_COLLIDE(2)
         MPCD_COLLIDE(3)
+        MPCD_COLLIDE(4)
+        MPCD_COLLIDE(5)
+        MPCD_COLLIDE(6)
         default: return set_err(MPCD_ERR_INVALID_ARG, "collision tile shape out of range");
     }
 #undef MPCD_COLLIDE
@@ -1300,6 +1303,9 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
         MPCD_COLLIDE_ATTR(1)
         MPCD_COLLIDE_ATTR(2)
         MPCD_COLLIDE_ATTR(3)
+        MPCD_COLLIDE_ATTR(4)
+        MPCD_COLLIDE_ATTR(5)
+        MPCD_COLLIDE_ATTR(6)
 #undef MPCD_COLLIDE_ATTR
         if (!ok) return fail(set_err(MPCD_ERR_CUDA, "collision shared memory attribute"));
     }

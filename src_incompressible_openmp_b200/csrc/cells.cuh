@@ -106,8 +106,9 @@ __device__ __forceinline__ bool collide_cell(const DevParams& P, uint64_t start0
 struct CollideShape {
     int cells, threads;
 };
-constexpr int kCollideShapes = 4;
-constexpr CollideShape kCollideShape[kCollideShapes] = {{32, 128}, {64, 256}, {128, 256}, {256, 512}};
+constexpr int kCollideShapes = 7;
+constexpr CollideShape kCollideShape[kCollideShapes] = {{32, 128}, {64, 256}, {128, 256}, {256, 512},
+                                                        {16, 128}, {32, 256},  {16, 64}};
 
 template <class V, int kCollideCells, int kCollideThreads>
 __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, const uint64_t* __restrict__ start,
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_srd_collide(DevParams P, co
         }
         return;
     }
+#pragma unroll 4
     for (int i = t; i < B - A; i += blockDim.x) {
         const int sl = slots[A + i];
         ts[i] = sl;

@@ -223,15 +223,17 @@ inline int rank_cells_per_block(int64_t n, int Nc) {
 
 __device__ __forceinline__ int seg_lo(uint64_t s) { return (int)(uint32_t)s; }
 
-// slots[start[c] + rank] = slot of the key of that rank among cell c's keys (pid, then slot:
-// ascending particle id). A block takes cellsPerBlock consecutive cells, stages their keys in
-// shared memory (splitting the run of cells where it exceeds kRankCap keys) and ranks each key
-// against its own cell's keys. A cell above kRankCap keys on its own is ranked from global memory.
+// slots[start[c] + rank] = slot of the key of that rank among cell c's keys (ascending
+// particle id; ids are unique, so they alone rank a cell's keys). A block takes cellsPerBlock
+// consecutive cells, stages their ids and slots in shared memory (splitting the run of cells
+// where it exceeds kRankCap keys) and ranks each key against its own cell's ids. A cell above
+// kRankCap keys on its own is ranked from global memory.
 __global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __restrict__ start, int Nc,
                                                             int cellsPerBlock, const uint64_t* __restrict__ keys,
                                                             int* __restrict__ slots) {
-    __shared__ uint64_t key[kRankCap];
-    __shared__ uint32_t seg[kRankCap];  // per key: its cell's segment [a, b) in the tile, a | b << 16
+    __shared__ uint32_t kid[kRankCap];   // particle id
+    __shared__ int ksl[kRankCap];        // slot
+    __shared__ uint32_t seg[kRankCap];   // per key: its cell's segment [a, b) in the tile, a | b << 16
     const int t = threadIdx.x;
     const int c0 = (int)min((int64_t)blockIdx.x * cellsPerBlock, (int64_t)Nc);
     const int c1 = min(Nc, c0 + cellsPerBlock);
@@ -254,8 +256,9 @@ __global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __re
             const int b = seg_lo(start[cs + 1]);
             for (int i = A + t; i < b; i += kRankThreads) {
                 const uint64_t k = keys[i];
+                const uint32_t id = (uint32_t)(k >> 32);
                 int r = 0;
-                for (int j = A; j < b; ++j) r += keys[j] < k;
+                for (int j = A; j < b; ++j) r += (uint32_t)(keys[j] >> 32) < id;
                 slots[A + r] = (int)(uint32_t)k;
             }
             ++cs;
@@ -263,7 +266,11 @@ __global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __re
         }
         const int m = seg_lo(start[ce]) - A;
 #pragma unroll 4
-        for (int i = t; i < m; i += kRankThreads) key[i] = keys[A + i];
+        for (int i = t; i < m; i += kRankThreads) {
+            const uint64_t k = keys[A + i];
+            kid[i] = (uint32_t)(k >> 32);
+            ksl[i] = (int)(uint32_t)k;
+        }
         for (int c = cs + t; c < ce; c += kRankThreads) {
             const int a = seg_lo(start[c]) - A, b = seg_lo(start[c + 1]) - A;
             for (int j = a; j < b; ++j) seg[j] = (uint32_t)a | ((uint32_t)b << 16);
@@ -272,10 +279,11 @@ __global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __re
         for (int i = t; i < m; i += kRankThreads) {
             const uint32_t sg = seg[i];
             const int a = (int)(sg & 0xffffu), b = (int)(sg >> 16);
-            const uint64_t k = key[i];
+            const uint32_t id = kid[i];
             int r = 0;
-            for (int j = a; j < b; ++j) r += key[j] < k;
-            slots[A + a + r] = (int)(uint32_t)k;
+#pragma unroll 4
+            for (int j = a; j < b; ++j) r += kid[j] < id;
+            slots[A + a + r] = ksl[i];
         }
         __syncthreads();
         cs = ce;

@@ -165,6 +165,7 @@ def cell_fields_static(params, x_ptr, v_ptr, n, rho_target, out_ptrs, stream=0):
 
 
 FORMS = {"f64": 0, "f32": 1}  # mpcd_state_form
+COLLIDE_SHAPES = 7  # MPCD_COLLIDE_SHAPES
 
 
 class Context:
@@ -327,7 +328,7 @@ class Context:
         return int(lib().mpcd_launch_count(self.h))
 
     def collide_shape(self, shape=-1):
-        """mpcd_ctx_collide_shape: set the collision tile shape (0..3) or, with -1, only query;
+        """mpcd_ctx_collide_shape: set the collision tile shape (0 .. COLLIDE_SHAPES-1) or, with -1, only query;
         returns the shape in use (-1 before the autotuner has run)."""
         r = C.c_int32()
         _check(lib().mpcd_ctx_collide_shape(self.h, shape, C.byref(r)))

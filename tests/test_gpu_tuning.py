@@ -28,9 +28,9 @@ def test_every_collision_shape_gives_the_same_state():
         ctx.step(0, 1)
         assert ctx.collide_shape() == -1  # the first step sorts the uploaded slots
         ctx.step(1, 2)
-        assert 0 <= ctx.collide_shape() < 4  # picked by timing
+        assert 0 <= ctx.collide_shape() < native.COLLIDE_SHAPES  # picked by timing
         out.append(ctx.get_state())
-    for shape in range(4):
+    for shape in range(native.COLLIDE_SHAPES):
         with native.Context(p) as ctx:
             ctx.set_state(x, v)
             assert ctx.collide_shape(shape) == shape
@@ -46,7 +46,7 @@ def test_shape_out_of_range_rejected():
     p = poiseuille_params(16, 16, 5)
     with native.Context(p) as ctx:
         with pytest.raises(native.MpcdError):
-            ctx.collide_shape(4)
+            ctx.collide_shape(native.COLLIDE_SHAPES)
 
 
 def test_contexts_of_different_density_keep_their_shared_memory():
@@ -61,7 +61,7 @@ def test_contexts_of_different_density_keep_their_shared_memory():
         with native.Context(sparse) as b:
             xs, vs = uniform_state(sparse, 4)
             b.set_state(xs, vs)
-            for shape in range(4):
+            for shape in range(native.COLLIDE_SHAPES):
                 a.collide_shape(shape)
                 a.step(shape, 1)
                 b.collide_shape(shape)
