@@ -910,27 +910,41 @@ int zone_pass_kernel(mpcd_ctx* c) {
     return MPCD_OK;
 }
 
-int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
-    const ZoneArgs& A = c->zA;
-    const int mode = c->zMode;
-    ZoneArgs B = A;
-    B.order = nullptr;
-    B.maxCells = c->ovMaxCells;
-    B.winCap = c->ovWinCap;
-    B.arenaCap = c->ovArenaCap;
-    B.nsmCap = c->ovNsmCap;
-    double* mout = c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0);
-    if (c->f32)
-        k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock, c->ovDone, mout);
-    else
-        k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(B, c->ovMem, c->ovPerBlock, c->ovDone, mout);
-    ++c->launches;
-    CUDA_TRY(cudaGetLastError());
-    mark(c, pf, 8);
+// the overflow kernel's job for the pass in progress (its arguments with the global-memory
+// working set's capacities)
+OverflowJob overflow_job(const mpcd_ctx* c) {
+    OverflowJob J{};
+    J.A = c->zA;
+    J.A.order = nullptr;
+    J.A.maxCells = c->ovMaxCells;
+    J.A.winCap = c->ovWinCap;
+    J.A.arenaCap = c->ovArenaCap;
+    J.A.nsmCap = c->ovNsmCap;
+    J.gmem = c->ovMem;
+    J.perBlock = c->ovPerBlock;
+    J.blocksDone = c->ovDone;
+    J.metricsOut = c->passOut + (c->zMode == MPCD_LAYOUT_SHIFTED ? 4 : 0);
+    return J;
+}
+
+// host-side state after a pass: velocities in the other buffer, positions in place
+void zone_pass_flip(mpcd_ctx* c) {
     c->xv ^= 1;
     c->xflip ^= 1;
     c->idxStdValid = false;  // cid was updated for moved particles; positions changed
     c->srdCellsValid = false;
+}
+
+int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
+    const OverflowJob J = overflow_job(c);
+    if (c->f32)
+        k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(J.A, J.gmem, J.perBlock, J.blocksDone, J.metricsOut);
+    else
+        k_zone_overflow<false><<<c->ovBlocks, 32, 0, c->stream>>>(J.A, J.gmem, J.perBlock, J.blocksDone, J.metricsOut);
+    ++c->launches;
+    CUDA_TRY(cudaGetLastError());
+    mark(c, pf, 8);
+    zone_pass_flip(c);
     return MPCD_OK;
 }
 
@@ -1760,15 +1774,16 @@ static int count_metrics(mpcd_ctx* c, double* dst /* device: 3 doubles */) {
 // reference fields, base-pass prep), mid (base-pass finish, shifted-pass prep), tail
 // (shifted-pass finish, closure and re-sort). step_once runs them with each replica's own
 // zone kernels; a batch runs the zone kernels of all its replicas in one launch.
+// step_mid and step_tail begin with the finish of a zone pass; their _b parts are the rest, so
+// that a batch can run the finish and the following index build for all replicas at once.
 static int step_head(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     const uint64_t s = (uint64_t)step;
-    int rc;
     if (metrics) CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
     mark(c, pf, -1);
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift,
                                         c->graphMode ? c->stepSeeds : nullptr, c->graphMode ? c->dStep : nullptr,
                                         c->stepSeeds); ++c->launches;
-    rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
+    int rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
     if (rc) return rc;
     c->cidStdValid = true;
     c->srdCellsValid = true;
@@ -1781,10 +1796,9 @@ static int step_head(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     return zone_pass_prep(c, MPCD_LAYOUT_BASE, 88172645463325252ULL + 10007ULL * s, pf);
 }
 
-static int step_mid(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
+static int step_mid_b(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     const uint64_t s = (uint64_t)step;
-    int rc = zone_pass_finish(c, pf);
-    if (rc) return rc;
+    int rc = MPCD_OK;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
         rc = ensure_std_index(c);
@@ -1796,9 +1810,13 @@ static int step_mid(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     return zone_pass_prep(c, MPCD_LAYOUT_SHIFTED, 88172645463325252ULL + 4099ULL + 10007ULL * s, pf);
 }
 
-static int step_tail(mpcd_ctx* c, bool metrics, Prof* pf) {
-    int rc = zone_pass_finish(c, pf);
-    if (rc) return rc;
+static int step_mid(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
+    const int rc = zone_pass_finish(c, pf);
+    return rc ? rc : step_mid_b(c, step, metrics, pf);
+}
+
+static int step_tail_b(mpcd_ctx* c, bool metrics, Prof* pf) {
+    int rc = MPCD_OK;
     if (metrics) {
         CUDA_TRY(cudaEventRecord(c->ev[4], c->stream));
         rc = ensure_std_index(c);
@@ -1832,6 +1850,11 @@ static int step_tail(mpcd_ctx* c, bool metrics, Prof* pf) {
     }
     if (c->graphMode) CUDA_TRY(cudaStreamWaitEvent(c->stream, c->sideDone, 0));  // join the sign prefetch
     return MPCD_OK;
+}
+
+static int step_tail(mpcd_ctx* c, bool metrics, Prof* pf) {
+    const int rc = zone_pass_finish(c, pf);
+    return rc ? rc : step_tail_b(c, metrics, pf);
 }
 
 static int step_once(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf = nullptr) {
@@ -2325,12 +2348,22 @@ struct mpcd_batch {
     ZoneArgs* dArgs = nullptr;
     int* dOffs = nullptr;
     size_t zSmem = 0;
+    OverflowJob* hOv = nullptr;  // the overflow kernels' jobs, staged the same way
+    OverflowJob* dOv = nullptr;
+    int ovBlocks = 0;            // overflow blocks per replica (the same for all)
     // whole batched steps replayed from CUDA graphs, one per buffer parity of the replicas
     bool useGraphs = true;
     cudaGraphExec_t gexec[8] = {};  // by (xv, pp, xflip) of the replicas at step entry
     std::vector<mpcd_ctx::HostFlags> gpost[8];
     std::vector<int64_t> gkernels[8];
     long long** dStepPtrs = nullptr;  // each replica's device step counter
+    // the replicas' standard-grid index builds after a zone pass as one launch per kernel
+    // (batch_index): job tables per particle-id buffer parity, block prefix sums
+    bool indexBatched = false;  // every replica has Nc <= kSmallScan
+    IndexJob* dJobs[2] = {};
+    int* dOffsHist = nullptr;   // count + 1: blocks of the histogram and the scatter
+    int* dOffsRank = nullptr;   // count + 1: blocks of the rank sort
+    int histBlocks = 0, rankBlocks = 0;
 };
 
 __global__ void k_set_steps(long long** steps, int n, long long value) {
@@ -2362,28 +2395,75 @@ static int batch_zone_kernel(mpcd_batch* b, int pass) {
     return MPCD_OK;
 }
 
-// one batched step: each replica's parts on its own streams, the zone kernels of all
-// replicas as one launch per pass on the batch stream (fork/join by events)
-static int batch_step_body(mpcd_batch* b, int64_t step) {
-    const int n = (int)b->members.size();
-    int rc;
-    for (int part = 0; part < 3; ++part) {
-        CUDA_TRY(cudaEventRecord(b->fork, b->stream));
-        for (int r = 0; r < n; ++r) {
-            mpcd_ctx* c = b->members[r];
-            CUDA_TRY(cudaStreamWaitEvent(c->stream, b->fork, 0));
-            rc = part == 0 ? step_head(c, step, false, nullptr) : part == 1 ? step_mid(c, step, false, nullptr)
-                                                                         : step_tail(c, false, nullptr);
-            if (rc) return rc;
-            CUDA_TRY(cudaEventRecord(b->done[r], c->stream));
-            CUDA_TRY(cudaStreamWaitEvent(b->stream, b->done[r], 0));
-        }
-        if (part < 2) {
-            rc = batch_zone_kernel(b, part);
-            if (rc) return rc;
-        }
+// f(c) on every replica, each on its own stream, forked from and joined back into the batch
+// stream by events
+template <class F>
+static int batch_each(mpcd_batch* b, F f) {
+    CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+    for (size_t r = 0; r < b->members.size(); ++r) {
+        mpcd_ctx* c = b->members[r];
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, b->fork, 0));
+        const int rc = f(c);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(b->done[r], c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(b->stream, b->done[r], 0));
     }
     return MPCD_OK;
+}
+
+// the standard-grid cell index of every replica, built by one launch per kernel on the batch
+// stream (the replicas share one particle-id buffer parity)
+static int batch_index(mpcd_batch* b) {
+    const int n = (int)b->members.size();
+    const IndexJob* jobs = b->dJobs[b->members[0]->pp];
+    mpcd_ctx* c0 = b->members[0];
+    if (b->histBlocks > 0) {
+        k_histogram_batch<<<b->histBlocks, kThreads, 0, b->stream>>>(jobs, b->dOffsHist, n); ++c0->launches;
+    }
+    k_scan_counts_small_batch<<<n, kScanThreads, 0, b->stream>>>(jobs); ++c0->launches;
+    if (b->histBlocks > 0) {
+        k_scatter_keys_batch<<<b->histBlocks, kThreads, 0, b->stream>>>(jobs, b->dOffsHist, n); ++c0->launches;
+    }
+    k_cell_rank_batch<<<b->rankBlocks, kRankThreads, 0, b->stream>>>(jobs, b->dOffsRank, n); ++c0->launches;
+    CUDA_TRY(cudaGetLastError());
+    for (mpcd_ctx* c : b->members) c->idxStdValid = true;
+    return MPCD_OK;
+}
+
+// the overflow kernels of pass `pass` of every replica in one launch on the batch stream (after
+// the batched zone kernel), then each replica's host-side flip; staged like the zone arguments
+static int batch_zone_finish(mpcd_batch* b, int pass) {
+    const int n = (int)b->members.size();
+    const int slot = (b->members[0]->xv & 1) * 2 + pass;
+    OverflowJob* h = b->hOv + (size_t)slot * n;
+    for (int r = 0; r < n; ++r) h[r] = overflow_job(b->members[r]);
+    OverflowJob* d = b->dOv + (size_t)slot * n;
+    CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(OverflowJob) * n, cudaMemcpyHostToDevice, b->stream));
+    k_zone_overflow_batch<<<n * b->ovBlocks, 32, 0, b->stream>>>(d, b->ovBlocks);
+    ++b->members[0]->launches;
+    CUDA_TRY(cudaGetLastError());
+    for (mpcd_ctx* c : b->members) zone_pass_flip(c);
+    return MPCD_OK;
+}
+
+// one batched step: each replica's parts on its own streams, forked from and joined into the
+// batch stream. Where the replicas are joined anyway (around the zone kernels), the batch
+// stream also runs the overflow kernels of all replicas as one launch and, when every replica
+// is small enough for the one-block scan and all share a particle-id buffer parity, the
+// standard-grid index builds that follow each pass.
+static int batch_step_body(mpcd_batch* b, int64_t step) {
+    bool idx = b->indexBatched;
+    for (mpcd_ctx* c : b->members) idx = idx && c->pp == b->members[0]->pp;
+    int rc = batch_each(b, [&](mpcd_ctx* c) { return step_head(c, step, false, nullptr); });
+    if (!rc) rc = batch_zone_kernel(b, 0);
+    if (!rc) rc = batch_zone_finish(b, 0);
+    if (!rc && idx) rc = batch_index(b);
+    if (!rc) rc = batch_each(b, [&](mpcd_ctx* c) { return step_mid_b(c, step, false, nullptr); });
+    if (!rc) rc = batch_zone_kernel(b, 1);
+    if (!rc) rc = batch_zone_finish(b, 1);
+    if (!rc && idx) rc = batch_index(b);
+    if (!rc) rc = batch_each(b, [&](mpcd_ctx* c) { return step_tail_b(c, false, nullptr); });
+    return rc;
 }
 
 // a batched step replayed from the graph of the replicas' buffer parity (captured on first
@@ -2480,7 +2560,13 @@ int mpcd_batch_destroy(mpcd_batch* b) {
     if (b->hOffs) cudaFreeHost(b->hOffs);
     if (b->dArgs) cudaFree(b->dArgs);
     if (b->dOffs) cudaFree(b->dOffs);
+    if (b->hOv) cudaFreeHost(b->hOv);
+    if (b->dOv) cudaFree(b->dOv);
     if (b->dStepPtrs) cudaFree(b->dStepPtrs);
+    for (IndexJob* j : b->dJobs)
+        if (j) cudaFree(j);
+    if (b->dOffsHist) cudaFree(b->dOffsHist);
+    if (b->dOffsRank) cudaFree(b->dOffsRank);
     if (b->fork) cudaEventDestroy(b->fork);
     for (mpcd_ctx* c : b->members) mpcd_ctx_destroy(c);
     for (cudaEvent_t e : b->done)
@@ -2523,10 +2609,18 @@ int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_b
             b->zSmem = std::max(b->zSmem, b->members[r]->zSmem + (size_t)kZoneArgsSmem);
             steps[(size_t)r] = b->members[r]->dStep;
         }
+        b->ovBlocks = b->members[0]->ovBlocks;
+        for (mpcd_ctx* c : b->members)
+            if (c->ovBlocks != b->ovBlocks) {
+                mpcd_batch_destroy(b);
+                return set_err(MPCD_ERR_INVALID_ARG, "replicas with different overflow block counts");
+            }
         if (cudaMallocHost((void**)&b->hArgs, sizeof(ZoneArgs) * count * nslots) != cudaSuccess ||
             cudaMallocHost((void**)&b->hOffs, sizeof(int) * (count + 1) * nslots) != cudaSuccess ||
             cudaMalloc((void**)&b->dArgs, sizeof(ZoneArgs) * count * nslots) != cudaSuccess ||
             cudaMalloc((void**)&b->dOffs, sizeof(int) * (count + 1) * nslots) != cudaSuccess ||
+            cudaMallocHost((void**)&b->hOv, sizeof(OverflowJob) * count * nslots) != cudaSuccess ||
+            cudaMalloc((void**)&b->dOv, sizeof(OverflowJob) * count * nslots) != cudaSuccess ||
             cudaMalloc((void**)&b->dStepPtrs, sizeof(long long*) * count) != cudaSuccess ||
             cudaMemcpy(b->dStepPtrs, steps.data(), sizeof(long long*) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
             !raise_smem((const void*)k_zone_pass_batch<false>, b->zSmem, device)) {
@@ -2542,6 +2636,38 @@ int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_b
             mpcd_batch_destroy(b);
             return set_err(MPCD_ERR_CUDA, "batch events");
         }
+    {
+        // job tables of the batched index builds (the buffers they name never move)
+        b->indexBatched = true;
+        std::vector<int> oh(1, 0), orank(1, 0);
+        for (mpcd_ctx* c : b->members) {
+            b->indexBatched = b->indexBatched && c->Nc <= kSmallScan;
+            oh.push_back(oh.back() + (c->n > 0 ? blocks_for(c->n, kThreads * kIndexItems) : 0));
+            orank.push_back(orank.back() + blocks_for(c->Nc, c->rankCells));
+        }
+        b->histBlocks = oh.back();
+        b->rankBlocks = orank.back();
+        bool ok = cudaMalloc((void**)&b->dOffsHist, sizeof(int) * oh.size()) == cudaSuccess &&
+                  cudaMalloc((void**)&b->dOffsRank, sizeof(int) * orank.size()) == cudaSuccess &&
+                  cudaMemcpy(b->dOffsHist, oh.data(), sizeof(int) * oh.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(b->dOffsRank, orank.data(), sizeof(int) * orank.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+        for (int q = 0; q < 2 && ok; ++q) {
+            std::vector<IndexJob> jobs;
+            for (mpcd_ctx* c : b->members) {
+                CellIndex& I = c->idxStd;
+                jobs.push_back(IndexJob{c->cidStd, I.count, I.pos, I.start, I.slots, c->pidb[q], c->sortKeys, c->n,
+                                        c->Nc, c->rankCells});
+            }
+            ok = cudaMalloc((void**)&b->dJobs[q], sizeof(IndexJob) * jobs.size()) == cudaSuccess &&
+                 cudaMemcpy(b->dJobs[q], jobs.data(), sizeof(IndexJob) * jobs.size(), cudaMemcpyHostToDevice) ==
+                     cudaSuccess;
+        }
+        if (!ok) {
+            cudaGetLastError();
+            mpcd_batch_destroy(b);
+            return set_err(MPCD_ERR_CUDA, "batch index tables");
+        }
+    }
     *out = b;
     return MPCD_OK;
 }

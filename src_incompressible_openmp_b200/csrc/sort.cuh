@@ -135,8 +135,7 @@ __global__ void k_count_scan_apply(int* __restrict__ count, int64_t n, const uin
 }
 
 // one block: the packed counts' exclusive scan into start (Nc <= kSmallScan), clearing the counts
-__global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restrict__ count, int Nc,
-                                                                     uint64_t* __restrict__ start) {
+__device__ __forceinline__ void scan_counts_small_block(int* __restrict__ count, int Nc, uint64_t* __restrict__ start) {
     __shared__ uint64_t sh[32];
     const int per = (Nc + kScanThreads - 1) / kScanThreads;
     const int a = min(Nc, (int)threadIdx.x * per), b = min(Nc, a + per);
@@ -155,15 +154,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restr
     if (threadIdx.x == 0) start[Nc] = tot;
 }
 
+__global__ void __launch_bounds__(kScanThreads) k_scan_counts_small(int* __restrict__ count, int Nc,
+                                                                     uint64_t* __restrict__ start) {
+    scan_counts_small_block(count, Nc, start);
+}
+
 // pos[s] = arrival order of slot s within its cell (any order; fixed by k_cell_rank).
 // One atomic per run of equal cell ids among consecutive lanes: after the end-of-step
 // re-sort, slots are ordered by cell, so a warp's lanes form a few long runs. Each warp
 // covers kIndexItems runs of 32 consecutive slots, whose atomics are in flight together.
 constexpr int kIndexItems = 4;
 
-__global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict__ count, int* __restrict__ pos) {
+__device__ __forceinline__ void histogram_block(int blk, const int* __restrict__ cid, int n, int* __restrict__ count,
+                                                int* __restrict__ pos) {
     const int lane = threadIdx.x & 31;
-    const int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
+    const int base = ((blk * (int)blockDim.x + (int)threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
     int c[kIndexItems], got[kIndexItems], runStart[kIndexItems];
 #pragma unroll
     for (int k = 0; k < kIndexItems; ++k) c[k] = (base + 32 * k < n) ? cid[base + 32 * k] : -1;
@@ -185,12 +190,17 @@ __global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict_
     }
 }
 
+__global__ void k_histogram(const int* __restrict__ cid, int n, int* __restrict__ count, int* __restrict__ pos) {
+    histogram_block((int)blockIdx.x, cid, n, count, pos);
+}
+
 // keys[start[cid[s]] + pos[s]] = (pid[s] << 32) | s: each cell's segment holds its
 // particles' keys in arrival order (same slot coverage as k_histogram)
-__global__ void k_scatter_keys(const int* __restrict__ cid, const int* __restrict__ pos, const int* __restrict__ pid,
-                               int n, const uint64_t* __restrict__ start, uint64_t* __restrict__ keys) {
+__device__ __forceinline__ void scatter_keys_block(int blk, const int* __restrict__ cid, const int* __restrict__ pos,
+                                                   const int* __restrict__ pid, int n,
+                                                   const uint64_t* __restrict__ start, uint64_t* __restrict__ keys) {
     const int lane = threadIdx.x & 31;
-    const int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
+    const int base = ((blk * (int)blockDim.x + (int)threadIdx.x) >> 5) * (32 * kIndexItems) + lane;
     int c[kIndexItems], p[kIndexItems], q[kIndexItems];
 #pragma unroll
     for (int k = 0; k < kIndexItems; ++k) {
@@ -207,6 +217,11 @@ __global__ void k_scatter_keys(const int* __restrict__ cid, const int* __restric
         const int s = base + 32 * k;
         if (s < n) keys[at[k] + p[k]] = ((uint64_t)(uint32_t)q[k] << 32) | (uint32_t)s;
     }
+}
+
+__global__ void k_scatter_keys(const int* __restrict__ cid, const int* __restrict__ pos, const int* __restrict__ pid,
+                               int n, const uint64_t* __restrict__ start, uint64_t* __restrict__ keys) {
+    scatter_keys_block((int)blockIdx.x, cid, pos, pid, n, start, keys);
 }
 
 constexpr int kRankThreads = 128;
@@ -228,14 +243,13 @@ __device__ __forceinline__ int seg_lo(uint64_t s) { return (int)(uint32_t)s; }
 // consecutive cells, stages their ids and slots in shared memory (splitting the run of cells
 // where it exceeds kRankCap keys) and ranks each key against its own cell's ids. A cell above
 // kRankCap keys on its own is ranked from global memory.
-__global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __restrict__ start, int Nc,
-                                                            int cellsPerBlock, const uint64_t* __restrict__ keys,
-                                                            int* __restrict__ slots) {
+__device__ __forceinline__ void cell_rank_block(int blk, const uint64_t* __restrict__ start, int Nc, int cellsPerBlock,
+                                                const uint64_t* __restrict__ keys, int* __restrict__ slots) {
     __shared__ uint32_t kid[kRankCap];   // particle id
     __shared__ int ksl[kRankCap];        // slot
     __shared__ uint32_t seg[kRankCap];   // per key: its cell's segment [a, b) in the tile, a | b << 16
     const int t = threadIdx.x;
-    const int c0 = (int)min((int64_t)blockIdx.x * cellsPerBlock, (int64_t)Nc);
+    const int c0 = (int)min((int64_t)blk * cellsPerBlock, (int64_t)Nc);
     const int c1 = min(Nc, c0 + cellsPerBlock);
     int cs = c0;
     while (cs < c1) {  // block-uniform
@@ -288,6 +302,72 @@ __global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __re
         __syncthreads();
         cs = ce;
     }
+}
+
+__global__ void __launch_bounds__(kRankThreads) k_cell_rank(const uint64_t* __restrict__ start, int Nc,
+                                                            int cellsPerBlock, const uint64_t* __restrict__ keys,
+                                                            int* __restrict__ slots) {
+    cell_rank_block((int)blockIdx.x, start, Nc, cellsPerBlock, keys, slots);
+}
+
+// ------------------------------------------------------------------ batched index builds
+// The index builds of many contexts (the replicas of a batch) as one launch per kernel: job r
+// is one context's build; blocks [offs[r], offs[r + 1]) of a launch are its blocks.
+struct IndexJob {
+    const int* cid;
+    int* count;
+    int* pos;
+    uint64_t* start;
+    int* slots;
+    const int* pid;
+    uint64_t* keys;
+    int n, Nc, rankCells;
+};
+
+// the job r with offs[r] <= b < offs[r + 1] (offs ascending, offs[0] = 0)
+__device__ __forceinline__ int job_of(const int* __restrict__ offs, int nJobs, int b) {
+    int lo = 0, hi = nJobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offs[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// offs: blocks of kThreads threads covering each job's slots (kIndexItems per thread)
+__global__ void k_histogram_batch(const IndexJob* __restrict__ jobs, const int* __restrict__ offs, int nJobs) {
+    const int b = (int)blockIdx.x;
+    if (nJobs <= 0 || b >= offs[nJobs]) return;
+    const int r = job_of(offs, nJobs, b);
+    const IndexJob J = jobs[r];
+    histogram_block(b - offs[r], J.cid, J.n, J.count, J.pos);
+}
+
+// one block per job (every job has Nc <= kSmallScan)
+__global__ void __launch_bounds__(kScanThreads) k_scan_counts_small_batch(const IndexJob* __restrict__ jobs) {
+    const IndexJob J = jobs[blockIdx.x];
+    scan_counts_small_block(J.count, J.Nc, J.start);
+}
+
+__global__ void k_scatter_keys_batch(const IndexJob* __restrict__ jobs, const int* __restrict__ offs, int nJobs) {
+    const int b = (int)blockIdx.x;
+    if (nJobs <= 0 || b >= offs[nJobs]) return;
+    const int r = job_of(offs, nJobs, b);
+    const IndexJob J = jobs[r];
+    scatter_keys_block(b - offs[r], J.cid, J.pos, J.pid, J.n, J.start, J.keys);
+}
+
+// offs: blocks of each job's rank sort (ceil(Nc / rankCells))
+__global__ void __launch_bounds__(kRankThreads) k_cell_rank_batch(const IndexJob* __restrict__ jobs,
+                                                                  const int* __restrict__ offs, int nJobs) {
+    const int b = (int)blockIdx.x;
+    if (nJobs <= 0 || b >= offs[nJobs]) return;
+    const int r = job_of(offs, nJobs, b);
+    const IndexJob J = jobs[r];
+    cell_rank_block(b - offs[r], J.start, J.Nc, J.rankCells, J.keys, J.slots);
 }
 
 }  // namespace mpcd_dev

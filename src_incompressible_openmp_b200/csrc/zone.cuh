@@ -1398,20 +1398,22 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 // resets the overflow and block counters for the next pass.
 __device__ void zone_metrics_warp(const int2* __restrict__ moved, const double2* __restrict__ corr, int nZones,
                                   double* __restrict__ out);
+// block blk of nblk: the overflow zones blk, blk + nblk, ...; the last block to finish
+// computes the pass metrics and resets the counters
 template <bool kF32>
-__global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock, int* blocksDone,
-                                                      double* metricsOut) {
+__device__ __forceinline__ void zone_overflow_block(const ZoneArgs& A, char* gmem, size_t perBlock, int* blocksDone,
+                                                    double* metricsOut, int blk, int nblk) {
     const int nov = *A.nOverflow;
-    for (int i = blockIdx.x; i < nov; i += gridDim.x)
-        if (!zone_body<false, int, kF32>(A, A.overflow[i], gmem + perBlock * blockIdx.x, A.maxCells, A.winCap, A.arenaCap,
-                                   A.nsmCap) &&
+    for (int i = blk; i < nov; i += nblk)
+        if (!zone_body<false, int, kF32>(A, A.overflow[i], gmem + perBlock * blk, A.maxCells, A.winCap, A.arenaCap,
+                                         A.nsmCap) &&
             (threadIdx.x & 31) == 0)
             raise_error(A.st, kErrZoneCapacity, A.overflow[i]);
     __syncwarp();
     int last = 0;
     if (threadIdx.x == 0) {
         __threadfence();
-        last = atomicAdd(blocksDone, 1) == (int)gridDim.x - 1;
+        last = atomicAdd(blocksDone, 1) == nblk - 1;
     }
     last = __shfl_sync(0xffffffffu, last, 0);
     if (!last) return;
@@ -1421,6 +1423,27 @@ __global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, si
         *blocksDone = 0;
         *A.nOverflow = 0;
     }
+}
+
+template <bool kF32>
+__global__ void __launch_bounds__(32) k_zone_overflow(ZoneArgs A, char* gmem, size_t perBlock, int* blocksDone,
+                                                      double* metricsOut) {
+    zone_overflow_block<kF32>(A, gmem, perBlock, blocksDone, metricsOut, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// The overflow kernels of many contexts (a batch's replicas) as one launch: job r takes
+// blocks [r * perJob, (r + 1) * perJob).
+struct OverflowJob {
+    ZoneArgs A;  // with the overflow path's capacities
+    char* gmem;
+    size_t perBlock;
+    int* blocksDone;
+    double* metricsOut;
+};
+
+__global__ void __launch_bounds__(32) k_zone_overflow_batch(const OverflowJob* __restrict__ jobs, int perJob) {
+    const OverflowJob& J = jobs[blockIdx.x / perJob];
+    zone_overflow_block<false>(J.A, J.gmem, J.perBlock, J.blocksDone, J.metricsOut, (int)(blockIdx.x % perJob), perJob);
 }
 
 // run_zone_pass (src/zone_pass.cpp:1096-1163): one warp runs the zones in id order on the

@@ -66,3 +66,42 @@ def test_batch_equals_replicas_alone(oracle):
         xo, vo, _ = oracle.step(p, xo, vo, s)
     rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))))
     assert rel(alone[0][0][0], xo) <= 1e-9 and rel(alone[0][0][1], vo) <= 1e-9
+
+
+def _alone(native, p, x, v, step0, nsteps):
+    with native.Context(p) as ctx:
+        ctx.set_state(x, v)
+        ctx.step(step0, nsteps)
+        return ctx.get_state()
+
+
+def test_batch_index_fallbacks():
+    """The replicas' cell indexes are built by one launch per kernel when every replica fits
+    the one-block scan (Nc <= 65,536) and all share a particle-id buffer parity; otherwise each
+    replica builds its own. Both give the replicas' results alone."""
+    native = _native()
+    big = _case(dict(Nx=320, Ny=240, ppc=2), "uniform", 61)  # 76,800 cells: per-replica builds
+    small = _case(dict(Nx=32, Ny=16, ppc=9), "uniform", 62)
+    with native.Batch([big[0], small[0]]) as B:
+        for i, (p, x, v) in enumerate((big, small)):
+            B.member(i).set_state(x, v)
+        B.step(0, 3)
+        for i, (p, x, v) in enumerate((big, small)):
+            xg, vg = B.member(i).get_state()
+            xa, va = _alone(native, p, x, v, 0, 3)
+            assert np.array_equal(xg, xa) and np.array_equal(vg, va), i
+    # parities differ after one member's state is uploaded again mid-run
+    other = _case(dict(Nx=28, Ny=20, ppc=7), "uniform", 63)
+    x2, v2 = uniform_state(other[0], 64)
+    with native.Batch([small[0], other[0]]) as B:
+        B.member(0).set_state(small[1], small[2])
+        B.member(1).set_state(other[1], other[2])
+        B.step(0, 1)
+        B.member(1).set_state(x2, v2)
+        B.step(1, 3)
+        xg, vg = B.member(0).get_state()
+        xa, va = _alone(native, small[0], small[1], small[2], 0, 4)
+        assert np.array_equal(xg, xa) and np.array_equal(vg, va)
+        xg, vg = B.member(1).get_state()
+        xa, va = _alone(native, other[0], x2, v2, 1, 3)
+        assert np.array_equal(xg, xa) and np.array_equal(vg, va)
