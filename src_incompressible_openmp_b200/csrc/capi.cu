@@ -911,8 +911,9 @@ int zone_pass_kernel(mpcd_ctx* c) {
 }
 
 // the overflow kernel's job for the pass in progress (its arguments with the global-memory
-// working set's capacities)
-OverflowJob overflow_job(const mpcd_ctx* c) {
+// working set's capacities); the pass metrics (a serial sum over the zones) only if wanted:
+// the phase API and the metrics step of mpcd_step report them, plain steps do not
+OverflowJob overflow_job(const mpcd_ctx* c, bool metrics) {
     OverflowJob J{};
     J.A = c->zA;
     J.A.order = nullptr;
@@ -923,7 +924,7 @@ OverflowJob overflow_job(const mpcd_ctx* c) {
     J.gmem = c->ovMem;
     J.perBlock = c->ovPerBlock;
     J.blocksDone = c->ovDone;
-    J.metricsOut = c->passOut + (c->zMode == MPCD_LAYOUT_SHIFTED ? 4 : 0);
+    J.metricsOut = metrics ? c->passOut + (c->zMode == MPCD_LAYOUT_SHIFTED ? 4 : 0) : nullptr;
     return J;
 }
 
@@ -935,8 +936,8 @@ void zone_pass_flip(mpcd_ctx* c) {
     c->srdCellsValid = false;
 }
 
-int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr) {
-    const OverflowJob J = overflow_job(c);
+int zone_pass_finish(mpcd_ctx* c, Prof* pf = nullptr, bool metrics = true) {
+    const OverflowJob J = overflow_job(c, metrics);
     if (c->f32)
         k_zone_overflow<true><<<c->ovBlocks, 32, 0, c->stream>>>(J.A, J.gmem, J.perBlock, J.blocksDone, J.metricsOut);
     else
@@ -1811,7 +1812,7 @@ static int step_mid_b(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
 }
 
 static int step_mid(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
-    const int rc = zone_pass_finish(c, pf);
+    const int rc = zone_pass_finish(c, pf, metrics);
     return rc ? rc : step_mid_b(c, step, metrics, pf);
 }
 
@@ -1853,7 +1854,7 @@ static int step_tail_b(mpcd_ctx* c, bool metrics, Prof* pf) {
 }
 
 static int step_tail(mpcd_ctx* c, bool metrics, Prof* pf) {
-    const int rc = zone_pass_finish(c, pf);
+    const int rc = zone_pass_finish(c, pf, metrics);
     return rc ? rc : step_tail_b(c, metrics, pf);
 }
 
@@ -2436,7 +2437,7 @@ static int batch_zone_finish(mpcd_batch* b, int pass) {
     const int n = (int)b->members.size();
     const int slot = (b->members[0]->xv & 1) * 2 + pass;
     OverflowJob* h = b->hOv + (size_t)slot * n;
-    for (int r = 0; r < n; ++r) h[r] = overflow_job(b->members[r]);
+    for (int r = 0; r < n; ++r) h[r] = overflow_job(b->members[r], false);
     OverflowJob* d = b->dOv + (size_t)slot * n;
     CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(OverflowJob) * n, cudaMemcpyHostToDevice, b->stream));
     k_zone_overflow_batch<<<n * b->ovBlocks, 32, 0, b->stream>>>(d, b->ovBlocks);

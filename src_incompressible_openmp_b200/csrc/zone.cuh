@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(1024) k_zone_order(const int* __restrict__ cos
 __device__ void zone_metrics_warp(const int2* __restrict__ moved, const double2* __restrict__ corr, int nZones,
                                   double* __restrict__ out);
 // block blk of nblk: the overflow zones blk, blk + nblk, ...; the last block to finish
-// computes the pass metrics and resets the counters
+// computes the pass metrics (when metricsOut is given) and resets the counters
 template <bool kF32>
 __device__ __forceinline__ void zone_overflow_block(const ZoneArgs& A, char* gmem, size_t perBlock, int* blocksDone,
                                                     double* metricsOut, int blk, int nblk) {
@@ -1418,7 +1418,7 @@ __device__ __forceinline__ void zone_overflow_block(const ZoneArgs& A, char* gme
     last = __shfl_sync(0xffffffffu, last, 0);
     if (!last) return;
     __threadfence();
-    zone_metrics_warp(A.zoneMoved, A.zoneCorr, A.nZones, metricsOut);
+    if (metricsOut) zone_metrics_warp(A.zoneMoved, A.zoneCorr, A.nZones, metricsOut);
     if (threadIdx.x == 0) {
         *blocksDone = 0;
         *A.nOverflow = 0;
