@@ -1070,7 +1070,7 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
         ++c->launches;
     }
     if (flat) {
-        WITH_VIEWS(nx, nx ^ 1, k_kick_flat<<<blocks_for(c->n), kThreads, 0, c->stream>>>(
+        WITH_VIEWS(nx, nx ^ 1, k_kick_flat<<<blocks_for(c->n, kThreads * kKickItems), kThreads, 0, c->stream>>>(
                                    c->P, c->n, c->cellOf, c->idxStd.slots, c->red, c->duRX, c->duRY, c->eosX, c->eosY, S,
                                    c->pidb[np], T, c->pidb[np ^ 1], learned ? c->lmode : nullptr, c->duLX, c->duLY,
                                    reinterpret_cast<const long long*>(c->duLSum)));

@@ -236,8 +236,11 @@ __global__ void k_kick(DevParams P, const uint64_t* __restrict__ start, const in
     }
 }
 
-// The two kicks for one index position j (flat, coalesced), writing the particle at
-// position j of the next step's layout: (cell, particle id) order.
+// The two kicks for index positions j (flat, coalesced), writing the particle at position j
+// of the next step's layout: (cell, particle id) order. Each thread takes kKickItems positions
+// (independent gathers in flight); the launch-wide factors (beta, or the learned kick's
+// particle mean) are computed once per block.
+constexpr int kKickItems = 2;
 template <class V>
 __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, const int* __restrict__ slots,
                             const double* __restrict__ numden, const double* __restrict__ duRX,
@@ -246,25 +249,51 @@ __global__ void k_kick_flat(DevParams P, int n, const int* __restrict__ cellOf, 
                             int* __restrict__ pido, const int* learned,
                             const double* __restrict__ duLX, const double* __restrict__ duLY,
                             const long long* __restrict__ duLSum) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const int c = cellOf[j];
-    const int s = slots[j];
-    const double2 w = S.vel(s);
-    if (learned && *learned) {
-        // the learned closure's kick less its particle mean (sum over cells of N du, int64 at
-        // 2^-32), so that it leaves the total momentum unchanged
-        const double mx = __ddiv_rn((double)duLSum[0] * 0x1p-32, (double)P.n);
-        const double my = __ddiv_rn((double)duLSum[1] * 0x1p-32, (double)P.n);
-        T.set_vel(j, make_double2(__dadd_rn(w.x, __dsub_rn(duLX[c], mx)), __dadd_rn(w.y, __dsub_rn(duLY[c], my))));
-    } else {
-        const double beta = beta_applied(P, numden[0], numden[1]);
-        const double kx = __dmul_rn(beta, duRX[c]), ky = __dmul_rn(beta, duRY[c]);
-        const double2 r = make_double2(__dadd_rn(w.x, kx), __dadd_rn(w.y, ky));
-        T.set_vel(j, make_double2(__dadd_rn(r.x, eosX[c]), __dadd_rn(r.y, eosY[c])));
+    __shared__ double fac[2];  // beta, or the learned kick's particle mean (x, y)
+    __shared__ int lrn;
+    if (threadIdx.x == 0) {
+        lrn = learned ? *learned : 0;
+        if (lrn) {
+            // the learned closure's kick less its particle mean (sum over cells of N du, int64
+            // at 2^-32), so that it leaves the total momentum unchanged
+            fac[0] = __ddiv_rn((double)duLSum[0] * 0x1p-32, (double)P.n);
+            fac[1] = __ddiv_rn((double)duLSum[1] * 0x1p-32, (double)P.n);
+        } else {
+            fac[0] = beta_applied(P, numden[0], numden[1]);
+        }
     }
-    T.copy_pos(j, S, s);
-    pido[j] = pid[s];
+    __syncthreads();
+    const int j0 = blockIdx.x * (blockDim.x * kKickItems) + threadIdx.x;
+    int c[kKickItems], s[kKickItems];
+#pragma unroll
+    for (int k = 0; k < kKickItems; ++k) {
+        const int j = j0 + k * (int)blockDim.x;
+        c[k] = j < n ? cellOf[j] : 0;
+        s[k] = j < n ? slots[j] : 0;
+    }
+    double2 w[kKickItems];
+    int q[kKickItems];
+#pragma unroll
+    for (int k = 0; k < kKickItems; ++k) {
+        const bool in = j0 + k * (int)blockDim.x < n;
+        w[k] = in ? S.vel(s[k]) : make_double2(0.0, 0.0);
+        q[k] = in ? pid[s[k]] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kKickItems; ++k) {
+        const int j = j0 + k * (int)blockDim.x;
+        if (j >= n) continue;
+        if (lrn) {
+            T.set_vel(j, make_double2(__dadd_rn(w[k].x, __dsub_rn(duLX[c[k]], fac[0])),
+                                      __dadd_rn(w[k].y, __dsub_rn(duLY[c[k]], fac[1]))));
+        } else {
+            const double kx = __dmul_rn(fac[0], duRX[c[k]]), ky = __dmul_rn(fac[0], duRY[c[k]]);
+            const double2 r = make_double2(__dadd_rn(w[k].x, kx), __dadd_rn(w[k].y, ky));
+            T.set_vel(j, make_double2(__dadd_rn(r.x, eosX[c[k]]), __dadd_rn(r.y, eosY[c[k]])));
+        }
+        T.copy_pos(j, S, s[k]);
+        pido[j] = q[k];
+    }
 }
 
 // identity cell index after a permuting kick: slots[j] = j
