@@ -94,6 +94,12 @@ struct mpcd_ctx {
     int* cidStd = nullptr;
     int* cidSrd = nullptr;
     uint64_t* sortKeys = nullptr;  // n: (particle id, slot) keys of the index being built
+    // The step's first standard-grid index is built on the walls stream, beside the SRD index
+    // and the collision (it needs the streamed cell ids only), with its own keys; the main
+    // stream joins it at its first use (ensure_std_index).
+    uint64_t* sortKeysSide = nullptr;  // n
+    cudaEvent_t stdIdxDone = nullptr;
+    bool stdIdxPending = false;
     int rankCells = 1;             // cells per block of k_cell_rank
     bool cidStdValid = false;
     bool srdCellsValid = false;
@@ -487,26 +493,32 @@ int scan_u64(mpcd_ctx* c, const uint64_t* in, int64_t n, uint64_t* out, cudaStre
     return MPCD_OK;
 }
 
-// I.count is all zero between builds (set at creation, cleared again by the scan's read)
-int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, int label = -1) {
+// I.count is all zero between builds (set at creation, cleared again by the scan's read).
+// s, keys, sums: the stream and scratch buffers (default: the context's stream, sortKeys and
+// blockSums).
+int build_index(mpcd_ctx* c, const int* cid, CellIndex& I, Prof* pf = nullptr, int label = -1,
+                cudaStream_t s = nullptr, uint64_t* keys = nullptr, uint64_t* sums = nullptr) {
+    if (!s) s = c->stream;
+    if (!keys) keys = c->sortKeys;
+    if (!sums) sums = c->blockSums;
     if (c->n > 0) {
-        k_histogram<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(cid, c->n, I.count, I.pos);
+        k_histogram<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, s>>>(cid, c->n, I.count, I.pos);
         ++c->launches;
     }
     if (c->Nc <= kSmallScan) {
-        k_scan_counts_small<<<1, kScanThreads, 0, c->stream>>>(I.count, c->Nc, I.start); ++c->launches;
+        k_scan_counts_small<<<1, kScanThreads, 0, s>>>(I.count, c->Nc, I.start); ++c->launches;
     } else {
         const int nb = (c->Nc + kScanTile - 1) / kScanTile;
         if (nb > c->blockSumsCap) return set_err(MPCD_ERR_CAPACITY, "scan block buffer too small");
-        k_count_scan_reduce<<<nb, kScanThreads, 0, c->stream>>>(I.count, c->Nc, c->blockSums); ++c->launches;
-        k_scan_blocks<<<1, kScanThreads, 0, c->stream>>>(c->blockSums, nb); ++c->launches;
-        k_count_scan_apply<<<nb, kScanThreads, 0, c->stream>>>(I.count, c->Nc, c->blockSums, I.start); ++c->launches;
+        k_count_scan_reduce<<<nb, kScanThreads, 0, s>>>(I.count, c->Nc, sums); ++c->launches;
+        k_scan_blocks<<<1, kScanThreads, 0, s>>>(sums, nb); ++c->launches;
+        k_count_scan_apply<<<nb, kScanThreads, 0, s>>>(I.count, c->Nc, sums, I.start); ++c->launches;
     }
     if (c->n > 0) {
-        k_scatter_keys<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, c->stream>>>(
-            cid, I.pos, c->pidb[c->pp], c->n, I.start, c->sortKeys); ++c->launches;
-        k_cell_rank<<<blocks_for(c->Nc, c->rankCells), kRankThreads, 0, c->stream>>>(I.start, c->Nc, c->rankCells,
-                                                                                    c->sortKeys, I.slots); ++c->launches;
+        k_scatter_keys<<<blocks_for(c->n, kThreads * kIndexItems), kThreads, 0, s>>>(
+            cid, I.pos, c->pidb[c->pp], c->n, I.start, keys); ++c->launches;
+        k_cell_rank<<<blocks_for(c->Nc, c->rankCells), kRankThreads, 0, s>>>(I.start, c->Nc, c->rankCells, keys,
+                                                                            I.slots); ++c->launches;
     }
     CUDA_TRY(cudaGetLastError());
     mark(c, pf, label);
@@ -552,6 +564,10 @@ __global__ void k_std_cells(DevParams P, V S, int* __restrict__ cid) {
 }
 
 int ensure_std_index(mpcd_ctx* c, Prof* pf = nullptr) {
+    if (c->stdIdxPending) {  // built on the walls stream
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->stdIdxDone, 0));
+        c->stdIdxPending = false;
+    }
     if (c->idxStdValid) return MPCD_OK;
     if (!c->cidStdValid) {
         WITH_VIEW(c->xv, k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, S, c->cidStd));
@@ -1134,7 +1150,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     if (!c) return MPCD_OK;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->offb[0], c->offb[1], c->cellb[0], c->cellb[1],
-                    c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd, c->sortKeys,
+                    c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd, c->sortKeys, c->sortKeysSide,
                     c->idxStd.count, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
                     c->idxSrd.count, c->idxSrd.start, c->idxSrd.pos, c->idxSrd.slots,
                     c->blockSums, c->blockSumsWalls, c->W.bitsX, c->W.bitsY, c->W.wordCount, c->W.wordPrefix, c->W.events,
@@ -1158,7 +1174,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
     if (c->walls) cudaStreamSynchronize(c->walls);
     for (cudaStream_t q : {c->up, c->down})
         if (q) cudaStreamSynchronize(q);
-    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone, c->sideDone,
+    for (cudaEvent_t e : {c->signsReady[0], c->signsReady[1], c->collDone, c->bcDone, c->wallsDone, c->sideDone, c->stdIdxDone,
                           c->upDone[0], c->upDone[1], c->inFree[0], c->inFree[1], c->outReady[0], c->outReady[1],
                           c->downDone[0], c->downDone[1]})
         if (e) cudaEventDestroy(e);
@@ -1226,6 +1242,7 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     ALLOC(c->cidStd, (size_t)n);
     ALLOC(c->cidSrd, (size_t)n);
     ALLOC(c->sortKeys, (size_t)n);
+    ALLOC(c->sortKeysSide, (size_t)n);
     c->rankCells = rank_cells_per_block(n, Nc);
     for (CellIndex* I : {&c->idxStd, &c->idxSrd}) {
         ALLOC(I->count, (size_t)Nc);
@@ -1265,6 +1282,7 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
         cudaStreamCreateWithFlags(&c->walls, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->bcDone, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->wallsDone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->stdIdxDone, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->sideDone, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_err(MPCD_ERR_CUDA, "side stream"));
     ALLOC(c->dStep, 1);
@@ -1784,11 +1802,21 @@ static int step_head(mpcd_ctx* c, int64_t step, bool metrics, Prof* pf) {
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, 130363ULL + 10007ULL * s, c->W.srdShift,
                                         c->graphMode ? c->stepSeeds : nullptr, c->graphMode ? c->dStep : nullptr,
                                         c->stepSeeds); ++c->launches;
-    int rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, pf == nullptr);
+    const bool overlap = pf == nullptr && c->walls;
+    int rc = run_bc(c, true, 104729ULL + 10007ULL * s, c->cidStd, c->cidSrd, metrics, pf, overlap);
     if (rc) return rc;
     c->cidStdValid = true;
     c->srdCellsValid = true;
     c->idxStdValid = false;
+    if (overlap) {
+        // the standard-grid index on the walls stream, after the wall kernels (whose end the
+        // collision waits for), beside the SRD index and the collision on the main stream
+        rc = build_index(c, c->cidStd, c->idxStd, nullptr, -1, c->walls, c->sortKeysSide, c->blockSumsWalls);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(c->stdIdxDone, c->walls));
+        c->stdIdxPending = true;
+        c->idxStdValid = true;
+    }
     rc = run_collide(c, 433494437ULL + 10007ULL * s, pf, step);
     if (rc) return rc;
     rc = run_save_ref(c, pf, true);
