@@ -191,13 +191,13 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
 #undef PAIR
     // final wrap / clamp (src/boundary_conditions.cpp:178-202)
     if (P.perx) {
-        x = __dsub_rn(x, __dmul_rn(floor(__ddiv_rn(x, Lx)), Lx));
+        x = __dsub_rn(x, __dmul_rn(floor_div(x, Lx, P.invLx), Lx));
     } else {
         if (x < 0.0) x = 0.0;
         if (x > Lx) x = Lx;
     }
     if (P.pery) {
-        y = __dsub_rn(y, __dmul_rn(floor(__ddiv_rn(y, Ly)), Ly));
+        y = __dsub_rn(y, __dmul_rn(floor_div(y, Ly, P.invLy), Ly));
     } else {
         if (y < 0.0) y = 0.0;
         if (y > Ly) y = Ly;
@@ -209,18 +209,18 @@ __device__ __forceinline__ bool bc_replay(double& x, double& y, double& vx, doub
 __device__ __forceinline__ int srd_cell(double x, double y, double sx, double sy, const DevParams& P) {
     double xs = __dadd_rn(x, sx), ys = __dadd_rn(y, sy);
     if (P.perx) {
-        xs = __dsub_rn(xs, __dmul_rn(floor(__ddiv_rn(xs, P.Lx)), P.Lx));
+        xs = __dsub_rn(xs, __dmul_rn(floor_div(xs, P.Lx, P.invLx), P.Lx));
     } else {
         if (xs < 0.0) xs = 0.0;
         if (xs >= P.Lx) xs = nextafter(P.Lx, 0.0);
     }
     if (P.pery) {
-        ys = __dsub_rn(ys, __dmul_rn(floor(__ddiv_rn(ys, P.Ly)), P.Ly));
+        ys = __dsub_rn(ys, __dmul_rn(floor_div(ys, P.Ly, P.invLy), P.Ly));
     } else {
         if (ys < 0.0) ys = 0.0;
         if (ys >= P.Ly) ys = nextafter(P.Ly, 0.0);
     }
-    int ix = (int)floor(__ddiv_rn(xs, P.a0)), iy = (int)floor(__ddiv_rn(ys, P.a0));
+    int ix = (int)floor_div(xs, P.a0, P.invA0), iy = (int)floor_div(ys, P.a0, P.invA0);
     if (ix < 0) ix = 0;
     if (ix >= P.Nx) ix = P.Nx - 1;
     if (iy < 0) iy = 0;

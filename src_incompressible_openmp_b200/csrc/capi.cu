@@ -425,6 +425,11 @@ DevParams make_dev_params(const mpcd_params_c& p) {
     d.dx = p.Lx / (double)p.Nx;
     d.dy = p.Ly / (double)p.Ny;
     d.Vc = d.dx * d.dy;
+    d.invDx = 1.0 / d.dx;
+    d.invDy = 1.0 / d.dy;
+    d.invA0 = 1.0 / d.a0;
+    d.invLx = 1.0 / d.Lx;
+    d.invLy = 1.0 / d.Ly;
     d.alpha = p.alpha; d.kBT = p.kBT; d.g = p.g; d.bodyForceX = p.bodyForceX;
     d.useThermostat = p.useThermostat; d.keepMeanFlow = p.keepMeanFlow;
     d.bc[0] = p.boundary_left; d.bc[1] = p.boundary_right; d.bc[2] = p.boundary_bottom; d.bc[3] = p.boundary_top;

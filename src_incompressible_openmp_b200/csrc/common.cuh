@@ -47,6 +47,7 @@ __device__ __forceinline__ void raise_error(DevStatus* st, int code, int detail)
 struct DevParams {
     int Nx, Ny, Nc, n;
     double Lx, Ly, dt, a0, dx, dy, Vc;
+    double invDx, invDy, invA0, invLx, invLy;  // correctly rounded reciprocals (floor_div)
     double alpha, kBT, g, bodyForceX;
     int useThermostat, keepMeanFlow;
     int bc[4];  // left, right, bottom, top (mpcd_bc_mode)
@@ -94,8 +95,23 @@ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b 
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
 
 // reference src/common_grid.cpp:9-19
+// floor(x / d) with the quotient correctly rounded, as floor(x / d) computes it, given
+// invd = RN(1 / d). q = RN(x * invd) is within 2^-51 |q| of RN(x / d) (two roundings of
+// 2^-53 each on the way to x / d, one more to RN(x / d)), so the two floors can differ only if
+// an integer lies within 2^-51 |q| of q. Outside 2^-49 |q| of every integer floor(q) is
+// returned; otherwise (cell boundaries hit exactly, |q| >= 2^52, NaN) the quotient is divided
+// out. The multiply stands in for a division sequence of about twenty FP64 operations.
+__device__ __forceinline__ double floor_div(double x, double d, double invd) {
+    const double q = __dmul_rn(x, invd);
+    const double f = floor(q);
+    const double r = __dsub_rn(q, f);  // exact: q and floor(q) differ by less than one
+    const double tol = __dmul_rn(fabs(q), 0x1p-49);
+    if (r > tol && r < __dsub_rn(1.0, tol)) return f;
+    return floor(__ddiv_rn(x, d));
+}
+
 __device__ __forceinline__ int cell_of(double x, double y, const DevParams& P) {
-    int ix = (int)floor(x / P.dx), iy = (int)floor(y / P.dy);
+    int ix = (int)floor_div(x, P.dx, P.invDx), iy = (int)floor_div(y, P.dy, P.invDy);
     if (ix < 0) ix = 0;
     if (ix >= P.Nx) ix = P.Nx - 1;
     if (iy < 0) iy = 0;

@@ -7,7 +7,9 @@
 - tiny periodic: a 4x3 domain periodic in both axes, smaller than one zone tile, where
   range-2 neighbour offsets wrap onto the same cell;
 - no particles at all;
-- an unsupported wall mode, which fails only once a particle crosses that wall.
+- an unsupported wall mode, which fails only once a particle crosses that wall;
+- positions on cell and period boundaries and one ulp either side, where the kernels' floor
+  of x / dx (a multiply by the reciprocal, certified, else a division) must take the division.
 Bars as in test_gpu_parity: positions, counts and moves bit-exact; velocities within 1e-12
 relative per step.
 """
@@ -128,3 +130,40 @@ def test_unsupported_wall_mode_fails_on_crossing(oracle):
     xs, vs = oracle.stream(p, x, v)
     with pytest.raises(Exception):
         oracle.apply_bc(p, xs, vs, 104729)
+
+
+def boundary_state(p, seed):
+    """Uniform state whose positions are moved onto cell and period boundaries: k dx exactly
+    (as rounded), the neighbouring doubles, 0, Lx and the double below Lx."""
+    x, v = uniform_state(p, seed)
+    rng = np.random.default_rng(seed + 7)
+    X = x.reshape(-1, 2)
+    n = len(X)
+    dx, dy = p["Lx"] / p["Nx"], p["Ly"] / p["Ny"]
+    kx = rng.integers(0, p["Nx"] + 1, n)
+    ky = rng.integers(1, p["Ny"], n)
+    bx = kx * dx
+    by = ky * dy
+    which = rng.integers(0, 4, n)
+    bx = np.where(which == 1, np.nextafter(bx, -np.inf), np.where(which == 2, np.nextafter(bx, np.inf), bx))
+    by = np.where(which == 3, np.nextafter(by, np.inf), np.where(which == 1, np.nextafter(by, -np.inf), by))
+    pick = rng.random(n) < 0.5
+    X[pick, 0] = np.clip(bx[pick], 0.0, np.nextafter(p["Lx"], 0.0))
+    X[pick, 1] = by[pick]
+    X[:4, 0] = [0.0, np.nextafter(p["Lx"], 0.0), p["Lx"] * 0.5, np.nextafter(0.0, 1.0)]
+    return X.reshape(-1).copy(), v
+
+
+def test_positions_on_cell_boundaries(oracle):
+    native = _native()
+    p = poiseuille_params(64, 32, 8)
+    x, v = boundary_state(p, 81)
+    rho_t = p["gamma"] / ((p["Lx"] / p["Nx"]) * (p["Ly"] / p["Ny"]))
+    with native.Context(p) as ctx:
+        ctx.set_state(x, v)
+        fg = ctx.cell_fields(rho_t)
+        fo = oracle.cell_fields(p, x, v, rho_t)
+        assert np.array_equal(fg["N"], fo["N"]), "cell counts"
+        for seed in (5, 130363, 991):
+            assert np.array_equal(ctx.srd_shift_cells(seed), oracle.srd_shift_cells(p, x, seed)), seed
+    run_steps_both(native, oracle, p, x, v, 3)
