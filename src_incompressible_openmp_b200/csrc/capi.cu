@@ -910,10 +910,17 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
     A.zoneMoved = c->zoneMoved;
     A.zoneCorr = c->zoneCorr;
     A.st = c->st;
-    k_zone_cost<<<blocks_for(L.nZones), kThreads, 0, c->stream>>>(c->P, L.rects, c->idxStd.start, L.nZones, c->zoneCost,
-                                                                   c->zoneHist); ++c->launches;
-    k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
-    A.order = c->zoneOrder;
+    // heaviest zones first (by estimated dense-phase work) in the base pass; the shifted pass
+    // runs after the base pass has evened the counts, its zones cost about the same, and the
+    // two ordering kernels would cost more than the tail they save
+    if (mode == MPCD_LAYOUT_SHIFTED) {
+        A.order = nullptr;
+    } else {
+        k_zone_cost<<<blocks_for(L.nZones), kThreads, 0, c->stream>>>(c->P, L.rects, c->idxStd.start, L.nZones,
+                                                                       c->zoneCost, c->zoneHist); ++c->launches;
+        k_zone_order<<<1, 1024, 0, c->stream>>>(c->zoneCost, c->zoneHist, L.nZones, c->zoneOrder); ++c->launches;
+        A.order = c->zoneOrder;
+    }
     CUDA_TRY(cudaGetLastError());
     c->zA = A;
     c->zMode = mode;
