@@ -872,12 +872,14 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
     }
     int rc = ensure_std_index(c, pf);
     if (rc) return rc;
+    // the seed of the shifted pass (seedBase + 4099) also when the single full-domain zone runs it
+    const bool shiftedPass = mode == MPCD_LAYOUT_SHIFTED;
     if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
     if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
     Layout& L = c->lay[mode];
     k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
-        seedBase, L.nZones, c->seeds, c->graphMode ? c->stepSeeds : nullptr,
-        mode == MPCD_LAYOUT_SHIFTED ? kSeedShifted : kSeedBase); ++c->launches;
+        seedBase, L.nZones, c->seeds, c->graphMode ? c->stepSeeds : nullptr, shiftedPass ? kSeedShifted : kSeedBase);
+    ++c->launches;
     mark(c, pf, 7);
     // velocities out of place (output starts as a copy of the input; zones write what they
     // change), positions in place (the zone kernel never reads them)

@@ -167,3 +167,19 @@ def test_positions_on_cell_boundaries(oracle):
         for seed in (5, 130363, 991):
             assert np.array_equal(ctx.srd_shift_cells(seed), oracle.srd_shift_cells(p, x, seed)), seed
     run_steps_both(native, oracle, p, x, v, 3)
+
+
+def test_single_full_domain_graph_replay_matches_eager():
+    """With the single full-domain zone, the second pass of a step still takes the shifted
+    pass's seed (seedBase + 4099), in eager steps and in graph replays alike."""
+    native = _native()
+    p = poiseuille_params(16, 12, 10, zoneSingleFullDomainMode=True)
+    x, v = uniform_state(p, 91)
+    res = []
+    for graphs in (True, False):
+        with native.Context(p) as ctx:
+            ctx.set_graphs(graphs)
+            ctx.set_state(x, v)
+            ctx.step(0, 6)
+            res.append(ctx.get_state())
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
