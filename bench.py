@@ -50,13 +50,13 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["channel_2048x512_ppc10"]
 DATA = "synthetic: seeded uniform positions, Maxwellian velocities (kT=1, mean removed)"
 # algorithmic bytes per particle (P) and per cell (C) of one launch of each phase's main
-# kernel, FP64 plain form ("Roofline")
+# kernel, FP64 plain form: the least each launch must read and write
 PHASE_BYTES = {
     "stream_bc": (72, 0),       # read x,v 32 B; write x,v 32 B; write 2 cell ids 8 B
     "zone_pass": (68, 8),       # read slot 4, x 16, v 16; write x 16, v 16 | counts 8 per cell
     "kick_resort": (76, 32),    # read slot 4, x,v 32, pid 4; write x,v,pid 36 | duR, duEOS 32 per cell
     "collide": (36, 16),        # read slot 4, v 16; write v 16 | segment starts 16 per cell
-    "cell_index": (32, 24),     # cid 2x4, pos 2x4, slots 2x4, pid 4, slot rewrite 4 | count, scan 24
+    "cell_index": (40, 24),     # cid, pos 8; cid, pos, pid 12 + key 8; key 8 + slot 4 | count, scan 24
     "ref_fields": (20, 96),     # read slot 4, v 16 | 10 field arrays + start
     "closure_cells": (20, 64),
 }
@@ -67,7 +67,7 @@ PHASE_BYTES_F32 = {
     "zone_pass": (44, 8),       # read slot 4, state 20; write state 20 | counts 8 per cell
     "kick_resort": (52, 32),    # read slot 4, state 20, pid 4; write state, pid 24 | 32 per cell
     "collide": (20, 16),        # read slot 4, v 8; write v 8 | segment starts 16 per cell
-    "cell_index": (32, 24),
+    "cell_index": (40, 24),     # as the FP64 form: ids, positions in cells, keys and slots
     "ref_fields": (12, 96),     # read slot 4, v 8 | 10 field arrays + start
     "closure_cells": (12, 64),
 }
