@@ -142,6 +142,27 @@ struct RunOutStep {
     int nZonesExecuted = 0;
 };
 
+// reference include/zone_pass.h:12-30: one zone of a layout and the layout
+struct ZoneDescriptor {
+    int id = 0;
+    std::vector<int> cellIds;
+    std::vector<char> maskVec;
+};
+
+struct ZoneLayout {
+    std::string mode;
+    std::vector<ZoneDescriptor> zones;
+    std::vector<std::int32_t> ownerMap;  // Nc entries, c = iy + Ny * ix
+};
+
+// reference include/zone_pass.h:24-29: what run_zone_kernel_inplace reports
+struct ZoneKernelStats {
+    std::array<double, 6> stats{};
+    std::array<double, 10> diag{};
+    int movedDense = 0;
+    int movedSparse = 0;
+};
+
 // reference include/zone_pass.h: the serial pass's result
 struct ZonePassMetrics {
     double occStdBefore = 0.0;
@@ -588,6 +609,93 @@ inline ZonePassResult run_zone_pass(const State& stateIn, const Params& params, 
     M.momentumDeltaX = p1.first - p0.first;
     M.momentumDeltaY = p1.second - p0.second;
     return out;
+}
+
+// reference src/zone_pass.cpp:1049-1063 (build_layout :173-221): the zones as cell lists in
+// ix-outer, iy-inner order, each with its Nc-cell mask, and the ownership map
+inline ZoneLayout build_zone_layout(const Params& params, const std::string& mode) {
+    const mpcd_params_c pc = b200::to_c(params);
+    const int m = (mode == "single_full") ? MPCD_LAYOUT_SINGLE_FULL : (mode == "shifted") ? MPCD_LAYOUT_SHIFTED : MPCD_LAYOUT_BASE;
+    std::int32_t nz = 0;
+    b200::check(mpcd_zone_layout(&pc, m, &nz, nullptr, 0));
+    std::vector<std::int32_t> r(4u * (std::size_t)nz);
+    b200::check(mpcd_zone_layout(&pc, m, &nz, r.data(), nz));
+    ZoneLayout L;
+    L.mode = mode;
+    L.ownerMap.assign(static_cast<std::size_t>(params.Nc), 0);
+    L.zones.reserve(static_cast<std::size_t>(nz));
+    for (int z = 0; z < nz; ++z) {
+        ZoneDescriptor d;
+        d.id = z + 1;
+        d.maskVec.assign(static_cast<std::size_t>(params.Nc), 0);
+        for (int ix = r[4 * z]; ix < r[4 * z + 1]; ++ix)
+            for (int iy = r[4 * z + 2]; iy < r[4 * z + 3]; ++iy) {
+                const int c = iy + params.Ny * ix;
+                d.cellIds.push_back(c);
+                d.maskVec[static_cast<std::size_t>(c)] = 1;
+                L.ownerMap[static_cast<std::size_t>(c)] = d.id;
+            }
+        L.zones.push_back(std::move(d));
+    }
+    return L;
+}
+
+namespace b200 {
+// The cell rectangle [x0, x1) x [y0, y1) a zone covers. The GPU kernels run rectangular zones,
+// which is what every layout of build_zone_layout holds; any other cell set is rejected.
+inline std::array<int, 4> zone_rect(const ZoneDescriptor& zone, const Params& p) {
+    if (zone.cellIds.empty()) throw std::runtime_error("zone has no cells");
+    int x0 = p.Nx, x1 = -1, y0 = p.Ny, y1 = -1;
+    for (int c : zone.cellIds) {
+        if (c < 0 || c >= p.Nc) throw std::runtime_error("zone cell id out of range");
+        const int ix = c / p.Ny, iy = c - ix * p.Ny;
+        x0 = std::min(x0, ix); x1 = std::max(x1, ix + 1);
+        y0 = std::min(y0, iy); y1 = std::max(y1, iy + 1);
+    }
+    const std::size_t area = (std::size_t)(x1 - x0) * (std::size_t)(y1 - y0);
+    std::size_t inMask = 0;
+    if (zone.maskVec.size() == static_cast<std::size_t>(p.Nc))
+        for (int ix = x0; ix < x1; ++ix)
+            for (int iy = y0; iy < y1; ++iy) inMask += zone.maskVec[(std::size_t)iy + (std::size_t)p.Ny * ix] ? 1u : 0u;
+    if (zone.cellIds.size() != area || inMask != area)
+        throw std::runtime_error("zone is not a rectangle of cells: the GPU zone kernel runs the rectangular zones of build_zone_layout");
+    return {x0, x1, y0, y1};
+}
+}  // namespace b200
+
+// reference src/zone_pass.cpp:1065-1081: one zone's redistribution, in place, on the GPU
+inline ZoneKernelStats run_zone_kernel_inplace(std::vector<double>& x, std::vector<double>& v, const Params& params,
+                                               const ZoneDescriptor& zone, std::uint64_t rngSeed) {
+    if (x.size() != 2u * (std::size_t)params.n || v.size() != 2u * (std::size_t)params.n)
+        throw std::runtime_error("run_zone_kernel_inplace: unexpected state size");
+    const auto r = b200::zone_rect(zone, params);
+    mpcd_ctx* c = b200::context_for(params);
+    b200::upload(c, x, v, params.n);
+    mpcd_zone_kernel_stats_c s;
+    b200::check(mpcd_zone_kernel_inplace(c, r[0], r[1], r[2], r[3], rngSeed, &s));
+    b200::check(mpcd_get_state(c, x.data(), v.data()));
+    ZoneKernelStats out;
+    std::copy(s.stats, s.stats + 6, out.stats.begin());
+    std::copy(s.diag, s.diag + 10, out.diag.begin());
+    out.movedDense = s.movedDense;
+    out.movedSparse = s.movedSparse;
+    return out;
+}
+
+// reference src/zone_pass.cpp:1083-1094: ids (ascending) of the particles whose cell is in the zone
+inline std::vector<int> build_particle_ids_in_zone(const std::vector<double>& x, const Params& params,
+                                                   const ZoneDescriptor& zone) {
+    if (x.size() != 2u * (std::size_t)params.n) throw std::runtime_error("build_particle_ids_in_zone: unexpected state size");
+    const auto r = b200::zone_rect(zone, params);
+    mpcd_ctx* c = b200::context_for(params);
+    const std::vector<double> v(x.size(), 0.0);
+    b200::upload(c, x, v, params.n);
+    std::vector<int> ids(static_cast<std::size_t>(params.n));
+    std::int64_t count = 0;
+    static_assert(sizeof(int) == sizeof(std::int32_t), "int32 ids");
+    b200::check(mpcd_particle_ids_in_rect(c, r[0], r[1], r[2], r[3], reinterpret_cast<std::int32_t*>(ids.data()), &count));
+    ids.resize(static_cast<std::size_t>(count));
+    return ids;
 }
 
 // reference src/liquid_closure.cpp:329-444

@@ -200,9 +200,12 @@ int mpcd_cell_fields(mpcd_ctx* ctx, double rho_target, mpcd_cellfields_c* out);
  *   stream   a cudaStream_t (NULL: the legacy default stream); the call only enqueues work
  * Returns MPCD_ERR_CAPACITY if Nc > MPCD_STATIC_FIELDS_MAX_CELLS. The first call on a device
  * looks up the array's device address (and may load the module there): make that first call
- * before any stream capture. Every call on a device shares the array and zeroes it first;
- * calls that overlap on the GPU race. Sums are accumulated with atomics, so the fields may
- * differ from mpcd_cell_fields in the last bits (counts are exact). */
+ * before any stream capture. The address is kept for the life of the process, so a device
+ * reset (cudaDeviceReset, or a reset of the primary context) after the first call is not
+ * supported: the module may then be loaded at another address. Every call on a device shares
+ * the array and zeroes it first; calls that overlap on the GPU race. Sums are accumulated
+ * with atomics, so the fields may differ from mpcd_cell_fields in the last bits (counts are
+ * exact). */
 #define MPCD_STATIC_FIELDS_MAX_CELLS 1048576
 int mpcd_cell_fields_static(const mpcd_params_c* params, const double* d_x, const double* d_v, int64_t n,
                             double rho_target, const mpcd_cellfields_c* d_out, void* stream);
@@ -225,6 +228,31 @@ int mpcd_zone_pass_serial(mpcd_ctx* ctx, int32_t mode, uint64_t seed_base, mpcd_
 int mpcd_liquid_closure(mpcd_ctx* ctx, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail);
 /* Zone ownership map of a layout (reference src/zone_pass.cpp:1049-1063), Nc int32. */
 int mpcd_zone_owner_map(mpcd_ctx* ctx, int32_t mode, int32_t* owner_out);
+
+/* mpcd::ZoneKernelStats (reference include/zone_pass.h:24-29) */
+typedef struct mpcd_zone_kernel_stats_c {
+    double stats[6];  /* dense cells handled (all passes), sparse cells, moved out, moved in, corrRmsDU, corrMaxDU */
+    double diag[10];  /* occStd, outBand, |dP global|, rms dPx, rms dPy, dE, NaN, 0, rms uxNow, rms uyNow */
+    int32_t movedDense, movedSparse;
+} mpcd_zone_kernel_stats_c;
+/* mpcd::build_zone_layout (reference src/zone_pass.cpp:1049-1063 over build_layout :173-221,
+ * include/zone_pass.h:58): the zones of a layout as cell rectangles. Zone id k + 1 covers
+ * the cells with ix in [rects[4k], rects[4k+1]) and iy in [rects[4k+2], rects[4k+3]); zones
+ * are numbered y-outer, x-inner. Host only (no device, no context). Writes *nzones; rects
+ * may be NULL to query the count, else it holds 4 * cap int32. */
+int mpcd_zone_layout(const mpcd_params_c* params, int32_t mode, int32_t* nzones, int32_t* rects, int32_t cap);
+/* mpcd::run_zone_kernel_inplace (reference src/zone_pass.cpp:1065-1081 over run_zone_kernel
+ * :669-973, include/zone_pass.h:60-64): the redistribution of one zone, the cell rectangle
+ * [x0, x1) x [y0, y1), in place on the current state, with the draws of mt19937_64(seed).
+ * Every cell is active (the reference's build_active_mask_vec). stats nullable. */
+int mpcd_zone_kernel_inplace(mpcd_ctx* ctx, int32_t x0, int32_t x1, int32_t y0, int32_t y1, uint64_t seed,
+                             mpcd_zone_kernel_stats_c* stats);
+/* mpcd::build_particle_ids_in_zone (reference src/zone_pass.cpp:1083-1094,
+ * include/zone_pass.h:66-68): the ids, ascending, of the particles of the current state whose
+ * standard-grid cell lies in [x0, x1) x [y0, y1). *count receives their number; ids_out
+ * (host, n int32) may be NULL to count only. */
+int mpcd_particle_ids_in_rect(mpcd_ctx* ctx, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t* ids_out,
+                              int64_t* count);
 
 /* ---------------------------------------------------------------- the step */
 /* Runs steps step0+1 .. step0+nsteps of the profiled benchmark loop on the device

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <random>
@@ -162,6 +163,11 @@ struct mpcd_ctx {
     int* liveTop = nullptr;
     double2* duScratch = nullptr;
     int64_t liveCap = 0;
+    // single-zone API (allocated on first use): the zone's rectangle, its kernel-side
+    // diagnostics (8 doubles) and the global sums around it (32 doubles)
+    int4* zkRect = nullptr;
+    double* zkDiag = nullptr;
+    double* zkOut = nullptr;
     // learned closure (mpcd_learned_set): parameters, the per-step mode flag (1 learned,
     // 0 plain) decided on the device from the previous step's occupancy spread, step counts
     // per mode, the spread sums, the predicted kick, and the red fields the stencil reads
@@ -997,8 +1003,12 @@ __global__ void k_live_init(const uint64_t* __restrict__ start, int Nc, int* __r
     if (c == 0) *top = n;
 }
 
-// run_zone_pass (src/zone_pass.cpp:1096-1163) on the current state, in place
-int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
+// The serial zone kernel over nZones rectangles (device), in place on the current state; zone
+// k draws from mt19937_64(seedBase + 104729 (k + 1)) (src/zone_pass_openmp.cpp:78 and the
+// serial pass). Pass metrics go to metricsOut (4 doubles); zoneDiag (nullable) receives the
+// single-zone diagnostics of ZoneArgs::zoneDiag.
+static int launch_zone_serial(mpcd_ctx* c, const int4* rects, const int* owner, int nZones, uint64_t seedBase,
+                              double* zoneDiag, double* metricsOut) {
     if (!c->cidStdValid) {
         k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view64(c, c->xv), c->cidStd); ++c->launches;
         c->cidStdValid = true;
@@ -1016,19 +1026,16 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
         CUDA_TRY(cudaMalloc(&c->liveTop, sizeof(int)));
         CUDA_TRY(cudaMalloc(&c->duScratch, sizeof(double2) * (size_t)std::max(std::max(c->zMaxCells, c->ovMaxCells), 1)));
     }
-    if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
-    if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
-    Layout& L = c->lay[mode];
-    k_zone_seeds<<<(L.nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
-        seedBase, L.nZones, c->seeds, nullptr, kSeedBase); ++c->launches;
+    k_zone_seeds<<<(nZones + kSeedZonesPerBlock - 1) / kSeedZonesPerBlock, kSeedZonesPerBlock * 2, 0, c->stream>>>(
+        seedBase, nZones, c->seeds, nullptr, kSeedBase); ++c->launches;
     if (c->n > 0)
         CUDA_TRY(cudaMemcpyAsync(c->slotsLive, c->idxStd.slots, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->stream));
     k_live_init<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->liveCnt, c->liveStart, c->liveTop,
                                                                c->n); ++c->launches;
     ZoneArgs A{};
     A.P = c->P;
-    A.rects = L.rects;
-    A.owner = L.owner;
+    A.rects = rects;
+    A.owner = owner;
     A.start = c->idxStd.start;
     A.slots = c->slotsLive;
     A.vin = c->vb[c->xv];
@@ -1036,7 +1043,7 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     A.vout = c->vb[c->xv];
     A.cid = c->cidStd;
     A.seeds = c->seeds;
-    A.nZones = L.nZones;
+    A.nZones = nZones;
     A.maxCells = c->zMaxCells;
     A.winCap = c->zWinCap;
     A.arenaCap = c->zArenaCap;
@@ -1055,18 +1062,28 @@ int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
     A.liveEnd = (int)(c->n + c->liveCap);
     A.pid = c->pidb[c->pp];
     A.duScratch = c->duScratch;
+    A.zoneDiag = zoneDiag;
     ZoneArgs B = A;
     B.maxCells = c->ovMaxCells;
     B.winCap = c->ovWinCap;
     B.arenaCap = c->ovArenaCap;
     B.nsmCap = c->ovNsmCap;
     k_zone_serial<<<1, 32, c->zSmem, c->stream>>>(A, B, c->ovMem); ++c->launches;
-    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, L.nZones, c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0), c->nOverflow); ++c->launches;
+    k_zone_metrics<<<1, 256, 0, c->stream>>>(c->zoneMoved, c->zoneCorr, nZones, metricsOut, c->nOverflow); ++c->launches;
     CUDA_TRY(cudaGetLastError());
     c->idxStdValid = false;  // positions and velocities changed in place
     c->cidStdValid = false;
     c->srdCellsValid = false;
     return MPCD_OK;
+}
+
+// run_zone_pass (src/zone_pass.cpp:1096-1163) on the current state, in place
+int run_zone_pass_serial(mpcd_ctx* c, int mode, uint64_t seedBase) {
+    if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
+    if (c->pc.zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
+    const Layout& L = c->lay[mode];
+    return launch_zone_serial(c, L.rects, L.owner, L.nZones, seedBase, nullptr,
+                              c->passOut + (mode == MPCD_LAYOUT_SHIFTED ? 4 : 0));
 }
 
 // closure on the current (red) state; permute: write particles in (cell, id) order into the
@@ -1171,7 +1188,7 @@ int mpcd_ctx_destroy(mpcd_ctx* c) {
                     c->W.nEvents, c->W.normals, c->W.contrib, c->W.blockPartial, c->W.ints, c->W.srdShift,
                     c->wallOut, c->signs, c->seeds, c->zoneMoved, c->zoneCorr, c->overflow, c->nOverflow, c->ovDone,
                     c->zoneCost, c->zoneHist, c->zoneOrder, c->dStep, c->stepSeeds,
-                    c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch,
+                    c->slotsLive, c->liveCnt, c->liveStart, c->liveTop, c->duScratch, c->zkRect, c->zkDiag, c->zkOut,
                     c->lparams, c->lmode, c->lcount, c->lsums, c->duLX, c->duLY, c->duLSum, c->redFeat,
                     c->ovMem, c->passOut, c->mask, c->refPx, c->refPy, c->refUx, c->refUy, c->refT, c->refRho,
                     c->refPkin, c->refPvir, c->refP, c->refNi, c->pdRaw, c->pdrive, c->eosX, c->eosY, c->duRX,
@@ -1714,6 +1731,226 @@ int mpcd_zone_pass_serial(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pa
         metrics->nThreadsUsed = 1;
         metrics->timeKernel = ms * 1e-3;
     }
+    return MPCD_OK;
+}
+
+// ---------------------------------------------------------------- single zones
+// (reference include/zone_pass.h:60-72: build_zone_layout, run_zone_kernel_inplace,
+// build_particle_ids_in_zone)
+
+int mpcd_zone_layout(const mpcd_params_c* params, int32_t mode, int32_t* nzones, int32_t* rects, int32_t cap) {
+    if (!params || !nzones) return set_err(MPCD_ERR_INVALID_ARG, "mpcd_zone_layout: null argument");
+    if (params->Nx <= 0 || params->Ny <= 0 || params->zoneTileNx <= 0 || params->zoneTileNy <= 0)
+        return set_err(MPCD_ERR_INVALID_ARG, "mpcd_zone_layout: grid and tile sizes must be positive");
+    if (mode != MPCD_LAYOUT_SHIFTED && mode != MPCD_LAYOUT_SINGLE_FULL) mode = MPCD_LAYOUT_BASE;
+    if (params->zoneSingleFullDomainMode) mode = MPCD_LAYOUT_SINGLE_FULL;
+    mpcd_params_c p = *params;
+    p.Nc = p.Nx * p.Ny;
+    Layout L;
+    build_layout(p, mode, L);
+    *nzones = L.nZones;
+    if (rects) {
+        if (cap < L.nZones) return set_err(MPCD_ERR_CAPACITY, "mpcd_zone_layout: rects holds fewer than nzones zones");
+        for (int z = 0; z < L.nZones; ++z) {
+            rects[4 * z] = L.hrects[z].x;
+            rects[4 * z + 1] = L.hrects[z].y;
+            rects[4 * z + 2] = L.hrects[z].z;
+            rects[4 * z + 3] = L.hrects[z].w;
+        }
+    }
+    return MPCD_OK;
+}
+
+}  // extern "C"
+
+namespace mpcd_dev {
+// per cell of a cell index: count, count^2, out-of-band flag (bulk thresholds), non-empty flag
+__global__ void k_zone_count_cols(const uint64_t* __restrict__ start, int Nc, double highThr, double lowThr,
+                                  double* __restrict__ cols) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nc) return;
+    const double n = (double)((uint32_t)start[c + 1] - (uint32_t)start[c]);
+    cols[4 * (size_t)c] = n;
+    cols[4 * (size_t)c + 1] = __dmul_rn(n, n);
+    cols[4 * (size_t)c + 2] = ((n > highThr) || (n > 0.0 && n < lowThr)) ? 1.0 : 0.0;
+    cols[4 * (size_t)c + 3] = (n > 0.0) ? 1.0 : 0.0;
+}
+
+// flag[pid] = 1 for the particles whose standard-grid cell lies in R = (x0, x1, y0, y1)
+__global__ void k_rect_flags(const int* __restrict__ cid, const int* __restrict__ pid, int n, int Ny, int4 R,
+                             uint8_t* __restrict__ flag) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int c = cid[s];
+    const int ix = c / Ny, iy = c - ix * Ny;
+    flag[pid[s]] = (ix >= R.x && ix < R.y && iy >= R.z && iy < R.w) ? 1 : 0;
+}
+
+// per chunk of `chunk` consecutive ids: the number of flagged ids
+__global__ void k_rect_chunk_counts(const uint8_t* __restrict__ flag, int n, int chunk, uint64_t* __restrict__ counts) {
+    __shared__ int sh[kThreads];
+    const int64_t a = (int64_t)blockIdx.x * chunk, b = min((int64_t)n, a + chunk);
+    int k = 0;
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) k += flag[i];
+    sh[threadIdx.x] = k;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[blockIdx.x] = (uint64_t)sh[0];
+}
+
+// per chunk: its flagged ids, ascending, from the chunk's offset on
+__global__ void k_rect_chunk_write(const uint8_t* __restrict__ flag, int n, int chunk, const uint64_t* __restrict__ offs,
+                                   int* __restrict__ ids) {
+    __shared__ int warpTot[kThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int64_t a = (int64_t)blockIdx.x * chunk, b = min((int64_t)n, a + chunk);
+    int64_t base = (int64_t)offs[blockIdx.x];
+    for (int64_t i0 = a; i0 < b; i0 += blockDim.x) {
+        const int64_t i = i0 + t;
+        const bool f = i < b && flag[i];
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) warpTot[w] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            if (k < w) before += warpTot[k];
+            total += warpTot[k];
+        }
+        if (f) ids[base + before + __popc(m & ((1u << lane) - 1u))] = (int)i;
+        base += total;
+        __syncthreads();
+    }
+}
+}  // namespace mpcd_dev
+
+extern "C" {
+
+static int check_rect(const mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int32_t y1) {
+    if (x0 < 0 || y0 < 0 || x1 > c->pc.Nx || y1 > c->pc.Ny || x0 >= x1 || y0 >= y1)
+        return set_err(MPCD_ERR_INVALID_ARG, "zone rectangle outside the grid or empty");
+    return MPCD_OK;
+}
+
+int mpcd_particle_ids_in_rect(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t* ids_out,
+                              int64_t* count) {
+    if (!c || !count) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    int rc = check_rect(c, x0, x1, y0, y1);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(c->device));
+    *count = 0;
+    if (c->n == 0) return MPCD_OK;
+    if (!c->cidStdValid) {
+        k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view64(c, c->xv), c->cidStd); ++c->launches;
+        c->cidStdValid = true;
+    }
+    // scratch in sortKeys (8n bytes): n flag bytes, then the chunk counts and their scan
+    const int chunk = (int)std::max<int64_t>(4096, ((int64_t)c->n + kSmallScan - 1) / kSmallScan);
+    const int nChunks = (int)(((int64_t)c->n + chunk - 1) / chunk);
+    uint8_t* flag = reinterpret_cast<uint8_t*>(c->sortKeys);
+    uint64_t* counts = c->sortKeys + ((size_t)c->n + 7) / 8;
+    uint64_t* offs = counts + nChunks;
+    if ((size_t)(((size_t)c->n + 7) / 8 + 2 * (size_t)nChunks + 1) > (size_t)c->n)
+        return set_err(MPCD_ERR_CAPACITY, "particle ids: scratch too small");
+    k_rect_flags<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->cidStd, c->pidb[c->pp], c->n, c->pc.Ny,
+                                                               make_int4(x0, x1, y0, y1), flag); ++c->launches;
+    k_rect_chunk_counts<<<nChunks, kThreads, 0, c->stream>>>(flag, c->n, chunk, counts); ++c->launches;
+    rc = scan_u64(c, counts, nChunks, offs);
+    if (rc) return rc;
+    uint64_t total = 0;
+    CUDA_TRY(cudaMemcpyAsync(&total, offs + nChunks, sizeof total, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *count = (int64_t)total;
+    if (ids_out && total > 0) {
+        int* dIds = c->cidSrd;  // n ints, free outside the SRD phase
+        k_rect_chunk_write<<<nChunks, kThreads, 0, c->stream>>>(flag, c->n, chunk, offs, dIds); ++c->launches;
+        CUDA_TRY(cudaMemcpyAsync(ids_out, dIds, sizeof(int32_t) * (size_t)total, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        c->srdCellsValid = false;
+    }
+    return check_device(c);
+}
+
+int mpcd_zone_kernel_inplace(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int32_t y1, uint64_t seed,
+                             mpcd_zone_kernel_stats_c* out) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
+        return set_err(MPCD_ERR_INVALID_ARG, "run_zone_kernel is restricted to no surface / no wetting / no reorientation");
+    int rc = check_rect(c, x0, x1, y0, y1);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->zkRect) {
+        CUDA_TRY(cudaMalloc(&c->zkRect, sizeof(int4)));
+        CUDA_TRY(cudaMalloc(&c->zkDiag, 8 * sizeof(double)));
+        CUDA_TRY(cudaMalloc(&c->zkOut, 32 * sizeof(double)));
+    }
+    const int4 R = make_int4(x0, x1, y0, y1);
+    CUDA_TRY(cudaMemcpyAsync(c->zkRect, &R, sizeof R, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->zkOut, 0, 32 * sizeof(double), c->stream));
+    // global kinetic energy and momentum before (zk[0..2]: E, Px, Py)
+    if (c->n > 0) {
+        WITH_VIEW(c->xv, k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->cols)); ++c->launches;
+        rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->zkOut);
+        if (rc) return rc;
+    }
+    // the zone: seed = seedBase + 104729 (0 + 1) in the serial kernel's schedule
+    rc = launch_zone_serial(c, c->zkRect, c->lay[MPCD_LAYOUT_BASE].owner, 1, seed - 104729ULL, c->zkDiag, c->zkOut + 8);
+    if (rc) return rc;
+    // after: counts (zk[12..15]) and global sums (zk[3..5])
+    k_std_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, view64(c, c->xv), c->cidStd); ++c->launches;
+    c->cidStdValid = true;
+    rc = ensure_std_index(c);
+    if (rc) return rc;
+    k_zone_count_cols<<<blocks_for(c->Nc), kThreads, 0, c->stream>>>(c->idxStd.start, c->Nc, c->P.highThr, c->P.lowThrBulk,
+                                                                      c->cols); ++c->launches;
+    rc = reduce_cols(c, c->cols, c->Nc, 4, 0u, c->zkOut + 12);
+    if (rc) return rc;
+    if (c->n > 0) {
+        WITH_VIEW(c->xv, k_particle_cols<<<blocks_for(c->n), kThreads, 0, c->stream>>>(S, c->n, c->cols)); ++c->launches;
+        rc = reduce_cols(c, c->cols, c->n, 3, 0u, c->zkOut + 3);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaGetLastError());
+    rc = check_device(c);
+    if (rc) return rc;
+    if (!out) return MPCD_OK;
+    double zk[32], dg[8];
+    int2 moved;
+    double2 corr;
+    CUDA_TRY(cudaMemcpy(zk, c->zkOut, sizeof zk, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(dg, c->zkDiag, sizeof dg, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&moved, c->zoneMoved, sizeof moved, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&corr, c->zoneCorr, sizeof corr, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof *out);
+    // stats (src/zone_pass.cpp:764-767,855-858,911-922)
+    out->stats[0] = dg[6];
+    out->stats[1] = dg[7];
+    out->stats[2] = out->stats[3] = (double)moved.x + (double)moved.y;
+    out->stats[4] = corr.x;
+    out->stats[5] = corr.y;
+    out->movedDense = moved.x;
+    out->movedSparse = moved.y;
+    // diag (src/zone_pass.cpp:924-970); every cell is active (build_active_mask_vec)
+    const double Nc = (double)std::max(1, c->Nc);
+    const double mean = zk[12] / Nc;
+    double var = zk[13] / Nc - mean * mean;
+    if (var < 0.0) var = 0.0;
+    out->diag[0] = std::sqrt(var) / std::max(c->pc.gamma, 1e-30);
+    out->diag[1] = zk[14] / Nc;
+    const double dPx = zk[4] - zk[1], dPy = zk[5] - zk[2];
+    out->diag[2] = std::sqrt(dPx * dPx + dPy * dPy);
+    out->diag[3] = dg[3] > 0.0 ? std::sqrt(dg[2] / dg[3]) : 0.0;
+    out->diag[4] = dg[5] > 0.0 ? std::sqrt(dg[4] / dg[5]) : 0.0;
+    out->diag[5] = zk[3] - zk[0];
+    out->diag[6] = std::numeric_limits<double>::quiet_NaN();
+    out->diag[7] = 0.0;
+    const double nVel = zk[15];
+    out->diag[8] = nVel > 0.0 ? std::sqrt(dg[0] / nVel) : 0.0;
+    out->diag[9] = nVel > 0.0 ? std::sqrt(dg[1] / nVel) : 0.0;
     return MPCD_OK;
 }
 

@@ -73,6 +73,11 @@ struct ZoneArgs {
     int liveEnd;
     const int* pid;           // particle id per slot
     double2* duScratch;       // momentum correction per cell of the running zone
+    // single-zone in-place API (serial kernel only; nullptr otherwise): per zone, the kernel-side
+    // diagnostics of run_zone_kernel (src/zone_pass.cpp:857-972): sum of uxNow^2, sum of uyNow^2
+    // over the zone's non-empty cells, sum and count of the non-zero dPx^2, the same for dPy,
+    // the dense cells handled over the passes (nHigh) and the sparse ones (nLow)
+    double* zoneDiag;
     // FP32 precision form (f32 != 0): the pass input and output states are these views and
     // vin, xout, vout are unused
     int f32;
@@ -1200,10 +1205,12 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     S.rng.init(M.mt, M.carry, A.seeds + (size_t)z * kMtN, lane);
 
     // dense passes (src/zone_pass.cpp:708-781)
+    int nHighAll = 0, nLowAll = 0;  // dense cells over the passes, sparse cells (stats[0], stats[1])
     for (int pass = 0; pass < p.maxPasses && !S.failed && !S.fatal; ++pass) {
         if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
         const int nd = S.collect([&](int l) { return (double)M.len[l] > S.map_high(l); });
+        nHighAll += nd;
         zone_shuffle_fast(M.list, nd, S.rng, lane);
         for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
     }
@@ -1214,6 +1221,7 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         if (p.useLFF) S.compute_nsm();
         S.mark_bulk();
         const int nlow = S.collect([&](int l) { return M.len[l] > 0 && (double)M.len[l] < S.map_low(l); });
+        nLowAll = nlow;
         if (!p.useLFF && nlow > 0) S.compute_nsm();
         zone_shuffle_fast(M.list, nlow, S.rng, lane);
         for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
@@ -1225,11 +1233,26 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     // its input list and of its final list, both in list order; owned particles of
     // corrected cells get v + du
     double* du2 = M.nsm;
+    const bool wantDiag = kSerial && A.zoneDiag != nullptr;
+    double dgUx2 = 0.0, dgUy2 = 0.0, dgPx2 = 0.0, dgPy2 = 0.0;
+    int dgNPx = 0, dgNPy = 0;
     for (int l = lane; l < S.nl; l += kWarp) {
         double d2 = 0.0;
         const uint8_t f = M.cflags[l];
         const int n = M.len[l];
         if (kSerial) A.duScratch[l] = make_double2(0.0, 0.0);  // cells left unchanged get none
+        if (wantDiag && !(f & kCChanged) && n > 0) {
+            // an unchanged cell: uxNow from its input list (ascending id), no momentum error
+            double sx = 0.0, sy = 0.0;
+            for (int j = 0; j < n; ++j) {
+                const double2 w = zone_vin<kF32>(A, A.slots[M.gstart[l] + j]);
+                sx = __dadd_rn(sx, w.x);
+                sy = __dadd_rn(sy, w.y);
+            }
+            const double ux = __ddiv_rn(sx, (double)n), uy = __ddiv_rn(sy, (double)n);
+            dgUx2 = __dadd_rn(dgUx2, __dmul_rn(ux, ux));
+            dgUy2 = __dadd_rn(dgUy2, __dmul_rn(uy, uy));
+        }
         if ((f & kCChanged) && n > 0) {
             double bx = 0.0, by = 0.0, axs = 0.0, ays = 0.0;
             const int n0 = M.cnt0[l], g0 = M.gstart[l];
@@ -1270,6 +1293,15 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
             const double ux = __ddiv_rn(__dsub_rn(bx, axs), (double)n);
             const double uy = __ddiv_rn(__dsub_rn(by, ays), (double)n);
             d2 = __dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy));
+            if (wantDiag) {
+                const double ax = __ddiv_rn(axs, (double)n), ay = __ddiv_rn(ays, (double)n);
+                dgUx2 = __dadd_rn(dgUx2, __dmul_rn(ax, ax));
+                dgUy2 = __dadd_rn(dgUy2, __dmul_rn(ay, ay));
+                const double dpx = __dsub_rn(bx, axs), dpy = __dsub_rn(by, ays);
+                const double ex = __dmul_rn(dpx, dpx), ey = __dmul_rn(dpy, dpy);
+                if (ex > 0.0) { dgPx2 = __dadd_rn(dgPx2, ex); ++dgNPx; }
+                if (ey > 0.0) { dgPy2 = __dadd_rn(dgPy2, ey); ++dgNPy; }
+            }
             bool doCorr = p.momCorr != 0;
             if (doCorr && (f & kCSkip)) doCorr = false;
             if (doCorr && (f & kCRecv) && !(f & kCBulkBulk)) doCorr = false;
@@ -1290,6 +1322,22 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
         du2[l] = d2;
     }
     __syncwarp();
+    if (wantDiag) {
+        for (int o = 16; o > 0; o >>= 1) {
+            dgUx2 = __dadd_rn(dgUx2, __shfl_xor_sync(0xffffffffu, dgUx2, o));
+            dgUy2 = __dadd_rn(dgUy2, __shfl_xor_sync(0xffffffffu, dgUy2, o));
+            dgPx2 = __dadd_rn(dgPx2, __shfl_xor_sync(0xffffffffu, dgPx2, o));
+            dgPy2 = __dadd_rn(dgPy2, __shfl_xor_sync(0xffffffffu, dgPy2, o));
+            dgNPx += __shfl_xor_sync(0xffffffffu, dgNPx, o);
+            dgNPy += __shfl_xor_sync(0xffffffffu, dgNPy, o);
+        }
+        if (lane == 0) {
+            double* d = A.zoneDiag + 8 * (size_t)z;
+            d[0] = dgUx2; d[1] = dgUy2; d[2] = dgPx2; d[3] = (double)dgNPx; d[4] = dgPy2; d[5] = (double)dgNPy;
+            d[6] = (double)nHighAll; d[7] = (double)nLowAll;
+        }
+        __syncwarp();
+    }
     if (kSerial) serial_finish(S, A, p);
     // zone stats[4], stats[5] (src/zone_pass.cpp:911-922): the sum of positive dU2 in
     // ascending cell order and their maximum (zero entries change neither)

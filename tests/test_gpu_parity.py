@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from src_incompressible_openmp_b200.cases import modulated_state, poiseuille_params, uniform_state
+from tests.parity_checks import check_phases
 
 pytestmark = pytest.mark.gpu
 
@@ -58,65 +59,7 @@ def make_case(over, kind, seed):
 def test_phases_match_oracle(oracle, name, over, kind, seed):
     native = _native()
     p, x, v = make_case(over, kind, seed)
-    with native.Context(p) as ctx:
-        # stream + BC
-        ctx.set_state(x, v)
-        ctx.stream()
-        xs_o, vs_o = oracle.stream(p, x, v)
-        xg, vg = ctx.get_state()
-        assert np.array_equal(xg, xs_o) and np.array_equal(vg, vs_o), "stream"
-        w_g = ctx.apply_bc(104729 + 10007 * S)
-        xb_o, vb_o, w_o = oracle.apply_bc(p, xs_o, vs_o, 104729 + 10007 * S)
-        xg, vg = ctx.get_state()
-        assert np.array_equal(xg, xb_o), "bc positions"
-        assert vclose(vg, vb_o) <= REL, "bc velocities"
-        assert np.count_nonzero(vg != vb_o) <= max(2, vg.size // 500), "bc velocities: too many inexact draws"
-        for k in ("nBot", "nTop", "nLeft", "nRight"):
-            assert w_g[k] == w_o[k], k
-        # SRD cells and collision, from the oracle's state so the phase is isolated
-        ctx.set_state(xb_o, vb_o)
-        cid_g = ctx.srd_shift_cells(130363 + 10007 * S)
-        cid_o = oracle.srd_shift_cells(p, xb_o, 130363 + 10007 * S)
-        assert np.array_equal(cid_g, cid_o), "srd cells"
-        ctx.srd_collide(433494437 + 10007 * S)
-        vc_o = oracle.srd_collide(p, vb_o, cid_o, 433494437 + 10007 * S)
-        _, vg = ctx.get_state()
-        assert np.array_equal(vg, vc_o), "collision"
-        # cell fields
-        rho_t = p["gamma"] / ((p["Lx"] / p["Nx"]) * (p["Ly"] / p["Ny"]))
-        fg = ctx.cell_fields(rho_t)
-        fo = oracle.cell_fields(p, xb_o, vc_o, rho_t)
-        for k in fo:
-            assert np.array_equal(fg[k], fo[k]), f"cell field {k}"
-        # zone passes
-        ctx.save_ref()
-        for mode, seed_b in (("base", 88172645463325252 + 10007 * S), ("shifted", 88172645463325252 + 4099 + 10007 * S)):
-            xin, vin = ctx.get_state()
-            mg = ctx.zone_pass(mode, seed_b)
-            xo, vo, mo = oracle.zone_pass(p, xin, vin, mode, seed_b)
-            xg, vg = ctx.get_state()
-            assert mg["nParticlesMovedDense"] == mo["nParticlesMovedDense"], mode
-            assert mg["nParticlesMovedSparse"] == mo["nParticlesMovedSparse"], mode
-            assert np.array_equal(xg, xo), f"{mode} pass positions"
-            assert np.array_equal(vg, vo), f"{mode} pass velocities"
-            assert abs(mg["corrMaxDU"] - mo["corrMaxDU"]) == 0.0
-            assert abs(mg["corrRmsDU"] - mo["corrRmsDU"]) <= 1e-12 * max(1.0, mo["corrRmsDU"])
-        # closure (ref = post-collision state, red = shifted output)
-        xr, vr = ctx.get_state()
-        mg, dg = ctx.liquid_closure(detail=True)
-        xo, vo, mo, do = oracle.liquid_closure(p, xb_o, vc_o, xr, vr)
-        xg, vg = ctx.get_state()
-        assert np.array_equal(xg, xo), "closure positions"
-        assert vclose(vg, vo) <= REL, "closure velocities"
-        assert mg["nMaskedInterzoneCells"] == mo["nMaskedInterzoneCells"]
-        for k in ("pdriveRaw", "pdrive", "duRepairX", "duRepairY", "duEOSX", "duEOSY", "interzoneMask"):
-            assert np.array_equal(dg[k], do[k]), f"closure {k}"
-        for f in ("refFields", "redFields"):
-            for k in do[f]:
-                assert np.array_equal(dg[f][k], do[f][k]), f"{f}.{k}"
-        for k in ("betaRepairNum", "betaRepairDen", "meanPdriveRaw", "meanPdrive", "rmsEOSDU", "maxEOSDU"):
-            assert abs(mg[k] - mo[k]) <= 1e-11 * max(1.0, abs(mo[k])), k
-        assert mg["betaRepairApplied"] == pytest.approx(mo["betaRepairApplied"], rel=1e-10, abs=1e-14)
+    check_phases(native, oracle, p, x, v, S)
 
 
 @pytest.mark.parametrize("name,over,kind,seed", CASES[:3], ids=[c[0] for c in CASES[:3]])
