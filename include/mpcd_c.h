@@ -160,7 +160,22 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out);
  * rounded to FP32 on every store. An FP32 context runs the whole step (mpcd_step,
  * mpcd_step_timed, mpcd_step_profile, mpcd_step_metrics, the learned closure) and state I/O in
  * FP64 particle-id order; the phase functions return MPCD_ERR_INVALID_ARG. */
-enum mpcd_state_form { MPCD_FORM_F64 = 0, MPCD_FORM_F32 = 1 };
+enum mpcd_state_form { MPCD_FORM_F64 = 0, MPCD_FORM_F32 = 1, MPCD_FORM_FAST = 2 };
+/* MPCD_FORM_FAST, the fast form (no counterpart in the reference, which has one form): the
+ * FP32 precision form with the redistribution decided in parallel. Same phases and rules as
+ * the plain form (stream, walls, shifted-grid SRD rotation with thermostat, base and shifted
+ * zone passes, liquid closure), but every random draw comes from a hash of (step, what the
+ * draw is for), so zones, cells and particles proceed independently; results are therefore
+ * not the reference's trajectories but the same physics, judged statistically against the
+ * plain form. State: per cell a bin of FP32 offsets inside the cell, FP32 velocities on the
+ * 2^-20 grid and particle ids; cell sums are exact int64 sums, so the collision keeps every
+ * SRD cell's momentum and each redistribution keeps the momentum of every cell it corrects,
+ * to the last grid unit. Results do not depend on the order of particles in memory: the same
+ * input gives the same output in particle-id order. Runs the whole step, state I/O and
+ * metrics rows; rejects local fluid-fraction thresholds, keepMeanFlow, the single full-domain
+ * zone, zone tiles above 128 cells and cells that are not squares of side a0. A cell that
+ * grows beyond its bin (about 2 gamma + 8 sqrt(gamma) particles) fails the step with
+ * MPCD_ERR_CAPACITY. */
 int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, mpcd_ctx** out);
 int mpcd_ctx_destroy(mpcd_ctx* ctx);
 /* The stream every kernel of this context runs on (a cudaStream_t). */
@@ -271,6 +286,14 @@ int mpcd_step(mpcd_ctx* ctx, int64_t step0, int64_t nsteps, mpcd_step_metrics_c*
  * unspecified. No counterpart in the reference: its state lives in host memory. */
 int mpcd_run_jobs(mpcd_ctx* ctx, int64_t njobs, const double* const* x_in, const double* const* v_in,
                   int64_t step0, int64_t nsteps, double* const* x_out, double* const* v_out);
+/* Time-averaged velocity profile across the channel (no counterpart in the reference, whose
+ * MATLAB tooling averages dumped states). mpcd_profile_reset clears the accumulators and, with
+ * enable != 0, makes every following step of mpcd_step / mpcd_step_timed add each row's
+ * momentum along x and particle count (exact int64 sums at 2^-32). mpcd_profile_read writes,
+ * per row iy (Ny doubles), the accumulated momentum divided by the accumulated count, and the
+ * number of steps accumulated. */
+int mpcd_profile_reset(mpcd_ctx* ctx, int32_t enable);
+int mpcd_profile_read(mpcd_ctx* ctx, double* ux_rows, int64_t* nsteps);
 /* Device-side metrics row of the current state after a step (see mpcd_step). */
 int mpcd_step_metrics(mpcd_ctx* ctx, mpcd_step_metrics_c* out);
 /* mpcd_step without metrics, timed with CUDA events recorded on the context's stream

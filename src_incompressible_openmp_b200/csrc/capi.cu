@@ -23,6 +23,7 @@
 #include "cells.cuh"
 #include "closure.cuh"
 #include "common.cuh"
+#include "fast.cuh"
 #include "learned.cuh"
 #include "sort.cuh"
 #include "zone.cuh"
@@ -163,6 +164,29 @@ struct mpcd_ctx {
     int* liveTop = nullptr;
     double2* duScratch = nullptr;
     int64_t liveCap = 0;
+    // fast form (MPCD_FORM_FAST): per-cell bins (ping-pong), the running step, wall hits, the
+    // reference sums of the step-start state, the red momenta, the pending closure kick, the
+    // moved counts, and the two zone layouts with the zone kernel's working-set sizes
+    bool fast = false;
+    FastParams F{};
+    FastBins fb[2] = {};
+    int fcur = 0;
+    FastStep* fstep = nullptr;
+    FastWall* fwall = nullptr;
+    longlong4* fref = nullptr;
+    longlong2* fred = nullptr;
+    int2* fkick = nullptr;
+    bool fkickPending = false;
+    int* fmoved = nullptr;  // base dense, base sparse, shifted dense, shifted sparse, zones out of records
+    int4* frects[2] = {nullptr, nullptr};
+    int fnz[2] = {0, 0};
+    int fzMaxCells = 0, fzWinCap = 0, fzNsmCap = 0, fzRecCap = 0;
+    size_t fzSmem = 0;
+    // velocity profile accumulation (mpcd_profile_*): per row, momentum (int64 at 2^-32) and count
+    bool profOn = false;
+    unsigned long long* profP = nullptr;
+    unsigned long long* profN = nullptr;
+    int64_t profSteps = 0;
     // single-zone API (allocated on first use): the zone's rectangle, its kernel-side
     // diagnostics (8 doubles) and the global sums around it (32 doubles)
     int4* zkRect = nullptr;
@@ -1159,6 +1183,8 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     return MPCD_OK;
 }
 
+#include "fast_host.inc"
+
 }  // namespace
 
 // ====================================================================== C-ABI
@@ -1180,6 +1206,9 @@ int mpcd_device_available(void) {
 int mpcd_ctx_destroy(mpcd_ctx* c) {
     if (!c) return MPCD_OK;
     cudaSetDevice(c->device);
+    fast_free(c);
+    if (c->profP) cudaFree(c->profP);
+    if (c->profN) cudaFree(c->profN);
     void* ptrs[] = {c->xb[0], c->xb[1], c->vb[0], c->vb[1], c->offb[0], c->offb[1], c->cellb[0], c->cellb[1],
                     c->v32b[0], c->v32b[1], c->pidb[0], c->pidb[1], c->cidStd, c->cidSrd, c->sortKeys, c->sortKeysSide,
                     c->idxStd.count, c->idxStd.start, c->idxStd.pos, c->idxStd.slots,
@@ -1231,7 +1260,8 @@ int mpcd_ctx_create(const mpcd_params_c* params, int device, mpcd_ctx** out) {
 }
 
 int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, mpcd_ctx** out) {
-    if (form != MPCD_FORM_F64 && form != MPCD_FORM_F32) return set_err(MPCD_ERR_INVALID_ARG, "unknown state form");
+    if (form != MPCD_FORM_F64 && form != MPCD_FORM_F32 && form != MPCD_FORM_FAST)
+        return set_err(MPCD_ERR_INVALID_ARG, "unknown state form");
     if (!params || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     int rc = validate(*params);
@@ -1256,6 +1286,12 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
     if (cudaSetDevice(device) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "cudaSetDevice failed"));
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(set_err(MPCD_ERR_CUDA, "stream"));
     const int n = c->n, Nc = c->Nc;
+    if (form == MPCD_FORM_FAST) {
+        rc = fast_create(c, *params, device);
+        if (rc) return fail(rc);
+        *out = c;
+        return MPCD_OK;
+    }
 #define ALLOC(p, cnt) \
     if ((rc = dalloc(&(p), (cnt)))) return fail(rc)
     c->f32 = form == MPCD_FORM_F32;
@@ -1444,6 +1480,7 @@ static int set_state_impl(mpcd_ctx* c, const double* x, const double* v, int64_t
     if (!c || !x || !v) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
     if (n != c->n) return set_err(MPCD_ERR_INVALID_ARG, "state size does not match params.n");
     CUDA_TRY(cudaSetDevice(c->device));
+    if (c->fast) return fast_set_state(c, x, v, kind);
     c->xv = 0;
     c->pp = 0;
     c->xflip = 0;
@@ -1484,6 +1521,7 @@ int mpcd_set_state_device(mpcd_ctx* c, const double* x, const double* v, int64_t
 static int get_state_impl(mpcd_ctx* c, double* x, double* v, bool toHost) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
+    if (c->fast) return fast_get_state(c, x, v, toHost);
     if (c->n == 0) return MPCD_OK;
     const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (c->f32) {
@@ -1517,7 +1555,7 @@ int mpcd_get_state_device(mpcd_ctx* c, double* x, double* v) { return get_state_
 
 int mpcd_stream(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     k_stream_only<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, cur_x(c), c->vb[c->xv]); ++c->launches;
     CUDA_TRY(cudaGetLastError());
@@ -1527,7 +1565,7 @@ int mpcd_stream(mpcd_ctx* c) {
 
 int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_bc(c, false, seed, nullptr, nullptr, info != nullptr);
     if (rc) return rc;
@@ -1548,7 +1586,7 @@ int mpcd_apply_bc(mpcd_ctx* c, uint64_t seed, mpcd_wallinfo_c* info) {
 
 int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     k_srd_shift<<<1, 1, 0, c->stream>>>(c->P, seed, c->W.srdShift, nullptr); ++c->launches;
     k_srd_cells<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, cur_x(c), c->W.srdShift, c->cidSrd); ++c->launches;
@@ -1564,7 +1602,7 @@ int mpcd_srd_shift_cells(mpcd_ctx* c, uint64_t seed, int32_t* cid_out) {
 
 int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->srdCellsValid) return set_err(MPCD_ERR_STATE, "no SRD cell ids: call mpcd_srd_shift_cells first");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_collide(c, seed);
@@ -1574,7 +1612,7 @@ int mpcd_srd_collide(mpcd_ctx* c, uint64_t seed) {
 
 int mpcd_srd_collide_cells(mpcd_ctx* c, const int32_t* cid, uint64_t seed) {
     if (!c || !cid) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     if (c->n > 0) {
         int* tmp = c->idxSrd.pos;
@@ -1610,7 +1648,7 @@ static FieldsOut tmp_fields(mpcd_ctx* c) {
 
 int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
     if (!c || !out) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = ensure_std_index(c);
     if (rc) return rc;
@@ -1624,7 +1662,7 @@ int mpcd_cell_fields(mpcd_ctx* c, double rho_target, mpcd_cellfields_c* out) {
 
 int mpcd_save_ref(mpcd_ctx* c) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc = run_save_ref(c);
     if (rc) return rc;
@@ -1648,7 +1686,7 @@ static int pass_metrics_to_host(mpcd_ctx* c, int mode, mpcd_pass_metrics_c* m) {
 
 int mpcd_zone_pass(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
@@ -1706,7 +1744,7 @@ static void closure_metrics_from(mpcd_ctx* c, const double* r, mpcd_closure_metr
 
 int mpcd_zone_pass_serial(mpcd_ctx* c, int32_t mode, uint64_t seed_base, mpcd_pass_metrics_c* metrics) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass requires useIncompressibleRedistribution=true and useZoneRedistribution=true");
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
@@ -1837,7 +1875,7 @@ static int check_rect(const mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int
 int mpcd_particle_ids_in_rect(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t* ids_out,
                               int64_t* count) {
     if (!c || !count) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     int rc = check_rect(c, x0, x1, y0, y1);
     if (rc) return rc;
     CUDA_TRY(cudaSetDevice(c->device));
@@ -1877,7 +1915,7 @@ int mpcd_particle_ids_in_rect(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, i
 int mpcd_zone_kernel_inplace(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, int32_t y1, uint64_t seed,
                              mpcd_zone_kernel_stats_c* out) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_kernel is restricted to no surface / no wetting / no reorientation");
     int rc = check_rect(c, x0, x1, y0, y1);
@@ -1956,7 +1994,7 @@ int mpcd_zone_kernel_inplace(mpcd_ctx* c, int32_t x0, int32_t x1, int32_t y0, in
 
 int mpcd_liquid_closure(mpcd_ctx* c, mpcd_closure_metrics_c* metrics, mpcd_closure_detail_c* detail) {
     if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
-    if (c->f32) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision form runs the whole step only (mpcd_step*, state I/O, metrics)");
+    if (c->f32 || c->fast) return set_err(MPCD_ERR_INVALID_ARG, "the FP32 precision and fast forms run the whole step only (mpcd_step*, state I/O, metrics)");
     if (!c->pc.useLiquidClosure) return set_err(MPCD_ERR_INVALID_ARG, "run_liquid_closure requires useLiquidClosure=true");
     CUDA_TRY(cudaSetDevice(c->device));
     const bool wantRep = detail && (detail->repairedV || detail->repairedX || detail->repairedFields.N ||
@@ -2198,6 +2236,15 @@ static int graph_step(mpcd_ctx* c, int64_t step) {
 // steps step0+1 .. step0+nsteps; the metrics step (if any), steps whose sign stream was
 // not prefetched and steps before the collision tile shape is tuned run eagerly, the others
 // from graphs
+static int profile_accumulate(mpcd_ctx* c) {
+    if (!c->profOn) return MPCD_OK;
+    WITH_VIEW(c->xv, k_profile_slots<<<blocks_for(c->n), kThreads, 0, c->stream>>>(c->P, S, c->n, c->profP, c->profN));
+    ++c->launches;
+    ++c->profSteps;
+    CUDA_TRY(cudaGetLastError());
+    return MPCD_OK;
+}
+
 static int run_steps(mpcd_ctx* c, int64_t step0, int64_t nsteps, bool metricsLast) {
     for (int64_t k = 1; k <= nsteps; ++k) {
         const int64_t s = step0 + k;
@@ -2207,6 +2254,7 @@ static int run_steps(mpcd_ctx* c, int64_t step0, int64_t nsteps, bool metricsLas
             rc = graph_step(c, s);
         else
             rc = step_once(c, s, m);
+        if (!rc) rc = profile_accumulate(c);
         if (rc) return rc;
     }
     return MPCD_OK;
@@ -2229,6 +2277,15 @@ int mpcd_step(mpcd_ctx* c, int64_t step0, int64_t nsteps, mpcd_step_metrics_c* l
     if (c->pc.redistributionEnableSurfaceTopology || c->pc.redistributionWallWettingEnabled || c->pc.useInterfaceVelocityReorientation)
         return set_err(MPCD_ERR_INVALID_ARG, "run_zone_pass_snapshot_impl is restricted to no surface / no wetting / no reorientation");
     CUDA_TRY(cudaSetDevice(c->device));
+    if (c->fast) {
+        int rc = fast_steps(c, step0, nsteps, nullptr);
+        if (!rc) rc = check_device(c);
+        if (!rc && last && nsteps > 0) {
+            rc = fast_metrics(c, last, step0 + nsteps);
+            if (!rc) c->last = *last;
+        }
+        return rc;
+    }
     {
         const int rc = run_steps(c, step0, nsteps, last != nullptr);
         if (rc) return rc;
@@ -2391,6 +2448,37 @@ int mpcd_step_metrics(mpcd_ctx* c, mpcd_step_metrics_c* out) {
     return MPCD_OK;
 }
 
+int mpcd_profile_reset(mpcd_ctx* c, int32_t enable) {
+    if (!c) return set_err(MPCD_ERR_INVALID_ARG, "null context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int Ny = c->pc.Ny;
+    if (!c->profP) {
+        CUDA_TRY(cudaMalloc(&c->profP, sizeof(unsigned long long) * (size_t)Ny));
+        CUDA_TRY(cudaMalloc(&c->profN, sizeof(unsigned long long) * (size_t)Ny));
+    }
+    CUDA_TRY(cudaMemsetAsync(c->profP, 0, sizeof(unsigned long long) * (size_t)Ny, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->profN, 0, sizeof(unsigned long long) * (size_t)Ny, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->profOn = enable != 0;
+    c->profSteps = 0;
+    return MPCD_OK;
+}
+
+int mpcd_profile_read(mpcd_ctx* c, double* ux_rows, int64_t* nsteps) {
+    if (!c || !ux_rows) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
+    if (!c->profP) return set_err(MPCD_ERR_INVALID_ARG, "profile accumulation was never reset");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int Ny = c->pc.Ny;
+    std::vector<unsigned long long> P((size_t)Ny), N((size_t)Ny);
+    CUDA_TRY(cudaMemcpy(P.data(), c->profP, sizeof(unsigned long long) * (size_t)Ny, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(N.data(), c->profN, sizeof(unsigned long long) * (size_t)Ny, cudaMemcpyDeviceToHost));
+    for (int iy = 0; iy < Ny; ++iy)
+        ux_rows[iy] = N[(size_t)iy] ? (double)(long long)P[(size_t)iy] * 0x1p-32 / (double)N[(size_t)iy] : 0.0;
+    if (nsteps) *nsteps = c->profSteps;
+    return MPCD_OK;
+}
+
 
 int mpcd_step_timed(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* device_seconds) {
     if (!c || !device_seconds) return set_err(MPCD_ERR_INVALID_ARG, "null argument");
@@ -2401,7 +2489,15 @@ int mpcd_step_timed(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* device_s
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     CUDA_TRY(cudaEventRecord(a, c->stream));
     int rc = MPCD_OK;
-    rc = run_steps(c, step0, nsteps, false);
+    if (c->fast) {
+        // the device step counter is set before the timed region
+        const long long s0 = (long long)step0;
+        CUDA_TRY(cudaMemcpy(&c->fstep->step, &s0, sizeof s0, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaEventRecord(a, c->stream));
+        for (int64_t k = 0; k < nsteps && rc == MPCD_OK; ++k) rc = fast_step(c, nullptr);
+    } else {
+        rc = run_steps(c, step0, nsteps, false);
+    }
     CUDA_TRY(cudaEventRecord(b, c->stream));
     CUDA_TRY(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -2428,9 +2524,13 @@ int mpcd_step_profile(mpcd_ctx* c, int64_t step0, int64_t nsteps, double* phase_
     Prof pf;
     for (auto& e : pf.ev) CUDA_TRY(cudaEventCreate(&e));
     int rc = MPCD_OK;
+    if (c->fast) {
+        const long long s0 = (long long)step0;
+        CUDA_TRY(cudaMemcpy(&c->fstep->step, &s0, sizeof s0, cudaMemcpyHostToDevice));
+    }
     for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) {
         pf.n = 0;
-        rc = step_once(c, step0 + k, false, &pf);
+        rc = c->fast ? fast_step(c, &pf) : step_once(c, step0 + k, false, &pf);
         if (rc) break;
         CUDA_TRY(cudaStreamSynchronize(c->stream));
         for (int i = 1; i < pf.n; ++i) {

@@ -313,6 +313,31 @@ __global__ void k_particle_cols(V S, int n, double* __restrict__ cols) {
     cols[3 * (size_t)i + 2] = w.y;
 }
 
+// Poiseuille profile of the slot state: per row iy, the momentum along x (int64 at 2^-32,
+// each particle rounded once, so the sums are exact and independent of order) and the count,
+// added over the steps. Lanes of one row are summed in the warp before the atomics.
+template <class V>
+__global__ void k_profile_slots(DevParams P, V S, int n, unsigned long long* __restrict__ rowP,
+                                unsigned long long* __restrict__ rowN) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!live) return;
+    const int row = S.std_cell(i, P) % P.Ny;
+    const long long q = llrint(S.vel(i).x * 0x1p32);
+    const unsigned grp = __match_any_sync(act, row);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    long long sum = 0;
+    for (unsigned m = grp; m; m &= m - 1) {
+        const long long t = __shfl_sync(grp, q, __ffs(m) - 1);
+        sum += t;
+    }
+    if (lane == leader) {
+        atomicAdd(rowP + row, (unsigned long long)sum);
+        atomicAdd(rowN + row, (unsigned long long)__popc(grp));
+    }
+}
+
 // per-cell columns for occStd / outBand from a cell index (counts), and mean Ux / Uy
 __global__ void k_count_cols(const uint64_t* __restrict__ start, int Nc, double highThr, double lowThr,
                              double* __restrict__ cols) {

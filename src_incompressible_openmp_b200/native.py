@@ -98,6 +98,9 @@ def lib():
         "mpcd_learned_set": ([C.c_void_p, _fp, C.c_double], C.c_int),
         "mpcd_learned_stats": ([C.c_void_p, P(C.c_int64), P(C.c_int64), P(C.c_int32)], C.c_int),
         "mpcd_learned_options": ([C.c_void_p, C.c_int32], C.c_int),
+        "mpcd_profile_reset": ([C.c_void_p, C.c_int32], C.c_int),
+        "mpcd_profile_read": ([C.c_void_p, _dp, P(C.c_int64)], C.c_int),
+        "mpcd_zone_layout": ([P(_abi.ParamsC), C.c_int32, P(C.c_int32), C.c_void_p, C.c_int32], C.c_int),
         "mpcd_host_alloc": ([C.c_size_t], C.c_void_p),
         "mpcd_host_free": ([C.c_void_p], None),
     }
@@ -164,13 +167,14 @@ def cell_fields_static(params, x_ptr, v_ptr, n, rho_target, out_ptrs, stream=0):
                                          C.byref(s), C.c_void_p(stream)))
 
 
-FORMS = {"f64": 0, "f32": 1}  # mpcd_state_form
+FORMS = {"f64": 0, "f32": 1, "fast": 2}  # mpcd_state_form
 COLLIDE_SHAPES = 7  # MPCD_COLLIDE_SHAPES
 
 
 class Context:
     """A device-resident MPCD state for one parameter set (one GPU). form "f64" is the plain
-    form; "f32" the FP32 precision form (whole steps and state I/O only)."""
+    form; "f32" the FP32 precision form; "fast" the fast form (FP32 bins, draws from hashes,
+    order-free); the last two run whole steps and state I/O only."""
 
     def __init__(self, params, device=0, form="f64"):
         self.params = dict(params)
@@ -337,6 +341,17 @@ class Context:
     def set_graphs(self, enable):
         """Step replay from CUDA graphs (on by default)."""
         _check(lib().mpcd_ctx_set_graphs(self.h, 1 if enable else 0))
+
+    def profile_reset(self, enable=True):
+        """Clears the velocity-profile accumulators; with enable, every following step adds to them."""
+        _check(lib().mpcd_profile_reset(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """(time-averaged mean vx per row iy, steps accumulated)."""
+        ux = np.zeros(int(self.params["Ny"]))
+        k = C.c_int64()
+        _check(lib().mpcd_profile_read(self.h, ux, C.byref(k)))
+        return ux, k.value
 
     def step(self, step0, nsteps, metrics=False):
         m = _abi.StepMetricsC() if metrics else None
