@@ -1,23 +1,30 @@
 #!/usr/bin/env python
-"""Benchmark of the SRC/MPCD time step on B200: particle-steps/s of the FP64 plain form.
+"""Benchmark of the SRC/MPCD time step on B200: FP64 plain vs FP32 fast form with the learned
+closure, in particle-steps/s, with the fast form's profile error against the plain form.
 
-Workload: the large plain-FP64 Poiseuille channel, 2048 x 512 cells (a = 0.2), 10 particles
-per cell (10,485,760 particles), dt = 0.1, alpha = 130 deg, body force 1e-3 along +x,
-periodic x, thermalising walls at y = 0 and y = Ly, 10 x 10 redistribution tiles with a
-shifted second pass, closure stiffness 1. Synthetic seeded state (uniform positions,
-Maxwellian velocities with kT = 1, mean removed). The state (378 MB) is larger than L2
-(126 MB), so no L2 flush is needed between steps.
+Workload (default): the Poiseuille channel of 4096 x 1024 cells (a = 0.2) at 20 particles per
+cell (83,886,080 particles), dt = 0.1, alpha = 130 deg, body force 1e-3 along +x, periodic x,
+thermalising walls at y = 0 and y = Ly, 10 x 10 redistribution tiles with a shifted second
+pass, closure stiffness 1. Synthetic seeded state (uniform positions, Maxwellian velocities
+with kT = 1, mean removed). The state (3 GB in the plain form) is larger than L2 (126 MB), so
+no L2 flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
 ours: W warm-up steps, then K steps timed with CUDA events on the context's stream,
 bracketed by a barrier and a device synchronisation on every rank; value = all ranks'
-particle-steps / max-over-ranks time. Under torchrun every rank advances its own replica on
-its own GPU (the step has no cross-replica exchange).
+particle-steps / max-over-ranks time of the FP64 plain form. In the same line, "chosen_form"
+gives the same measurement of the fast form (FP32 bins, parallel redistribution) with the
+learned closure, its ratio to the plain form, and the L2 error of its time-averaged velocity
+profile against the plain form's over --profile-steps steps (averaged over the second half),
+beside the plain form's own seed-to-seed difference (the noise floor). Under torchrun every
+rank advances its own replica on its own GPU (the step has no cross-replica exchange).
 
-reference: the unmodified reference (oracle/_ref/ref_sampled, built from the reference's
-own sources) on the host cores, on a bounded sample of the same workload: one full step of
-everything but the zone passes, plus a sample of zones per pass scaled to all zones.
+reference: the unmodified reference (built from the reference's own sources by
+oracle/Makefile) on the host cores: on the workload, one step of everything but the zone
+passes plus a sample of zones per pass scaled to all zones (labelled extrapolated); and, in the
+same line, the reference's own benchmark driver on its own 50 x 50 case for all 1,500 steps,
+timed in full.
 """
 import argparse
 import json
@@ -35,19 +42,19 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s on 1 B200: FP64 plain vs FP32+learned closure, at ≤1% profile err"
 UNIT = "particle-steps/s"
 WORKLOADS = {
-    # the benchmark workload: the large plain-FP64 channel
+    # the benchmark workload: the target's channel (83.9 M particles)
+    "channel_4096x1024_ppc20": dict(name="channel_4096x1024_ppc20", Nx=4096, Ny=1024, ppc=20),
+    # the large plain-FP64 channel (10.5 M particles)
     "channel_2048x512_ppc10": dict(name="channel_2048x512_ppc10", Nx=2048, Ny=512, ppc=10),
     # a smaller channel of the same physics, for profiler captures (state 47 MB)
     "channel_512x256_ppc10": dict(name="channel_512x256_ppc10", Nx=512, Ny=256, ppc=10),
-    # the precision-form domain at full size, here in the plain FP64 form (83.9 M particles)
-    "channel_4096x1024_ppc20": dict(name="channel_4096x1024_ppc20", Nx=4096, Ny=1024, ppc=20),
     # the reference's own benchmark case (50x50 cells, 25,000 particles)
     "channel_50x50_ppc10": dict(name="channel_50x50_ppc10", Nx=50, Ny=50, ppc=10),
     # batched ensemble: 256 independent channels, Nx ~ U[32,512], Ny ~ U[16,128],
     # ppc ~ U[5,20], bodyForceX log-uniform in [1e-4, 1e-2], one initial-state seed each
     "ensemble_256": dict(name="ensemble_256", replicas=256, seed=2024),
 }
-WORKLOAD = WORKLOADS["channel_2048x512_ppc10"]
+WORKLOAD = WORKLOADS["channel_4096x1024_ppc20"]
 DATA = "synthetic: seeded uniform positions, Maxwellian velocities (kT=1, mean removed)"
 # algorithmic bytes per particle (P) and per cell (C) of one launch of each phase's main
 # kernel, FP64 plain form: the least each launch must read and write
@@ -60,16 +67,13 @@ PHASE_BYTES = {
     "ref_fields": (20, 96),     # read slot 4, v 16 | 10 field arrays + start
     "closure_cells": (20, 64),
 }
-# the same for the FP32 precision form: 20 B of state per particle (cell 4, FP32 offset 8,
-# FP32 velocity 8) instead of 32
-PHASE_BYTES_F32 = {
-    "stream_bc": (48, 0),       # read cell, offset, v 20 B; write 20 B; write 2 cell ids 8 B
-    "zone_pass": (44, 8),       # read slot 4, state 20; write state 20 | counts 8 per cell
-    "kick_resort": (52, 32),    # read slot 4, state 20, pid 4; write state, pid 24 | 32 per cell
-    "collide": (20, 16),        # read slot 4, v 8; write v 8 | segment starts 16 per cell
-    "cell_index": (40, 24),     # as the FP64 form: ids, positions in cells, keys and slots
-    "ref_fields": (12, 96),     # read slot 4, v 8 | 10 field arrays + start
-    "closure_cells": (12, 64),
+# the fast form: FP32 bins (offset 8, velocity 8, id 4 bytes per particle)
+PHASE_BYTES_FAST = {
+    "stream_bc": (40, 8),       # read 20 B, write 20 B | count, kick 8 per cell
+    "collide": (28, 4),         # read offset, velocity, id 20; write velocity 8 | count
+    "zone_pass": (40, 40),      # read 20, write 20 | counts in and out 8, cell sums 32
+    "closure_cells": (0, 92),   # reference and red sums 48 + counts 4; pdrive, duRepair, beta terms 40
+    "kick_resort": (0, 48),     # pressure drive and duRepair read 24 (+ stencil), kick written 8
 }
 LAUNCHES_PER_STEP = {"zone_pass": 2, "cell_index": 4}
 
@@ -172,28 +176,33 @@ def whole_job_value(world, n_per_rank, steps, t_max):
     return world * n_per_rank * steps / t_max
 
 
-def config_dict(p, world, closure="plain", form="f64"):
-    state_bytes = 36 if form == "f64" else 24
+def config_dict(p, world, form="plain_f64"):
     return {
         "workload": WORKLOAD["name"], "Nx": p["Nx"], "Ny": p["Ny"], "particles_per_cell": WORKLOAD["ppc"],
-        "n_particles": p["n"], "n_cells": p["Nc"],
-        "form": ("plain_" if closure == "plain" else "learned_closure_") + form,
-        "state": "FP64 x, v" if form == "f64" else "int32 cell, FP32 offset in cell, FP32 v (FP64 arithmetic)",
-        "dt": p["dt"],
+        "n_particles": p["n"], "n_cells": p["Nc"], "form": form, "state": "FP64 x, v", "dt": p["dt"],
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        "l2_policy": f"state ({state_bytes * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
+        "l2_policy": f"state ({36 * p['n'] / 1e6:.0f} MB) vs L2 126 MB; no flush",
+        "metricsEvery": "none inside the timed steps (one metrics row after them)",
     }
 
 
-def cpu_baseline_port(p, x, v):
-    """The oracle port (single thread) on one full step of the workload."""
+def cpu_baseline_port(p):
+    """The oracle port (single thread) on one full step of a bounded sub-case of the workload
+    (the same channel physics and density on a quarter of the cells in each direction when the
+    workload is large); the rate per particle does not depend on the domain size."""
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
     from tests.oracle_libs import Oracle
+    sub = p
+    if p["n"] > 12_000_000:
+        sub = poiseuille_params(p["Nx"] // 4, p["Ny"] // 2, WORKLOAD["ppc"])
+    x, v = uniform_state(sub, 1)
     O = Oracle()
     t0 = time.perf_counter()
-    O.step(p, x, v, 1)
+    O.step(sub, x, v, 1)
     dt = time.perf_counter() - t0
-    return {"value": p["n"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"one full step of {WORKLOAD['name']} ({p['n']} particles) with the C oracle, one thread: {dt:.1f} s"}
+    return {"value": sub["n"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one full step of the {sub['Nx']}x{sub['Ny']} channel at {WORKLOAD['ppc']} per cell "
+                      f"({sub['n']} particles) with the C oracle, one thread: {dt:.1f} s"}
 
 
 def measured_peaks():
@@ -209,7 +218,7 @@ def measured_traffic(kernel, form="f64"):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             d = json.load(f)
-        e = d.get(kernel)
+        e = d.get(kernel if form == "f64" else f"{kernel}:{form}")
         if e and e.get("workload") == WORKLOAD["name"] and e.get("form", "f64") == form:
             return float(e["bytes_per_launch"])
     except (OSError, ValueError):
@@ -217,27 +226,22 @@ def measured_traffic(kernel, form="f64"):
     return None
 
 
-def run_ours(args):
-    from src_incompressible_openmp_b200 import native
-    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
+def roofline(phases, KP, p, table, form):
+    """Roofline of the dominant kernel: its algorithmic bytes per launch over its live launch time."""
+    peak, peak_src = measured_peaks()
+    dom = max((k for k in phases if k in table), key=lambda k: phases[k])
+    per_launch_s = phases[dom] / (KP * LAUNCHES_PER_STEP.get(dom, 1))
+    bp, bc = table[dom]
+    alg = bp * p["n"] + bc * p["Nc"]
+    achieved = alg / per_launch_s / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": measured_traffic(dom, form), "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
+            "avg_launch_ms": 1e3 * per_launch_s}
 
-    world, rank, local, dist, torch = dist_setup(args.gpus)
-    p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
-    x, v = uniform_state(p, 1 + rank)
-    learned = None
-    if args.closure == "learned":
-        learned = learned_network(args, local)
-    ctx = native.Context(p, device=local, form=args.form)
-    ctx.set_state(x, v)
-    W, K = args.warmup, args.steps
-    if learned is not None:
-        # fallback limit: 1.2 x the plain closure's occupancy spread, taken from a plain step
-        occ_plain = ctx.step(0, 1, metrics=True)["occStd"]
-        ctx.learned_set(learned["params"], 1.2 * occ_plain)
-        learned["occ_limit"] = 1.2 * occ_plain
-        ctx.step(1, W - 1)
-    else:
-        ctx.step(0, W)
+
+def timed_steps(native, ctx, W, K, KP, dist, torch, world, n, local):
+    """W warm-up steps, K timed steps (device time, max over ranks), KP profiled steps."""
+    ctx.step(0, W)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -250,10 +254,42 @@ def run_ours(args):
     l1 = ctx.launch_count()
     clocks = sampler.stop(t_wall0, t_wall1)
     t_max = reduce_max(t_dev, dist, torch)
-    value = whole_job_value(world, p["n"], K, t_max)
-    # live per-phase timing (separate run: one synchronisation per step)
-    KP = max(1, min(K, args.profile_steps))
     phases = ctx.step_profile(W + K, KP)
+    return t_max, clocks, l1 - l0, phases
+
+
+def profile_run(native, p, seed, form, steps, network=None, occ_limit=0.0, device=0):
+    """Velocity profile across the channel, averaged over the second half of `steps` steps."""
+    from src_incompressible_openmp_b200.cases import uniform_state
+    x, v = uniform_state(p, seed)
+    with native.Context(p, device=device, form=form) as ctx:
+        ctx.set_state(x, v)
+        if network is not None:
+            ctx.learned_set(network, occ_limit)
+        ctx.step(0, steps // 2)
+        ctx.profile_reset(True)
+        m = ctx.step(steps // 2, steps - steps // 2, metrics=True)
+        ux, k = ctx.profile_read()
+        stats = ctx.learned_stats() if network is not None else None
+    return ux, m, stats
+
+
+def run_ours(args):
+    import numpy as np
+
+    from src_incompressible_openmp_b200 import native
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state
+
+    world, rank, local, dist, torch = dist_setup(args.gpus)
+    p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
+    x, v = uniform_state(p, 1 + rank)
+    W, K = args.warmup, args.steps
+    KP = max(1, min(K, args.profile_steps))
+    # ---- the FP64 plain form (value)
+    ctx = native.Context(p, device=local, form="f64")
+    ctx.set_state(x, v)
+    t_max, clocks, launches, phases = timed_steps(native, ctx, W, K, KP, dist, torch, world, p["n"], local)
+    value = whole_job_value(world, p["n"], K, t_max)
     # end-to-end through the C-ABI with pinned host buffers (mpcd_run_jobs): every step is a
     # job that uploads its input state, runs one step and downloads the resulting state; the
     # copies of neighbouring jobs overlap each job's step
@@ -264,8 +300,7 @@ def run_ours(args):
     hv[:] = v
     outs_x = [host[2].array, host[3].array]
     outs_v = [host[4].array, host[5].array]
-    # untimed warm-up call: allocates the job staging buffers and copy streams
-    ctx.run_jobs([hx] * 2, [hv] * 2, W + K + KP, 1, outs_x, outs_v)
+    ctx.run_jobs([hx] * 2, [hv] * 2, W + K + KP, 1, outs_x, outs_v)  # untimed: allocates the staging
     barrier(dist, torch)
     t0 = time.perf_counter()
     ctx.run_jobs([hx] * KE, [hv] * KE, W + K + KP + 2, 1, [outs_x[k % 2] for k in range(KE)],
@@ -274,57 +309,90 @@ def run_ours(args):
     te = reduce_max(time.perf_counter() - t0, dist, torch)
     for h in host:
         h.close()
-    ctx_stats = ctx.learned_stats()
+    ctx.close()
     e2e = {"value": whole_job_value(world, p["n"], KE, te), "unit": UNIT, "h2d_bytes_per_step": 32 * p["n"],
            "d2h_bytes_per_step": 32 * p["n"], "steps": KE,
            "note": "per step: upload of the input state from pinned host memory, one step, download of the "
-                   "resulting state (mpcd_run_jobs: copies of neighbouring steps overlap the step)"}
-    ctx.close()
+                   "resulting state (mpcd_run_jobs: copies of neighbouring steps overlap the step); bound by the "
+                   "host link at 32 B per particle each way"}
+    # ---- the chosen form: fast form with the learned closure
+    chosen = None
+    if args.chosen != "none":
+        net = learned_network(args, local) if args.chosen == "learned" else None
+        cf = native.Context(p, device=local, form="fast")
+        cf.set_state(x, v)
+        occ_limit = 0.0
+        if net is not None:
+            occ_plain = cf.step(0, 1, metrics=True)["occStd"]
+            occ_limit = 1.2 * occ_plain
+            cf.learned_set(net["params"], occ_limit)
+        tf, clocks_f, launches_f, phases_f = timed_steps(native, cf, W, K, KP, dist, torch, world, p["n"], local)
+        stats = cf.learned_stats() if net is not None else None
+        cf.close()
+        vf = whole_job_value(world, p["n"], K, tf)
+        chosen = {
+            "form": "fast_f32_" + args.chosen + "_closure", "value": vf, "unit": UNIT, "ms_per_step": 1e3 * tf / K,
+            "ratio_vs_plain": vf / value,
+            "state": "per-cell bins: FP32 offset in cell, FP32 velocity on the 2^-20 grid, particle id (int64 cell sums)",
+            "phases_ms_per_step": {k: 1e3 * t / KP for k, t in phases_f.items() if t > 0},
+            "roofline": roofline({k: t for k, t in phases_f.items() if t > 0}, KP, p, PHASE_BYTES_FAST, "fast"),
+            "step_hbm": {"algorithmic_bytes_per_step": 128 * p["n"] + 128 * p["Nc"],
+                         "achieved_GBps": (128 * p["n"] + 128 * p["Nc"]) * K / tf / 1e9 * world,
+                         "note": "128 B per particle + 128 B per cell per step (FP32 state)"},
+            "gpu_launches": int(launches_f * world), "clocks": clocks_f,
+        }
+        if net is not None:
+            chosen["learned_closure"] = {k: v for k, v in net.items() if k != "params"}
+            chosen["learned_closure"].update({"occ_limit": occ_limit, "steps_plain": stats[0], "steps_learned": stats[1]})
+        if args.profile_steps_long > 0 and world == 1:
+            S = args.profile_steps_long
+            pa, ma, _ = profile_run(native, p, 1, "f64", S, device=local)
+            pb, mb, _ = profile_run(native, p, 2, "f64", S, device=local)
+            pc, mc, st2 = profile_run(native, p, 1, "fast", S, None if net is None else net["params"], occ_limit, local)
+            na = float(np.linalg.norm(pa))
+            chosen["profile"] = {
+                "steps": S, "averaged_over": f"steps {S // 2 + 1}-{S}",
+                "profile_l2_err": float(np.linalg.norm(pc - pa)) / na,
+                "noise_floor": float(np.linalg.norm(pb - pa)) / na,
+                "noise_floor_note": "plain form, initial state seed 2 against seed 1",
+                "mean_ux_plain": float(np.mean(pa)), "mean_ux_chosen": float(np.mean(pc)),
+                "meanKinetic_plain": ma["meanKinetic"], "meanKinetic_chosen": mc["meanKinetic"],
+                "occStd_plain": ma["occStd"], "occStd_chosen": mc["occStd"],
+            }
+            if st2 is not None:
+                chosen["profile"]["steps_learned"] = st2[1]
+                chosen["profile"]["steps_plain_fallback"] = st2[0]
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
-    # roofline of the dominant kernel
-    peak, peak_src = measured_peaks()
-    table = PHASE_BYTES if args.form == "f64" else PHASE_BYTES_F32
-    dom = max((k for k in phases if k in table), key=lambda k: phases[k])
-    per_launch_s = phases[dom] / (KP * LAUNCHES_PER_STEP.get(dom, 1))
-    bp, bc = table[dom]
-    alg = bp * p["n"] + bc * p["Nc"]
-    achieved = alg / per_launch_s / 1e9
-    bp_step = 256 if args.form == "f64" else 160  # 4 state sweeps, read + write
-    step_bytes = bp_step * p["n"] + 128 * p["Nc"]
+    step_bytes = 256 * p["n"] + 128 * p["Nc"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": 1e3 * t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": args.form, "data": DATA, "config": config_dict(p, world, args.closure, args.form),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": measured_traffic(dom, args.form),
-                     "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
-                     "avg_launch_ms": 1e3 * per_launch_s},
+        "dtype": "f64", "data": DATA, "config": config_dict(p, world),
+        "roofline": roofline(phases, KP, p, PHASE_BYTES, "f64"),
         "step_hbm": {"algorithmic_bytes_per_step": step_bytes,
                      "achieved_GBps": step_bytes * K / t_max / 1e9 * world,
-                     "note": f"{bp_step} B per particle + 128 B per cell per step"},
+                     "note": "256 B per particle + 128 B per cell per step"},
         "phases_ms_per_step": {k: 1e3 * t / KP for k, t in phases.items()},
         "e2e": e2e,
-        "gpu_launches": int((l1 - l0) * world),
+        "gpu_launches": int(launches * world),
         "clocks": clocks,
     }
-    if learned is not None:
-        plain_steps, learned_steps, _ = ctx_stats
-        line["learned_closure"] = {k: learned[k] for k in learned if k != "params"}
-        line["learned_closure"].update({"steps_plain": plain_steps, "steps_learned": learned_steps})
+    if chosen is not None:
+        line["chosen_form"] = chosen
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_port(p, x, v)
+        line["cpu_baseline"] = cpu_baseline_port(p)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
 
 
 def learned_network(args, device):
-    """The learned closure's network: loaded from --network, or collected and trained here on
-    the ensemble family (the plain closure's kicks in 200 seeded channels, up to 2 M cells, with
-    their mirror images; Adam on the GPU)."""
+    """The fast form's learned closure: loaded from --network, or collected and trained here on
+    the ensemble family (the fast form's plain EOS kicks in 200 seeded channels, up to 2 M
+    cells, with their mirror images; Adam on the GPU)."""
     import numpy as np
 
     from src_incompressible_openmp_b200 import learned as L
@@ -332,12 +400,14 @@ def learned_network(args, device):
     if args.network:
         return {"params": np.load(args.network), "source": args.network}
     t0 = time.perf_counter()
-    X, Y = L.collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=2_000_000, device=device)
+    X, Y = L.collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=2_000_000, device=device, form="fast")
     t1 = time.perf_counter()
-    net, losses = L.train(X, Y, epochs=6, device=device)
+    net, losses = L.train(X, Y, epochs=6, device=device, form="fast")
     t2 = time.perf_counter()
-    return {"params": net, "source": "trained in this run", "train_samples": int(len(X)),
-            "collect_s": t1 - t0, "train_s": t2 - t1, "final_loss": float(losses[-1])}
+    held = L.unexplained(net, X[::97], Y[::97])
+    return {"params": net, "source": "trained in this run (fast form, ensemble family, 200 channels)",
+            "train_samples": int(len(X)), "collect_s": t1 - t0, "train_s": t2 - t1, "final_loss": float(losses[-1]),
+            "unexplained_variance_train_sample": held}
 
 
 def ensemble_params(W):
@@ -387,6 +457,39 @@ def run_ensemble(args):
     print(json.dumps(line))
 
 
+def reference_measured_leg(threads):
+    """The reference's own profiled benchmark driver (oracle/_ref/ref_bench, unmodified) on its
+    own case, 50 x 50 cells at 10 per cell (25,000 particles), all 1,500 steps, timed in full."""
+    from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state, write_case
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        return None
+    p = poiseuille_params(50, 50, 10)
+    x, v = uniform_state(p, 1)
+    steps = 1500
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as d:
+        write_case(d, p, x, v, {"benchmark_nSteps": steps, "benchmark_metricsEvery": 100, "benchmark_dumpSteps": ""})
+        c = os.path.join(d, "")
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, c + "params.kv", c + "in_x.bin", c + "in_v.bin", c + "in_type.bin", c + "in_r0.bin",
+                            c + "out", "0", "0", str(threads)], capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"unavailable": "reference driver failed: " + r.stderr.strip()[-200:]}
+        kv = {}
+        with open(c + "out_runout.kv") as f:
+            for line in f:
+                if "=" in line:
+                    k, val = line.strip().split("=", 1)
+                    kv[k] = val
+    per_step = float(kv.get("timePerStepMean", wall / steps))
+    return {"workload": "channel_50x50_ppc10 (the reference's own case)", "steps": steps, "threads": threads,
+            "value": p["n"] / per_step, "unit": UNIT, "s_per_step": per_step, "wall_s": wall,
+            "note": "timePerStepMean of the driver's own _runout.kv (step loop only, metrics every 100 steps); "
+                    "measured, not extrapolated"}
+
+
 def run_reference(args):
     from src_incompressible_openmp_b200.cases import poiseuille_params, uniform_state, write_case
 
@@ -397,16 +500,17 @@ def run_reference(args):
     p = poiseuille_params(WORKLOAD["Nx"], WORKLOAD["Ny"], WORKLOAD["ppc"])
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_sampled")
     threads = os.cpu_count() or 1
-    x, v = uniform_state(p, 1)
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_sampled was not built (reference sources absent at build time)"}))
         return
+    measured = reference_measured_leg(threads)
+    x, v = uniform_state(p, 1)
     budget = args.reference_budget_s
     with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as d:
         write_case(d, p, x, v, {"benchmark_nSteps": 1, "benchmark_metricsEvery": 1, "benchmark_dumpSteps": ""})
+        del x, v
         runs = []
         t_start = time.time()
-        n_warm = min(args.warmup, 1)
         k = 0
         while True:
             r = subprocess.run([exe, os.path.join(d, "params.kv"), os.path.join(d, "in_x.bin"), os.path.join(d, "in_v.bin"),
@@ -417,25 +521,27 @@ def run_reference(args):
             runs.append(json.loads(r.stdout))
             k += 1
             elapsed = time.time() - t_start
-            timed = len(runs) - n_warm
             per = elapsed / len(runs)
-            if timed >= args.steps or (timed >= 1 and elapsed + per > budget):
+            # each sampled step is a one-shot CPU computation: no warm-up; stop at the budget
+            if len(runs) >= args.steps or elapsed + per > budget:
                 break
-    timed_runs = runs[n_warm:]
-    t_step = statistics.mean(r["t_step_extrapolated"] for r in timed_runs)
+    t_step = statistics.mean(r["t_step_extrapolated"] for r in runs)
     value = p["n"] / t_step
-    sample = (f"{len(timed_runs)} sampled steps of {WORKLOAD['name']} on {threads} threads: full stream/BC/SRD and closure, "
-              f"{timed_runs[0]['base_sampled']}/{timed_runs[0]['base_zones']} base and {timed_runs[0]['shifted_sampled']}/"
-              f"{timed_runs[0]['shifted_zones']} shifted zones per step through the reference's own per-zone body, "
-              f"scaled to all zones")
+    sample = (f"{len(runs)} sampled steps of {WORKLOAD['name']} on {threads} threads: full stream/BC/SRD and closure, "
+              f"{runs[0]['base_sampled']}/{runs[0]['base_zones']} base and {runs[0]['shifted_sampled']}/"
+              f"{runs[0]['shifted_zones']} shifted zones per step through the reference's own per-zone body, "
+              f"scaled to all zones (extrapolated)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": len(timed_runs), "warmup": n_warm, "ms_per_step": 1e3 * t_step, "higher_is_better": True,
+        "steps": len(runs), "warmup": 0, "ms_per_step": 1e3 * t_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA, "config": config_dict(p, 1),
+        "extrapolated": True,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "phases_s": {k: statistics.mean(r[k] for r in timed_runs) for k in ("t_refbuild", "base_extrapolated", "shifted_extrapolated", "t_closure")},
+        "phases_s": {k: statistics.mean(r[k] for r in runs) for k in ("t_refbuild", "base_extrapolated", "shifted_extrapolated", "t_closure")},
     }
+    if measured is not None:
+        line["measured_reference_case"] = measured
     print(json.dumps(line))
 
 
@@ -449,12 +555,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel_2048x512_ppc10")
-    ap.add_argument("--closure", choices=["plain", "learned"], default="plain",
-                    help="learned: the stencil-MLP closure with the plain closure as fallback")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel_4096x1024_ppc20")
+    ap.add_argument("--chosen", choices=["learned", "plain", "none"], default="learned",
+                    help="the chosen form's closure (fast form): learned (stencil MLP with the plain "
+                         "closure as fallback), plain, or none (skip the chosen form)")
     ap.add_argument("--network", default=None, help="learned closure parameters (.npy); default: train here")
-    ap.add_argument("--form", choices=["f64", "f32"], default="f64",
-                    help="f32: the FP32 precision form (FP32 cell-relative positions and velocities)")
+    ap.add_argument("--profile-steps-long", type=int, default=2000,
+                    help="steps of the profile-error runs (0: skip); the profile is averaged over the second half")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]

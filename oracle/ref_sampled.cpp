@@ -55,6 +55,7 @@ struct PassTime {
     double layoutPerZone = 0, wallSample = 0, mergePerParticle = 0;
     int nZones = 0, nSample = 0;
     double extrapolated = 0;
+    State out;  // the input with the sampled zones' results merged in
 };
 
 static PassTime sampled_pass(const State& in, const Params& p, bool shifted, std::uint64_t seedBase, int T, int k) {
@@ -99,7 +100,8 @@ static PassTime sampled_pass(const State& in, const Params& p, bool shifted, std
         }
     }
     t.wallSample = secs(t0, Clock::now());
-    State out = in;
+    t.out = in;
+    State& out = t.out;
     t0 = Clock::now();
     std::size_t merged = 0;
     for (int j = 0; j < S; ++j)
@@ -129,23 +131,26 @@ int main(int argc, char** argv) {
         const int T = std::max(1, std::stoi(argv[4]));
         const int k = std::max(1, std::stoi(argv[5]));
         const std::uint64_t step = static_cast<std::uint64_t>(std::stoll(argv[6]));
+        // the step of src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:237-279:
+        // stateRef is the streamed, wall-treated and collided state; the base pass reads it, the
+        // shifted pass the base pass's output, and the closure gets (stateRef, shifted output)
         auto t0 = Clock::now();
-        State ref = state;
+        State cur = state;
         for (int i = 0; i < params.n; ++i) {
-            ref.v[2 * i] += params.bodyForceX * params.dt;
-            ref.v[2 * i + 1] += params.g * params.dt;
-            ref.x[2 * i] += params.dt * ref.v[2 * i];
-            ref.x[2 * i + 1] += params.dt * ref.v[2 * i + 1];
+            cur.v[2 * i] += params.bodyForceX * params.dt;
+            cur.v[2 * i + 1] += params.g * params.dt;
+            cur.x[2 * i] += params.dt * cur.v[2 * i];
+            cur.x[2 * i + 1] += params.dt * cur.v[2 * i + 1];
         }
         WallInfo w;
-        apply_bc_general(ref.x, ref.v, params, w, 104729ULL + 10007ULL * step);
-        const auto cid = srd_cell_id_with_random_shift(ref.x, params, 130363ULL + 10007ULL * step);
-        srd_collision_step(ref.v, cid, params, 433494437ULL + 10007ULL * step);
+        apply_bc_general(cur.x, cur.v, params, w, 104729ULL + 10007ULL * step);
+        const auto cid = srd_cell_id_with_random_shift(cur.x, params, 130363ULL + 10007ULL * step);
+        srd_collision_step(cur.v, cid, params, 433494437ULL + 10007ULL * step);
         const double tRef = secs(t0, Clock::now());
-        const PassTime b = sampled_pass(ref, params, false, 88172645463325252ULL + 10007ULL * step, T, k);
-        const PassTime s = sampled_pass(ref, params, true, 88172645463325252ULL + 4099ULL + 10007ULL * step, T, k);
+        const PassTime b = sampled_pass(cur, params, false, 88172645463325252ULL + 10007ULL * step, T, k);
+        const PassTime s = sampled_pass(b.out, params, true, 88172645463325252ULL + 4099ULL + 10007ULL * step, T, k);
         t0 = Clock::now();
-        const auto cl = run_liquid_closure(ref, ref, params);
+        const auto cl = run_liquid_closure(cur, s.out, params);
         const double tClosure = secs(t0, Clock::now());
         const double tStep = tRef + b.extrapolated + s.extrapolated + tClosure;
         std::printf("{\"n\": %d, \"Nc\": %d, \"threads\": %d, \"t_refbuild\": %.6f, \"t_closure\": %.6f, "

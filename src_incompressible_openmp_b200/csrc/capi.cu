@@ -170,6 +170,7 @@ struct mpcd_ctx {
     bool fast = false;
     FastParams F{};
     FastBins fb[2] = {};
+    FastBins sb{};  // the SRD bins of the collision (with each particle's standard cell)
     int fcur = 0;
     FastStep* fstep = nullptr;
     FastWall* fwall = nullptr;
@@ -206,7 +207,7 @@ struct mpcd_ctx {
     double* lsums = nullptr;
     double* duLX = nullptr;
     double* duLY = nullptr;
-    unsigned long long* duLSum = nullptr;  // sum over cells of N du (x, y), int64 at 2^-32
+    unsigned long long* duLSum = nullptr;  // sum over cells of N du (x, y), int64 at 2^-32; particles kicked
     float4* redFeat = nullptr;  // per cell of the red state: (N/gamma - 1, Ux, Uy, 0)
     ZoneArgs zA{};             // the zone pass in progress (zone_pass_prep .. zone_pass_finish)
     int zMode = 0;
@@ -265,7 +266,11 @@ const char* dev_error_text(int code) {
         case kErrCellId: return "cell id outside [0, Nc)";
         case kErrTargetIsSource: return "a dense cell targeted itself (periodic axis shorter than 3 cells)";
         case kErrRngCapacity: return "collision sign stream shorter than the number of cells with >= 2 particles";
-        case kErrTensorWait: return "a tensor-core MMA of the learned closure did not complete within the wait limit";
+        case kErrTensorWait: return "a tensor-core MMA of the learned closure did not complete within the wait limit; "
+                                    "the step's learned kicks are not trusted (results of every CTA of that launch)";
+        case kErrBinCapacity: return "fast form: a cell holds more particles than its bin (capacity K)";
+        case kErrRecordCapacity: return "fast form: a zone's moves outgrew its record area";
+        case kErrLearnedRange: return "learned closure: a cell's kick N du exceeds the bound of its exact int64 sum (2^8 per cell)";
         default: return "device error";
     }
 }
@@ -335,7 +340,8 @@ int check_device(mpcd_ctx* c) {
         const int detail = c->hst->detail;
         cudaMemset(c->st, 0, sizeof(DevStatus));
         const int rc = (code >= kErrUnsupportedBcLeft && code <= kErrUnsupportedBcTop) ? MPCD_ERR_UNSUPPORTED_BC
-                       : (code == kErrZoneCapacity || code == kErrEventCapacity || code == kErrRngCapacity) ? MPCD_ERR_CAPACITY
+                       : (code == kErrZoneCapacity || code == kErrEventCapacity || code == kErrRngCapacity ||
+                          code == kErrBinCapacity || code == kErrRecordCapacity) ? MPCD_ERR_CAPACITY
                        : (code == kErrCellId) ? MPCD_ERR_INVALID_ARG
                                               : MPCD_ERR_DEVICE;
         return set_err(rc, std::string(dev_error_text(code)) + " (detail " + std::to_string(detail) + ")");
@@ -1134,7 +1140,7 @@ int run_closure(mpcd_ctx* c, bool permute, bool wantRep, bool wantStats, Prof* p
     mark(c, pf, 9);
     const int nx = c->xv, np = c->pp;
     if (learned) {
-        CUDA_TRY(cudaMemsetAsync(c->duLSum, 0, 2 * sizeof(unsigned long long), c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->duLSum, 0, 3 * sizeof(unsigned long long), c->stream));
         k_mlp_tc<false><<<c->tcGrid, kTcThreads, kTcSmem, c->stream>>>(c->P, c->redFeat, nullptr, 0,
                                                                         c->lparams, c->duLX, c->duLY, nullptr, c->lmode,
                                                                         c->duLSum, c->learnedBulkOnly, c->st);
@@ -3126,7 +3132,7 @@ static int ensure_learned_buffers(mpcd_ctx* c) {
     if (rc) return rc;
     if ((rc = dalloc(&c->lparams, kParams)) || (rc = dalloc(&c->lmode, 1)) || (rc = dalloc(&c->lcount, 2)) ||
         (rc = dalloc(&c->lsums, 3)) || (rc = dalloc(&c->duLX, (size_t)c->Nc)) || (rc = dalloc(&c->duLY, (size_t)c->Nc)) ||
-        (rc = dalloc(&c->redFeat, (size_t)c->Nc)) || (rc = dalloc(&c->duLSum, 2)))
+        (rc = dalloc(&c->redFeat, (size_t)c->Nc)) || (rc = dalloc(&c->duLSum, 3)))
         return rc;
     return MPCD_OK;
 }
@@ -3266,7 +3272,11 @@ int mpcd_learned_samples(mpcd_ctx* c, int64_t step0, int64_t nsteps, int32_t str
         return rc;
     }
     int64_t got = 0;
-    c->sampling = true;
+    if (c->fast) {
+        rc = fast_samples(c, step0, nsteps, stride, dX, dY, total, &got);
+        nsteps = 0;  // the loop below is the slot forms'
+    }
+    c->sampling = !c->fast;
     for (int64_t k = 1; k <= nsteps && rc == MPCD_OK; ++k) {
         const int64_t s = step0 + k;
         rc = step_once(c, s, false);

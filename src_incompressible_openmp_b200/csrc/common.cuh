@@ -28,7 +28,9 @@ enum DevError : int {
     kErrCellId = 9,             // a caller-given cell id outside [0, Nc)
     kErrTargetIsSource = 10,    // a dense cell targeting itself (periodic axis shorter than 3)
     kErrRngCapacity = 11,       // the collision sign stream was shorter than needed
-    kErrTensorWait = 12         // a tensor-core MMA did not complete within the wait limit
+    kErrTensorWait = 12,        // a tensor-core MMA did not complete within the wait limit
+    // 13, 14: the fast form's bin and record capacities (fast.cuh)
+    kErrLearnedRange = 15       // a learned kick N du beyond the bound that keeps its int64 sum exact
 };
 
 struct DevStatus {

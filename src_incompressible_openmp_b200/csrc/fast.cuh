@@ -49,6 +49,7 @@ struct FastBins {
     float2* vel;
     int* pid;
     int* cnt;
+    int* cell;  // SRD bins only: each particle's standard cell (its offset is relative to it)
 };
 
 // Values of the running step, derived on the device by k_fast_step_begin (graph replay keeps
@@ -111,6 +112,13 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+__device__ __forceinline__ unsigned long long warp_min_u64_c(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, v, o);
+        v = x < v ? x : v;
+    }
+    return v;
+}
 __device__ __forceinline__ int warp_sum_i(int v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -134,31 +142,31 @@ __global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W) {
 
 // ------------------------------------------------------------------ stream + walls + binning
 // One warp per source cell. Applies the pending closure kick of the previous step (kick[c],
-// grid units, nullable), sums the kicked state per cell (the closure's reference fields:
-// ref[c] = (sum qx, sum qy, sum |q|^2, N)), then body force, streaming and the walls of
+// grid units, nullable), then body force, streaming and the walls of
 // apply_bc_general (src/boundary_conditions.cpp:37-202: up to four sweeps of left, right,
-// bottom, top, then the final wrap or clamp), and files each particle into the bin of its new
-// cell (warp-aggregated slot claims).
-__global__ void __launch_bounds__(256) k_fast_stream(DevParams P, FastParams F, const FastStep* __restrict__ S,
+// bottom, top, then the final wrap or clamp), and files each particle into the bin of its
+// SRD cell, the cell of the grid shifted by this step's (sx, sy) (srd_cell_id_with_random_shift,
+// src/srd_collision.cpp:9-45: wrapped on periodic axes, clamped on the others), with its
+// standard cell and its offset inside that cell (warp-aggregated slot claims).
+__global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams F, const FastStep* __restrict__ S,
                                                      FastBins in, FastBins out, const int2* __restrict__ kick,
-                                                     longlong4* __restrict__ ref, FastWall* __restrict__ W,
-                                                     DevStatus* st) {
+                                                     FastWall* __restrict__ W, DevStatus* st) {
     const int c = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (c >= P.Nc) return;
     const int n = min(in.cnt[c], F.K);  // a count above K (a failed step) reads no further
     const int ix = c / P.Ny, iy = c - ix * P.Ny;
     const int fqx = S->fqx, fqy = S->fqy;
+    const double ssx = S->sx, ssy = S->sy;
     const uint64_t seed = S->seed;
     const int2 kq = kick ? kick[c] : make_int2(0, 0);
-    long long sx = 0, sy = 0, sqq = 0;
     int hits[4] = {0, 0, 0, 0};
     long long dE2 = 0;
     const double Nx = (double)P.Nx, Ny = (double)P.Ny;
     for (int j0 = 0; j0 < n; j0 += 32) {
         const int j = j0 + lane;
         const bool live = j < n;
-        int newc = 0;
+        int newc = 0, stdc = 0;
         float2 o = make_float2(0.f, 0.f);
         int qx = 0, qy = 0, pid = 0;
         if (live) {
@@ -166,16 +174,12 @@ __global__ void __launch_bounds__(256) k_fast_stream(DevParams P, FastParams F, 
             const float2 off = in.off[s];
             const float2 w = in.vel[s];
             pid = in.pid[s];
-            qx = fq_of(w.x) + kq.x;
-            qy = fq_of(w.y) + kq.y;
-            sx += qx;
-            sy += qy;
-            sqq += (long long)qx * qx + (long long)qy * qy;
-            qx += fqx;
-            qy += fqy;
+            qx = fq_of(w.x) + kq.x + fqx;
+            qy = fq_of(w.y) + kq.y + fqy;
             double X = (double)ix + (double)off.x + (double)qx * F.dtqx;
             double Y = (double)iy + (double)off.y + (double)qy * F.dtqy;
-            for (int sweep = 0; sweep < 4; ++sweep) {
+            const bool inside0 = X >= 0.0 && X <= Nx && Y >= 0.0 && Y <= Ny;
+            for (int sweep = 0; sweep < 4 && !inside0; ++sweep) {
                 const long long e0 = (long long)qx * qx + (long long)qy * qy;
                 bool hit = false;
                 const uint64_t hk = fhash(seed, (uint64_t)(uint32_t)pid, (uint64_t)sweep);
@@ -262,16 +266,32 @@ __global__ void __launch_bounds__(256) k_fast_stream(DevParams P, FastParams F, 
                 if (hit) dE2 += (long long)qx * qx + (long long)qy * qy - e0;
                 if (X >= 0.0 && X <= Nx && Y >= 0.0 && Y <= Ny) break;
             }
-            if (P.perx) X = X - floor(X / Nx) * Nx;
-            else X = fmin(fmax(X, 0.0), Nx);
-            if (P.pery) Y = Y - floor(Y / Ny) * Ny;
-            else Y = fmin(fmax(Y, 0.0), Ny);
+            // the final wrap x - floor(x / L) L or clamp (src/boundary_conditions.cpp:178-202);
+            // after the sweeps a particle is within one period of the box
+            if (P.perx) {
+                if (X < 0.0) X += Nx;
+                if (X >= Nx) X -= Nx;
+            } else {
+                X = fmin(fmax(X, 0.0), Nx);
+            }
+            if (P.pery) {
+                if (Y < 0.0) Y += Ny;
+                if (Y >= Ny) Y -= Ny;
+            } else {
+                Y = fmin(fmax(Y, 0.0), Ny);
+            }
             int jx = (int)floor(X), jy = (int)floor(Y);
             jx = min(max(jx, 0), P.Nx - 1);
             jy = min(max(jy, 0), P.Ny - 1);
             o.x = fminf(fmaxf((float)(X - (double)jx), 0.0f), kFastOffMax);
             o.y = fminf(fmaxf((float)(Y - (double)jy), 0.0f), kFastOffMax);
-            newc = jy + P.Ny * jx;
+            stdc = jy + P.Ny * jx;
+            int sxc = (int)floor(X + ssx), syc = (int)floor(Y + ssy);
+            if (P.perx) sxc = sxc < 0 ? sxc + P.Nx : (sxc >= P.Nx ? sxc - P.Nx : sxc);
+            else sxc = min(max(sxc, 0), P.Nx - 1);
+            if (P.pery) syc = syc < 0 ? syc + P.Ny : (syc >= P.Ny ? syc - P.Ny : syc);
+            else syc = min(max(syc, 0), P.Ny - 1);
+            newc = syc + P.Ny * sxc;
         }
         // warp-aggregated slot claims in the destination bins
         const unsigned act = __ballot_sync(0xffffffffu, live);
@@ -287,15 +307,12 @@ __global__ void __launch_bounds__(256) k_fast_stream(DevParams P, FastParams F, 
                 out.off[d] = o;
                 out.vel[d] = make_float2(fv_of(qx), fv_of(qy));
                 out.pid[d] = pid;
+                out.cell[d] = stdc;
             } else if (st) {
                 raise_error(st, kErrBinCapacity, newc);
             }
         }
     }
-    sx = warp_sum_ll(sx);
-    sy = warp_sum_ll(sy);
-    sqq = warp_sum_ll(sqq);
-    if (lane == 0 && ref) ref[c] = make_longlong4(sx, sy, sqq, n);
     if (W) {
         for (int k = 0; k < 4; ++k) {
             const int h = warp_sum_i(hits[k]);
@@ -307,84 +324,53 @@ __global__ void __launch_bounds__(256) k_fast_stream(DevParams P, FastParams F, 
 }
 
 // ------------------------------------------------------------------ SRD collision
-// One warp per SRD cell (jx, jy) of the grid shifted by (sx, sy) cell units: its particles
-// come from the 2 x 2 standard cells that overlap it (a particle in cell (ix, iy) at offset
-// (ox, oy) lies in SRD cell (ix + floor(ox + sx), iy + floor(oy + sy)), wrapped on periodic
-// axes and clamped on the others, as srd_cell_id_with_random_shift does, src/srd_collision.cpp:9-45).
+// One warp per SRD cell: its members are the particles the stream kernel filed into its bin.
 // Rotation of the velocities relative to the cell mean by +-alpha, the sign drawn per SRD cell,
 // and the isokinetic thermostat (src/srd_collision.cpp:47-140). Sums are exact in grid units;
 // the rounding of the new velocities to the grid leaves an integer residual that goes to the
-// member with the smallest particle id, so every SRD cell keeps its momentum exactly.
-__device__ __forceinline__ int fast_srd_index(int i, double o, double s, int N, bool per) {
-    int j = i + (int)floor((double)o + s);
-    if (per) j = wrap_index(j, N);
-    else j = min(max(j, 0), N - 1);
-    return j;
-}
-
-__global__ void __launch_bounds__(256) k_fast_collide(DevParams P, FastParams F, const FastStep* __restrict__ S,
-                                                      FastBins b) {
+// member with the smallest particle id, so every SRD cell keeps its momentum exactly. Each
+// member is then filed into the bin of its standard cell (warp-aggregated slot claims).
+__global__ void __launch_bounds__(256, 4) k_fast_collide(DevParams P, FastParams F, const FastStep* __restrict__ S,
+                                                         FastBins sb, FastBins out, DevStatus* st) {
     const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (w >= P.Nc) return;
-    const int jx = w / P.Ny, jy = w - jx * P.Ny;
-    const double sxs = S->sx, sys = S->sy;
-    const int fx = (sxs < 0.0) ? -1 : 0, fy = (sys < 0.0) ? -1 : 0;
-    int src[4], n[4];
-    int total = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int ax = jx - fx - 1 + (k & 1), ay = jy - fy - 1 + (k >> 1);
-        bool ok = true;
-        if (P.perx) ax = wrap_index(ax, P.Nx);
-        else ok = ok && ax >= 0 && ax < P.Nx;
-        if (P.pery) ay = wrap_index(ay, P.Ny);
-        else ok = ok && ay >= 0 && ay < P.Ny;
-        src[k] = ok ? ay + P.Ny * ax : -1;
-        n[k] = ok ? min(b.cnt[src[k]], F.K) : 0;
-        total += n[k];
-    }
-    // duplicate sources (a periodic axis of one or two cells) are read once
-    if (src[1] == src[0]) n[1] = 0;
-    if (src[2] == src[0] || src[2] == src[1]) n[2] = 0;
-    if (src[3] == src[0] || src[3] == src[1] || src[3] == src[2]) n[3] = 0;
-    total = n[0] + n[1] + n[2] + n[3];
-    // pass 1: membership and exact sums
+    const int n = min(sb.cnt[w], F.K);
+    if (n == 0) return;
+    const size_t base = (size_t)w * F.K;
+    // members in registers, up to four per lane
+    int qx[4], qy[4], pid[4], cel[4];
+    float2 off[4];
     long long Sx = 0, Sy = 0, Sqq = 0;
-    int N = 0;
-    for (int t0 = 0; t0 < total; t0 += 32) {
-        const int t = t0 + lane;
-        bool mem = false;
-        int qx = 0, qy = 0;
-        if (t < total) {
-            int k = 0, j = t;
-            while (j >= n[k]) { j -= n[k]; ++k; }
-            const size_t s = (size_t)src[k] * F.K + j;
-            const int ix = src[k] / P.Ny, iy = src[k] - ix * P.Ny;
-            const float2 o = b.off[s];
-            mem = fast_srd_index(ix, o.x, sxs, P.Nx, P.perx) == jx && fast_srd_index(iy, o.y, sys, P.Ny, P.pery) == jy;
-            if (mem) {
-                const float2 v = b.vel[s];
-                qx = fq_of(v.x);
-                qy = fq_of(v.y);
-            }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int j = 32 * r + lane;
+        qx[r] = qy[r] = 0;
+        pid[r] = 0x7fffffff;
+        cel[r] = -1;
+        if (j < n) {
+            const float2 v = sb.vel[base + j];
+            qx[r] = fq_of(v.x);
+            qy[r] = fq_of(v.y);
+            pid[r] = sb.pid[base + j];
+            cel[r] = sb.cell[base + j];
+            off[r] = sb.off[base + j];
+            Sx += qx[r];
+            Sy += qy[r];
+            Sqq += (long long)qx[r] * qx[r] + (long long)qy[r] * qy[r];
         }
-        N += __popc(__ballot_sync(0xffffffffu, mem));
-        Sx += qx;
-        Sy += qy;
-        Sqq += (long long)qx * qx + (long long)qy * qy;
     }
-    if (N == 0) return;
     Sx = warp_sum_ll(Sx);
     Sy = warp_sum_ll(Sy);
     Sqq = warp_sum_ll(Sqq);
+    const int N = n;
     const double ux = (double)Sx / N, uy = (double)Sy / N;
     double ct = 1.0, sn = 0.0;
     if (N >= 2) {
         const uint64_t h = fhash(S->seed, (uint64_t)w, 0x5349474EULL);
-        const int r = (h >> 63) ? 1 : 2;  // +alpha or -alpha
-        ct = P.rotCos[r];
-        sn = P.rotSin[r];
+        const int rr = (h >> 63) ? 1 : 2;  // +alpha or -alpha
+        ct = P.rotCos[rr];
+        sn = P.rotSin[rr];
     }
     double lam = 1.0;
     if (P.useThermostat && N > 1) {
@@ -393,46 +379,54 @@ __global__ void __launch_bounds__(256) k_fast_collide(DevParams P, FastParams F,
         const double s2 = (double)num / (double)N;
         if (s2 > 0.0) lam = sqrt(2.0 * (double)(N - 1) * P.kBT * kFastQ * kFastQ / s2);
     }
-    // pass 2: new velocities rounded to the grid; their sum and the smallest-id member
     long long Tx = 0, Ty = 0;
-    unsigned long long best = ~0ULL;  // (pid, slot) of the member that takes the residual
-    for (int t0 = 0; t0 < total; t0 += 32) {
-        const int t = t0 + lane;
-        if (t < total) {
-            int k = 0, j = t;
-            while (j >= n[k]) { j -= n[k]; ++k; }
-            const size_t s = (size_t)src[k] * F.K + j;
-            const int ix = src[k] / P.Ny, iy = src[k] - ix * P.Ny;
-            const float2 o = b.off[s];
-            if (fast_srd_index(ix, o.x, sxs, P.Nx, P.perx) == jx && fast_srd_index(iy, o.y, sys, P.Ny, P.pery) == jy) {
-                const float2 v = b.vel[s];
-                const double rx = (double)fq_of(v.x) - ux, ry = (double)fq_of(v.y) - uy;
-                const long long nx = llrint(ux + lam * (ct * rx - sn * ry));
-                const long long ny = llrint(uy + lam * (sn * rx + ct * ry));
-                Tx += nx;
-                Ty += ny;
-                b.vel[s] = make_float2(fv_of(nx), fv_of(ny));
-                if (llabs(nx) < (1LL << 22) && llabs(ny) < (1LL << 22)) {
-                    const unsigned long long key = ((unsigned long long)(uint32_t)b.pid[s] << 32) | (unsigned long long)t;
-                    best = key < best ? key : best;
-                }
+    long long nx[4], ny[4];
+    unsigned long long best = ~0ULL;  // (pid << 8 | member) of the member that takes the residual
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        nx[r] = ny[r] = 0;
+        if (32 * r + lane < n) {
+            const double rx = (double)qx[r] - ux, ry = (double)qy[r] - uy;
+            nx[r] = llrint(ux + lam * (ct * rx - sn * ry));
+            ny[r] = llrint(uy + lam * (sn * rx + ct * ry));
+            Tx += nx[r];
+            Ty += ny[r];
+            if (llabs(nx[r]) < (1LL << 22) && llabs(ny[r]) < (1LL << 22)) {
+                const unsigned long long key = ((unsigned long long)(uint32_t)pid[r] << 8) | (unsigned long long)r;
+                best = key < best ? key : best;
             }
         }
     }
     Tx = warp_sum_ll(Tx);
     Ty = warp_sum_ll(Ty);
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
-        best = x < best ? x : best;
-    }
-    __syncwarp();
+    const unsigned long long bestAll = warp_min_u64_c(best);
     const long long rx = Sx - Tx, ry = Sy - Ty;
-    if (lane == 0 && best != ~0ULL && (rx != 0 || ry != 0)) {
-        int k = 0, j = (int)(best & 0xffffffffu);
-        while (j >= n[k]) { j -= n[k]; ++k; }
-        const size_t s = (size_t)src[k] * F.K + j;
-        const float2 v = b.vel[s];
-        b.vel[s] = make_float2(fv_of(fq_of(v.x) + rx), fv_of(fq_of(v.y) + ry));
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const bool live = 32 * r + lane < n;
+        if (live && best == bestAll && (int)(bestAll & 0xff) == r) {
+            nx[r] += rx;
+            ny[r] += ry;
+        }
+        const unsigned act = __ballot_sync(0xffffffffu, live);
+        if (!act) break;
+        if (live) {
+            const int c = cel[r];
+            const unsigned grp = __match_any_sync(act, c);
+            const int leader = __ffs(grp) - 1;
+            int b0 = 0;
+            if (lane == leader) b0 = atomicAdd(out.cnt + c, __popc(grp));
+            b0 = __shfl_sync(grp, b0, leader);
+            const int slot = b0 + __popc(grp & lanemask_lt());
+            if (slot < F.K) {
+                const size_t d = (size_t)c * F.K + slot;
+                out.off[d] = off[r];
+                out.vel[d] = make_float2(fv_of(nx[r]), fv_of(ny[r]));
+                out.pid[d] = pid[r];
+            } else if (st) {
+                raise_error(st, kErrBinCapacity, c);
+            }
+        }
     }
 }
 
@@ -450,36 +444,53 @@ struct FastZoneArgs {
     const FastStep* S;
     FastBins in, out;
     longlong2* red;            // nullable: per cell the output's momentum sum (closure input)
+    longlong4* ref;            // nullable: per cell the input's (sum qx, sum qy, sum |q|^2, N): the
+                               // closure's reference fields (stateRef is the collided state,
+                               // src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:241-251)
     int* moved;                // (dense, sparse) over all zones
     int* recOverflow;          // zones that ran out of records (their remaining moves are skipped)
     DevStatus* st;
     int maxCells, winCap, nsmCap, recCap;
 };
 
+// The 24 range-2 neighbour offsets grouped by the angular bin of atan2(dy, dx)
+// (src/zone_pass.cpp:447-457: bin = floor((angle + pi) / (pi / 4)) mod 8): three per bin, bin b
+// in lanes 3b .. 3b + 2. For |d| <= 2 on axes of at least 5 cells the minimal-image step is
+// the offset itself.
+__constant__ signed char kFastNb[24][2] = {
+    {-2, -1}, {-2, 0}, {-1, 0},  {-2, -2}, {-1, -2}, {-1, -1}, {0, -2}, {1, -2}, {0, -1}, {2, -2}, {1, -1}, {2, -1},
+    {1, 0},   {2, 0},  {2, 1},   {1, 1},   {1, 2},   {2, 2},   {0, 1},  {-1, 2}, {0, 2},  {-2, 1}, {-1, 1}, {-2, 2}};
+
 // zone working set layout (bytes), carved per warp
 struct FastZoneMem {
-    short* win;       // winCap: counts of the window (zone + 2-cell halo); -1 outside the domain
-    uint8_t* n0;      // cell: particles at the pass start
-    uint8_t* flg;     // cell: flags
-    uint8_t* nrecv;   // cell: records currently in the cell
-    uint32_t* rm;     // cell x 4: originals removed
-    int* recPid;      // recCap
-    uint16_t* recSrc; // recCap: (origin cell << 7) | slot
-    uint8_t* recCur;  // recCap: current cell
-    float2* recOff;   // recCap: position in the current cell
-    float* nsm;       // nsmCap: smoothed occupancy of the zone and a one-cell ring
-    uint32_t* keys;   // 128: order keys (dense / low cells), sort scratch
-    int* tgt;         // 32: ordered targets or donors
-    float* tgtMap;    // 32
-    int* pidBuf;      // kFastMaxK: member ids (momentum correction)
+    short* win;        // winCap: counts of the window (zone + 2-cell halo); -1 outside the domain
+    uint16_t* wi;      // cell: its window index
+    uint8_t* cx;       // cell: local x
+    uint8_t* cy;       // cell: local y
+    uint8_t* n0;       // cell: particles at the pass start
+    uint8_t* flg;      // cell: flags
+    uint8_t* nrecv;    // cell: records currently in the cell
+    uint32_t* rm;      // cell x 4: originals removed
+    int* minPid;       // cell: the smallest id among the output members (takes the remainder)
+    int* sums;         // cell x 4: the arrivals' momentum (2); then the correction's share (2),
+                       // remainders (x low, y high half) and the next free output slot
+    int* recPid;       // recCap
+    uint16_t* recSrc;  // recCap: (origin cell << 7) | slot
+    uint8_t* recCur;   // recCap: current cell
+    float2* recOff;    // recCap: position in the current cell
+    float* nsm;        // nsmCap: smoothed occupancy of the zone and a one-cell ring
+    uint32_t* keys;    // 128: order keys (dense / low cells), sort scratch
+    int* tgt;          // 32: ordered targets or donors
+    int* tgt2;         // 32: receivers of a dense cell's first phase
 
     __host__ __device__ static size_t bytes(int maxCells, int winCap, int nsmCap, int recCap) {
         size_t b = 0;
         auto add = [&](size_t n, size_t a) { b = (b + a - 1) / a * a + n; };
         add((size_t)winCap * 2, 2);
-        add((size_t)maxCells, 1);
-        add((size_t)maxCells, 1);
-        add((size_t)maxCells, 1);
+        add((size_t)maxCells * 2, 2);
+        for (int k = 0; k < 5; ++k) add((size_t)maxCells, 1);
+        add((size_t)maxCells * 16, 4);
+        add((size_t)maxCells * 4, 4);
         add((size_t)maxCells * 16, 4);
         add((size_t)recCap * 4, 4);
         add((size_t)recCap * 2, 2);
@@ -489,7 +500,6 @@ struct FastZoneMem {
         add(128 * 4, 4);
         add(32 * 4, 4);
         add(32 * 4, 4);
-        add((size_t)kFastMaxK * 4, 4);
         return (b + 15) / 16 * 16;
     }
     __device__ void carve(char* base, int maxCells, int winCap, int nsmCap, int recCap) {
@@ -501,10 +511,15 @@ struct FastZoneMem {
             return p;
         };
         win = (short*)take((size_t)winCap * 2, 2);
+        wi = (uint16_t*)take((size_t)maxCells * 2, 2);
+        cx = (uint8_t*)take((size_t)maxCells, 1);
+        cy = (uint8_t*)take((size_t)maxCells, 1);
         n0 = (uint8_t*)take((size_t)maxCells, 1);
         flg = (uint8_t*)take((size_t)maxCells, 1);
         nrecv = (uint8_t*)take((size_t)maxCells, 1);
         rm = (uint32_t*)take((size_t)maxCells * 16, 4);
+        minPid = (int*)take((size_t)maxCells * 4, 4);
+        sums = (int*)take((size_t)maxCells * 16, 4);
         recPid = (int*)take((size_t)recCap * 4, 4);
         recSrc = (uint16_t*)take((size_t)recCap * 2, 2);
         recCur = (uint8_t*)take((size_t)recCap, 1);
@@ -512,8 +527,7 @@ struct FastZoneMem {
         nsm = (float*)take((size_t)nsmCap * 4, 4);
         keys = (uint32_t*)take(128 * 4, 4);
         tgt = (int*)take(32 * 4, 4);
-        tgtMap = (float*)take(32 * 4, 4);
-        pidBuf = (int*)take((size_t)kFastMaxK * 4, 4);
+        tgt2 = (int*)take(32 * 4, 4);
     }
 };
 
@@ -524,7 +538,9 @@ __device__ __forceinline__ void warp_sort128(uint32_t* a, int lane) {
     for (int k = 2; k <= 128; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
             __syncwarp();
-            for (int i = lane; i < 128; i += 32) {
+#pragma unroll
+            for (int i0 = 0; i0 < 128; i0 += 32) {
+                const int i = i0 + lane;
                 const int p = i ^ j;
                 if (p > i) {
                     const uint32_t x = a[i], y = a[p];
@@ -540,6 +556,8 @@ __device__ __forceinline__ void warp_sort128(uint32_t* a, int lane) {
     __syncwarp();
 }
 
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) { return warp_min_u64_c(v); }
+
 struct FastZone {
     const FastZoneArgs* A;
     FastZoneMem M;
@@ -551,24 +569,28 @@ struct FastZone {
     bool failed;        // out of records: remaining moves skipped
     int movedDense, movedSparse;
 
-    __device__ __forceinline__ int widx(int lx, int ly) const { return (lx + 2) * WY + (ly + 2); }
-    __device__ __forceinline__ int cnt(int l) const { return M.win[widx(l / TY, l % TY)]; }
-    __device__ __forceinline__ void add_cnt(int l, int d) { M.win[widx(l / TY, l % TY)] += (short)d; }
-    __device__ __forceinline__ int gcell(int l) const { return (y0 + l % TY) + A->P.Ny * (x0 + l / TY); }
+    __device__ __forceinline__ int cnt(int l) const { return M.win[M.wi[l]]; }
+    __device__ __forceinline__ void add_cnt(int l, int d) { M.win[M.wi[l]] += (short)d; }
+    __device__ __forceinline__ int gcell(int l) const { return (y0 + M.cy[l]) + A->P.Ny * (x0 + M.cx[l]); }
     __device__ __forceinline__ double low_map(bool bulk) const { return bulk ? A->P.lowThrBulk : A->F.lowMapEmpty; }
     __device__ __forceinline__ double high_map(bool bulk) const { return bulk ? A->P.highThr : A->F.highMapEmpty; }
 
-    // local cell of the zone cell at local (lx, ly) moved by (dx, dy), wrapping periodic axes;
-    // -1 outside the domain or outside the zone
+    // the zone cell at local (lx + dx, ly + dy), wrapping periodic axes; -1 outside the domain
+    // or outside the zone
     __device__ __forceinline__ int neighbour(int l, int dx, int dy) const {
         const DevParams& P = A->P;
-        int gx = x0 + l / TY + dx, gy = y0 + l % TY + dy;
-        if (P.perx) gx = wrap_index(gx, P.Nx);
+        int gx = x0 + M.cx[l] + dx, gy = y0 + M.cy[l] + dy;
+        if (P.perx) gx = gx < 0 ? gx + P.Nx : (gx >= P.Nx ? gx - P.Nx : gx);
         else if (gx < 0 || gx >= P.Nx) return -1;
-        if (P.pery) gy = wrap_index(gy, P.Ny);
+        if (P.pery) gy = gy < 0 ? gy + P.Ny : (gy >= P.Ny ? gy - P.Ny : gy);
         else if (gy < 0 || gy >= P.Ny) return -1;
         if (gx < x0 || gx >= x1 || gy < y0 || gy >= y1) return -1;
         return (gx - x0) * TY + (gy - y0);
+    }
+
+    __device__ __forceinline__ uint64_t member_key(bool dense, uint32_t salt, uint32_t pid, int rec) const {
+        if (dense) return rec < 0 ? (uint64_t)pid : ((1ULL << 31) + (uint64_t)rec);
+        return ((fmix64(zseed ^ ((uint64_t)salt << 32) ^ (uint64_t)pid) >> 41) << 31) | (uint64_t)(pid & 0x7fffffffu);
     }
 
     // Removes nt members of cell l and files them into cell t at fresh uniform positions.
@@ -576,25 +598,28 @@ struct FastZone {
     // then the arrivals in order: src/zone_pass.cpp:541-583 takes the first ids); otherwise
     // members chosen uniformly at random (the sparse phase shuffles the donor's list). A
     // candidate is (key << 10) | (record flag << 9) | index: keys of at most 54 bits, original
-    // slots below 128 and records below 512.
-    __device__ __forceinline__ uint64_t member_key(bool dense, uint32_t salt, uint32_t pid, int rec) const {
-        if (dense) return rec < 0 ? (uint64_t)pid : ((1ULL << 31) + (uint64_t)rec);
-        return ((fhash(zseed, salt, pid) >> 41) << 31) | (uint64_t)(pid & 0x7fffffffu);
-    }
+    // slots below 128 and records below 512. Each lane keeps the keys of its originals
+    // (slots lane + 32 k) in registers for the whole call.
     __device__ void move_members(int l, int t, int nt, bool dense) {
         const FastBins& B = A->in;
         const int c = gcell(l);
         const int n0 = M.n0[l];
         const uint32_t salt = ++op;
+        unsigned long long cand[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int j = lane + 32 * r;
+            cand[r] = ~0ULL;
+            if (j < n0 && !(M.rm[4 * l + r] & (1u << lane))) {
+                const uint32_t pid = (uint32_t)B.pid[(size_t)c * A->F.K + j];
+                cand[r] = (member_key(dense, salt, pid, -1) << 10) | (unsigned long long)j;
+            }
+        }
         for (int k = 0; k < nt; ++k) {
             if (failed) return;
-            unsigned long long best = ~0ULL;
-            for (int j = lane; j < n0; j += 32) {
-                if (M.rm[4 * l + (j >> 5)] & (1u << (j & 31))) continue;
-                const uint32_t pid = (uint32_t)B.pid[(size_t)c * A->F.K + j];
-                const unsigned long long v = (member_key(dense, salt, pid, -1) << 10) | (unsigned long long)j;
-                best = v < best ? v : best;
-            }
+            unsigned long long best = cand[0];
+#pragma unroll
+            for (int r = 1; r < 4; ++r) best = cand[r] < best ? cand[r] : best;
             if (M.nrecv[l] > 0) {
                 for (int r = lane; r < nrec; r += 32) {
                     if (M.recCur[r] != l) continue;
@@ -603,19 +628,19 @@ struct FastZone {
                     best = v < best ? v : best;
                 }
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
-                best = x < best ? x : best;
-            }
+            best = warp_min_u64(best);
             if (best == ~0ULL) return;  // no member left (cannot happen while counts agree)
-            const uint64_t hp = fhash(zseed, salt, 0x504F53ULL + (uint64_t)k);
-            const float2 pos = make_float2(fminf((float)fu01(hp), kFastOffMax), fminf((float)fu01(fmix64(hp)), kFastOffMax));
+            // the new position: two 24-bit uniforms of one draw
+            const uint64_t hp = fmix64(zseed ^ ((uint64_t)salt << 20) ^ (0x504F53ULL + (uint64_t)k));
+            const float2 pos = make_float2(fminf((float)(hp >> 40) * 0x1.0p-24f, kFastOffMax),
+                                           fminf((float)((hp >> 8) & 0xFFFFFFu) * 0x1.0p-24f, kFastOffMax));
             if (!(best & 512ULL)) {  // an original of cell l
                 const int j = (int)(best & 511ULL);
                 if (nrec >= A->recCap) {
                     failed = true;
                     return;
                 }
+                if ((j & 31) == lane) cand[j >> 5] = ~0ULL;
                 if (lane == 0) {
                     M.rm[4 * l + (j >> 5)] |= 1u << (j & 31);
                     M.recPid[nrec] = B.pid[(size_t)c * A->F.K + j];
@@ -636,38 +661,19 @@ struct FastZone {
         }
     }
 
-    // update_transfer_correction_masks (src/zone_pass.cpp:492-525) for source l and the
-    // receivers recv (bit k: target k of tgt[]), bulk flag bit `bf`
-    __device__ void update_masks(int l, unsigned recvBits, uint8_t bf) {
-        bool allBulk = (M.flg[l] & bf) != 0;
-        for (int k = 0; k < 32; ++k)
-            if (recvBits & (1u << k)) allBulk = allBulk && (M.flg[M.tgt[k]] & bf);
-        if (lane == 0) {
-            auto set = [&](int c) {
-                if (allBulk) M.flg[c] |= kZBB;
-                else M.flg[c] = (uint8_t)((M.flg[c] | kZSkip) & ~kZBB);
-            };
-            set(l);
-            for (int k = 0; k < 32; ++k)
-                if (recvBits & (1u << k)) set(M.tgt[k]);
-        }
-        __syncwarp();
-    }
-
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589) over the
     // targets ranked as rank_dense_targets_unified does (:436-490); map: 0 low, 1 high.
-    // Returns the particles moved; receivers are added to *recvBits (bits index M.tgt).
-    __device__ int spread(int l, int needOut, int mapKind, unsigned* recvBits) {
+    // Returns the particles moved; the receivers go to rcv[*nr ...].
+    __device__ int spread(int l, int needOut, int mapKind, int* rcv, int* nr) {
         const DevParams& P = A->P;
-        // candidates: range-2 neighbours in dy-outer, dx-inner order (lane k < 24)
+        // lane k < 24: the k-th neighbour of the bin-grouped offset table
         const int k = lane;
         int t = -1, ddx = 0, ddy = 0;
         double map = 0.0;
         bool adm = false;
         if (k < 24) {
-            const int idx = k < 12 ? k : k + 1;
-            ddx = idx % 5 - 2;
-            ddy = idx / 5 - 2;
+            ddx = kFastNb[k][0];
+            ddy = kFastNb[k][1];
             t = neighbour(l, ddx, ddy);
             if (t >= 0) {
                 const bool bulk = M.flg[t] & kZBulkD;
@@ -679,35 +685,26 @@ struct FastZone {
         const int T = __popc(admMask);
         if (T == 0) return 0;
         const uint32_t salt = ++op;
-        const int startBin = (int)(fhash(zseed, salt, 0x42494EULL) & 7);
+        const int startBin = (int)(fmix64(zseed ^ ((uint64_t)salt << 12) ^ 0x42494EULL) >> 61);
         // sort key (-deficit, cnt, chebyshev, distance^2, random); inward weight is 0 here
         unsigned long long key = ~0ULL;
-        int bin = 0;
         if (adm) {
             const double deficit = fmax(0.0, map - (double)cnt(t));
             const unsigned long long dq = (unsigned long long)min(llrint(deficit * 4096.0), (long long)0xFFFFF);
             const int cheb = max(abs(ddx), abs(ddy)), d2 = ddx * ddx + ddy * ddy;
             key = ((0xFFFFFULL - dq) << 44) | ((unsigned long long)min(cnt(t), 255) << 36) |
                   ((unsigned long long)cheb << 34) | ((unsigned long long)d2 << 30) |
-                  (fhash(zseed, salt, (uint64_t)k) & 0x3FFFFFFFULL);
-            bin = P.atanBin[(ddx + 2) + 5 * (ddy + 2)];
+                  (fmix64(zseed ^ ((uint64_t)salt << 8) ^ (uint64_t)k) & 0x3FFFFFFFULL);
         }
-        int rank = 0;
-        for (int j = 0; j < 24; ++j) {
-            const unsigned long long kj = __shfl_sync(0xffffffffu, key, j);
-            const int bj = __shfl_sync(0xffffffffu, bin, j);
-            if (adm && ((admMask >> j) & 1u) && bj == bin && kj < key) ++rank;
-        }
-        const int pos = rank * 8 + ((bin - startBin + 8) & 7);
-        int ord = 0;
-        for (int j = 0; j < 24; ++j) {
-            const int pj = __shfl_sync(0xffffffffu, pos, j);
-            if (adm && ((admMask >> j) & 1u) && pj < pos) ++ord;
-        }
-        if (adm) {
-            M.tgt[ord] = t;
-            M.tgtMap[ord] = (float)map;
-        }
+        // rank inside the bin: the two other lanes of the bin
+        const int b = k / 3, base = 3 * b;
+        const unsigned long long ka = __shfl_sync(0xffffffffu, key, base + ((k - base + 1) % 3));
+        const unsigned long long kb = __shfl_sync(0xffffffffu, key, base + ((k - base + 2) % 3));
+        const int rank = (ka < key) + (kb < key);
+        const int pos = rank * 8 + ((b - startBin + 8) & 7);
+        const unsigned posMask = __reduce_or_sync(0xffffffffu, adm ? (1u << pos) : 0u);
+        const int ord = __popc(posMask & ((1u << pos) - 1u));
+        if (adm) M.tgt[ord] = t;
         __syncwarp();
         // per ordered target (lane o < T): its current integer deficit
         int def = 0;
@@ -721,6 +718,7 @@ struct FastZone {
         }
         int avail = cnt(l);
         int moved = 0;
+        unsigned got = 0;
         while (needOut > 0 && avail > 0 && !failed) {
             bool progressed = false;
             for (int kk = 0; kk < T; ++kk) {
@@ -738,8 +736,7 @@ struct FastZone {
                 }
                 __syncwarp();
                 if (lane == kk) def = max(0, (int)floor(mapO - (double)cnt(tO)));
-                // the receiver's index in M.tgt for the masks
-                *recvBits |= 1u << kk;
+                got |= 1u << kk;
                 avail -= nt;
                 needOut -= nt;
                 moved += nt;
@@ -748,7 +745,29 @@ struct FastZone {
             }
             if (!progressed) break;
         }
+        // receivers, in target order
+        if ((got >> lane) & 1u) rcv[*nr + __popc(got & ((1u << lane) - 1u))] = tO;
+        *nr += __popc(got);
+        __syncwarp();
         return moved;
+    }
+
+    // the transfer masks (src/zone_pass.cpp:492-525) for a source and its receivers rcv[0..nr),
+    // bulk flag bit bf
+    __device__ void masks(int src, const int* rcv, int nr, uint8_t bf) {
+        bool allBulk = (M.flg[src] & bf) != 0;
+        const bool mine = lane < nr;
+        const int rc = mine ? rcv[lane] : src;
+        allBulk = allBulk && __all_sync(0xffffffffu, !mine || (M.flg[rc] & bf));
+        __syncwarp();
+        if (lane <= nr) {
+            const int cc = lane < nr ? rc : src;
+            uint8_t f = M.flg[cc];
+            if (lane < nr) f |= kZRecv;
+            f = allBulk ? (uint8_t)(f | kZBB) : (uint8_t)((f | kZSkip) & ~kZBB);
+            M.flg[cc] = f;
+        }
+        __syncwarp();
     }
 
     // redistribute_dense_cell_at_range_zone_local (src/zone_pass.cpp:591-634) and the mask
@@ -758,40 +777,14 @@ struct FastZone {
         const double hi = high_map(bulk);
         const int nc = cnt(l);
         if (nc <= 0 || (double)nc <= hi) return;
-        int needOut = max(0, (int)ceil((double)nc - hi));
-        unsigned recvPoor = 0, recvRelief = 0;
+        const int needOut = max(0, (int)ceil((double)nc - hi));
+        int nr = 0;
         int moved = 0;
-        if (needOut > 0) moved += spread(l, needOut, 0, &recvPoor);
-        // the poor targets are in M.tgt now; keep their cells before the relief ranking
-        int poorCells[24];
-        int np = 0;
-        for (int k = 0; k < 24; ++k)
-            if (recvPoor & (1u << k)) poorCells[np++] = M.tgt[k];
+        if (needOut > 0) moved += spread(l, needOut, 0, M.tgt2, &nr);
         const int remainingOut = max(0, (int)ceil((double)cnt(l) - hi));
-        if (remainingOut > 0 && !failed) moved += spread(l, remainingOut, 1, &recvRelief);
-        // masks over the union of both phases' receivers
-        bool allBulk = (M.flg[l] & kZBulkD) != 0;
-        for (int k = 0; k < np; ++k) allBulk = allBulk && (M.flg[poorCells[k]] & kZBulkD);
-        for (int k = 0; k < 24; ++k)
-            if (recvRelief & (1u << k)) allBulk = allBulk && (M.flg[M.tgt[k]] & kZBulkD);
-        __syncwarp();
-        if (lane == 0) {
-            auto set = [&](int c) {
-                if (allBulk) M.flg[c] |= kZBB;
-                else M.flg[c] = (uint8_t)((M.flg[c] | kZSkip) & ~kZBB);
-            };
-            set(l);
-            for (int k = 0; k < np; ++k) {
-                M.flg[poorCells[k]] |= kZRecv;
-                set(poorCells[k]);
-            }
-            for (int k = 0; k < 24; ++k)
-                if (recvRelief & (1u << k)) {
-                    M.flg[M.tgt[k]] |= kZRecv;
-                    set(M.tgt[k]);
-                }
-        }
-        __syncwarp();
+        if (remainingOut > 0 && !failed) moved += spread(l, remainingOut, 1, M.tgt2, &nr);
+        // the receivers of the two phases may repeat a cell; flags are idempotent
+        masks(l, M.tgt2, min(nr, 31), kZBulkD);
         movedDense += moved;
     }
 
@@ -802,20 +795,22 @@ struct FastZone {
         const int RY = TY + 2, total = (TX + 2) * RY;
         for (int i = lane; i < total; i += 32) {
             const int rx = i / RY - 1, ry = i % RY - 1;  // local coordinates, -1 .. TX
-            int cx = x0 + rx, cy = y0 + ry;
-            if (P.perx) cx = wrap_index(cx, P.Nx);
-            if (P.pery) cy = wrap_index(cy, P.Ny);
+            int cxx = x0 + rx, cyy = y0 + ry;
+            if (P.perx) cxx = cxx < 0 ? cxx + P.Nx : (cxx >= P.Nx ? cxx - P.Nx : cxx);
+            if (P.pery) cyy = cyy < 0 ? cyy + P.Ny : (cyy >= P.Ny ? cyy - P.Ny : cyy);
             float v = 0.0f;
-            if (cx >= 0 && cx < P.Nx && cy >= 0 && cy < P.Ny) {
-                double acc = 0.0, ws = 0.0;
+            if (cxx >= 0 && cxx < P.Nx && cyy >= 0 && cyy < P.Ny) {
+                float acc = 0.0f, ws = 0.0f;
+#pragma unroll
                 for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
                     for (int dx = -1; dx <= 1; ++dx) {
-                        if (cx + dx < 0 || cx + dx >= P.Nx || cy + dy < 0 || cy + dy >= P.Ny) continue;
-                        const double w = (double)((2 - abs(dx)) * (2 - abs(dy))) * 0.0625;
-                        acc += w * (double)M.win[(rx + dx + 2) * WY + (ry + dy + 2)];
+                        if (cxx + dx < 0 || cxx + dx >= P.Nx || cyy + dy < 0 || cyy + dy >= P.Ny) continue;
+                        const float w = (float)((2 - abs(dx)) * (2 - abs(dy))) * 0.0625f;
+                        acc += w * (float)M.win[(rx + dx + 2) * WY + (ry + dy + 2)];
                         ws += w;
                     }
-                v = (float)(acc / fmax(ws, 1e-30));
+                v = acc / ws;
             }
             M.nsm[i] = v;
         }
@@ -830,19 +825,19 @@ struct FastZone {
         if (nc <= 0) return;
         int need = max(0, P.lowThrBulkInt - nc);
         if (need <= 0) return;
-        const int lx = l / TY, ly = l % TY;
+        const int lx = M.cx[l], ly = M.cy[l];
         // inward direction from the local gradient of the smoothed occupancy (:375-411)
         const int gx = x0 + lx, gy = y0 + ly;
-        double dirx, diry;
-        if (P.perx) dirx = 0.5 * ((double)nsm_at(lx + 1, ly) - (double)nsm_at(lx - 1, ly));
-        else if (gx == 0) dirx = (double)nsm_at(lx + 1, ly) - (double)nsm_at(lx, ly);
-        else if (gx == P.Nx - 1) dirx = (double)nsm_at(lx, ly) - (double)nsm_at(lx - 1, ly);
-        else dirx = 0.5 * ((double)nsm_at(lx + 1, ly) - (double)nsm_at(lx - 1, ly));
-        if (P.pery) diry = 0.5 * ((double)nsm_at(lx, ly + 1) - (double)nsm_at(lx, ly - 1));
-        else if (gy == 0) diry = (double)nsm_at(lx, ly + 1) - (double)nsm_at(lx, ly);
-        else if (gy == P.Ny - 1) diry = (double)nsm_at(lx, ly) - (double)nsm_at(lx, ly - 1);
-        else diry = 0.5 * ((double)nsm_at(lx, ly + 1) - (double)nsm_at(lx, ly - 1));
-        const double ndir = hypot(dirx, diry);
+        float dirx, diry;
+        if (P.perx) dirx = 0.5f * (nsm_at(lx + 1, ly) - nsm_at(lx - 1, ly));
+        else if (gx == 0) dirx = nsm_at(lx + 1, ly) - nsm_at(lx, ly);
+        else if (gx == P.Nx - 1) dirx = nsm_at(lx, ly) - nsm_at(lx - 1, ly);
+        else dirx = 0.5f * (nsm_at(lx + 1, ly) - nsm_at(lx - 1, ly));
+        if (P.pery) diry = 0.5f * (nsm_at(lx, ly + 1) - nsm_at(lx, ly - 1));
+        else if (gy == 0) diry = nsm_at(lx, ly + 1) - nsm_at(lx, ly);
+        else if (gy == P.Ny - 1) diry = nsm_at(lx, ly) - nsm_at(lx, ly - 1);
+        else diry = 0.5f * (nsm_at(lx, ly + 1) - nsm_at(lx, ly - 1));
+        const float ndir = hypotf(dirx, diry);
         // donors: in-zone 8-neighbours above ceil(lowThrBulk), ranked by
         // 100 align + Nsm (+ a random tie-break) descending (rank_admissible_neighbors_inward, :636-667)
         const int k = lane;
@@ -858,18 +853,19 @@ struct FastZone {
         const unsigned donMask = __ballot_sync(0xffffffffu, don);
         if (!donMask) return;
         const uint32_t salt = ++op;
-        double score = -1e300;
+        float score = -1e30f;
         uint32_t tie = 0;
         if (don) {
-            const double nstep = P.hypotTab[(ddx + 2) + 5 * (ddy + 2)];
-            double align = 0.0;
-            if (ndir >= 1e-14 && nstep >= 1e-14) align = ((double)ddx * dirx + (double)ddy * diry) / (ndir * nstep);
-            score = 100.0 * align + (double)nsm_at(lx + ddx, ly + ddy);
-            tie = (uint32_t)fhash(zseed, salt, (uint64_t)k);
+            const float nstep = (ddx != 0 && ddy != 0) ? 1.41421356f : 1.0f;
+            float align = 0.0f;
+            if (ndir >= 1e-14f) align = ((float)ddx * dirx + (float)ddy * diry) / (ndir * nstep);
+            score = 100.0f * align + nsm_at(lx + ddx, ly + ddy);
+            tie = (uint32_t)fmix64(zseed ^ ((uint64_t)salt << 8) ^ (uint64_t)k);
         }
         int ord = 0;
+#pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const double sj = __shfl_sync(0xffffffffu, score, j);
+            const float sj = __shfl_sync(0xffffffffu, score, j);
             const uint32_t tj = __shfl_sync(0xffffffffu, tie, j);
             if (don && ((donMask >> j) & 1u) && (sj > score || (sj == score && tj < tie))) ++ord;
         }
@@ -887,174 +883,167 @@ struct FastZone {
             if (lane == 0) {
                 add_cnt(dn, -nt);
                 add_cnt(l, nt);
-                M.flg[l] |= kZRecv;
             }
             __syncwarp();
-            // update_transfer_correction_masks(d, {c}, bulkMaskLowBefore)
-            const bool allBulk = (M.flg[dn] & kZBulkS) && (M.flg[l] & kZBulkS);
-            if (lane == 0) {
-                for (int c2 : {dn, l}) {
-                    if (allBulk) M.flg[c2] |= kZBB;
-                    else M.flg[c2] = (uint8_t)((M.flg[c2] | kZSkip) & ~kZBB);
-                }
-            }
-            __syncwarp();
+            // update_transfer_correction_masks(d, {c}, bulkMaskLowBefore), recvMask[c]
+            const int one[1] = {l};
+            masks(dn, one, 1, kZBulkS);
             movedSparse += nt;
             need -= nt;
         }
     }
 };
 
-// Output of one zone cell: its members (the originals still there, then the arrivals), with
-// the momentum correction of src/zone_pass.cpp:870-909 restoring the cell's momentum exactly
-// (an integer share per member, the remainder one unit each to the members of smallest id).
-__device__ void fast_zone_output_cell(FastZone& Z, int l) {
+// Output of the zone (src/zone_pass.cpp:870-909): every cell's members (the originals still
+// there, then the arrivals) into its output bin, with the momentum correction restoring each
+// corrected cell's pass-input momentum exactly (an integer share per member, the remainder to
+// the member of smallest id). Lanes own cells (lane + 32 r) and walk their particles with
+// independent loads; the arrivals are added by record, lane-parallel.
+__device__ void fast_zone_output(FastZone& Z) {
     const FastZoneArgs& A = *Z.A;
     FastZoneMem& M = Z.M;
-    const int lane = Z.lane, K = A.F.K;
-    const int c = Z.gcell(l);
-    const int n0 = M.n0[l];
-    const size_t ib = (size_t)c * K;
-    const uint32_t* rm = M.rm + 4 * l;
-    const bool changed = (rm[0] | rm[1] | rm[2] | rm[3]) != 0 || M.nrecv[l] > 0;
-    long long fx = 0, fy = 0;  // final momentum of the cell
-    if (!changed) {
-        for (int j = lane; j < n0; j += 32) {
-            const float2 o = A.in.off[ib + j];
-            const float2 v = A.in.vel[ib + j];
-            const int p = A.in.pid[ib + j];
-            A.out.off[ib + j] = o;
-            A.out.vel[ib + j] = v;
-            A.out.pid[ib + j] = p;
-            fx += fq_of(v.x);
-            fy += fq_of(v.y);
-        }
-        if (lane == 0) A.out.cnt[c] = n0;
-    } else {
-        // members: originals not removed (compacted), then records in this cell
-        long long bx = 0, by = 0, ax = 0, ay = 0;
-        int nOrig = 0;
-        for (int j0 = 0; j0 < n0; j0 += 32) {
-            const int j = j0 + lane;
-            const bool in0 = j < n0;
-            const bool keep = in0 && !(rm[j >> 5] & (1u << (j & 31)));
-            const unsigned kb = __ballot_sync(0xffffffffu, keep);
-            if (in0) {
-                const float2 v = A.in.vel[ib + j];
-                bx += fq_of(v.x);
-                by += fq_of(v.y);
-                if (keep) {
-                    ax += fq_of(v.x);
-                    ay += fq_of(v.y);
-                    M.pidBuf[nOrig + __popc(kb & lanemask_lt())] = A.in.pid[ib + j];
-                }
-            }
-            nOrig += __popc(kb);
-        }
-        int nAll = nOrig;
-        for (int r0 = 0; r0 < Z.nrec; r0 += 32) {
-            const int r = r0 + lane;
-            const bool here = r < Z.nrec && M.recCur[r] == l;
-            const unsigned hb = __ballot_sync(0xffffffffu, here);
-            if (here) {
-                const int src = M.recSrc[r];
-                const float2 v = A.in.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
-                ax += fq_of(v.x);
-                ay += fq_of(v.y);
-                const int slot = nAll + __popc(hb & lanemask_lt());
-                if (slot < kFastMaxK) M.pidBuf[slot] = M.recPid[r];
-            }
-            nAll += __popc(hb);
-        }
-        bx = warp_sum_ll(bx);
-        by = warp_sum_ll(by);
-        ax = warp_sum_ll(ax);
-        ay = warp_sum_ll(ay);
-        __syncwarp();
-        if (nAll > K) {
-            if (lane == 0) raise_error(A.st, kErrBinCapacity, c);
-            nAll = K;
-        }
-        const uint8_t f = M.flg[l];
-        bool doCorr = A.P.momCorr != 0;
-        if (doCorr && (f & kZSkip)) doCorr = false;
-        if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
-        long long shx = 0, shy = 0, remx = 0, remy = 0;
-        if (doCorr && nAll > 0) {
-            const long long dx = bx - ax, dy = by - ay;
-            shx = floor_div_ll(dx, nAll);
-            shy = floor_div_ll(dy, nAll);
-            remx = dx - shx * nAll;
-            remy = dy - shy * nAll;
-        }
-        // rank of a member by id among the cell's members (the remainder goes to the lowest)
-        auto id_rank = [&](int p) {
-            int r = 0;
-            for (int i = 0; i < nAll; ++i) r += M.pidBuf[i] < p;
-            return r;
-        };
-        int k = 0;
-        for (int j0 = 0; j0 < n0; j0 += 32) {
-            const int j = j0 + lane;
-            const bool keep = j < n0 && !(rm[j >> 5] & (1u << (j & 31)));
-            const unsigned kb = __ballot_sync(0xffffffffu, keep);
-            if (keep) {
-                const int slot = k + __popc(kb & lanemask_lt());
-                if (slot < K) {
-                    const int p = A.in.pid[ib + j];
-                    const float2 v = A.in.vel[ib + j];
-                    long long qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
-                    if (remx || remy) {
-                        const int rk = id_rank(p);
-                        if (rk < remx) ++qx;
-                        if (rk < remy) ++qy;
-                    }
-                    A.out.off[ib + slot] = A.in.off[ib + j];
-                    A.out.vel[ib + slot] = make_float2(fv_of(qx), fv_of(qy));
-                    A.out.pid[ib + slot] = p;
-                    fx += qx;
-                    fy += qy;
-                }
-            }
-            k += __popc(kb);
-        }
-        for (int r0 = 0; r0 < Z.nrec; r0 += 32) {
-            const int r = r0 + lane;
-            const bool here = r < Z.nrec && M.recCur[r] == l;
-            const unsigned hb = __ballot_sync(0xffffffffu, here);
-            if (here) {
-                const int slot = k + __popc(hb & lanemask_lt());
-                if (slot < K) {
-                    const int src = M.recSrc[r];
-                    const size_t s = (size_t)Z.gcell(src >> 7) * K + (src & 127);
-                    const int p = M.recPid[r];
-                    const float2 v = A.in.vel[s];
-                    long long qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
-                    if (remx || remy) {
-                        const int rk = id_rank(p);
-                        if (rk < remx) ++qx;
-                        if (rk < remy) ++qy;
-                    }
-                    A.out.off[ib + slot] = M.recOff[r];
-                    A.out.vel[ib + slot] = make_float2(fv_of(qx), fv_of(qy));
-                    A.out.pid[ib + slot] = p;
-                    fx += qx;
-                    fy += qy;
-                }
-            }
-            k += __popc(hb);
-        }
-        if (lane == 0) A.out.cnt[c] = nAll;
+    const int lane = Z.lane, K = A.F.K, nl = Z.nl;
+    // the arrivals' momentum and smallest id per receiving cell (few, low contention)
+    for (int l = lane; l < nl; l += 32) {
+        M.sums[4 * l] = M.sums[4 * l + 1] = 0;
+        M.minPid[l] = 0x7fffffff;
     }
-    if (A.red) {
-        fx = warp_sum_ll(fx);
-        fy = warp_sum_ll(fy);
-        if (lane == 0) A.red[c] = make_longlong2(fx, fy);
+    __syncwarp();
+    for (int r = lane; r < Z.nrec; r += 32) {
+        const int src = M.recSrc[r];
+        const int l = M.recCur[r];
+        const float2 v = A.in.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
+        // an arrival's momentum fits in 32 bits with room for a cell's worth (|q| < 2^24)
+        atomicAdd(M.sums + 4 * l, fq_of(v.x));
+        atomicAdd(M.sums + 4 * l + 1, fq_of(v.y));
+        atomicMin(M.minPid + l, M.recPid[r]);
+    }
+    __syncwarp();
+    // per cell: input sums, kept sums, the correction; then the kept originals, compacted
+    for (int l = lane; l < nl; l += 32) {
+        const int c = Z.gcell(l);
+        const size_t ib = (size_t)c * K;
+        const int n0 = M.n0[l];
+        const uint32_t* rm = M.rm + 4 * l;
+        const bool changed = (rm[0] | rm[1] | rm[2] | rm[3]) != 0 || M.nrecv[l] > 0;
+        long long bx = 0, by = 0, qq = 0, ax = M.sums[4 * l], ay = M.sums[4 * l + 1];
+        int mp = M.minPid[l];
+        for (int j0 = 0; j0 < n0; j0 += 4) {  // four independent loads in flight
+            float2 v[4];
+            int pp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] = make_float2(0.f, 0.f);
+                pp[u] = 0x7fffffff;
+                if (j0 + u < n0) {
+                    v[u] = A.in.vel[ib + j0 + u];
+                    if (changed) pp[u] = A.in.pid[ib + j0 + u];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u;
+                if (j >= n0) break;
+                const long long qx = fq_of(v[u].x), qy = fq_of(v[u].y);
+                bx += qx;
+                by += qy;
+                qq += qx * qx + qy * qy;
+                if (changed && !(rm[j >> 5] & (1u << (j & 31)))) {
+                    ax += qx;
+                    ay += qy;
+                    mp = min(mp, pp[u]);
+                }
+            }
+        }
+        if (A.ref) A.ref[c] = make_longlong4(bx, by, qq, n0);
+        const int kept = n0 - (__popc(rm[0]) + __popc(rm[1]) + __popc(rm[2]) + __popc(rm[3]));
+        const int nAll = kept + M.nrecv[l];
+        long long shx = 0, shy = 0, remx = 0, remy = 0;
+        if (changed) {
+            const uint8_t f = M.flg[l];
+            bool doCorr = A.P.momCorr != 0;
+            if (doCorr && (f & kZSkip)) doCorr = false;
+            if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
+            if (doCorr && nAll > 0) {
+                const long long dx = bx - ax, dy = by - ay;
+                shx = floor_div_ll(dx, nAll);
+                shy = floor_div_ll(dy, nAll);
+                remx = dx - shx * nAll;
+                remy = dy - shy * nAll;
+            }
+        } else {
+            ax = bx;
+            ay = by;
+        }
+        if (A.red) A.red[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
+        if (nAll > K) raise_error(A.st, kErrBinCapacity, c);
+        A.out.cnt[c] = min(nAll, K);
+        // the share, remainder and next free slot, for the arrivals below
+        // shares are below the cell's momentum change, remainders below its count
+        M.sums[4 * l] = (int)shx;
+        M.sums[4 * l + 1] = (int)shy;
+        M.sums[4 * l + 2] = (int)((remx & 0xffff) | (remy << 16));
+        M.sums[4 * l + 3] = kept;
+        M.minPid[l] = mp;
+        // kept originals into slots 0 .. kept - 1
+        int slot = 0;
+        for (int j0 = 0; j0 < n0; j0 += 4) {
+            float2 v[4], o[4];
+            int pp[4];
+            bool keep[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u;
+                keep[u] = j < n0 && !(changed && (rm[j >> 5] & (1u << (j & 31))));
+                if (keep[u]) {
+                    v[u] = A.in.vel[ib + j];
+                    o[u] = A.in.off[ib + j];
+                    pp[u] = A.in.pid[ib + j];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (!keep[u]) continue;
+                long long qx = fq_of(v[u].x) + shx, qy = fq_of(v[u].y) + shy;
+                if (pp[u] == mp) {
+                    qx += remx;
+                    qy += remy;
+                }
+                if (slot < K) {
+                    A.out.off[ib + slot] = o[u];
+                    A.out.vel[ib + slot] = make_float2(fv_of(qx), fv_of(qy));
+                    A.out.pid[ib + slot] = pp[u];
+                }
+                ++slot;
+            }
+        }
+    }
+    __syncwarp();
+    // the arrivals after the kept originals, in claim order (order-free)
+    for (int r = lane; r < Z.nrec; r += 32) {
+        const int l = M.recCur[r];
+        const int src = M.recSrc[r];
+        int* sm = M.sums + 4 * l;
+        const int slot = atomicAdd(sm + 3, 1);
+        const int c = Z.gcell(l);
+        const int p = M.recPid[r];
+        const float2 v = A.in.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
+        long long qx = fq_of(v.x) + sm[0], qy = fq_of(v.y) + sm[1];
+        if (p == M.minPid[l]) {
+            qx += sm[2] & 0xffff;
+            qy += (sm[2] >> 16) & 0xffff;
+        }
+        if (slot < K) {
+            const size_t d = (size_t)c * K + slot;
+            A.out.off[d] = M.recOff[r];
+            A.out.vel[d] = make_float2(fv_of(qx), fv_of(qy));
+            A.out.pid[d] = p;
+        }
     }
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * kFastZoneWarps) k_fast_zone(FastZoneArgs A) {
+__global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int wib = threadIdx.x >> 5;
     const int z = blockIdx.x * kFastZoneWarps + wib;
@@ -1088,6 +1077,12 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps) k_fast_zone(FastZoneArgs 
         if (P.pery) gy = wrap_index(gy, P.Ny);
         const bool ok = gx >= 0 && gx < P.Nx && gy >= 0 && gy < P.Ny;
         M.win[w] = ok ? (short)min(A.in.cnt[gy + P.Ny * gx], A.F.K) : (short)-1;
+    }
+    for (int l = lane; l < Z.nl; l += 32) {
+        const int lx = l / Z.TY, ly = l - lx * Z.TY;
+        M.cx[l] = (uint8_t)lx;
+        M.cy[l] = (uint8_t)ly;
+        M.wi[l] = (uint16_t)((lx + 2) * Z.WY + (ly + 2));
     }
     __syncwarp();
     for (int l = lane; l < Z.nl; l += 32) {
@@ -1147,7 +1142,7 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps) k_fast_zone(FastZoneArgs 
     }
     __syncwarp();
     // output with the momentum correction
-    for (int l = 0; l < Z.nl; ++l) fast_zone_output_cell(Z, l);
+    fast_zone_output(Z);
     if (lane == 0) {
         if (Z.movedDense || Z.movedSparse) {
             atomicAdd(A.moved, Z.movedDense);
@@ -1158,8 +1153,8 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps) k_fast_zone(FastZoneArgs 
 }
 
 // ------------------------------------------------------------------ closure
-// Per cell, from the exact sums: the reference fields of the step-start state (N, Ux, Uy, T,
-// rho, Pkin, Pvir: src/common_grid.cpp:32-100) and pdriveRaw = Pkin + Pvir
+// Per cell, from the exact sums: the reference fields of stateRef, the collided state the base
+// pass read (N, Ux, Uy, T, rho, Pkin, Pvir: src/common_grid.cpp:32-100), and pdriveRaw = Pkin + Pvir
 // (src/liquid_closure.cpp:401-405); the red momenta, duRepair = (P_ref - P_red) / gamma and the
 // beta_opt terms (:343-360) into cols (num term, den term).
 __global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ ref, const longlong2* __restrict__ red,
@@ -1196,23 +1191,39 @@ __global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ 
     duRY[c] = ay;
     cols[2 * (size_t)c] = -(ex * ax + ey * ay);
     cols[2 * (size_t)c + 1] = ax * ax + ay * ay;
-    if (feat) feat[c] = make_float4((float)((double)n / P.gamma - 1.0), (float)uxr, (float)uyr, (float)n);
+    // the learned closure's stencil input: occupancy, kinetic pressure relative to the target
+    // rho* kBT, and the mean velocity along x (the network predicts the EOS kick, which the
+    // pressure drive Pkin + Pvir of these fields determines)
+    if (feat) {  // .w: the red count, the weight of the cell's kick in the momentum sum
+        const double pkRel = pk / (P.rhoTarget * P.kBT) - 1.0;
+        feat[c] = make_float4((float)((double)n / P.gamma - 1.0), (float)pkRel, (float)uxr, (float)m);
+    }
 }
 
 // EOS kick from the blended pressure drive (src/liquid_closure.cpp:243-295, :424-430) plus
 // beta_applied * duRepair, rounded per cell to the grid (the pending kick of the next step).
-// learned (nullable): per cell (duX, duY) of the learned closure replacing the EOS kick.
+// learned (nullable): per cell (duX, duY) of the learned closure replacing the EOS kick where
+// it is a number and the step's mode (nullable) is learned; elsewhere the plain EOS kick. The
+// learned kicks are taken less their particle-weighted mean (learnedSum: sum of N du at 2^-32
+// and the particles kicked), so they carry no net momentum: the plain EOS kick is the gradient
+// of a field and moves the mean flow by a negligible amount, while a network's residual bias,
+// though small against the kick, is of the size of the body force per step.
+// eosX, eosY (nullable): the plain EOS kick per cell (training samples).
 __global__ void k_fast_kick_cells(DevParams P, const double* __restrict__ pd, const double* __restrict__ duRX,
                                   const double* __restrict__ duRY, const double* __restrict__ numDen,
                                   const double* __restrict__ learnedX, const double* __restrict__ learnedY,
-                                  int2* __restrict__ kick) {
+                                  const long long* __restrict__ learnedSum, const int* __restrict__ mode,
+                                  int2* __restrict__ kick, double* __restrict__ eosX, double* __restrict__ eosY) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const double beta = beta_applied(P, numDen[0], numDen[1]);
     double ex, ey;
-    if (learnedX) {
-        ex = learnedX[c];
-        ey = learnedY[c];
+    if (learnedX && (!mode || *mode) && !isnan(learnedX[c])) {
+        const double nk = learnedSum ? (double)learnedSum[2] : 0.0;
+        const double mx = nk > 0.0 ? (double)learnedSum[0] * 0x1p-32 / nk : 0.0;
+        const double my = nk > 0.0 ? (double)learnedSum[1] * 0x1p-32 / nk : 0.0;
+        ex = learnedX[c] - mx;
+        ey = learnedY[c] - my;
     } else {
         const int ix = c / P.Ny, iy = c - ix * P.Ny;
         double gx, gy;
@@ -1227,9 +1238,22 @@ __global__ void k_fast_kick_cells(DevParams P, const double* __restrict__ pd, co
         const double k = -P.dt / P.rhoTarget * P.betaEOS;
         ex = k * gx;
         ey = k * gy;
+        if (eosX) {
+            eosX[c] = ex;
+            eosY[c] = ey;
+        }
     }
     const double dx = beta * duRX[c] + ex, dy = beta * duRY[c] + ey;
     kick[c] = make_int2((int)llrint(dx * kFastQ), (int)llrint(dy * kFastQ));
+}
+
+// per cell of the bins: count and count^2 (the learned closure's occupancy-variance check)
+__global__ void k_fast_count_cols(const int* __restrict__ cnt, int Nc, double* __restrict__ cols) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nc) return;
+    const double n = (double)cnt[c];
+    cols[2 * (size_t)c] = n;
+    cols[2 * (size_t)c + 1] = n * n;
 }
 
 // Applies the pending kick to the bins in place (before the state is read out).

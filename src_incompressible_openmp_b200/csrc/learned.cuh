@@ -99,6 +99,21 @@ __device__ __forceinline__ void cell_features(const DevParams& P, const float4* 
         for (int k = 0; k < 25; ++k) f[25 * ch + k] = stencil_value(S, feat, k, ch);
 }
 
+// training samples of the fast form's learned closure: the stencil features of every
+// stride-th cell from offset (the collided state's occupancy, kinetic pressure and mean vx),
+// and the plain closure's EOS kick there (the part the network replaces)
+__global__ void k_fast_learned_samples(DevParams P, const float4* __restrict__ feat, const double* __restrict__ eosX,
+                                       const double* __restrict__ eosY, int stride, int offset, int count,
+                                       float* __restrict__ X, float* __restrict__ Y) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const int c = offset + s * stride;
+    if (c >= P.Nc) return;
+    cell_features(P, feat, c, X + (size_t)s * kFeat);
+    Y[2 * (size_t)s] = (float)eosX[c];
+    Y[2 * (size_t)s + 1] = (float)eosY[c];
+}
+
 __device__ __forceinline__ void stage_weights(const float* __restrict__ params, __nv_bfloat16* sw) {
     for (int i = threadIdx.x; i < kTrained; i += blockDim.x) sw[i] = __float2bfloat16_rn(params[i]);
 }
@@ -476,7 +491,8 @@ __global__ void __launch_bounds__(kTcThreads, 4)
             bool inside = true;
 #pragma unroll
             for (int d = 0; d < 5; ++d) inside = inside && S.col[d] >= 0 && S.row[d] >= 0;
-            if (!inside) o0 = o1 = 0.0f;
+            // bulkOnly 2: a NaN marks the cell, whose kick the caller computes itself
+            if (!inside) o0 = o1 = (bulkOnly == 2) ? __int_as_float(0x7fc00000) : 0.0f;
         }
         if (live) {
             if (kRows) {
@@ -487,21 +503,32 @@ __global__ void __launch_bounds__(kTcThreads, 4)
                 duY[r] = (double)(o1 * scale);
             }
         }
-        if (!kRows) {  // sum of N du over the cells, int64 at 2^-32 (exact and order-free)
-            long long qx = 0, qy = 0;
-            if (live) {
+        if (!kRows) {  // sum of N du over the cells, int64 at 2^-32 (exact and order-free), and
+                       // the particles of the cells that take a learned kick
+            long long qx = 0, qy = 0, qn = 0;
+            if (live && !isnan(o0)) {
+                // |N du| <= 2^8 per cell keeps the sum over up to 2^22 cells below 2^62 at 2^-32
+                // (exact, no wrap); a larger kick is a diverged network: flagged, not summed
                 const double nc = (double)__ldg(reinterpret_cast<const float*>(feat + r) + 3);
-                qx = __double2ll_rn(nc * (double)(o0 * scale) * 0x1p32);
-                qy = __double2ll_rn(nc * (double)(o1 * scale) * 0x1p32);
+                const double px = nc * (double)(o0 * scale), py = nc * (double)(o1 * scale);
+                if (fabs(px) <= 256.0 && fabs(py) <= 256.0) {
+                    qx = __double2ll_rn(px * 0x1p32);
+                    qy = __double2ll_rn(py * 0x1p32);
+                    qn = (long long)nc;
+                } else {
+                    raise_error(st, kErrLearnedRange, r);
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 qx += __shfl_xor_sync(0xffffffffu, qx, o);
                 qy += __shfl_xor_sync(0xffffffffu, qy, o);
+                qn += __shfl_xor_sync(0xffffffffu, qn, o);
             }
-            if ((t & 31) == 0 && (qx != 0 || qy != 0)) {
+            if ((t & 31) == 0 && (qx != 0 || qy != 0 || qn != 0)) {
                 atomicAdd(duSum, (unsigned long long)qx);
                 atomicAdd(duSum + 1, (unsigned long long)qy);
+                atomicAdd(duSum + 2, (unsigned long long)qn);
             }
         }
     }

@@ -20,13 +20,15 @@ from . import native
 from .cases import ensemble_family, uniform_state
 
 
-def collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=None, log=None, device=0):
+def collect(runs=200, seed=7, warmup=60, steps=20, stride=4, capacity=None, log=None, device=0, form="f64"):
     """Samples from `runs` channels of the ensemble family: each runs `warmup` plain steps, then
-    `steps` steps whose closure is sampled at every stride-th cell. Returns (X, Y) float32."""
+    `steps` steps whose closure is sampled at every stride-th cell. Returns (X, Y) float32.
+    form "fast": the fast form's closure, whose network sees the collided state's occupancy,
+    kinetic pressure and mean vx and predicts the EOS kick."""
     Xs, Ys, total = [], [], 0
     for r, (p, s) in enumerate(ensemble_family(runs, seed)):
         x, v = uniform_state(p, s)
-        with native.Context(p, device) as ctx:
+        with native.Context(p, device, form=form) as ctx:
             ctx.set_state(x, v)
             ctx.step(0, warmup)
             X, Y = ctx.learned_samples(warmup, steps, stride)
@@ -50,9 +52,12 @@ def _mirror_index():
     return 5 * dy + (4 - dx), 5 * (4 - dy) + dx
 
 
-def mirrored(X, Y):
+def mirrored(X, Y, form="f64"):
     """The samples with their mirror images in x, in y and in both: the closure commutes with
-    the channel's reflections (a reflected cell neighbourhood gets the reflected kick)."""
+    the channel's reflections (a reflected cell neighbourhood gets the reflected kick). Feature
+    channels 1 and 2 are Ux and Uy (plain and precision forms) or the kinetic pressure and Ux
+    (fast form): a reflection negates the velocity channels along its axis."""
+    flipx_ch, flipy_ch = ((1,), (2,)) if form != "fast" else ((2,), ())
     mx, my = _mirror_index()
     outX, outY = [X], [Y]
     for flip_x, flip_y in ((True, False), (False, True), (True, True)):
@@ -64,21 +69,23 @@ def mirrored(X, Y):
         Z = np.concatenate([X[:, perm], X[:, 25 + perm], X[:, 50 + perm]], axis=1)
         W = Y.copy()
         if flip_x:
-            Z[:, 25:50] *= -1
+            for ch in flipx_ch:
+                Z[:, 25 * ch:25 * ch + 25] *= -1
             W[:, 0] *= -1
         if flip_y:
-            Z[:, 50:75] *= -1
+            for ch in flipy_ch:
+                Z[:, 25 * ch:25 * ch + 25] *= -1
             W[:, 1] *= -1
         outX.append(Z)
         outY.append(W)
     return np.concatenate(outX), np.concatenate(outY)
 
 
-def train(X, Y, epochs=6, batch=512, lr=1e-3, seed=3, init_seed=1, mirror=True, device=0):
+def train(X, Y, epochs=6, batch=512, lr=1e-3, seed=3, init_seed=1, mirror=True, device=0, form="f64"):
     """Adam on the device from Glorot weights, on the samples and (mirror) their reflections;
     returns (params, mean loss per epoch)."""
     if mirror:
-        X, Y = mirrored(X, Y)
+        X, Y = mirrored(X, Y, form)
     return native.learned_train(X, Y, native.learned_init(init_seed), epochs, batch, lr, seed, device)
 
 
