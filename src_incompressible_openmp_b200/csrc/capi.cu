@@ -169,9 +169,10 @@ struct mpcd_ctx {
     // moved counts, and the two zone layouts with the zone kernel's working-set sizes
     bool fast = false;
     FastParams F{};
-    FastBins fb[2] = {};
+    FastBins fb{};      // the standard-cell bins (the zone passes update them in place)
+    int* fcnt2 = nullptr;  // the second count array (the zone passes' counts ping-pong)
+    longlong2* fmid = nullptr;  // per cell the base pass's output momentum
     FastBins sb{};  // the SRD bins of the collision (with each particle's standard cell)
-    int fcur = 0;
     FastStep* fstep = nullptr;
     FastWall* fwall = nullptr;
     longlong4* fref = nullptr;

@@ -442,8 +442,11 @@ struct FastZoneArgs {
     int nZones;
     int pass;                  // 0 base, 1 shifted (salts the draws)
     const FastStep* S;
-    FastBins in, out;
-    longlong2* red;            // nullable: per cell the output's momentum sum (closure input)
+    FastBins b;                // the bins, updated in place (cnt unused: cntIn / cntOut)
+    const int* cntIn;          // pass-input counts (the snapshot every zone reads)
+    int* cntOut;               // pass-output counts
+    const longlong2* sumsIn;   // nullable: per cell the input's momentum (cells left unchanged pass it on)
+    longlong2* sumsOut;        // per cell the output's momentum (the next pass's input; red state: closure)
     longlong4* ref;            // nullable: per cell the input's (sum qx, sum qy, sum |q|^2, N): the
                                // closure's reference fields (stateRef is the collided state,
                                // src/main_benchmark_poiseuille_openmp_profiled_shifted_profiled.cpp:241-251)
@@ -475,6 +478,10 @@ struct FastZoneMem {
     int* sums;         // cell x 4: the arrivals' momentum (2); then the correction's share (2),
                        // remainders (x low, y high half) and the next free output slot
     int* recPid;       // recCap
+    int* recV;         // recCap x 2: the moved particle's velocity (grid units)
+    uint16_t* recList; // recCap: records grouped by current cell
+    uint16_t* recStart;// cell + 1: start of each cell's records in recList
+    int* rfill;        // cell: records filed so far
     uint16_t* recSrc;  // recCap: (origin cell << 7) | slot
     uint8_t* recCur;   // recCap: current cell
     float2* recOff;    // recCap: position in the current cell
@@ -493,6 +500,10 @@ struct FastZoneMem {
         add((size_t)maxCells * 4, 4);
         add((size_t)maxCells * 16, 4);
         add((size_t)recCap * 4, 4);
+        add((size_t)recCap * 8, 4);
+        add((size_t)recCap * 2, 2);
+        add((size_t)(maxCells + 1) * 2, 2);
+        add((size_t)maxCells * 4, 4);
         add((size_t)recCap * 2, 2);
         add((size_t)recCap, 1);
         add((size_t)recCap * 8, 8);
@@ -521,6 +532,10 @@ struct FastZoneMem {
         minPid = (int*)take((size_t)maxCells * 4, 4);
         sums = (int*)take((size_t)maxCells * 16, 4);
         recPid = (int*)take((size_t)recCap * 4, 4);
+        recV = (int*)take((size_t)recCap * 8, 4);
+        recList = (uint16_t*)take((size_t)recCap * 2, 2);
+        recStart = (uint16_t*)take((size_t)(maxCells + 1) * 2, 2);
+        rfill = (int*)take((size_t)maxCells * 4, 4);
         recSrc = (uint16_t*)take((size_t)recCap * 2, 2);
         recCur = (uint8_t*)take((size_t)recCap, 1);
         recOff = (float2*)take((size_t)recCap * 8, 8);
@@ -601,7 +616,7 @@ struct FastZone {
     // slots below 128 and records below 512. Each lane keeps the keys of its originals
     // (slots lane + 32 k) in registers for the whole call.
     __device__ void move_members(int l, int t, int nt, bool dense) {
-        const FastBins& B = A->in;
+        const FastBins& B = A->b;
         const int c = gcell(l);
         const int n0 = M.n0[l];
         const uint32_t salt = ++op;
@@ -894,38 +909,63 @@ struct FastZone {
     }
 };
 
-// Output of the zone (src/zone_pass.cpp:870-909): every cell's members (the originals still
-// there, then the arrivals) into its output bin, with the momentum correction restoring each
-// corrected cell's pass-input momentum exactly (an integer share per member, the remainder to
-// the member of smallest id). Lanes own cells (lane + 32 r) and walk their particles with
-// independent loads; the arrivals are added by record, lane-parallel.
+// Output of the zone (src/zone_pass.cpp:870-909), in place: only the cells whose members
+// changed are rewritten. A changed cell's final members are its kept particles and its
+// arrivals; arrivals and the kept particles above the new count fill the holes the departed
+// left (then the slots above the old count). The momentum correction restores each corrected
+// cell's pass-input momentum exactly: an integer share per member, the remainder to the member
+// of smallest id. All reads a write could clobber (the departed particles' data) happen
+// before any write. Lanes own cells (lane + 32 r).
 __device__ void fast_zone_output(FastZone& Z) {
     const FastZoneArgs& A = *Z.A;
     FastZoneMem& M = Z.M;
     const int lane = Z.lane, K = A.F.K, nl = Z.nl;
-    // the arrivals' momentum and smallest id per receiving cell (few, low contention)
+    const FastBins& B = A.b;
     for (int l = lane; l < nl; l += 32) {
         M.sums[4 * l] = M.sums[4 * l + 1] = 0;
         M.minPid[l] = 0x7fffffff;
+        M.rfill[l] = 0;
+    }
+    // records grouped by cell (exclusive prefix of the arrivals per cell)
+    int base = 0;
+    for (int l0 = 0; l0 < nl; l0 += 32) {
+        const int l = l0 + lane;
+        const int v = l < nl ? M.nrecv[l] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (l < nl) M.recStart[l] = (uint16_t)(base + incl - v);
+        base += __shfl_sync(0xffffffffu, incl, 31);
     }
     __syncwarp();
+    // the arrivals' data, read before anything is written; their momentum and smallest id per cell
     for (int r = lane; r < Z.nrec; r += 32) {
         const int src = M.recSrc[r];
         const int l = M.recCur[r];
-        const float2 v = A.in.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
-        // an arrival's momentum fits in 32 bits with room for a cell's worth (|q| < 2^24)
-        atomicAdd(M.sums + 4 * l, fq_of(v.x));
-        atomicAdd(M.sums + 4 * l + 1, fq_of(v.y));
+        const float2 v = B.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
+        const int qx = fq_of(v.x), qy = fq_of(v.y);
+        M.recV[2 * r] = qx;
+        M.recV[2 * r + 1] = qy;
+        atomicAdd(M.sums + 4 * l, qx);  // a cell's arrivals' momentum fits in 32 bits (|q| < 2^24)
+        atomicAdd(M.sums + 4 * l + 1, qy);
         atomicMin(M.minPid + l, M.recPid[r]);
+        M.recList[M.recStart[l] + atomicAdd(M.rfill + l, 1)] = (uint16_t)r;
     }
     __syncwarp();
-    // per cell: input sums, kept sums, the correction; then the kept originals, compacted
+    // per cell: input sums, the correction, counts and output sums
     for (int l = lane; l < nl; l += 32) {
         const int c = Z.gcell(l);
         const size_t ib = (size_t)c * K;
         const int n0 = M.n0[l];
         const uint32_t* rm = M.rm + 4 * l;
         const bool changed = (rm[0] | rm[1] | rm[2] | rm[3]) != 0 || M.nrecv[l] > 0;
+        if (!changed && A.sumsIn) {  // nothing to read: the input passes through
+            A.cntOut[c] = n0;
+            A.sumsOut[c] = A.sumsIn[c];
+            continue;
+        }
         long long bx = 0, by = 0, qq = 0, ax = M.sums[4 * l], ay = M.sums[4 * l + 1];
         int mp = M.minPid[l];
         for (int j0 = 0; j0 < n0; j0 += 4) {  // four independent loads in flight
@@ -936,8 +976,8 @@ __device__ void fast_zone_output(FastZone& Z) {
                 v[u] = make_float2(0.f, 0.f);
                 pp[u] = 0x7fffffff;
                 if (j0 + u < n0) {
-                    v[u] = A.in.vel[ib + j0 + u];
-                    if (changed) pp[u] = A.in.pid[ib + j0 + u];
+                    v[u] = B.vel[ib + j0 + u];
+                    if (changed) pp[u] = B.pid[ib + j0 + u];
                 }
             }
 #pragma unroll
@@ -956,88 +996,118 @@ __device__ void fast_zone_output(FastZone& Z) {
             }
         }
         if (A.ref) A.ref[c] = make_longlong4(bx, by, qq, n0);
+        if (!changed) {
+            A.cntOut[c] = n0;
+            A.sumsOut[c] = make_longlong2(bx, by);
+            continue;
+        }
         const int kept = n0 - (__popc(rm[0]) + __popc(rm[1]) + __popc(rm[2]) + __popc(rm[3]));
         const int nAll = kept + M.nrecv[l];
         long long shx = 0, shy = 0, remx = 0, remy = 0;
-        if (changed) {
-            const uint8_t f = M.flg[l];
-            bool doCorr = A.P.momCorr != 0;
-            if (doCorr && (f & kZSkip)) doCorr = false;
-            if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
-            if (doCorr && nAll > 0) {
-                const long long dx = bx - ax, dy = by - ay;
-                shx = floor_div_ll(dx, nAll);
-                shy = floor_div_ll(dy, nAll);
-                remx = dx - shx * nAll;
-                remy = dy - shy * nAll;
-            }
-        } else {
-            ax = bx;
-            ay = by;
+        const uint8_t f = M.flg[l];
+        bool doCorr = A.P.momCorr != 0;
+        if (doCorr && (f & kZSkip)) doCorr = false;
+        if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
+        if (doCorr && nAll > 0) {
+            const long long dx = bx - ax, dy = by - ay;
+            shx = floor_div_ll(dx, nAll);
+            shy = floor_div_ll(dy, nAll);
+            remx = dx - shx * nAll;
+            remy = dy - shy * nAll;
         }
-        if (A.red) A.red[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
+        A.sumsOut[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
         if (nAll > K) raise_error(A.st, kErrBinCapacity, c);
-        A.out.cnt[c] = min(nAll, K);
-        // the share, remainder and next free slot, for the arrivals below
-        // shares are below the cell's momentum change, remainders below its count
+        A.cntOut[c] = min(nAll, K);
+        // shares below the cell's momentum change, remainders below its count
         M.sums[4 * l] = (int)shx;
         M.sums[4 * l + 1] = (int)shy;
         M.sums[4 * l + 2] = (int)((remx & 0xffff) | (remy << 16));
-        M.sums[4 * l + 3] = kept;
+        M.sums[4 * l + 3] = nAll;
         M.minPid[l] = mp;
-        // kept originals into slots 0 .. kept - 1
-        int slot = 0;
-        for (int j0 = 0; j0 < n0; j0 += 4) {
-            float2 v[4], o[4];
-            int pp[4];
-            bool keep[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                keep[u] = j < n0 && !(changed && (rm[j >> 5] & (1u << (j & 31))));
-                if (keep[u]) {
-                    v[u] = A.in.vel[ib + j];
-                    o[u] = A.in.off[ib + j];
-                    pp[u] = A.in.pid[ib + j];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (!keep[u]) continue;
-                long long qx = fq_of(v[u].x) + shx, qy = fq_of(v[u].y) + shy;
-                if (pp[u] == mp) {
-                    qx += remx;
-                    qy += remy;
-                }
-                if (slot < K) {
-                    A.out.off[ib + slot] = o[u];
-                    A.out.vel[ib + slot] = make_float2(fv_of(qx), fv_of(qy));
-                    A.out.pid[ib + slot] = pp[u];
-                }
-                ++slot;
-            }
-        }
     }
     __syncwarp();
-    // the arrivals after the kept originals, in claim order (order-free)
-    for (int r = lane; r < Z.nrec; r += 32) {
-        const int l = M.recCur[r];
-        const int src = M.recSrc[r];
-        int* sm = M.sums + 4 * l;
-        const int slot = atomicAdd(sm + 3, 1);
+    // placement and corrections, in place, cell by cell (each lane writes only its cells' bins)
+    for (int l = lane; l < nl; l += 32) {
+        const int n0 = M.n0[l];
+        const uint32_t* rm = M.rm + 4 * l;
+        const int nr = M.nrecv[l];
+        if (!((rm[0] | rm[1] | rm[2] | rm[3]) != 0 || nr > 0)) continue;
         const int c = Z.gcell(l);
-        const int p = M.recPid[r];
-        const float2 v = A.in.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
-        long long qx = fq_of(v.x) + sm[0], qy = fq_of(v.y) + sm[1];
-        if (p == M.minPid[l]) {
-            qx += sm[2] & 0xffff;
-            qy += (sm[2] >> 16) & 0xffff;
+        const size_t ib = (size_t)c * K;
+        const int shx = M.sums[4 * l], shy = M.sums[4 * l + 1];
+        const int remx = M.sums[4 * l + 2] & 0xffff, remy = (M.sums[4 * l + 2] >> 16) & 0xffff;
+        const int nAll = min(M.sums[4 * l + 3], K);
+        const int mp = M.minPid[l];
+        const int below = min(n0, nAll);
+        // kept particles that stay: velocity correction in place
+        if (shx | shy | remx | remy) {
+            for (int j0 = 0; j0 < below; j0 += 4) {
+                float2 v[4];
+                int pp[4];
+                bool kp[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int j = j0 + u;
+                    kp[u] = j < below && !(rm[j >> 5] & (1u << (j & 31)));
+                    if (kp[u]) {
+                        v[u] = B.vel[ib + j];
+                        pp[u] = (remx | remy) ? B.pid[ib + j] : 0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (!kp[u]) continue;
+                    int qx = fq_of(v[u].x) + shx, qy = fq_of(v[u].y) + shy;
+                    if ((remx | remy) && pp[u] == mp) {
+                        qx += remx;
+                        qy += remy;
+                    }
+                    B.vel[ib + j0 + u] = make_float2(fv_of(qx), fv_of(qy));
+                }
+            }
         }
-        if (slot < K) {
-            const size_t d = (size_t)c * K + slot;
-            A.out.off[d] = M.recOff[r];
-            A.out.vel[d] = make_float2(fv_of(qx), fv_of(qy));
-            A.out.pid[d] = p;
+        // free slots: the holes below the new count, then the slots from the old count on
+        int hole = 0, app = n0;
+        auto next_free = [&]() {
+            while (hole < below) {
+                const int j = hole++;
+                if (rm[j >> 5] & (1u << (j & 31))) return j;
+            }
+            return app++;
+        };
+        // kept particles above the new count move down into holes
+        for (int j = nAll; j < n0; ++j) {
+            if (rm[j >> 5] & (1u << (j & 31))) continue;
+            const size_t s = ib + j;
+            const float2 v = B.vel[s];
+            const float2 o = B.off[s];
+            const int p = B.pid[s];
+            int qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
+            if (p == mp) {
+                qx += remx;
+                qy += remy;
+            }
+            const int d = next_free();
+            B.off[ib + d] = o;
+            B.vel[ib + d] = make_float2(fv_of(qx), fv_of(qy));
+            B.pid[ib + d] = p;
+        }
+        // arrivals
+        const int rs = M.recStart[l];
+        for (int k = 0; k < nr; ++k) {
+            const int r = M.recList[rs + k];
+            const int p = M.recPid[r];
+            int qx = M.recV[2 * r] + shx, qy = M.recV[2 * r + 1] + shy;
+            if (p == mp) {
+                qx += remx;
+                qy += remy;
+            }
+            const int d = next_free();
+            if (d < K) {
+                B.off[ib + d] = M.recOff[r];
+                B.vel[ib + d] = make_float2(fv_of(qx), fv_of(qy));
+                B.pid[ib + d] = p;
+            }
         }
     }
     __syncwarp();
@@ -1076,7 +1146,7 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneAr
         if (P.perx) gx = wrap_index(gx, P.Nx);
         if (P.pery) gy = wrap_index(gy, P.Ny);
         const bool ok = gx >= 0 && gx < P.Nx && gy >= 0 && gy < P.Ny;
-        M.win[w] = ok ? (short)min(A.in.cnt[gy + P.Ny * gx], A.F.K) : (short)-1;
+        M.win[w] = ok ? (short)min(A.cntIn[gy + P.Ny * gx], A.F.K) : (short)-1;
     }
     for (int l = lane; l < Z.nl; l += 32) {
         const int lx = l / Z.TY, ly = l - lx * Z.TY;
