@@ -123,6 +123,24 @@ __device__ __forceinline__ int warp_sum_i(int v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Full-warp int64 sum with redux.sync: the two's-complement words summed in four 16-bit limbs
+// (a limb's sum over 32 lanes stays below 2^21), exact modulo 2^64.
+__device__ __forceinline__ long long warp_sum_i64(long long v) {
+    const unsigned long long u = (unsigned long long)v;
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        s += (unsigned long long)__reduce_add_sync(0xffffffffu, (unsigned)(u >> (16 * k)) & 0xFFFFu) << (16 * k);
+    return (long long)s;
+}
+// Full-warp u64 minimum with redux.sync: the high words' minimum, then the low words' among the
+// lanes that hold it.
+__device__ __forceinline__ unsigned long long warp_min_u64_r(unsigned long long v) {
+    const unsigned hi = (unsigned)(v >> 32);
+    const unsigned mh = __reduce_min_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_min_sync(0xffffffffu, hi == mh ? (unsigned)v : 0xFFFFFFFFu);
+    return ((unsigned long long)mh << 32) | ml;
+}
 
 // ------------------------------------------------------------------ step begin
 __global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W) {
@@ -474,11 +492,8 @@ struct FastZoneMem {
     uint8_t* flg;      // cell: flags
     uint8_t* nrecv;    // cell: records currently in the cell
     uint32_t* rm;      // cell x 4: originals removed
-    int* minPid;       // cell: the smallest id among the output members (takes the remainder)
-    int* sums;         // cell x 4: the arrivals' momentum (2); then the correction's share (2),
-                       // remainders (x low, y high half) and the next free output slot
     int* recPid;       // recCap
-    int* recV;         // recCap x 2: the moved particle's velocity (grid units)
+    int2* recV;        // recCap: the moved particle's velocity (grid units), gathered by the output
     uint16_t* recList; // recCap: records grouped by current cell
     uint16_t* recStart;// cell + 1: start of each cell's records in recList
     int* rfill;        // cell: records filed so far
@@ -486,92 +501,70 @@ struct FastZoneMem {
     uint8_t* recCur;   // recCap: current cell
     float2* recOff;    // recCap: position in the current cell
     float* nsm;        // nsmCap: smoothed occupancy of the zone and a one-cell ring
-    uint32_t* keys;    // 128: order keys (dense / low cells), sort scratch
+    uint32_t* keys;    // 128: order keys of the dense / low cells; the output's hole slots
+    uint8_t* ord;      // 128: those cells in key order
     int* tgt;          // 32: ordered targets or donors
     int* tgt2;         // 32: receivers of a dense cell's first phase
 
+    template <class F>
+    __host__ __device__ static void layout(int maxCells, int winCap, int nsmCap, int recCap, F&& take) {
+        take((size_t)winCap * 2, 2);
+        take((size_t)maxCells * 2, 2);
+        for (int k = 0; k < 5; ++k) take((size_t)maxCells, 1);
+        take((size_t)maxCells * 16, 4);
+        take((size_t)recCap * 4, 4);
+        take((size_t)recCap * 8, 8);
+        take((size_t)recCap * 2, 2);
+        take((size_t)(maxCells + 1) * 2, 2);
+        take((size_t)maxCells * 4, 4);
+        take((size_t)recCap * 2, 2);
+        take((size_t)recCap, 1);
+        take((size_t)recCap * 8, 8);
+        take((size_t)nsmCap * 4, 4);
+        take(128 * 4, 4);
+        take(128, 1);
+        take(32 * 4, 4);
+        take(32 * 4, 4);
+    }
     __host__ __device__ static size_t bytes(int maxCells, int winCap, int nsmCap, int recCap) {
         size_t b = 0;
-        auto add = [&](size_t n, size_t a) { b = (b + a - 1) / a * a + n; };
-        add((size_t)winCap * 2, 2);
-        add((size_t)maxCells * 2, 2);
-        for (int k = 0; k < 5; ++k) add((size_t)maxCells, 1);
-        add((size_t)maxCells * 16, 4);
-        add((size_t)maxCells * 4, 4);
-        add((size_t)maxCells * 16, 4);
-        add((size_t)recCap * 4, 4);
-        add((size_t)recCap * 8, 4);
-        add((size_t)recCap * 2, 2);
-        add((size_t)(maxCells + 1) * 2, 2);
-        add((size_t)maxCells * 4, 4);
-        add((size_t)recCap * 2, 2);
-        add((size_t)recCap, 1);
-        add((size_t)recCap * 8, 8);
-        add((size_t)nsmCap * 4, 4);
-        add(128 * 4, 4);
-        add(32 * 4, 4);
-        add(32 * 4, 4);
+        layout(maxCells, winCap, nsmCap, recCap, [&](size_t n, size_t a) { b = (b + a - 1) / a * a + n; });
         return (b + 15) / 16 * 16;
     }
     __device__ void carve(char* base, int maxCells, int winCap, int nsmCap, int recCap) {
         size_t b = 0;
-        auto take = [&](size_t n, size_t a) {
+        char* p[21];
+        int i = 0;
+        layout(maxCells, winCap, nsmCap, recCap, [&](size_t n, size_t a) {
             b = (b + a - 1) / a * a;
-            char* p = base + b;
+            p[i++] = base + b;
             b += n;
-            return p;
-        };
-        win = (short*)take((size_t)winCap * 2, 2);
-        wi = (uint16_t*)take((size_t)maxCells * 2, 2);
-        cx = (uint8_t*)take((size_t)maxCells, 1);
-        cy = (uint8_t*)take((size_t)maxCells, 1);
-        n0 = (uint8_t*)take((size_t)maxCells, 1);
-        flg = (uint8_t*)take((size_t)maxCells, 1);
-        nrecv = (uint8_t*)take((size_t)maxCells, 1);
-        rm = (uint32_t*)take((size_t)maxCells * 16, 4);
-        minPid = (int*)take((size_t)maxCells * 4, 4);
-        sums = (int*)take((size_t)maxCells * 16, 4);
-        recPid = (int*)take((size_t)recCap * 4, 4);
-        recV = (int*)take((size_t)recCap * 8, 4);
-        recList = (uint16_t*)take((size_t)recCap * 2, 2);
-        recStart = (uint16_t*)take((size_t)(maxCells + 1) * 2, 2);
-        rfill = (int*)take((size_t)maxCells * 4, 4);
-        recSrc = (uint16_t*)take((size_t)recCap * 2, 2);
-        recCur = (uint8_t*)take((size_t)recCap, 1);
-        recOff = (float2*)take((size_t)recCap * 8, 8);
-        nsm = (float*)take((size_t)nsmCap * 4, 4);
-        keys = (uint32_t*)take(128 * 4, 4);
-        tgt = (int*)take(32 * 4, 4);
-        tgt2 = (int*)take(32 * 4, 4);
+        });
+        win = (short*)p[0];
+        wi = (uint16_t*)p[1];
+        cx = (uint8_t*)p[2];
+        cy = (uint8_t*)p[3];
+        n0 = (uint8_t*)p[4];
+        flg = (uint8_t*)p[5];
+        nrecv = (uint8_t*)p[6];
+        rm = (uint32_t*)p[7];
+        recPid = (int*)p[8];
+        recV = (int2*)p[9];
+        recList = (uint16_t*)p[10];
+        recStart = (uint16_t*)p[11];
+        rfill = (int*)p[12];
+        recSrc = (uint16_t*)p[13];
+        recCur = (uint8_t*)p[14];
+        recOff = (float2*)p[15];
+        nsm = (float*)p[16];
+        keys = (uint32_t*)p[17];
+        ord = (uint8_t*)p[18];
+        tgt = (int*)p[19];
+        tgt2 = (int*)p[20];
     }
 };
 
 constexpr uint8_t kZBulkD = 1, kZBulkS = 2, kZRecv = 4, kZBB = 8, kZSkip = 16;
-
-// ascending sort of 128 u32 keys in shared memory by one warp (bitonic network)
-__device__ __forceinline__ void warp_sort128(uint32_t* a, int lane) {
-    for (int k = 2; k <= 128; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            __syncwarp();
-#pragma unroll
-            for (int i0 = 0; i0 < 128; i0 += 32) {
-                const int i = i0 + lane;
-                const int p = i ^ j;
-                if (p > i) {
-                    const uint32_t x = a[i], y = a[p];
-                    const bool up = (i & k) == 0;
-                    if ((x > y) == up) {
-                        a[i] = y;
-                        a[p] = x;
-                    }
-                }
-            }
-        }
-    }
-    __syncwarp();
-}
-
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) { return warp_min_u64_c(v); }
 
 struct FastZone {
     const FastZoneArgs* A;
@@ -608,28 +601,31 @@ struct FastZone {
         return ((fmix64(zseed ^ ((uint64_t)salt << 32) ^ (uint64_t)pid) >> 41) << 31) | (uint64_t)(pid & 0x7fffffffu);
     }
 
-    // Removes nt members of cell l and files them into cell t at fresh uniform positions.
-    // dense: the members in the reference's list order (the cell's particles in ascending id,
-    // then the arrivals in order: src/zone_pass.cpp:541-583 takes the first ids); otherwise
-    // members chosen uniformly at random (the sparse phase shuffles the donor's list). A
-    // candidate is (key << 10) | (record flag << 9) | index: keys of at most 54 bits, original
-    // slots below 128 and records below 512. Each lane keeps the keys of its originals
-    // (slots lane + 32 k) in registers for the whole call.
-    __device__ void move_members(int l, int t, int nt, bool dense) {
+    // The candidates of source cell l, one key per original not yet removed: slot j in lane
+    // j % 32, register j / 32. A candidate is (key << 10) | (record flag << 9) | index: keys of at
+    // most 54 bits whose low 31 bits are the particle id, original slots below 128 and records
+    // below 512.
+    __device__ __forceinline__ void load_candidates(int l, bool dense, uint32_t salt, unsigned long long (&cand)[4]) const {
         const FastBins& B = A->b;
-        const int c = gcell(l);
+        const size_t ib = (size_t)gcell(l) * A->F.K;
         const int n0 = M.n0[l];
-        const uint32_t salt = ++op;
-        unsigned long long cand[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int j = lane + 32 * r;
             cand[r] = ~0ULL;
-            if (j < n0 && !(M.rm[4 * l + r] & (1u << lane))) {
-                const uint32_t pid = (uint32_t)B.pid[(size_t)c * A->F.K + j];
-                cand[r] = (member_key(dense, salt, pid, -1) << 10) | (unsigned long long)j;
-            }
+            if (j < n0 && !(M.rm[4 * l + r] & (1u << lane)))
+                cand[r] = (member_key(dense, salt, (uint32_t)B.pid[ib + j], -1) << 10) | (unsigned long long)j;
         }
+    }
+
+    // Removes nt members of cell l and files them into cell t at fresh uniform positions.
+    // dense: the members in the reference's list order (the cell's particles in ascending id,
+    // then the arrivals in order: src/zone_pass.cpp:541-583 takes the first ids), from the
+    // candidates the caller loaded once for the cell; otherwise members chosen uniformly at
+    // random (the sparse phase shuffles the donor's list) from candidates keyed afresh.
+    __device__ __forceinline__ void move_members(int l, int t, int nt, bool dense, unsigned long long (&cand)[4]) {
+        const uint32_t salt = ++op;
+        if (!dense) load_candidates(l, false, salt, cand);
         for (int k = 0; k < nt; ++k) {
             if (failed) return;
             unsigned long long best = cand[0];
@@ -643,7 +639,7 @@ struct FastZone {
                     best = v < best ? v : best;
                 }
             }
-            best = warp_min_u64(best);
+            best = warp_min_u64_r(best);
             if (best == ~0ULL) return;  // no member left (cannot happen while counts agree)
             // the new position: two 24-bit uniforms of one draw
             const uint64_t hp = fmix64(zseed ^ ((uint64_t)salt << 20) ^ (0x504F53ULL + (uint64_t)k));
@@ -655,10 +651,12 @@ struct FastZone {
                     failed = true;
                     return;
                 }
-                if ((j & 31) == lane) cand[j >> 5] = ~0ULL;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r == (j >> 5) && (j & 31) == lane) cand[r] = ~0ULL;
                 if (lane == 0) {
                     M.rm[4 * l + (j >> 5)] |= 1u << (j & 31);
-                    M.recPid[nrec] = B.pid[(size_t)c * A->F.K + j];
+                    M.recPid[nrec] = (int)((best >> 10) & 0x7fffffffULL);
                     M.recSrc[nrec] = (uint16_t)((l << 7) | j);
                     M.recCur[nrec] = (uint8_t)t;
                     M.recOff[nrec] = pos;
@@ -679,8 +677,7 @@ struct FastZone {
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589) over the
     // targets ranked as rank_dense_targets_unified does (:436-490); map: 0 low, 1 high.
     // Returns the particles moved; the receivers go to rcv[*nr ...].
-    __device__ int spread(int l, int needOut, int mapKind, int* rcv, int* nr) {
-        const DevParams& P = A->P;
+    __device__ int spread(int l, int needOut, int mapKind, int* rcv, int* nr, unsigned long long (&cand)[4]) {
         // lane k < 24: the k-th neighbour of the bin-grouped offset table
         const int k = lane;
         int t = -1, ddx = 0, ddy = 0;
@@ -743,7 +740,7 @@ struct FastZone {
                 const int quota = max(1, (needOut + max(1, rem) - 1) / max(1, rem));
                 const int nt = max(1, min(min(quota, d), min(needOut, avail)));
                 const int tt = __shfl_sync(0xffffffffu, tO, kk);
-                move_members(l, tt, nt, true);
+                move_members(l, tt, nt, true, cand);
                 if (failed) break;
                 if (lane == 0) {
                     add_cnt(l, -nt);
@@ -767,12 +764,12 @@ struct FastZone {
         return moved;
     }
 
-    // the transfer masks (src/zone_pass.cpp:492-525) for a source and its receivers rcv[0..nr),
-    // bulk flag bit bf
-    __device__ void masks(int src, const int* rcv, int nr, uint8_t bf) {
+    // the transfer masks (src/zone_pass.cpp:492-525) for a source and its nr receivers (lane
+    // k < nr holds the k-th in myRcv), bulk flag bit bf
+    __device__ void masks(int src, int myRcv, int nr, uint8_t bf) {
         bool allBulk = (M.flg[src] & bf) != 0;
         const bool mine = lane < nr;
-        const int rc = mine ? rcv[lane] : src;
+        const int rc = mine ? myRcv : src;
         allBulk = allBulk && __all_sync(0xffffffffu, !mine || (M.flg[rc] & bf));
         __syncwarp();
         if (lane <= nr) {
@@ -795,11 +792,14 @@ struct FastZone {
         const int needOut = max(0, (int)ceil((double)nc - hi));
         int nr = 0;
         int moved = 0;
-        if (needOut > 0) moved += spread(l, needOut, 0, M.tgt2, &nr);
+        unsigned long long cand[4];
+        load_candidates(l, true, 0, cand);
+        if (needOut > 0) moved += spread(l, needOut, 0, M.tgt2, &nr, cand);
         const int remainingOut = max(0, (int)ceil((double)cnt(l) - hi));
-        if (remainingOut > 0 && !failed) moved += spread(l, remainingOut, 1, M.tgt2, &nr);
+        if (remainingOut > 0 && !failed) moved += spread(l, remainingOut, 1, M.tgt2, &nr, cand);
         // the receivers of the two phases may repeat a cell; flags are idempotent
-        masks(l, M.tgt2, min(nr, 31), kZBulkD);
+        const int nrc = min(nr, 31);
+        masks(l, lane < nrc ? M.tgt2[lane] : l, nrc, kZBulkD);
         movedDense += moved;
     }
 
@@ -893,7 +893,8 @@ struct FastZone {
             if (avail <= 0) continue;
             const int nt = min(need, min(avail, cnt(dn)));
             if (nt <= 0) continue;
-            move_members(dn, l, nt, false);
+            unsigned long long cand[4];
+            move_members(dn, l, nt, false, cand);
             if (failed) break;
             if (lane == 0) {
                 add_cnt(dn, -nt);
@@ -901,31 +902,64 @@ struct FastZone {
             }
             __syncwarp();
             // update_transfer_correction_masks(d, {c}, bulkMaskLowBefore), recvMask[c]
-            const int one[1] = {l};
-            masks(dn, one, 1, kZBulkS);
+            masks(dn, l, 1, kZBulkS);
             movedSparse += nt;
             need -= nt;
         }
     }
+
+    // The cells with a key (keyOf(l) != ~0) in ascending key order into M.ord: compacted by
+    // ballot, each placed by counting the smaller keys (keys are distinct: the cell index is
+    // their low byte). Returns how many.
+    template <class KeyOf>
+    __device__ int order_cells(KeyOf&& keyOf) {
+        int D = 0;
+        for (int l0 = 0; l0 < nl; l0 += 32) {
+            const int l = l0 + lane;
+            const uint32_t key = l < nl ? keyOf(l) : 0xFFFFFFFFu;
+            const bool on = key != 0xFFFFFFFFu;
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (on) M.keys[D + __popc(m & lanemask_lt())] = key;
+            D += __popc(m);
+        }
+        __syncwarp();
+        for (int i = lane; i < D; i += 32) {
+            const uint32_t k = M.keys[i];
+            int rank = 0;
+            for (int j = 0; j < D; ++j) rank += M.keys[j] < k;
+            M.ord[rank] = (uint8_t)(k & 0xFFu);
+        }
+        __syncwarp();
+        return D;
+    }
 };
+
+// floor(a / b) for b > 0, in 32 bits when a fits
+__device__ __forceinline__ long long floor_div_small(long long a, int b) {
+    if (a >= -2147483647LL - 1 && a <= 2147483647LL) {
+        const int ai = (int)a;
+        int q = ai / b;
+        if ((ai % b != 0) && (ai < 0)) --q;
+        return q;
+    }
+    return floor_div_ll(a, b);
+}
 
 // Output of the zone (src/zone_pass.cpp:870-909), in place: only the cells whose members
 // changed are rewritten. A changed cell's final members are its kept particles and its
-// arrivals; arrivals and the kept particles above the new count fill the holes the departed
-// left (then the slots above the old count). The momentum correction restores each corrected
-// cell's pass-input momentum exactly: an integer share per member, the remainder to the member
-// of smallest id. All reads a write could clobber (the departed particles' data) happen
-// before any write. Lanes own cells (lane + 32 r).
+// arrivals; the kept particles above the new count and then the arrivals fill the holes the
+// departed left (in slot order), then the slots from the old count on. The momentum correction
+// restores each corrected cell's pass-input momentum exactly: an integer share per member, the
+// remainder to the member of smallest id. The arrivals' velocities are gathered before anything
+// is written; then each lane takes its cells (lane + 32 r) and reads a cell four slots at a
+// time (32-byte loads: bins start on 128-byte boundaries, K being a multiple of 16), before it
+// writes that cell.
 __device__ void fast_zone_output(FastZone& Z) {
     const FastZoneArgs& A = *Z.A;
     FastZoneMem& M = Z.M;
     const int lane = Z.lane, K = A.F.K, nl = Z.nl;
     const FastBins& B = A.b;
-    for (int l = lane; l < nl; l += 32) {
-        M.sums[4 * l] = M.sums[4 * l + 1] = 0;
-        M.minPid[l] = 0x7fffffff;
-        M.rfill[l] = 0;
-    }
+    for (int l = lane; l < nl; l += 32) M.rfill[l] = 0;
     // records grouped by cell (exclusive prefix of the arrivals per cell)
     int base = 0;
     for (int l0 = 0; l0 < nl; l0 += 32) {
@@ -940,58 +974,52 @@ __device__ void fast_zone_output(FastZone& Z) {
         base += __shfl_sync(0xffffffffu, incl, 31);
     }
     __syncwarp();
-    // the arrivals' data, read before anything is written; their momentum and smallest id per cell
     for (int r = lane; r < Z.nrec; r += 32) {
         const int src = M.recSrc[r];
         const int l = M.recCur[r];
         const float2 v = B.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
-        const int qx = fq_of(v.x), qy = fq_of(v.y);
-        M.recV[2 * r] = qx;
-        M.recV[2 * r + 1] = qy;
-        atomicAdd(M.sums + 4 * l, qx);  // a cell's arrivals' momentum fits in 32 bits (|q| < 2^24)
-        atomicAdd(M.sums + 4 * l + 1, qy);
-        atomicMin(M.minPid + l, M.recPid[r]);
+        M.recV[r] = make_int2(fq_of(v.x), fq_of(v.y));
         M.recList[M.recStart[l] + atomicAdd(M.rfill + l, 1)] = (uint16_t)r;
     }
     __syncwarp();
-    // per cell: input sums, the correction, counts and output sums
     for (int l = lane; l < nl; l += 32) {
         const int c = Z.gcell(l);
-        const size_t ib = (size_t)c * K;
-        const int n0 = M.n0[l];
-        const uint32_t* rm = M.rm + 4 * l;
-        const bool changed = (rm[0] | rm[1] | rm[2] | rm[3]) != 0 || M.nrecv[l] > 0;
+        const int n0 = M.n0[l], nr = M.nrecv[l];
+        const uint32_t rm0 = M.rm[4 * l], rm1 = M.rm[4 * l + 1], rm2 = M.rm[4 * l + 2], rm3 = M.rm[4 * l + 3];
+        const bool changed = (rm0 | rm1 | rm2 | rm3) != 0 || nr > 0;
         if (!changed && A.sumsIn) {  // nothing to read: the input passes through
             A.cntOut[c] = n0;
             A.sumsOut[c] = A.sumsIn[c];
             continue;
         }
-        long long bx = 0, by = 0, qq = 0, ax = M.sums[4 * l], ay = M.sums[4 * l + 1];
-        int mp = M.minPid[l];
-        for (int j0 = 0; j0 < n0; j0 += 4) {  // four independent loads in flight
-            float2 v[4];
-            int pp[4];
+        // the removal bits of slots j0 .. j0 + 3 (j0 a multiple of 4)
+        auto rbits = [&](int j0) -> uint32_t {
+            const uint32_t w = j0 < 32 ? rm0 : (j0 < 64 ? rm1 : (j0 < 96 ? rm2 : rm3));
+            return (w >> (j0 & 31)) & 0xFu;
+        };
+        const size_t ib = (size_t)c * K;
+        const float4* v4 = reinterpret_cast<const float4*>(B.vel + ib);
+        const int4* p4 = reinterpret_cast<const int4*>(B.pid + ib);
+        long long bx = 0, by = 0, qq = 0, ax = 0, ay = 0;
+        int mp = 0x7fffffff;
+#pragma unroll 2
+        for (int j0 = 0; j0 < n0; j0 += 4) {
+            const float4 va = v4[j0 >> 1], vb = v4[(j0 >> 1) + 1];
+            const int4 pp = changed ? p4[j0 >> 2] : make_int4(0, 0, 0, 0);
+            const float vx[4] = {va.x, va.z, vb.x, vb.z}, vy[4] = {va.y, va.w, vb.y, vb.w};
+            const int pv[4] = {pp.x, pp.y, pp.z, pp.w};
+            const uint32_t rb = rbits(j0);
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                v[u] = make_float2(0.f, 0.f);
-                pp[u] = 0x7fffffff;
-                if (j0 + u < n0) {
-                    v[u] = B.vel[ib + j0 + u];
-                    if (changed) pp[u] = B.pid[ib + j0 + u];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                if (j >= n0) break;
-                const long long qx = fq_of(v[u].x), qy = fq_of(v[u].y);
+                if (j0 + u >= n0) break;
+                const long long qx = fq_of(vx[u]), qy = fq_of(vy[u]);
                 bx += qx;
                 by += qy;
                 qq += qx * qx + qy * qy;
-                if (changed && !(rm[j >> 5] & (1u << (j & 31)))) {
+                if (changed && !((rb >> u) & 1u)) {
                     ax += qx;
                     ay += qy;
-                    mp = min(mp, pp[u]);
+                    mp = min(mp, pv[u]);
                 }
             }
         }
@@ -1001,8 +1029,16 @@ __device__ void fast_zone_output(FastZone& Z) {
             A.sumsOut[c] = make_longlong2(bx, by);
             continue;
         }
-        const int kept = n0 - (__popc(rm[0]) + __popc(rm[1]) + __popc(rm[2]) + __popc(rm[3]));
-        const int nAll = kept + M.nrecv[l];
+        const int rs = M.recStart[l];
+        for (int k = 0; k < nr; ++k) {
+            const int r = M.recList[rs + k];
+            const int2 q = M.recV[r];
+            ax += q.x;
+            ay += q.y;
+            mp = min(mp, M.recPid[r]);
+        }
+        const int kept = n0 - (__popc(rm0) + __popc(rm1) + __popc(rm2) + __popc(rm3));
+        const int nAll = kept + nr;
         long long shx = 0, shy = 0, remx = 0, remy = 0;
         const uint8_t f = M.flg[l];
         bool doCorr = A.P.momCorr != 0;
@@ -1010,79 +1046,67 @@ __device__ void fast_zone_output(FastZone& Z) {
         if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
         if (doCorr && nAll > 0) {
             const long long dx = bx - ax, dy = by - ay;
-            shx = floor_div_ll(dx, nAll);
-            shy = floor_div_ll(dy, nAll);
+            shx = floor_div_small(dx, nAll);
+            shy = floor_div_small(dy, nAll);
             remx = dx - shx * nAll;
             remy = dy - shy * nAll;
         }
         A.sumsOut[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
         if (nAll > K) raise_error(A.st, kErrBinCapacity, c);
         A.cntOut[c] = min(nAll, K);
-        // shares below the cell's momentum change, remainders below its count
-        M.sums[4 * l] = (int)shx;
-        M.sums[4 * l + 1] = (int)shy;
-        M.sums[4 * l + 2] = (int)((remx & 0xffff) | (remy << 16));
-        M.sums[4 * l + 3] = nAll;
-        M.minPid[l] = mp;
-    }
-    __syncwarp();
-    // placement and corrections, in place, cell by cell (each lane writes only its cells' bins)
-    for (int l = lane; l < nl; l += 32) {
-        const int n0 = M.n0[l];
-        const uint32_t* rm = M.rm + 4 * l;
-        const int nr = M.nrecv[l];
-        if (!((rm[0] | rm[1] | rm[2] | rm[3]) != 0 || nr > 0)) continue;
-        const int c = Z.gcell(l);
-        const size_t ib = (size_t)c * K;
-        const int shx = M.sums[4 * l], shy = M.sums[4 * l + 1];
-        const int remx = M.sums[4 * l + 2] & 0xffff, remy = (M.sums[4 * l + 2] >> 16) & 0xffff;
-        const int nAll = min(M.sums[4 * l + 3], K);
-        const int mp = M.minPid[l];
         const int below = min(n0, nAll);
-        // kept particles that stay: velocity correction in place
+        // kept particles that stay: velocity corrected in place (whole 32-byte groups are
+        // rewritten; the other slots in them keep their values or are filled below)
         if (shx | shy | remx | remy) {
+            float4* w4 = reinterpret_cast<float4*>(B.vel + ib);
+            const bool rem = (remx | remy) != 0;
             for (int j0 = 0; j0 < below; j0 += 4) {
-                float2 v[4];
-                int pp[4];
-                bool kp[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int j = j0 + u;
-                    kp[u] = j < below && !(rm[j >> 5] & (1u << (j & 31)));
-                    if (kp[u]) {
-                        v[u] = B.vel[ib + j];
-                        pp[u] = (remx | remy) ? B.pid[ib + j] : 0;
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    if (!kp[u]) continue;
-                    int qx = fq_of(v[u].x) + shx, qy = fq_of(v[u].y) + shy;
-                    if ((remx | remy) && pp[u] == mp) {
+                float4 va = w4[j0 >> 1], vb = w4[(j0 >> 1) + 1];
+                const int4 pp = rem ? p4[j0 >> 2] : make_int4(-1, -1, -1, -1);
+                const uint32_t rb = rbits(j0);
+                auto fix = [&](float& x, float& y, int p, int u) {
+                    if (j0 + u >= below || ((rb >> u) & 1u)) return;
+                    long long qx = fq_of(x) + shx, qy = fq_of(y) + shy;
+                    if (p == mp) {
                         qx += remx;
                         qy += remy;
                     }
-                    B.vel[ib + j0 + u] = make_float2(fv_of(qx), fv_of(qy));
-                }
+                    x = fv_of(qx);
+                    y = fv_of(qy);
+                };
+                fix(va.x, va.y, pp.x, 0);
+                fix(va.z, va.w, pp.y, 1);
+                fix(vb.x, vb.y, pp.z, 2);
+                fix(vb.z, vb.w, pp.w, 3);
+                w4[j0 >> 1] = va;
+                w4[(j0 >> 1) + 1] = vb;
             }
         }
-        // free slots: the holes below the new count, then the slots from the old count on
-        int hole = 0, app = n0;
-        auto next_free = [&]() {
-            while (hole < below) {
-                const int j = hole++;
-                if (rm[j >> 5] & (1u << (j & 31))) return j;
+        // holes below the new count, in slot order, then the slots from the old count on
+        int hw = 0;
+        uint32_t hbits = rm0;
+        int app = n0;
+        auto next_free = [&]() -> int {
+            for (;;) {
+                if (hbits) {
+                    const int j = 32 * hw + __ffs(hbits) - 1;
+                    hbits &= hbits - 1;
+                    if (j < below) return j;
+                    hbits = 0;
+                    hw = 4;
+                }
+                if (++hw >= 4) return app++;
+                hbits = hw == 1 ? rm1 : (hw == 2 ? rm2 : rm3);
             }
-            return app++;
         };
-        // kept particles above the new count move down into holes
+        // kept particles above the new count
         for (int j = nAll; j < n0; ++j) {
-            if (rm[j >> 5] & (1u << (j & 31))) continue;
+            if ((rbits(j & ~3) >> (j & 3)) & 1u) continue;
             const size_t s = ib + j;
             const float2 v = B.vel[s];
             const float2 o = B.off[s];
             const int p = B.pid[s];
-            int qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
+            long long qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
             if (p == mp) {
                 qx += remx;
                 qy += remy;
@@ -1093,11 +1117,11 @@ __device__ void fast_zone_output(FastZone& Z) {
             B.pid[ib + d] = p;
         }
         // arrivals
-        const int rs = M.recStart[l];
         for (int k = 0; k < nr; ++k) {
             const int r = M.recList[rs + k];
             const int p = M.recPid[r];
-            int qx = M.recV[2 * r] + shx, qy = M.recV[2 * r + 1] + shy;
+            const int2 q = M.recV[r];
+            long long qx = q.x + shx, qy = q.y + shy;
             if (p == mp) {
                 qx += remx;
                 qy += remy;
@@ -1169,21 +1193,13 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneAr
             M.flg[l] = (uint8_t)((M.flg[l] & ~kZBulkD) | (bulk ? kZBulkD : 0));
         }
         __syncwarp();
-        for (int i = lane; i < 128; i += 32) {
-            uint32_t key = 0xFFFFFFFFu;
-            if (i < Z.nl) {
-                const bool bulk = M.flg[i] & kZBulkD;
-                if ((double)Z.cnt(i) > Z.high_map(bulk))
-                    key = ((uint32_t)fhash(Z.zseed, 0x44454EULL + (uint64_t)pass, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
-            }
-            M.keys[i] = key;
-        }
-        warp_sort128(M.keys, lane);
-        for (int q = 0; q < 128 && !Z.failed; ++q) {
-            const uint32_t key = M.keys[q];
-            if (key == 0xFFFFFFFFu) break;
-            Z.dense_cell((int)(key & 0xFFu));
-        }
+        const int D = Z.order_cells([&](int i) -> uint32_t {
+            const bool bulk = M.flg[i] & kZBulkD;
+            if ((double)Z.cnt(i) > Z.high_map(bulk))
+                return ((uint32_t)fhash(Z.zseed, 0x44454EULL + (uint64_t)pass, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
+            return 0xFFFFFFFFu;
+        });
+        for (int q = 0; q < D && !Z.failed; ++q) Z.dense_cell(M.ord[q]);
         __syncwarp();
     }
     // sparse phase (src/zone_pass.cpp:783-854)
@@ -1194,21 +1210,13 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneAr
         }
         __syncwarp();
         Z.compute_nsm();
-        for (int i = lane; i < 128; i += 32) {
-            uint32_t key = 0xFFFFFFFFu;
-            if (i < Z.nl) {
-                const int cn = Z.cnt(i);
-                if (cn > 0 && (double)cn < Z.low_map(true))
-                    key = ((uint32_t)fhash(Z.zseed, 0x4C4F57ULL, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
-            }
-            M.keys[i] = key;
-        }
-        warp_sort128(M.keys, lane);
-        for (int q = 0; q < 128 && !Z.failed; ++q) {
-            const uint32_t key = M.keys[q];
-            if (key == 0xFFFFFFFFu) break;
-            Z.sparse_cell((int)(key & 0xFFu));
-        }
+        const int L = Z.order_cells([&](int i) -> uint32_t {
+            const int cn = Z.cnt(i);
+            if (cn > 0 && (double)cn < Z.low_map(true))
+                return ((uint32_t)fhash(Z.zseed, 0x4C4F57ULL, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
+            return 0xFFFFFFFFu;
+        });
+        for (int q = 0; q < L && !Z.failed; ++q) Z.sparse_cell(M.ord[q]);
     }
     __syncwarp();
     // output with the momentum correction
