@@ -9,12 +9,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
 #include <mutex>
 #include <random>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mpcd_c.h"
@@ -172,7 +174,11 @@ struct mpcd_ctx {
     FastBins fb{};      // the standard-cell bins (the zone passes update them in place)
     int* fcnt2 = nullptr;  // the second count array (the zone passes' counts ping-pong)
     longlong2* fmid = nullptr;  // per cell the base pass's output momentum
-    FastBins sb{};  // the SRD bins of the collision (with each particle's standard cell)
+    FastBins sb{};  // the stream's destination bins (swapped with fb after the stream)
+    int* fspill = nullptr;   // collision tiles left to the spill kernel, and their count
+    int* fnSpill = nullptr;
+    int fcTY = 16, fcTilesY = 0, fcTiles = 0, fcPcap = 0;  // collision tiles: rows, tile rows, tiles, capacity
+    size_t fcSmem = 0;
     FastStep* fstep = nullptr;
     FastWall* fwall = nullptr;
     longlong4* fref = nullptr;
@@ -184,6 +190,12 @@ struct mpcd_ctx {
     int fnz[2] = {0, 0};
     int fzMaxCells = 0, fzWinCap = 0, fzNsmCap = 0, fzRecCap = 0;
     size_t fzSmem = 0;
+    // zone decisions handed to the apply kernel: per cell summary and removal masks, per zone records
+    unsigned long long* fzMeta = nullptr;
+    uint4* fzRm = nullptr;
+    int* fzRecPid = nullptr;
+    float2* fzRecOff = nullptr;
+    int2* fzRecQ = nullptr;
     // velocity profile accumulation (mpcd_profile_*): per row, momentum (int64 at 2^-32) and count
     bool profOn = false;
     unsigned long long* profP = nullptr;

@@ -49,7 +49,6 @@ struct FastBins {
     float2* vel;
     int* pid;
     int* cnt;
-    int* cell;  // SRD bins only: each particle's standard cell (its offset is relative to it)
 };
 
 // Values of the running step, derived on the device by k_fast_step_begin (graph replay keeps
@@ -65,7 +64,7 @@ struct FastParams {
     int K;
     int zoneWY;                  // unused padding for alignment
     double fqx, fqy;             // body force * dt in grid units (fractional)
-    double dtqx, dtqy;           // cell units moved per grid unit of velocity in one step
+    float dtqx, dtqy;            // cell units moved per grid unit of velocity in one step
     double sigmaQ, UtopQ, UbottomQ;  // wall temperature and wall speeds in grid units
     double lowMapEmpty, highMapEmpty;  // threshold maps of empty cells (src/zone_pass.cpp:321-345)
     unsigned long long seed;     // run seed
@@ -99,7 +98,8 @@ __device__ __forceinline__ double fnormal(uint64_t h1, uint64_t h2) {
 }
 
 __device__ __forceinline__ int fq_of(float v) { return __float2int_rn(v * 1048576.0f); }
-__device__ __forceinline__ float fv_of(long long q) { return (float)((double)q * kFastInvQ); }
+// q / 2^20 rounded once to FP32 (scaling by a power of two commutes with the rounding)
+__device__ __forceinline__ float fv_of(long long q) { return __ll2float_rn(q) * 0x1.0p-20f; }
 
 // floor(a / b) for b > 0
 __device__ __forceinline__ long long floor_div_ll(long long a, long long b) {
@@ -143,8 +143,9 @@ __device__ __forceinline__ unsigned long long warp_min_u64_r(unsigned long long 
 }
 
 // ------------------------------------------------------------------ step begin
-__global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W) {
+__global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W, int* nSpill) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    *nSpill = 0;
     const long long s = S->step + 1;
     S->step = s;
     // the long-run force is exact: the increments of steps 1..s add up to round(s f)
@@ -159,53 +160,133 @@ __global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W) {
 }
 
 // ------------------------------------------------------------------ stream + walls + binning
-// One warp per source cell. Applies the pending closure kick of the previous step (kick[c],
-// grid units, nullable), then body force, streaming and the walls of
-// apply_bc_general (src/boundary_conditions.cpp:37-202: up to four sweeps of left, right,
-// bottom, top, then the final wrap or clamp), and files each particle into the bin of its
-// SRD cell, the cell of the grid shifted by this step's (sx, sy) (srd_cell_id_with_random_shift,
-// src/srd_collision.cpp:9-45: wrapped on periodic axes, clamped on the others), with its
-// standard cell and its offset inside that cell (warp-aggregated slot claims).
+constexpr int kStreamCells = 8;  // cells per warp of the stream kernel
+
+// A coordinate along one axis as (cell, offset in [0, 1)): integer arithmetic for the cell,
+// FP32 for the offset. Moving the integer part of the offset into the cell is exact for
+// offsets of at least 0; below 0 it rounds once (at most half a unit of 2^-24).
+__device__ __forceinline__ void fix_cell(int& c, float& r) {
+    const float f = floorf(r);
+    c += (int)f;
+    r -= f;
+    if (r >= 1.0f) {
+        ++c;
+        r = 0.0f;
+    }
+}
+// x -> -x
+__device__ __forceinline__ void reflect_low(int& c, float& r) {
+    if (r > 0.0f) {
+        c = -c - 1;
+        r = 1.0f - r;
+        fix_cell(c, r);
+    } else {
+        c = -c;
+    }
+}
+// x -> 2 L - x
+__device__ __forceinline__ void reflect_high(int& c, float& r, int L) {
+    if (r > 0.0f) {
+        c = 2 * L - c - 1;
+        r = 1.0f - r;
+        fix_cell(c, r);
+    } else {
+        c = 2 * L - c;
+    }
+}
+
+// One warp per run of kStreamCells consecutive source cells, the lanes over the run's particles
+// in order. Applies the pending closure kick of the previous step (kick[c], grid units,
+// nullable), then body force, streaming and the walls of apply_bc_general
+// (src/boundary_conditions.cpp:37-202: up to four sweeps of left, right, bottom, top, then the
+// final wrap or clamp), and files each particle into the bin of its new cell (warp-aggregated
+// slot claims).
 __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams F, const FastStep* __restrict__ S,
                                                      FastBins in, FastBins out, const int2* __restrict__ kick,
                                                      FastWall* __restrict__ W, DevStatus* st) {
-    const int c = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int c0 = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5) * kStreamCells;
     const int lane = threadIdx.x & 31;
-    if (c >= P.Nc) return;
-    const int n = min(in.cnt[c], F.K);  // a count above K (a failed step) reads no further
-    const int ix = c / P.Ny, iy = c - ix * P.Ny;
+    if (c0 >= P.Nc) return;
+    // lanes below kStreamCells: their cell's count and the exclusive prefix of the counts
+    int n = 0;
+    if (lane < kStreamCells && c0 + lane < P.Nc) n = min(in.cnt[c0 + lane], F.K);
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < kStreamCells; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    const int excl = incl - n;
+    const int total = __shfl_sync(0xffffffffu, incl, kStreamCells - 1);
+    const int ix0 = c0 / P.Ny, iy0 = c0 - ix0 * P.Ny;
     const int fqx = S->fqx, fqy = S->fqy;
-    const double ssx = S->sx, ssy = S->sy;
     const uint64_t seed = S->seed;
-    const int2 kq = kick ? kick[c] : make_int2(0, 0);
+    const int Nx = P.Nx, Ny = P.Ny;
     int hits[4] = {0, 0, 0, 0};
     long long dE2 = 0;
-    const double Nx = (double)P.Nx, Ny = (double)P.Ny;
-    for (int j0 = 0; j0 < n; j0 += 32) {
-        const int j = j0 + lane;
-        const bool live = j < n;
-        int newc = 0, stdc = 0;
+    // the particle i of the run: its cell g (the last whose start is at most i, by a binary
+    // search over the starts held in lanes 0 .. 7) and slot; each round's loads are issued
+    // before the previous round is processed
+    auto locate = [&](int i, int& g, int& slot) {
+        g = 0;
+#pragma unroll
+        for (int st = kStreamCells / 2; st >= 1; st >>= 1) {
+            const int sv = __shfl_sync(0xffffffffu, excl, g + st);
+            if (i >= sv) g += st;
+        }
+        slot = i - __shfl_sync(0xffffffffu, excl, g);
+    };
+    float2 offA = make_float2(0.f, 0.f), velA = offA;
+    int pidA = 0, gA = 0;
+    int2 kickA = make_int2(0, 0);
+    auto fetch = [&](int i) {
+        int g, slot;
+        locate(i, g, slot);
+        gA = g;
+        if (i < total) {
+            const size_t s = (size_t)(c0 + g) * F.K + slot;
+            offA = in.off[s];
+            velA = in.vel[s];
+            pidA = in.pid[s];
+            if (kick) kickA = kick[c0 + g];
+        }
+    };
+    fetch(lane);
+    for (int i0 = 0; i0 < total; i0 += 32) {
+        const int i = i0 + lane;
+        const bool live = i < total;
+        const float2 off = offA, w = velA;
+        const int g = gA;
+        int pid = pidA;
+        const int2 kq = kickA;
+        fetch(i + 32);
+        int newc = 0, qx = 0, qy = 0;
         float2 o = make_float2(0.f, 0.f);
-        int qx = 0, qy = 0, pid = 0;
         if (live) {
-            const size_t s = (size_t)c * F.K + j;
-            const float2 off = in.off[s];
-            const float2 w = in.vel[s];
-            pid = in.pid[s];
+            const int c = c0 + g;
+            int cx = ix0, cy = iy0 + g;
+            while (cy >= Ny) {
+                cy -= Ny;
+                ++cx;
+            }
             qx = fq_of(w.x) + kq.x + fqx;
             qy = fq_of(w.y) + kq.y + fqy;
-            double X = (double)ix + (double)off.x + (double)qx * F.dtqx;
-            double Y = (double)iy + (double)off.y + (double)qy * F.dtqy;
-            const bool inside0 = X >= 0.0 && X <= Nx && Y >= 0.0 && Y <= Ny;
-            for (int sweep = 0; sweep < 4 && !inside0; ++sweep) {
+            float rx = off.x + (float)qx * F.dtqx, ry = off.y + (float)qy * F.dtqy;
+            fix_cell(cx, rx);
+            fix_cell(cy, ry);
+            // x < 0 is cx < 0; x > L is cx > L or (cx == L and r > 0)
+            auto below = [](int cc) { return cc < 0; };
+            auto above = [](int cc, float r, int L) { return cc > L || (cc == L && r > 0.0f); };
+            bool inside = !below(cx) && !above(cx, rx, Nx) && !below(cy) && !above(cy, ry, Ny);
+            for (int sweep = 0; sweep < 4 && !inside; ++sweep) {
                 const long long e0 = (long long)qx * qx + (long long)qy * qy;
                 bool hit = false;
                 const uint64_t hk = fhash(seed, (uint64_t)(uint32_t)pid, (uint64_t)sweep);
-                if (X < 0.0) {
+                if (below(cx)) {
                     if (P.bc[0] == MPCD_BC_PERIODIC) {
-                        X += Nx;
+                        cx += Nx;
                     } else {
-                        X = -X;
+                        reflect_low(cx, rx);
                         if (P.bc[0] == MPCD_BC_THERMALIZE) {
                             qx = (int)llrint(fabs(F.sigmaQ * fnormal(fmix64(hk ^ 1), fmix64(hk ^ 2))));
                             qy = (int)llrint(F.sigmaQ * fnormal(fmix64(hk ^ 3), fmix64(hk ^ 4)));
@@ -221,11 +302,11 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
                         hit = true;
                     }
                 }
-                if (X > Nx) {
+                if (above(cx, rx, Nx)) {
                     if (P.bc[1] == MPCD_BC_PERIODIC) {
-                        X -= Nx;
+                        cx -= Nx;
                     } else {
-                        X = 2.0 * Nx - X;
+                        reflect_high(cx, rx, Nx);
                         if (P.bc[1] == MPCD_BC_THERMALIZE) {
                             qx = -(int)llrint(fabs(F.sigmaQ * fnormal(fmix64(hk ^ 5), fmix64(hk ^ 6))));
                             qy = (int)llrint(F.sigmaQ * fnormal(fmix64(hk ^ 7), fmix64(hk ^ 8)));
@@ -241,11 +322,11 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
                         hit = true;
                     }
                 }
-                if (Y < 0.0) {
+                if (below(cy)) {
                     if (P.bc[2] == MPCD_BC_PERIODIC) {
-                        Y += Ny;
+                        cy += Ny;
                     } else {
-                        Y = -Y;
+                        reflect_low(cy, ry);
                         if (P.bc[2] == MPCD_BC_THERMALIZE) {
                             qx = (int)llrint(F.UbottomQ + F.sigmaQ * fnormal(fmix64(hk ^ 9), fmix64(hk ^ 10)));
                             qy = (int)llrint(fabs(F.sigmaQ * fnormal(fmix64(hk ^ 11), fmix64(hk ^ 12))));
@@ -261,11 +342,11 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
                         hit = true;
                     }
                 }
-                if (Y > Ny) {
+                if (above(cy, ry, Ny)) {
                     if (P.bc[3] == MPCD_BC_PERIODIC) {
-                        Y -= Ny;
+                        cy -= Ny;
                     } else {
-                        Y = 2.0 * Ny - Y;
+                        reflect_high(cy, ry, Ny);
                         if (P.bc[3] == MPCD_BC_THERMALIZE) {
                             qx = (int)llrint(F.UtopQ + F.sigmaQ * fnormal(fmix64(hk ^ 13), fmix64(hk ^ 14)));
                             qy = -(int)llrint(fabs(F.sigmaQ * fnormal(fmix64(hk ^ 15), fmix64(hk ^ 16))));
@@ -282,34 +363,34 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
                     }
                 }
                 if (hit) dE2 += (long long)qx * qx + (long long)qy * qy - e0;
-                if (X >= 0.0 && X <= Nx && Y >= 0.0 && Y <= Ny) break;
+                inside = !below(cx) && !above(cx, rx, Nx) && !below(cy) && !above(cy, ry, Ny);
             }
             // the final wrap x - floor(x / L) L or clamp (src/boundary_conditions.cpp:178-202);
             // after the sweeps a particle is within one period of the box
             if (P.perx) {
-                if (X < 0.0) X += Nx;
-                if (X >= Nx) X -= Nx;
-            } else {
-                X = fmin(fmax(X, 0.0), Nx);
+                if (cx < 0) cx += Nx;
+                if (cx >= Nx) cx -= Nx;
+            } else if (cx < 0) {
+                cx = 0;
+                rx = 0.0f;
+            } else if (cx >= Nx) {
+                cx = Nx - 1;
+                rx = kFastOffMax;
             }
             if (P.pery) {
-                if (Y < 0.0) Y += Ny;
-                if (Y >= Ny) Y -= Ny;
-            } else {
-                Y = fmin(fmax(Y, 0.0), Ny);
+                if (cy < 0) cy += Ny;
+                if (cy >= Ny) cy -= Ny;
+            } else if (cy < 0) {
+                cy = 0;
+                ry = 0.0f;
+            } else if (cy >= Ny) {
+                cy = Ny - 1;
+                ry = kFastOffMax;
             }
-            int jx = (int)floor(X), jy = (int)floor(Y);
-            jx = min(max(jx, 0), P.Nx - 1);
-            jy = min(max(jy, 0), P.Ny - 1);
-            o.x = fminf(fmaxf((float)(X - (double)jx), 0.0f), kFastOffMax);
-            o.y = fminf(fmaxf((float)(Y - (double)jy), 0.0f), kFastOffMax);
-            stdc = jy + P.Ny * jx;
-            int sxc = (int)floor(X + ssx), syc = (int)floor(Y + ssy);
-            if (P.perx) sxc = sxc < 0 ? sxc + P.Nx : (sxc >= P.Nx ? sxc - P.Nx : sxc);
-            else sxc = min(max(sxc, 0), P.Nx - 1);
-            if (P.pery) syc = syc < 0 ? syc + P.Ny : (syc >= P.Ny ? syc - P.Ny : syc);
-            else syc = min(max(syc, 0), P.Ny - 1);
-            newc = syc + P.Ny * sxc;
+            cx = min(max(cx, 0), Nx - 1);
+            cy = min(max(cy, 0), Ny - 1);
+            o = make_float2(fminf(rx, kFastOffMax), fminf(ry, kFastOffMax));
+            newc = cy + Ny * cx;
         }
         // warp-aggregated slot claims in the destination bins
         const unsigned act = __ballot_sync(0xffffffffu, live);
@@ -325,7 +406,6 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
                 out.off[d] = o;
                 out.vel[d] = make_float2(fv_of(qx), fv_of(qy));
                 out.pid[d] = pid;
-                out.cell[d] = stdc;
             } else if (st) {
                 raise_error(st, kErrBinCapacity, newc);
             }
@@ -342,107 +422,409 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
 }
 
 // ------------------------------------------------------------------ SRD collision
-// One warp per SRD cell: its members are the particles the stream kernel filed into its bin.
-// Rotation of the velocities relative to the cell mean by +-alpha, the sign drawn per SRD cell,
-// and the isokinetic thermostat (src/srd_collision.cpp:47-140). Sums are exact in grid units;
-// the rounding of the new velocities to the grid leaves an integer residual that goes to the
-// member with the smallest particle id, so every SRD cell keeps its momentum exactly. Each
-// member is then filed into the bin of its standard cell (warp-aggregated slot claims).
-__global__ void __launch_bounds__(256, 4) k_fast_collide(DevParams P, FastParams F, const FastStep* __restrict__ S,
-                                                         FastBins sb, FastBins out, DevStatus* st) {
-    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= P.Nc) return;
-    const int n = min(sb.cnt[w], F.K);
-    if (n == 0) return;
-    const size_t base = (size_t)w * F.K;
-    // members in registers, up to four per lane
-    int qx[4], qy[4], pid[4], cel[4];
-    float2 off[4];
-    long long Sx = 0, Sy = 0, Sqq = 0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int j = 32 * r + lane;
-        qx[r] = qy[r] = 0;
-        pid[r] = 0x7fffffff;
-        cel[r] = -1;
-        if (j < n) {
-            const float2 v = sb.vel[base + j];
-            qx[r] = fq_of(v.x);
-            qy[r] = fq_of(v.y);
-            pid[r] = sb.pid[base + j];
-            cel[r] = sb.cell[base + j];
-            off[r] = sb.off[base + j];
-            Sx += qx[r];
-            Sy += qy[r];
-            Sqq += (long long)qx[r] * qx[r] + (long long)qy[r] * qy[r];
-        }
-    }
-    Sx = warp_sum_ll(Sx);
-    Sy = warp_sum_ll(Sy);
-    Sqq = warp_sum_ll(Sqq);
-    const int N = n;
-    const double ux = (double)Sx / N, uy = (double)Sy / N;
-    double ct = 1.0, sn = 0.0;
+// The SRD cell along one axis of a particle at standard cell g with offset r: the grid shifted
+// by ss in [-1/2, 1/2) cells (srd_cell_id_with_random_shift, src/srd_collision.cpp:9-45:
+// wrapped on periodic axes, clamped on the others). SRD cell s thus holds particles of the
+// standard cells s - 1 and s (ss >= 0) or s and s + 1 (ss < 0).
+__device__ __forceinline__ int srd_axis(int g, float r, float ss, int N, bool per) {
+    int s = g + (int)floorf(r + ss);
+    if (s < 0) s = per ? s + N : 0;
+    if (s >= N) s = per ? s - N : N - 1;
+    return s;
+}
+
+// Rotation of one SRD cell (src/srd_collision.cpp:47-140) from its exact sums in grid units:
+// velocities relative to the cell mean turned by +-alpha (the sign drawn per SRD cell) and
+// scaled by the isokinetic thermostat's factor.
+struct SrdRot {
+    double ux, uy, lam, ct, sn;
+};
+__device__ __forceinline__ SrdRot srd_rotation(const DevParams& P, uint64_t seed, int w, int N, long long Sx,
+                                               long long Sy, long long Sqq) {
+    SrdRot R;
+    R.ux = (double)Sx / N;
+    R.uy = (double)Sy / N;
+    R.ct = 1.0;
+    R.sn = 0.0;
     if (N >= 2) {
-        const uint64_t h = fhash(S->seed, (uint64_t)w, 0x5349474EULL);
+        const uint64_t h = fhash(seed, (uint64_t)w, 0x5349474EULL);
         const int rr = (h >> 63) ? 1 : 2;  // +alpha or -alpha
-        ct = P.rotCos[rr];
-        sn = P.rotSin[rr];
+        R.ct = P.rotCos[rr];
+        R.sn = P.rotSin[rr];
     }
-    double lam = 1.0;
+    R.lam = 1.0;
     if (P.useThermostat && N > 1) {
-        // sum |q - u|^2 = (N sum|q|^2 - |sum q|^2) / N, an exact integer numerator
-        const __int128 num = (__int128)N * Sqq - (__int128)Sx * Sx - (__int128)Sy * Sy;
-        const double s2 = (double)num / (double)N;
-        if (s2 > 0.0) lam = sqrt(2.0 * (double)(N - 1) * P.kBT * kFastQ * kFastQ / s2);
+        // sum |q - u|^2 = (N sum|q|^2 - |sum q|^2) / N, an exact integer numerator (in 64 bits
+        // when its terms stay below 2^62, else in 128)
+        double numd;
+        if (N < 512 && Sqq < (1LL << 53) && llabs(Sx) < (1LL << 31) && llabs(Sy) < (1LL << 31))
+            numd = (double)((long long)N * Sqq - Sx * Sx - Sy * Sy);
+        else
+            numd = (double)((__int128)N * Sqq - (__int128)Sx * Sx - (__int128)Sy * Sy);
+        const double s2 = numd / (double)N;
+        if (s2 > 0.0) R.lam = sqrt(2.0 * (double)(N - 1) * P.kBT * kFastQ * kFastQ / s2);
     }
-    long long Tx = 0, Ty = 0;
-    long long nx[4], ny[4];
-    unsigned long long best = ~0ULL;  // (pid << 8 | member) of the member that takes the residual
+    return R;
+}
+__device__ __forceinline__ void srd_rotate(const SrdRot& R, int qx, int qy, long long& nx, long long& ny) {
+    const double rx = (double)qx - R.ux, ry = (double)qy - R.uy;
+    nx = llrint(R.ux + R.lam * (R.ct * rx - R.sn * ry));
+    ny = llrint(R.uy + R.lam * (R.sn * rx + R.ct * ry));
+}
+// the members that may take an SRD cell's rounding residual: new velocities of |n| < 2^22
+__device__ __forceinline__ bool srd_eligible(long long nx, long long ny) {
+    return llabs(nx) < (1LL << 22) && llabs(ny) < (1LL << 22);
+}
+
+// SRD collision tiles: kCollTX x TY SRD cells per block of kCollThreads threads. The block
+// gathers the standard cells under its tile (one column and one row of halo on the side the
+// shift points to) into shared memory, sorts their particles by SRD cell, collides each SRD
+// cell with 32 / TY threads and writes the new velocities back in place. Each cell keeps its
+// momentum exactly: the rounding of the new velocities to the grid leaves an integer residual
+// that goes to the eligible member with the smallest particle id. A tile whose standard cells
+// hold more than pcap particles is left to k_fast_collide_spill.
+constexpr int kCollTX = 8;
+constexpr int kCollThreads = 256;
+constexpr int kCollMaxStd = (kCollTX + 1) * (32 + 1);  // standard cells under a tile (TY <= 32)
+
+struct CollideArgs {
+    DevParams P;
+    FastParams F;
+    const FastStep* S;
+    FastBins b;
+    int TY, tilesY, nTiles, pcap;
+    int* spill;   // tiles left to the spill kernel
+    int* nSpill;  // their number (zeroed by k_fast_step_begin)
+};
+
+// the shared layout of a tile: standard-cell tables, then per staged particle its velocity,
+// id, SRD cell and rank, home (local cell << 7 | slot) and the SRD-ordered member list
+struct CollideMem {
+    int* cstart;    // kCollMaxStd + 1
+    int* gcell;     // kCollMaxStd
+    short2* gxy;    // kCollMaxStd
+    int* scnt;      // 256
+    int* sstart;    // 257
+    int* wsum;      // 32
+    int2* q;        // pcap
+    int* pid;       // pcap
+    uint32_t* sr;   // pcap: (SRD cell << 16) | rank, ~0 outside the tile
+    uint16_t* home; // pcap
+    uint16_t* list; // pcap
+    __host__ __device__ static size_t bytes(int pcap) {
+        return (size_t)(kCollMaxStd + 1) * 4 + kCollMaxStd * 4 + kCollMaxStd * 4 + 256 * 4 + 257 * 4 + 32 * 4 +
+               (size_t)pcap * (8 + 4 + 4 + 2 + 2) + 64;
+    }
+    __device__ void carve(char* base, int pcap) {
+        char* p = base;
+        auto take = [&](size_t n, size_t a) {
+            p = (char*)(((uintptr_t)p + a - 1) / a * a);
+            char* r = p;
+            p += n;
+            return r;
+        };
+        q = (int2*)take((size_t)pcap * 8, 8);
+        pid = (int*)take((size_t)pcap * 4, 4);
+        sr = (uint32_t*)take((size_t)pcap * 4, 4);
+        cstart = (int*)take((size_t)(kCollMaxStd + 1) * 4, 4);
+        gcell = (int*)take((size_t)kCollMaxStd * 4, 4);
+        gxy = (short2*)take((size_t)kCollMaxStd * 4, 4);
+        scnt = (int*)take(256 * 4, 4);
+        sstart = (int*)take(257 * 4, 4);
+        wsum = (int*)take(32 * 4, 4);
+        home = (uint16_t*)take((size_t)pcap * 2, 2);
+        list = (uint16_t*)take((size_t)pcap * 2, 2);
+    }
+};
+
+// exclusive prefix of v[0..n) into out[0..n] (out[n] the total), n <= 512, all threads of a
+// kCollThreads block; v and out may alias
+__device__ void block_scan(const int* v, int* out, int n, int* wsum) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int carry = 0;
+    for (int b0 = 0; b0 < n; b0 += kCollThreads) {
+        const int t = b0 + tid;
+        const int x = t < n ? v[t] : 0;
+        int incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const int w = lane < kCollThreads / 32 ? wsum[lane] : 0;
+            int wi = w;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += u;
+            }
+            if (lane < kCollThreads / 32) wsum[lane] = wi - w;
+            if (lane == kCollThreads / 32 - 1) wsum[kCollThreads / 32] = wi;
+        }
+        __syncthreads();
+        if (t < n) out[t] = carry + wsum[wid] + incl - x;
+        carry += wsum[kCollThreads / 32];
+        __syncthreads();
+    }
+    if (tid == 0) out[n] = carry;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCollThreads) k_fast_collide_tile(CollideArgs A) {
+    extern __shared__ __align__(16) char smem[];
+    const DevParams& P = A.P;
+    const int K = A.F.K;
+    const int tid = threadIdx.x;
+    CollideMem M;
+    M.carve(smem, A.pcap);
+    const int tile = blockIdx.x;
+    const int X0 = (tile / A.tilesY) * kCollTX, Y0 = (tile % A.tilesY) * A.TY;
+    const int TXc = min(kCollTX, P.Nx - X0), TYc = min(A.TY, P.Ny - Y0);
+    const float ssx = (float)A.S->sx, ssy = (float)A.S->sy;
+    // the halo column: X0 - 1 for a shift >= 0, X0 + TXc for a shift < 0 (when that column
+    // exists and is not in the tile)
+    const bool upx = ssx < 0.0f, upy = ssy < 0.0f;
+    const int hx = (TXc < P.Nx && (P.perx || (upx ? X0 + TXc < P.Nx : X0 > 0))) ? 1 : 0;
+    const int hy = (TYc < P.Ny && (P.pery || (upy ? Y0 + TYc < P.Ny : Y0 > 0))) ? 1 : 0;
+    const int LX = TXc + hx, LY = TYc + hy, NL = LX * LY, NS = TXc * TYc;
+    const int gx0 = X0 - (upx ? 0 : hx), gy0 = Y0 - (upy ? 0 : hy);
+    for (int t = tid; t < NL; t += kCollThreads) {
+        const int lx = t / LY, ly = t - lx * LY;
+        int gx = gx0 + lx, gy = gy0 + ly;
+        if (gx < 0) gx += P.Nx;
+        if (gx >= P.Nx) gx -= P.Nx;
+        if (gy < 0) gy += P.Ny;
+        if (gy >= P.Ny) gy -= P.Ny;
+        const int gc = gy + P.Ny * gx;
+        M.gcell[t] = gc;
+        M.gxy[t] = make_short2((short)gx, (short)gy);
+        M.cstart[t] = min(A.b.cnt[gc], K);
+    }
+    for (int t = tid; t < NS; t += kCollThreads) M.scnt[t] = 0;
+    __syncthreads();
+    block_scan(M.cstart, M.cstart, NL, M.wsum);
+    const int total = M.cstart[NL];
+    if (total > A.pcap) {
+        if (tid == 0) A.spill[atomicAdd(A.nSpill, 1)] = tile;
+        return;
+    }
+    // each particle's home (local cell << 7 | slot), cell by cell
+    for (int lc = tid; lc < NL; lc += kCollThreads) {
+        const int a = M.cstart[lc], e = M.cstart[lc + 1];
+        for (int f = a; f < e; ++f) M.home[f] = (uint16_t)((lc << 7) | (f - a));
+    }
+    __syncthreads();
+    // stage every particle of the standard cells; count the tile's members per SRD cell
+    // (four particles per thread and iteration, their loads issued together)
+    constexpr int kU = 4;
+    for (int fb = tid; fb < total; fb += kU * kCollThreads) {
+        int lcs[kU], js[kU];
+        float2 off[kU], vv[kU];
+        int pp[kU];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        nx[r] = ny[r] = 0;
-        if (32 * r + lane < n) {
-            const double rx = (double)qx[r] - ux, ry = (double)qy[r] - uy;
-            nx[r] = llrint(ux + lam * (ct * rx - sn * ry));
-            ny[r] = llrint(uy + lam * (sn * rx + ct * ry));
-            Tx += nx[r];
-            Ty += ny[r];
-            if (llabs(nx[r]) < (1LL << 22) && llabs(ny[r]) < (1LL << 22)) {
-                const unsigned long long key = ((unsigned long long)(uint32_t)pid[r] << 8) | (unsigned long long)r;
-                best = key < best ? key : best;
+        for (int u = 0; u < kU; ++u) {
+            const int f = fb + u * kCollThreads;
+            const int h = f < total ? M.home[f] : 0;
+            lcs[u] = h >> 7;
+            js[u] = h & 127;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (fb + u * kCollThreads < total) {
+                const size_t s = (size_t)M.gcell[lcs[u]] * K + js[u];
+                off[u] = A.b.off[s];
+                vv[u] = A.b.vel[s];
+                pp[u] = A.b.pid[s];
             }
         }
-    }
-    Tx = warp_sum_ll(Tx);
-    Ty = warp_sum_ll(Ty);
-    const unsigned long long bestAll = warp_min_u64_c(best);
-    const long long rx = Sx - Tx, ry = Sy - Ty;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const bool live = 32 * r + lane < n;
-        if (live && best == bestAll && (int)(bestAll & 0xff) == r) {
-            nx[r] += rx;
-            ny[r] += ry;
+        for (int u = 0; u < kU; ++u) {
+            const int f = fb + u * kCollThreads;
+            if (f >= total) break;
+            const short2 g = M.gxy[lcs[u]];
+            const int sx = srd_axis(g.x, off[u].x, ssx, P.Nx, P.perx) - X0;
+            const int sy = srd_axis(g.y, off[u].y, ssy, P.Ny, P.pery) - Y0;
+            uint32_t code = 0xFFFFFFFFu;
+            if (sx >= 0 && sx < TXc && sy >= 0 && sy < TYc) {
+                const int k = sx * TYc + sy;
+                code = ((uint32_t)k << 16) | (uint32_t)atomicAdd(M.scnt + k, 1);
+            }
+            M.q[f] = make_int2(fq_of(vv[u].x), fq_of(vv[u].y));
+            M.pid[f] = pp[u];
+            M.sr[f] = code;
         }
-        const unsigned act = __ballot_sync(0xffffffffu, live);
-        if (!act) break;
-        if (live) {
-            const int c = cel[r];
-            const unsigned grp = __match_any_sync(act, c);
-            const int leader = __ffs(grp) - 1;
-            int b0 = 0;
-            if (lane == leader) b0 = atomicAdd(out.cnt + c, __popc(grp));
-            b0 = __shfl_sync(grp, b0, leader);
-            const int slot = b0 + __popc(grp & lanemask_lt());
-            if (slot < F.K) {
-                const size_t d = (size_t)c * F.K + slot;
-                out.off[d] = off[r];
-                out.vel[d] = make_float2(fv_of(nx[r]), fv_of(ny[r]));
-                out.pid[d] = pid[r];
-            } else if (st) {
-                raise_error(st, kErrBinCapacity, c);
+    }
+    __syncthreads();
+    block_scan(M.scnt, M.sstart, NS, M.wsum);
+    for (int f = tid; f < total; f += kCollThreads) {
+        const uint32_t code = M.sr[f];
+        if (code != 0xFFFFFFFFu) M.list[M.sstart[code >> 16] + (code & 0xFFFFu)] = (uint16_t)f;
+    }
+    __syncthreads();
+    // collide: tpc threads per SRD cell (aligned lane groups)
+    const int tpc = kCollThreads / (kCollTX * A.TY);
+    const int k = tid / tpc, sub = tid - k * tpc;
+    const bool own = k < NS;
+    const int N = own ? M.scnt[k] : 0;
+    const int b0 = own ? M.sstart[k] : 0;
+    long long Sx = 0, Sy = 0, Sqq = 0;
+    for (int m = sub; m < N; m += tpc) {
+        const int2 q = M.q[M.list[b0 + m]];
+        Sx += q.x;
+        Sy += q.y;
+        Sqq += (long long)q.x * q.x + (long long)q.y * q.y;
+    }
+    for (int o = 1; o < tpc; o <<= 1) {
+        Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+        Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+        Sqq += __shfl_xor_sync(0xffffffffu, Sqq, o);
+    }
+    const int w = own ? (Y0 + k % TYc) + P.Ny * (X0 + k / TYc) : 0;
+    SrdRot R{};
+    if (N > 0) R = srd_rotation(P, A.S->seed, w, N, Sx, Sy, Sqq);
+    long long Tx = 0, Ty = 0;
+    int minPid = 0x7fffffff;
+    for (int m = sub; m < N; m += tpc) {
+        const int f = M.list[b0 + m];
+        const int2 q = M.q[f];
+        long long nx, ny;
+        srd_rotate(R, q.x, q.y, nx, ny);
+        Tx += nx;
+        Ty += ny;
+        if (srd_eligible(nx, ny)) minPid = min(minPid, M.pid[f]);
+        M.q[f] = make_int2((int)nx, (int)ny);
+    }
+    for (int o = 1; o < tpc; o <<= 1) {
+        Tx += __shfl_xor_sync(0xffffffffu, Tx, o);
+        Ty += __shfl_xor_sync(0xffffffffu, Ty, o);
+        minPid = min(minPid, __shfl_xor_sync(0xffffffffu, minPid, o));
+    }
+    const long long rx = Sx - Tx, ry = Sy - Ty;
+    for (int m = sub; m < N; m += tpc) {
+        const int f = M.list[b0 + m];
+        const int2 q = M.q[f];
+        long long nx = q.x, ny = q.y;
+        if (M.pid[f] == minPid) {
+            nx += rx;
+            ny += ry;
+        }
+        const int h = M.home[f];
+        A.b.vel[(size_t)M.gcell[h >> 7] * K + (h & 127)] = make_float2(fv_of(nx), fv_of(ny));
+    }
+}
+
+// The tiles the tile kernel left (more particles than its shared memory holds): one warp per
+// SRD cell, its members found among the particles of the two-by-two standard cells under it
+// and read twice from global memory. The same arithmetic as the tile kernel.
+__global__ void __launch_bounds__(256) k_fast_collide_spill(CollideArgs A) {
+    const DevParams& P = A.P;
+    const int K = A.F.K;
+    const int lane = threadIdx.x & 31;
+    const int nsp = *A.nSpill;
+    if (nsp == 0) return;
+    const float ssx = (float)A.S->sx, ssy = (float)A.S->sy;
+    const int ex = ssx < 0.0f ? 1 : 0, ey = ssy < 0.0f ? 1 : 0;
+    const int cellsPerTile = kCollTX * A.TY;
+    const long long items = (long long)nsp * cellsPerTile;
+    const long long wstep = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long it = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; it < items; it += wstep) {
+        const int tile = A.spill[it / cellsPerTile];
+        const int kk = (int)(it % cellsPerTile);
+        const int X0 = (tile / A.tilesY) * kCollTX, Y0 = (tile % A.tilesY) * A.TY;
+        const int TXc = min(kCollTX, P.Nx - X0), TYc = min(A.TY, P.Ny - Y0);
+        if (kk >= TXc * TYc) continue;
+        const int sx = X0 + kk / TYc, sy = Y0 + kk % TYc;
+        // the standard cells that can hold members: sx - 1 + ex .. sx + ex (wrapped; missing ones skipped)
+        int cells[4];
+        int nc = 0;
+        for (int a = 0; a < 2; ++a)
+            for (int bb = 0; bb < 2; ++bb) {
+                int gx = sx - 1 + ex + a, gy = sy - 1 + ey + bb;
+                if (gx < 0 || gx >= P.Nx) {
+                    if (!P.perx) continue;
+                    gx = gx < 0 ? gx + P.Nx : gx - P.Nx;
+                }
+                if (gy < 0 || gy >= P.Ny) {
+                    if (!P.pery) continue;
+                    gy = gy < 0 ? gy + P.Ny : gy - P.Ny;
+                }
+                cells[nc++] = gy + P.Ny * gx;
+            }
+        long long Sx = 0, Sy = 0, Sqq = 0;
+        int N = 0;
+        // pass 1: sums
+        for (int ci = 0; ci < nc; ++ci) {
+            const int gc = cells[ci];
+            const int gx = gc / P.Ny, gy = gc - gx * P.Ny;
+            const int n = min(A.b.cnt[gc], K);
+            for (int j = lane; j < n; j += 32) {
+                const size_t s = (size_t)gc * K + j;
+                const float2 off = A.b.off[s];
+                if (srd_axis(gx, off.x, ssx, P.Nx, P.perx) != sx || srd_axis(gy, off.y, ssy, P.Ny, P.pery) != sy) continue;
+                const float2 v = A.b.vel[s];
+                const long long qx = fq_of(v.x), qy = fq_of(v.y);
+                Sx += qx;
+                Sy += qy;
+                Sqq += qx * qx + qy * qy;
+                ++N;
+            }
+        }
+        Sx = warp_sum_ll(Sx);
+        Sy = warp_sum_ll(Sy);
+        Sqq = warp_sum_ll(Sqq);
+        N = warp_sum_i(N);
+        if (N == 0) continue;
+        const SrdRot R = srd_rotation(P, A.S->seed, sy + P.Ny * sx, N, Sx, Sy, Sqq);
+        // pass 2: the rounding residual and its taker
+        long long Tx = 0, Ty = 0;
+        int minPid = 0x7fffffff;
+        for (int ci = 0; ci < nc; ++ci) {
+            const int gc = cells[ci];
+            const int gx = gc / P.Ny, gy = gc - gx * P.Ny;
+            const int n = min(A.b.cnt[gc], K);
+            for (int j = lane; j < n; j += 32) {
+                const size_t s = (size_t)gc * K + j;
+                const float2 off = A.b.off[s];
+                if (srd_axis(gx, off.x, ssx, P.Nx, P.perx) != sx || srd_axis(gy, off.y, ssy, P.Ny, P.pery) != sy) continue;
+                const float2 v = A.b.vel[s];
+                long long nx, ny;
+                srd_rotate(R, fq_of(v.x), fq_of(v.y), nx, ny);
+                Tx += nx;
+                Ty += ny;
+                if (srd_eligible(nx, ny)) minPid = min(minPid, A.b.pid[s]);
+            }
+        }
+        Tx = warp_sum_ll(Tx);
+        Ty = warp_sum_ll(Ty);
+        minPid = (int)__reduce_min_sync(0xffffffffu, (unsigned)minPid);
+        const long long rx = Sx - Tx, ry = Sy - Ty;
+        // pass 3: the new velocities (every lane reads its members before the warp writes)
+        for (int ci = 0; ci < nc; ++ci) {
+            const int gc = cells[ci];
+            const int gx = gc / P.Ny, gy = gc - gx * P.Ny;
+            const int n = min(A.b.cnt[gc], K);
+            for (int j0 = 0; j0 < n; j0 += 32) {
+                const int j = j0 + lane;
+                const size_t s = (size_t)gc * K + j;
+                bool mem = false;
+                float2 nv = make_float2(0.f, 0.f);
+                if (j < n) {
+                    const float2 off = A.b.off[s];
+                    mem = srd_axis(gx, off.x, ssx, P.Nx, P.perx) == sx && srd_axis(gy, off.y, ssy, P.Ny, P.pery) == sy;
+                    if (mem) {
+                        const float2 v = A.b.vel[s];
+                        long long nx, ny;
+                        srd_rotate(R, fq_of(v.x), fq_of(v.y), nx, ny);
+                        if (A.b.pid[s] == minPid) {
+                            nx += rx;
+                            ny += ry;
+                        }
+                        nv = make_float2(fv_of(nx), fv_of(ny));
+                    }
+                }
+                __syncwarp();
+                if (mem) A.b.vel[s] = nv;
             }
         }
     }
@@ -472,6 +854,15 @@ struct FastZoneArgs {
     int* recOverflow;          // zones that ran out of records (their remaining moves are skipped)
     DevStatus* st;
     int maxCells, winCap, nsmCap, recCap;
+    // what the decision kernel hands the apply kernel: per cell a summary (bit 63 changed,
+    // bit 48 corrected, bits 32-47 arrivals, bits 0-31 its first arrival record) and the removal
+    // masks of changed cells; per zone (recCap records from z * recCap) the arrivals in cell
+    // order: id, position in the cell, velocity (grid units)
+    unsigned long long* meta;
+    uint4* cellRm;
+    int* recPidG;
+    float2* recOffG;
+    int2* recQG;
 };
 
 // The 24 range-2 neighbour offsets grouped by the angular bin of atan2(dy, dx)
@@ -493,9 +884,7 @@ struct FastZoneMem {
     uint8_t* nrecv;    // cell: records currently in the cell
     uint32_t* rm;      // cell x 4: originals removed
     int* recPid;       // recCap
-    int2* recV;        // recCap: the moved particle's velocity (grid units), gathered by the output
-    uint16_t* recList; // recCap: records grouped by current cell
-    uint16_t* recStart;// cell + 1: start of each cell's records in recList
+    uint16_t* recStart;// cell + 1: start of each cell's arrivals in the exported records
     int* rfill;        // cell: records filed so far
     uint16_t* recSrc;  // recCap: (origin cell << 7) | slot
     uint8_t* recCur;   // recCap: current cell
@@ -513,8 +902,6 @@ struct FastZoneMem {
         for (int k = 0; k < 5; ++k) take((size_t)maxCells, 1);
         take((size_t)maxCells * 16, 4);
         take((size_t)recCap * 4, 4);
-        take((size_t)recCap * 8, 8);
-        take((size_t)recCap * 2, 2);
         take((size_t)(maxCells + 1) * 2, 2);
         take((size_t)maxCells * 4, 4);
         take((size_t)recCap * 2, 2);
@@ -533,7 +920,7 @@ struct FastZoneMem {
     }
     __device__ void carve(char* base, int maxCells, int winCap, int nsmCap, int recCap) {
         size_t b = 0;
-        char* p[21];
+        char* p[19];
         int i = 0;
         layout(maxCells, winCap, nsmCap, recCap, [&](size_t n, size_t a) {
             b = (b + a - 1) / a * a;
@@ -549,18 +936,16 @@ struct FastZoneMem {
         nrecv = (uint8_t*)p[6];
         rm = (uint32_t*)p[7];
         recPid = (int*)p[8];
-        recV = (int2*)p[9];
-        recList = (uint16_t*)p[10];
-        recStart = (uint16_t*)p[11];
-        rfill = (int*)p[12];
-        recSrc = (uint16_t*)p[13];
-        recCur = (uint8_t*)p[14];
-        recOff = (float2*)p[15];
-        nsm = (float*)p[16];
-        keys = (uint32_t*)p[17];
-        ord = (uint8_t*)p[18];
-        tgt = (int*)p[19];
-        tgt2 = (int*)p[20];
+        recStart = (uint16_t*)p[9];
+        rfill = (int*)p[10];
+        recSrc = (uint16_t*)p[11];
+        recCur = (uint8_t*)p[12];
+        recOff = (float2*)p[13];
+        nsm = (float*)p[14];
+        keys = (uint32_t*)p[15];
+        ord = (uint8_t*)p[16];
+        tgt = (int*)p[17];
+        tgt2 = (int*)p[18];
     }
 };
 
@@ -729,6 +1114,52 @@ struct FastZone {
             def = max(0, (int)floor(mapO - (double)cnt(tO)));
         }
         int avail = cnt(l);
+        // With at most as many particles to move as targets with a deficit, the round-robin
+        // quota stays 1: the first needOut of those targets (in order) take one particle each,
+        // the i-th the i-th member in list order, drawn as the general loop below draws them
+        // (its i-th call's salt, first draw). Done in one step when the source holds no records.
+        const unsigned defMask = __ballot_sync(0xffffffffu, lane < T && def > 0);
+        if (needOut > 0 && needOut <= __popc(defMask) && needOut <= avail && M.nrecv[l] == 0 && !failed &&
+            nrec + needOut <= A->recCap) {
+            unsigned long long mine = ~0ULL;
+            for (int i = 0; i < needOut; ++i) {
+                unsigned long long best = cand[0];
+#pragma unroll
+                for (int r = 1; r < 4; ++r) best = cand[r] < best ? cand[r] : best;
+                best = warp_min_u64_r(best);
+                const int j = (int)(best & 511ULL);
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r == (j >> 5) && (j & 31) == lane) cand[r] = ~0ULL;
+                if (lane == i) mine = best;
+            }
+            const int drank = __popc(defMask & lanemask_lt());
+            __syncwarp();
+            if (lane < T && def > 0 && drank < needOut) M.tgt[drank] = tO;
+            __syncwarp();
+            if (lane < needOut) {
+                const int t = M.tgt[lane];
+                const int j = (int)(mine & 511ULL);
+                const uint32_t salt = op + 1 + (uint32_t)lane;
+                const uint64_t hp = fmix64(zseed ^ ((uint64_t)salt << 20) ^ 0x504F53ULL);
+                const int rec = nrec + lane;
+                M.recPid[rec] = (int)((mine >> 10) & 0x7fffffffULL);
+                M.recSrc[rec] = (uint16_t)((l << 7) | j);
+                M.recCur[rec] = (uint8_t)t;
+                M.recOff[rec] = make_float2(fminf((float)(hp >> 40) * 0x1.0p-24f, kFastOffMax),
+                                            fminf((float)((hp >> 8) & 0xFFFFFFu) * 0x1.0p-24f, kFastOffMax));
+                M.nrecv[t] += 1;
+                add_cnt(t, 1);
+                atomicOr(&M.rm[4 * l + (j >> 5)], 1u << (j & 31));
+                rcv[*nr + lane] = t;
+            }
+            if (lane == 0) add_cnt(l, -needOut);
+            op += (uint32_t)needOut;
+            nrec += needOut;
+            *nr += needOut;
+            __syncwarp();
+            return needOut;
+        }
         int moved = 0;
         unsigned got = 0;
         while (needOut > 0 && avail > 0 && !failed) {
@@ -794,9 +1225,13 @@ struct FastZone {
         int moved = 0;
         unsigned long long cand[4];
         load_candidates(l, true, 0, cand);
-        if (needOut > 0) moved += spread(l, needOut, 0, M.tgt2, &nr, cand);
-        const int remainingOut = max(0, (int)ceil((double)cnt(l) - hi));
-        if (remainingOut > 0 && !failed) moved += spread(l, remainingOut, 1, M.tgt2, &nr, cand);
+        // the low map first, then the high map for what is left (one call site: code size)
+#pragma unroll 1
+        for (int phase = 0; phase < 2; ++phase) {
+            const int out = phase == 0 ? needOut : max(0, (int)ceil((double)cnt(l) - hi));
+            if (out <= 0 || failed) continue;
+            moved += spread(l, out, phase, M.tgt2, &nr, cand);
+        }
         // the receivers of the two phases may repeat a cell; flags are idempotent
         const int nrc = min(nr, 31);
         masks(l, lane < nrc ? M.tgt2[lane] : l, nrc, kZBulkD);
@@ -934,31 +1369,13 @@ struct FastZone {
     }
 };
 
-// floor(a / b) for b > 0, in 32 bits when a fits
-__device__ __forceinline__ long long floor_div_small(long long a, int b) {
-    if (a >= -2147483647LL - 1 && a <= 2147483647LL) {
-        const int ai = (int)a;
-        int q = ai / b;
-        if ((ai % b != 0) && (ai < 0)) --q;
-        return q;
-    }
-    return floor_div_ll(a, b);
-}
-
-// Output of the zone (src/zone_pass.cpp:870-909), in place: only the cells whose members
-// changed are rewritten. A changed cell's final members are its kept particles and its
-// arrivals; the kept particles above the new count and then the arrivals fill the holes the
-// departed left (in slot order), then the slots from the old count on. The momentum correction
-// restores each corrected cell's pass-input momentum exactly: an integer share per member, the
-// remainder to the member of smallest id. The arrivals' velocities are gathered before anything
-// is written; then each lane takes its cells (lane + 32 r) and reads a cell four slots at a
-// time (32-byte loads: bins start on 128-byte boundaries, K being a multiple of 16), before it
-// writes that cell.
-__device__ void fast_zone_output(FastZone& Z) {
+// The zone's decisions for the apply kernel: its arrival records in cell order (with the moved
+// particles' velocities, read here, before any bin is rewritten) and per cell the summary and
+// removal masks.
+__device__ void fast_zone_export(FastZone& Z) {
     const FastZoneArgs& A = *Z.A;
     FastZoneMem& M = Z.M;
     const int lane = Z.lane, K = A.F.K, nl = Z.nl;
-    const FastBins& B = A.b;
     for (int l = lane; l < nl; l += 32) M.rfill[l] = 0;
     // records grouped by cell (exclusive prefix of the arrivals per cell)
     int base = 0;
@@ -974,167 +1391,203 @@ __device__ void fast_zone_output(FastZone& Z) {
         base += __shfl_sync(0xffffffffu, incl, 31);
     }
     __syncwarp();
+    const size_t zb = (size_t)Z.z * A.recCap;
     for (int r = lane; r < Z.nrec; r += 32) {
         const int src = M.recSrc[r];
         const int l = M.recCur[r];
-        const float2 v = B.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
-        M.recV[r] = make_int2(fq_of(v.x), fq_of(v.y));
-        M.recList[M.recStart[l] + atomicAdd(M.rfill + l, 1)] = (uint16_t)r;
+        const float2 v = A.b.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
+        const size_t g = zb + M.recStart[l] + atomicAdd(M.rfill + l, 1);
+        A.recPidG[g] = M.recPid[r];
+        A.recOffG[g] = M.recOff[r];
+        A.recQG[g] = make_int2(fq_of(v.x), fq_of(v.y));
     }
-    __syncwarp();
     for (int l = lane; l < nl; l += 32) {
         const int c = Z.gcell(l);
-        const int n0 = M.n0[l], nr = M.nrecv[l];
-        const uint32_t rm0 = M.rm[4 * l], rm1 = M.rm[4 * l + 1], rm2 = M.rm[4 * l + 2], rm3 = M.rm[4 * l + 3];
-        const bool changed = (rm0 | rm1 | rm2 | rm3) != 0 || nr > 0;
-        if (!changed && A.sumsIn) {  // nothing to read: the input passes through
-            A.cntOut[c] = n0;
-            A.sumsOut[c] = A.sumsIn[c];
-            continue;
+        const uint4 rm = make_uint4(M.rm[4 * l], M.rm[4 * l + 1], M.rm[4 * l + 2], M.rm[4 * l + 3]);
+        const int nr = M.nrecv[l];
+        const bool changed = (rm.x | rm.y | rm.z | rm.w) != 0 || nr > 0;
+        unsigned long long meta = 0;
+        if (changed) {
+            const uint8_t f = M.flg[l];
+            const bool corr = A.P.momCorr != 0 && !(f & kZSkip) && !((f & kZRecv) && !(f & kZBB));
+            meta = (1ULL << 63) | ((unsigned long long)corr << 48) | ((unsigned long long)nr << 32) |
+                   (unsigned long long)(zb + M.recStart[l]);
+            A.cellRm[c] = rm;
         }
-        // the removal bits of slots j0 .. j0 + 3 (j0 a multiple of 4)
-        auto rbits = [&](int j0) -> uint32_t {
-            const uint32_t w = j0 < 32 ? rm0 : (j0 < 64 ? rm1 : (j0 < 96 ? rm2 : rm3));
-            return (w >> (j0 & 31)) & 0xFu;
-        };
-        const size_t ib = (size_t)c * K;
-        const float4* v4 = reinterpret_cast<const float4*>(B.vel + ib);
-        const int4* p4 = reinterpret_cast<const int4*>(B.pid + ib);
-        long long bx = 0, by = 0, qq = 0, ax = 0, ay = 0;
-        int mp = 0x7fffffff;
+        A.meta[c] = meta;
+    }
+}
+
+// floor(a / b) for b > 0, in 32 bits when a fits
+__device__ __forceinline__ long long floor_div_small(long long a, int b) {
+    if (a >= -2147483647LL - 1 && a <= 2147483647LL) {
+        const int ai = (int)a;
+        int q = ai / b;
+        if ((ai % b != 0) && (ai < 0)) --q;
+        return q;
+    }
+    return floor_div_ll(a, b);
+}
+
+// Output of a zone pass (src/zone_pass.cpp:870-909), in place, one thread per cell: only the
+// cells whose members changed are rewritten. A changed cell's final members are its kept
+// particles and its arrivals; the kept particles above the new count and then the arrivals fill
+// the holes the departed left (in slot order), then the slots from the old count on. The
+// momentum correction restores each corrected cell's pass-input momentum exactly: an integer
+// share per member, the remainder to the member of smallest id. A cell is read four slots at a
+// time (32-byte loads: bins start on 128-byte boundaries, K being a multiple of 16) before it is
+// written; no thread reads another cell's slots (the arrivals come from the exported records).
+__global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
+    const int c = (int)(blockIdx.x * (size_t)blockDim.x + threadIdx.x);
+    if (c >= A.P.Nc) return;
+    const int K = A.F.K;
+    const FastBins& B = A.b;
+    const int n0 = min(A.cntIn[c], K);
+    const unsigned long long meta = A.meta[c];
+    const bool changed = (meta >> 63) != 0;
+    if (!changed && A.sumsIn) {  // nothing to read: the input passes through
+        A.cntOut[c] = n0;
+        A.sumsOut[c] = A.sumsIn[c];
+        return;
+    }
+    const uint4 rmv = changed ? A.cellRm[c] : make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t rm0 = rmv.x, rm1 = rmv.y, rm2 = rmv.z, rm3 = rmv.w;
+    const int nr = (int)((meta >> 32) & 0xFFFFu);
+    const size_t rs = (size_t)(meta & 0xFFFFFFFFULL);
+    // the removal bits of slots j0 .. j0 + 3 (j0 a multiple of 4)
+    auto rbits = [&](int j0) -> uint32_t {
+        const uint32_t w = j0 < 32 ? rm0 : (j0 < 64 ? rm1 : (j0 < 96 ? rm2 : rm3));
+        return (w >> (j0 & 31)) & 0xFu;
+    };
+    const size_t ib = (size_t)c * K;
+    const float4* v4 = reinterpret_cast<const float4*>(B.vel + ib);
+    const int4* p4 = reinterpret_cast<const int4*>(B.pid + ib);
+    long long bx = 0, by = 0, qq = 0, ax = 0, ay = 0;
+    int mp = 0x7fffffff;
 #pragma unroll 2
-        for (int j0 = 0; j0 < n0; j0 += 4) {
-            const float4 va = v4[j0 >> 1], vb = v4[(j0 >> 1) + 1];
-            const int4 pp = changed ? p4[j0 >> 2] : make_int4(0, 0, 0, 0);
-            const float vx[4] = {va.x, va.z, vb.x, vb.z}, vy[4] = {va.y, va.w, vb.y, vb.w};
-            const int pv[4] = {pp.x, pp.y, pp.z, pp.w};
-            const uint32_t rb = rbits(j0);
+    for (int j0 = 0; j0 < n0; j0 += 4) {
+        const float4 va = v4[j0 >> 1], vb = v4[(j0 >> 1) + 1];
+        const int4 pp = changed ? p4[j0 >> 2] : make_int4(0, 0, 0, 0);
+        const float vx[4] = {va.x, va.z, vb.x, vb.z}, vy[4] = {va.y, va.w, vb.y, vb.w};
+        const int pv[4] = {pp.x, pp.y, pp.z, pp.w};
+        const uint32_t rb = rbits(j0);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (j0 + u >= n0) break;
-                const long long qx = fq_of(vx[u]), qy = fq_of(vy[u]);
-                bx += qx;
-                by += qy;
-                qq += qx * qx + qy * qy;
-                if (changed && !((rb >> u) & 1u)) {
-                    ax += qx;
-                    ay += qy;
-                    mp = min(mp, pv[u]);
+        for (int u = 0; u < 4; ++u) {
+            if (j0 + u >= n0) break;
+            const long long qx = fq_of(vx[u]), qy = fq_of(vy[u]);
+            bx += qx;
+            by += qy;
+            qq += qx * qx + qy * qy;
+            if (changed && !((rb >> u) & 1u)) {
+                ax += qx;
+                ay += qy;
+                mp = min(mp, pv[u]);
+            }
+        }
+    }
+    if (A.ref) A.ref[c] = make_longlong4(bx, by, qq, n0);
+    if (!changed) {
+        A.cntOut[c] = n0;
+        A.sumsOut[c] = make_longlong2(bx, by);
+        return;
+    }
+    for (int k = 0; k < nr; ++k) {
+        const int2 q = A.recQG[rs + k];
+        ax += q.x;
+        ay += q.y;
+        mp = min(mp, A.recPidG[rs + k]);
+    }
+    const int kept = n0 - (__popc(rm0) + __popc(rm1) + __popc(rm2) + __popc(rm3));
+    const int nAll = kept + nr;
+    long long shx = 0, shy = 0, remx = 0, remy = 0;
+    if (((meta >> 48) & 1ULL) && nAll > 0) {
+        const long long dx = bx - ax, dy = by - ay;
+        shx = floor_div_small(dx, nAll);
+        shy = floor_div_small(dy, nAll);
+        remx = dx - shx * nAll;
+        remy = dy - shy * nAll;
+    }
+    A.sumsOut[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
+    if (nAll > K) raise_error(A.st, kErrBinCapacity, c);
+    A.cntOut[c] = min(nAll, K);
+    const int below = min(n0, nAll);
+    // kept particles that stay: velocity corrected in place (whole 32-byte groups are
+    // rewritten; the other slots in them keep their values or are filled below)
+    if (shx | shy | remx | remy) {
+        float4* w4 = reinterpret_cast<float4*>(B.vel + ib);
+        const bool rem = (remx | remy) != 0;
+        for (int j0 = 0; j0 < below; j0 += 4) {
+            float4 va = w4[j0 >> 1], vb = w4[(j0 >> 1) + 1];
+            const int4 pp = rem ? p4[j0 >> 2] : make_int4(-1, -1, -1, -1);
+            const uint32_t rb = rbits(j0);
+            auto fix = [&](float& x, float& y, int p, int u) {
+                if (j0 + u >= below || ((rb >> u) & 1u)) return;
+                long long qx = fq_of(x) + shx, qy = fq_of(y) + shy;
+                if (p == mp) {
+                    qx += remx;
+                    qy += remy;
                 }
+                x = fv_of(qx);
+                y = fv_of(qy);
+            };
+            fix(va.x, va.y, pp.x, 0);
+            fix(va.z, va.w, pp.y, 1);
+            fix(vb.x, vb.y, pp.z, 2);
+            fix(vb.z, vb.w, pp.w, 3);
+            w4[j0 >> 1] = va;
+            w4[(j0 >> 1) + 1] = vb;
+        }
+    }
+    // holes below the new count, in slot order, then the slots from the old count on
+    int hw = 0;
+    uint32_t hbits = rm0;
+    int app = n0;
+    auto next_free = [&]() -> int {
+        for (;;) {
+            if (hbits) {
+                const int j = 32 * hw + __ffs(hbits) - 1;
+                hbits &= hbits - 1;
+                if (j < below) return j;
+                hbits = 0;
+                hw = 4;
             }
+            if (++hw >= 4) return app++;
+            hbits = hw == 1 ? rm1 : (hw == 2 ? rm2 : rm3);
         }
-        if (A.ref) A.ref[c] = make_longlong4(bx, by, qq, n0);
-        if (!changed) {
-            A.cntOut[c] = n0;
-            A.sumsOut[c] = make_longlong2(bx, by);
-            continue;
+    };
+    // kept particles above the new count
+    for (int j = nAll; j < n0; ++j) {
+        if ((rbits(j & ~3) >> (j & 3)) & 1u) continue;
+        const size_t s = ib + j;
+        const float2 v = B.vel[s];
+        const float2 o = B.off[s];
+        const int p = B.pid[s];
+        long long qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
+        if (p == mp) {
+            qx += remx;
+            qy += remy;
         }
-        const int rs = M.recStart[l];
-        for (int k = 0; k < nr; ++k) {
-            const int r = M.recList[rs + k];
-            const int2 q = M.recV[r];
-            ax += q.x;
-            ay += q.y;
-            mp = min(mp, M.recPid[r]);
+        const int d = next_free();
+        B.off[ib + d] = o;
+        B.vel[ib + d] = make_float2(fv_of(qx), fv_of(qy));
+        B.pid[ib + d] = p;
+    }
+    // arrivals
+    for (int k = 0; k < nr; ++k) {
+        const int p = A.recPidG[rs + k];
+        const int2 q = A.recQG[rs + k];
+        long long qx = q.x + shx, qy = q.y + shy;
+        if (p == mp) {
+            qx += remx;
+            qy += remy;
         }
-        const int kept = n0 - (__popc(rm0) + __popc(rm1) + __popc(rm2) + __popc(rm3));
-        const int nAll = kept + nr;
-        long long shx = 0, shy = 0, remx = 0, remy = 0;
-        const uint8_t f = M.flg[l];
-        bool doCorr = A.P.momCorr != 0;
-        if (doCorr && (f & kZSkip)) doCorr = false;
-        if (doCorr && (f & kZRecv) && !(f & kZBB)) doCorr = false;
-        if (doCorr && nAll > 0) {
-            const long long dx = bx - ax, dy = by - ay;
-            shx = floor_div_small(dx, nAll);
-            shy = floor_div_small(dy, nAll);
-            remx = dx - shx * nAll;
-            remy = dy - shy * nAll;
-        }
-        A.sumsOut[c] = make_longlong2(ax + shx * nAll + remx, ay + shy * nAll + remy);
-        if (nAll > K) raise_error(A.st, kErrBinCapacity, c);
-        A.cntOut[c] = min(nAll, K);
-        const int below = min(n0, nAll);
-        // kept particles that stay: velocity corrected in place (whole 32-byte groups are
-        // rewritten; the other slots in them keep their values or are filled below)
-        if (shx | shy | remx | remy) {
-            float4* w4 = reinterpret_cast<float4*>(B.vel + ib);
-            const bool rem = (remx | remy) != 0;
-            for (int j0 = 0; j0 < below; j0 += 4) {
-                float4 va = w4[j0 >> 1], vb = w4[(j0 >> 1) + 1];
-                const int4 pp = rem ? p4[j0 >> 2] : make_int4(-1, -1, -1, -1);
-                const uint32_t rb = rbits(j0);
-                auto fix = [&](float& x, float& y, int p, int u) {
-                    if (j0 + u >= below || ((rb >> u) & 1u)) return;
-                    long long qx = fq_of(x) + shx, qy = fq_of(y) + shy;
-                    if (p == mp) {
-                        qx += remx;
-                        qy += remy;
-                    }
-                    x = fv_of(qx);
-                    y = fv_of(qy);
-                };
-                fix(va.x, va.y, pp.x, 0);
-                fix(va.z, va.w, pp.y, 1);
-                fix(vb.x, vb.y, pp.z, 2);
-                fix(vb.z, vb.w, pp.w, 3);
-                w4[j0 >> 1] = va;
-                w4[(j0 >> 1) + 1] = vb;
-            }
-        }
-        // holes below the new count, in slot order, then the slots from the old count on
-        int hw = 0;
-        uint32_t hbits = rm0;
-        int app = n0;
-        auto next_free = [&]() -> int {
-            for (;;) {
-                if (hbits) {
-                    const int j = 32 * hw + __ffs(hbits) - 1;
-                    hbits &= hbits - 1;
-                    if (j < below) return j;
-                    hbits = 0;
-                    hw = 4;
-                }
-                if (++hw >= 4) return app++;
-                hbits = hw == 1 ? rm1 : (hw == 2 ? rm2 : rm3);
-            }
-        };
-        // kept particles above the new count
-        for (int j = nAll; j < n0; ++j) {
-            if ((rbits(j & ~3) >> (j & 3)) & 1u) continue;
-            const size_t s = ib + j;
-            const float2 v = B.vel[s];
-            const float2 o = B.off[s];
-            const int p = B.pid[s];
-            long long qx = fq_of(v.x) + shx, qy = fq_of(v.y) + shy;
-            if (p == mp) {
-                qx += remx;
-                qy += remy;
-            }
-            const int d = next_free();
-            B.off[ib + d] = o;
+        const int d = next_free();
+        if (d < K) {
+            B.off[ib + d] = A.recOffG[rs + k];
             B.vel[ib + d] = make_float2(fv_of(qx), fv_of(qy));
             B.pid[ib + d] = p;
         }
-        // arrivals
-        for (int k = 0; k < nr; ++k) {
-            const int r = M.recList[rs + k];
-            const int p = M.recPid[r];
-            const int2 q = M.recV[r];
-            long long qx = q.x + shx, qy = q.y + shy;
-            if (p == mp) {
-                qx += remx;
-                qy += remy;
-            }
-            const int d = next_free();
-            if (d < K) {
-                B.off[ib + d] = M.recOff[r];
-                B.vel[ib + d] = make_float2(fv_of(qx), fv_of(qy));
-                B.pid[ib + d] = p;
-            }
-        }
     }
-    __syncwarp();
 }
 
 __global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneArgs A) {
@@ -1219,8 +1672,8 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneAr
         for (int q = 0; q < L && !Z.failed; ++q) Z.sparse_cell(M.ord[q]);
     }
     __syncwarp();
-    // output with the momentum correction
-    fast_zone_output(Z);
+    // the decisions for the apply kernel
+    fast_zone_export(Z);
     if (lane == 0) {
         if (Z.movedDense || Z.movedSparse) {
             atomicAdd(A.moved, Z.movedDense);

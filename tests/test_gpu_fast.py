@@ -13,6 +13,8 @@ oracle. It is held to what it promises instead:
     occupancy spread agree with the plain FP64 form within the plain form's own seed-to-seed
     spread.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -79,6 +81,28 @@ def test_momentum_exact_without_kicks():
             Pk = np.round(vk * Q).astype(np.int64).reshape(-1, 2).sum(axis=0)
             assert np.array_equal(Pk, P0), (k, Pk - P0)
     assert moved > 0
+
+
+def test_collision_spill_path_matches_tiles():
+    """SRD tiles whose standard cells hold more particles than the tile kernel's shared memory
+    are collided by the spill kernel; sending every tile there gives the same state."""
+    native = _native()
+    p = poiseuille_params(70, 45, 12)
+    x, v = uniform_state(p, 6)
+    out = []
+    for pcap in (None, "64"):
+        if pcap:
+            os.environ["MPCD_FAST_COLLIDE_PCAP"] = pcap
+        try:
+            with native.Context(p, form="fast") as ctx:
+                ctx.set_state(x, v)
+                ctx.step(0, 6)
+                out.append(ctx.get_state())
+        finally:
+            os.environ.pop("MPCD_FAST_COLLIDE_PCAP", None)
+    (x1, v1), (x2, v2) = out
+    assert not np.isnan(v1).any()
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
 
 
 def _profile(native, p, seed, form, steps, avg_from):
