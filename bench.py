@@ -67,15 +67,18 @@ PHASE_BYTES = {
     "ref_fields": (20, 96),     # read slot 4, v 16 | 10 field arrays + start
     "closure_cells": (20, 64),
 }
-# the fast form: FP32 bins (offset 8, velocity 8, id 4 bytes per particle)
+# the fast form: FP32 bins (offset 8, velocity 8, id 4 bytes per particle); bytes per step of
+# each phase (its kernels together)
 PHASE_BYTES_FAST = {
-    "stream_bc": (40, 8),       # read 20 B, write 20 B | count, kick 8 per cell
-    "collide": (28, 4),         # read offset, velocity, id 20; write velocity 8 | count
-    "zone_pass": (40, 40),      # read 20, write 20 | counts in and out 8, cell sums 32
+    "stream_bc": (40, 16),      # read 20 B, write 20 B | count read, count claimed, kick 16 per cell
+    "collide": (28, 4),         # tiles read offset, velocity, id 20; write velocity 8 | count
+    "zone_pass": (20, 128),     # both passes: base reads velocity and id 12, rewrites velocities 8 |
+                                # counts, summaries, momentum sums and reference sums 128 per cell
     "closure_cells": (0, 92),   # reference and red sums 48 + counts 4; pdrive, duRepair, beta terms 40
     "kick_resort": (0, 48),     # pressure drive and duRepair read 24 (+ stencil), kick written 8
 }
 LAUNCHES_PER_STEP = {"zone_pass": 2, "cell_index": 4}
+LAUNCHES_PER_STEP_FAST = {}
 
 
 def env_int(k, d):
@@ -230,7 +233,8 @@ def roofline(phases, KP, p, table, form):
     """Roofline of the dominant kernel: its algorithmic bytes per launch over its live launch time."""
     peak, peak_src = measured_peaks()
     dom = max((k for k in phases if k in table), key=lambda k: phases[k])
-    per_launch_s = phases[dom] / (KP * LAUNCHES_PER_STEP.get(dom, 1))
+    launches = (LAUNCHES_PER_STEP if form == "f64" else LAUNCHES_PER_STEP_FAST).get(dom, 1)
+    per_launch_s = phases[dom] / (KP * launches)
     bp, bc = table[dom]
     alg = bp * p["n"] + bc * p["Nc"]
     achieved = alg / per_launch_s / 1e9

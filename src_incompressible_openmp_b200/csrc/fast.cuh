@@ -888,7 +888,7 @@ struct FastZoneMem {
     int* rfill;        // cell: records filed so far
     uint16_t* recSrc;  // recCap: (origin cell << 7) | slot
     uint8_t* recCur;   // recCap: current cell
-    float2* recOff;    // recCap: position in the current cell
+    uint32_t* recDraw; // recCap: the draw of the position in the current cell (salt << 8 | k)
     float* nsm;        // nsmCap: smoothed occupancy of the zone and a one-cell ring
     uint32_t* keys;    // 128: order keys of the dense / low cells; the output's hole slots
     uint8_t* ord;      // 128: those cells in key order
@@ -906,7 +906,7 @@ struct FastZoneMem {
         take((size_t)maxCells * 4, 4);
         take((size_t)recCap * 2, 2);
         take((size_t)recCap, 1);
-        take((size_t)recCap * 8, 8);
+        take((size_t)recCap * 4, 4);
         take((size_t)nsmCap * 4, 4);
         take(128 * 4, 4);
         take(128, 1);
@@ -940,7 +940,7 @@ struct FastZoneMem {
         rfill = (int*)p[10];
         recSrc = (uint16_t*)p[11];
         recCur = (uint8_t*)p[12];
-        recOff = (float2*)p[13];
+        recDraw = (uint32_t*)p[13];
         nsm = (float*)p[14];
         keys = (uint32_t*)p[15];
         ord = (uint8_t*)p[16];
@@ -950,6 +950,14 @@ struct FastZoneMem {
 };
 
 constexpr uint8_t kZBulkD = 1, kZBulkS = 2, kZRecv = 4, kZBB = 8, kZSkip = 16;
+
+// A moved particle's position in its new cell: two 24-bit uniforms of one draw of the zone's
+// stream, keyed by the operation's salt and the move's index k in it (draw = salt << 8 | k)
+__device__ __forceinline__ float2 zone_draw_pos(uint64_t zseed, uint32_t draw) {
+    const uint64_t hp = fmix64(zseed ^ ((uint64_t)(draw >> 8) << 20) ^ (0x504F53ULL + (uint64_t)(draw & 0xFFu)));
+    return make_float2(fminf((float)(hp >> 40) * 0x1.0p-24f, kFastOffMax),
+                       fminf((float)((hp >> 8) & 0xFFFFFFu) * 0x1.0p-24f, kFastOffMax));
+}
 
 struct FastZone {
     const FastZoneArgs* A;
@@ -1026,10 +1034,8 @@ struct FastZone {
             }
             best = warp_min_u64_r(best);
             if (best == ~0ULL) return;  // no member left (cannot happen while counts agree)
-            // the new position: two 24-bit uniforms of one draw
-            const uint64_t hp = fmix64(zseed ^ ((uint64_t)salt << 20) ^ (0x504F53ULL + (uint64_t)k));
-            const float2 pos = make_float2(fminf((float)(hp >> 40) * 0x1.0p-24f, kFastOffMax),
-                                           fminf((float)((hp >> 8) & 0xFFFFFFu) * 0x1.0p-24f, kFastOffMax));
+            // the new position: the draw (salt, k), evaluated when the record is exported
+            const uint32_t draw = (salt << 8) | (uint32_t)k;
             if (!(best & 512ULL)) {  // an original of cell l
                 const int j = (int)(best & 511ULL);
                 if (nrec >= A->recCap) {
@@ -1044,14 +1050,14 @@ struct FastZone {
                     M.recPid[nrec] = (int)((best >> 10) & 0x7fffffffULL);
                     M.recSrc[nrec] = (uint16_t)((l << 7) | j);
                     M.recCur[nrec] = (uint8_t)t;
-                    M.recOff[nrec] = pos;
+                    M.recDraw[nrec] = draw;
                     M.nrecv[t] += 1;
                 }
                 ++nrec;
             } else if (lane == 0) {  // an arrival in cell l moves on
                 const int r = (int)(best & 511ULL);
                 M.recCur[r] = (uint8_t)t;
-                M.recOff[r] = pos;
+                M.recDraw[r] = draw;
                 M.nrecv[l] -= 1;
                 M.nrecv[t] += 1;
             }
@@ -1141,13 +1147,11 @@ struct FastZone {
                 const int t = M.tgt[lane];
                 const int j = (int)(mine & 511ULL);
                 const uint32_t salt = op + 1 + (uint32_t)lane;
-                const uint64_t hp = fmix64(zseed ^ ((uint64_t)salt << 20) ^ 0x504F53ULL);
                 const int rec = nrec + lane;
                 M.recPid[rec] = (int)((mine >> 10) & 0x7fffffffULL);
                 M.recSrc[rec] = (uint16_t)((l << 7) | j);
                 M.recCur[rec] = (uint8_t)t;
-                M.recOff[rec] = make_float2(fminf((float)(hp >> 40) * 0x1.0p-24f, kFastOffMax),
-                                            fminf((float)((hp >> 8) & 0xFFFFFFu) * 0x1.0p-24f, kFastOffMax));
+                M.recDraw[rec] = salt << 8;
                 M.nrecv[t] += 1;
                 add_cnt(t, 1);
                 atomicOr(&M.rm[4 * l + (j >> 5)], 1u << (j & 31));
@@ -1398,7 +1402,7 @@ __device__ void fast_zone_export(FastZone& Z) {
         const float2 v = A.b.vel[(size_t)Z.gcell(src >> 7) * K + (src & 127)];
         const size_t g = zb + M.recStart[l] + atomicAdd(M.rfill + l, 1);
         A.recPidG[g] = M.recPid[r];
-        A.recOffG[g] = M.recOff[r];
+        A.recOffG[g] = zone_draw_pos(Z.zseed, M.recDraw[r]);
         A.recQG[g] = make_int2(fq_of(v.x), fq_of(v.y));
     }
     for (int l = lane; l < nl; l += 32) {
@@ -1590,7 +1594,7 @@ __global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
     }
 }
 
-__global__ void __launch_bounds__(32 * kFastZoneWarps, 5) k_fast_zone(FastZoneArgs A) {
+__global__ void __launch_bounds__(32 * kFastZoneWarps, 6) k_fast_zone(FastZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int wib = threadIdx.x >> 5;
     const int z = blockIdx.x * kFastZoneWarps + wib;
