@@ -946,6 +946,12 @@ struct FastZoneMem {
         ord = (uint8_t*)p[16];
         tgt = (int*)p[17];
         tgt2 = (int*)p[18];
+        // all of them in shared memory (lets the compiler use shared-space accesses)
+        __builtin_assume(__isShared(win) && __isShared(wi) && __isShared(cx) && __isShared(cy) && __isShared(n0) &&
+                         __isShared(flg) && __isShared(nrecv) && __isShared(rm) && __isShared(recPid) &&
+                         __isShared(recStart) && __isShared(rfill) && __isShared(recSrc) && __isShared(recCur) &&
+                         __isShared(recDraw) && __isShared(nsm) && __isShared(keys) && __isShared(ord) &&
+                         __isShared(tgt) && __isShared(tgt2));
     }
 };
 
