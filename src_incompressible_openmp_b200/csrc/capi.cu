@@ -188,7 +188,8 @@ struct mpcd_ctx {
     int* fmoved = nullptr;  // base dense, base sparse, shifted dense, shifted sparse, zones out of records
     int4* frects[2] = {nullptr, nullptr};
     int fnz[2] = {0, 0};
-    int fzMaxCells = 0, fzWinCap = 0, fzNsmCap = 0, fzRecCap = 0;
+    int zSyncWarps = 0;  // zones per block of the phase-synchronous zone pass (0: one per block)
+    int fzMaxCells = 0, fzWinCap = 0, fzNsmCap = 0, fzRecCap = 0, fzWarps = 8;
     size_t fzSmem = 0;
     // zone decisions handed to the apply kernel: per cell summary and removal masks, per zone records
     unsigned long long* fzMeta = nullptr;
@@ -980,10 +981,22 @@ int zone_pass_prep(mpcd_ctx* c, int mode, uint64_t seedBase, Prof* pf = nullptr)
 
 int zone_pass_kernel(mpcd_ctx* c) {
     const ZoneArgs& A = c->zA;
-    if (c->f32)
+    const int W = c->zSyncWarps;
+    const int per = (int)c->zSmem;
+    const int blocks = W > 0 ? (A.nZones + W - 1) / W : 0;
+#define MPCD_ZONE_SYNC(F, K) k_zone_pass_sync<F, K><<<blocks, 32 * K, (size_t)K * per, c->stream>>>(A, per)
+    if (W == 16) {
+        if (c->f32) MPCD_ZONE_SYNC(true, 16); else MPCD_ZONE_SYNC(false, 16);
+    } else if (W == 8) {
+        if (c->f32) MPCD_ZONE_SYNC(true, 8); else MPCD_ZONE_SYNC(false, 8);
+    } else if (W == 4) {
+        if (c->f32) MPCD_ZONE_SYNC(true, 4); else MPCD_ZONE_SYNC(false, 4);
+    } else if (c->f32) {
         k_zone_pass<true><<<A.nZones, 32, c->zSmem, c->stream>>>(A);
-    else
+    } else {
         k_zone_pass<false><<<A.nZones, 32, c->zSmem, c->stream>>>(A);
+    }
+#undef MPCD_ZONE_SYNC
     ++c->launches;
     CUDA_TRY(cudaGetLastError());
     return MPCD_OK;
@@ -1452,6 +1465,29 @@ int mpcd_ctx_create_form(const mpcd_params_c* params, int device, int32_t form, 
             !raise_smem((const void*)k_zone_pass<true>, c->zSmem, device) ||
             !raise_smem((const void*)k_zone_serial, c->zSmem, device))
             return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
+        // the phase-synchronous kernel: the most warps per block (16, 8 or 4) whose working
+        // sets fit in 200 KB; MPCD_ZONE_SYNC_WARPS picks another (0: one zone per block)
+        c->zSyncWarps = 0;
+        if (c->zMaxCells > 0)
+            for (int W : {16, 8, 4})
+                if ((size_t)W * c->zSmem <= 200 * 1024) {
+                    c->zSyncWarps = W;
+                    break;
+                }
+        if (const char* e = std::getenv("MPCD_ZONE_SYNC_WARPS")) {
+            const int v = std::atoi(e);
+            if ((v == 0 || v == 4 || v == 8 || v == 16) && (size_t)v * c->zSmem <= 200 * 1024) c->zSyncWarps = v;
+        }
+        bool okSync = true;
+#define MPCD_ZONE_SYNC_ATTR(K)                                                                         \
+        if (c->zSyncWarps == K)                                                                        \
+            okSync = raise_smem((const void*)k_zone_pass_sync<false, K>, (size_t)K * c->zSmem, device) && \
+                     raise_smem((const void*)k_zone_pass_sync<true, K>, (size_t)K * c->zSmem, device);
+        MPCD_ZONE_SYNC_ATTR(4)
+        MPCD_ZONE_SYNC_ATTR(8)
+        MPCD_ZONE_SYNC_ATTR(16)
+#undef MPCD_ZONE_SYNC_ATTR
+        if (!okSync) return fail(set_err(MPCD_ERR_CUDA, "zone shared memory attribute"));
         c->ovMaxCells = maxArea;
         c->ovWinCap = (maxTX + 4) * (maxTY + 4);
         c->ovNsmCap = (maxTX + 2) * (maxTY + 2);

@@ -40,7 +40,7 @@ constexpr double kFastInvQ = 1.0 / 1048576.0;
 constexpr float kFastOffMax = 0x1.fffffep-1f;  // largest float below 1
 constexpr int kFastMaxK = 128;                 // bin capacity limit (removal masks of 4 words)
 constexpr int kFastMaxZoneCells = 128;         // zone cells (dense/low orders sort 128 keys)
-constexpr int kFastZoneWarps = 4;              // zones per block of the zone kernel
+constexpr int kFastZoneWarps = 8;              // zones per block of the zone decision kernel
 constexpr int kErrBinCapacity = 13;            // a cell above its bin capacity
 constexpr int kErrRecordCapacity = 14;         // a zone's moves outgrew its record area
 
@@ -1600,73 +1600,84 @@ __global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
     }
 }
 
-__global__ void __launch_bounds__(32 * kFastZoneWarps, 6) k_fast_zone(FastZoneArgs A) {
+// kW zones per block, in step: a block barrier after the set-up, after each dense pass and
+// after the sparse phase, so that the resident warps of an SM execute the same phase's code
+template <int kW>
+__global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int wib = threadIdx.x >> 5;
-    const int z = blockIdx.x * kFastZoneWarps + wib;
-    if (z >= A.nZones) return;
+    const int z = blockIdx.x * kW + wib;
     FastZone Z;
     Z.A = &A;
     Z.lane = threadIdx.x & 31;
     Z.z = z;
     const int lane = Z.lane;
     const DevParams& P = A.P;
-    const int4 R = A.rects[z];
-    Z.x0 = R.x; Z.x1 = R.y; Z.y0 = R.z; Z.y1 = R.w;
-    Z.TX = Z.x1 - Z.x0; Z.TY = Z.y1 - Z.y0; Z.nl = Z.TX * Z.TY; Z.WY = Z.TY + 4;
-    Z.zseed = fhash(A.S->seed, (uint64_t)z, 0x5A4F4E45ULL + (uint64_t)A.pass);
-    Z.op = 0;
-    Z.nrec = 0;
     Z.failed = false;
-    Z.movedDense = Z.movedSparse = 0;
-    if (Z.nl > A.maxCells || (Z.TX + 4) * Z.WY > A.winCap || (Z.TX + 2) * (Z.TY + 2) > A.nsmCap) {
-        if (lane == 0) raise_error(A.st, kErrZoneCapacity, z);
-        return;
+    bool ok = z < A.nZones;
+    if (ok) {
+        const int4 R = A.rects[z];
+        Z.x0 = R.x; Z.x1 = R.y; Z.y0 = R.z; Z.y1 = R.w;
+        Z.TX = Z.x1 - Z.x0; Z.TY = Z.y1 - Z.y0; Z.nl = Z.TX * Z.TY; Z.WY = Z.TY + 4;
+        Z.zseed = fhash(A.S->seed, (uint64_t)z, 0x5A4F4E45ULL + (uint64_t)A.pass);
+        Z.op = 0;
+        Z.nrec = 0;
+        Z.movedDense = Z.movedSparse = 0;
+        if (Z.nl > A.maxCells || (Z.TX + 4) * Z.WY > A.winCap || (Z.TX + 2) * (Z.TY + 2) > A.nsmCap) {
+            if (lane == 0) raise_error(A.st, kErrZoneCapacity, z);
+            ok = false;
+        }
     }
-    const size_t per = FastZoneMem::bytes(A.maxCells, A.winCap, A.nsmCap, A.recCap);
-    Z.M.carve(smem + per * wib, A.maxCells, A.winCap, A.nsmCap, A.recCap);
     FastZoneMem& M = Z.M;
-    // pass-input counts of the window (wrapped on periodic axes, -1 outside the domain)
-    const int W = (Z.TX + 4) * Z.WY;
-    for (int w = lane; w < W; w += 32) {
-        int gx = Z.x0 - 2 + w / Z.WY, gy = Z.y0 - 2 + w % Z.WY;
-        if (P.perx) gx = wrap_index(gx, P.Nx);
-        if (P.pery) gy = wrap_index(gy, P.Ny);
-        const bool ok = gx >= 0 && gx < P.Nx && gy >= 0 && gy < P.Ny;
-        M.win[w] = ok ? (short)min(A.cntIn[gy + P.Ny * gx], A.F.K) : (short)-1;
-    }
-    for (int l = lane; l < Z.nl; l += 32) {
-        const int lx = l / Z.TY, ly = l - lx * Z.TY;
-        M.cx[l] = (uint8_t)lx;
-        M.cy[l] = (uint8_t)ly;
-        M.wi[l] = (uint16_t)((lx + 2) * Z.WY + (ly + 2));
-    }
-    __syncwarp();
-    for (int l = lane; l < Z.nl; l += 32) {
-        M.n0[l] = (uint8_t)Z.cnt(l);
-        M.flg[l] = 0;
-        M.nrecv[l] = 0;
-        M.rm[4 * l] = M.rm[4 * l + 1] = M.rm[4 * l + 2] = M.rm[4 * l + 3] = 0;
-    }
-    __syncwarp();
-    // dense passes (src/zone_pass.cpp:708-781): cells above their high map, in random order
-    for (int pass = 0; pass < P.maxPasses && !Z.failed; ++pass) {
+    if (ok) {
+        const size_t per = FastZoneMem::bytes(A.maxCells, A.winCap, A.nsmCap, A.recCap);
+        Z.M.carve(smem + per * wib, A.maxCells, A.winCap, A.nsmCap, A.recCap);
+        // pass-input counts of the window (wrapped on periodic axes, -1 outside the domain)
+        const int W = (Z.TX + 4) * Z.WY;
+        for (int w = lane; w < W; w += 32) {
+            int gx = Z.x0 - 2 + w / Z.WY, gy = Z.y0 - 2 + w % Z.WY;
+            if (P.perx) gx = wrap_index(gx, P.Nx);
+            if (P.pery) gy = wrap_index(gy, P.Ny);
+            const bool in = gx >= 0 && gx < P.Nx && gy >= 0 && gy < P.Ny;
+            M.win[w] = in ? (short)min(A.cntIn[gy + P.Ny * gx], A.F.K) : (short)-1;
+        }
         for (int l = lane; l < Z.nl; l += 32) {
-            const bool bulk = Z.cnt(l) > 0;
-            M.flg[l] = (uint8_t)((M.flg[l] & ~kZBulkD) | (bulk ? kZBulkD : 0));
+            const int lx = l / Z.TY, ly = l - lx * Z.TY;
+            M.cx[l] = (uint8_t)lx;
+            M.cy[l] = (uint8_t)ly;
+            M.wi[l] = (uint16_t)((lx + 2) * Z.WY + (ly + 2));
         }
         __syncwarp();
-        const int D = Z.order_cells([&](int i) -> uint32_t {
-            const bool bulk = M.flg[i] & kZBulkD;
-            if ((double)Z.cnt(i) > Z.high_map(bulk))
-                return ((uint32_t)fhash(Z.zseed, 0x44454EULL + (uint64_t)pass, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
-            return 0xFFFFFFFFu;
-        });
-        for (int q = 0; q < D && !Z.failed; ++q) Z.dense_cell(M.ord[q]);
+        for (int l = lane; l < Z.nl; l += 32) {
+            M.n0[l] = (uint8_t)Z.cnt(l);
+            M.flg[l] = 0;
+            M.nrecv[l] = 0;
+            M.rm[4 * l] = M.rm[4 * l + 1] = M.rm[4 * l + 2] = M.rm[4 * l + 3] = 0;
+        }
         __syncwarp();
     }
+    __syncthreads();
+    // dense passes (src/zone_pass.cpp:708-781): cells above their high map, in random order
+    for (int pass = 0; pass < P.maxPasses; ++pass) {
+        if (ok && !Z.failed) {
+            for (int l = lane; l < Z.nl; l += 32) {
+                const bool bulk = Z.cnt(l) > 0;
+                M.flg[l] = (uint8_t)((M.flg[l] & ~kZBulkD) | (bulk ? kZBulkD : 0));
+            }
+            __syncwarp();
+            const int D = Z.order_cells([&](int i) -> uint32_t {
+                const bool bulk = M.flg[i] & kZBulkD;
+                if ((double)Z.cnt(i) > Z.high_map(bulk))
+                    return ((uint32_t)fhash(Z.zseed, 0x44454EULL + (uint64_t)pass, (uint64_t)i) & 0xFFFFFF00u) | (uint32_t)i;
+                return 0xFFFFFFFFu;
+            });
+            for (int q = 0; q < D && !Z.failed; ++q) Z.dense_cell(M.ord[q]);
+            __syncwarp();
+        }
+        __syncthreads();
+    }
     // sparse phase (src/zone_pass.cpp:783-854)
-    if (!Z.failed) {
+    if (ok && !Z.failed) {
         for (int l = lane; l < Z.nl; l += 32) {
             const bool bulk = Z.cnt(l) > 0;
             M.flg[l] = (uint8_t)((M.flg[l] & ~kZBulkS) | (bulk ? kZBulkS : 0));
@@ -1681,7 +1692,8 @@ __global__ void __launch_bounds__(32 * kFastZoneWarps, 6) k_fast_zone(FastZoneAr
         });
         for (int q = 0; q < L && !Z.failed; ++q) Z.sparse_cell(M.ord[q]);
     }
-    __syncwarp();
+    __syncthreads();
+    if (!ok) return;
     // the decisions for the apply kernel
     fast_zone_export(Z);
     if (lane == 0) {

@@ -83,6 +83,60 @@ __device__ __forceinline__ Stencil stencil_of(const DevParams& P, const float4* 
     return S;
 }
 
+// The layer-1 operands of cell c as BF16 pairs: operand column k is channel k % 3 of stencil
+// point k / 3 (the values stencil_value gives, the stencil mean taken in the same order as
+// stencil_of), column 75 the bias input 1, columns 76-79 zero. The 25 points are read twice
+// (the mean, then the values), each as one float4.
+template <int kCols>
+__device__ __forceinline__ void stencil_operands(const DevParams& P, const float4* __restrict__ feat, int c,
+                                                 uint32_t (&w)[kCols / 2]) {
+    const int ix = c / P.Ny, iy = c - ix * P.Ny;
+    int col[5], row[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        int jx = ix + d - 2, jy = iy + d - 2;
+        if (P.perx) jx = wrap_index(jx, P.Nx);
+        col[d] = (jx >= 0 && jx < P.Nx) ? jx * P.Ny : -1;
+        if (P.pery) jy = wrap_index(jy, P.Ny);
+        row[d] = (jy >= 0 && jy < P.Ny) ? jy : -1;
+    }
+    float sx = 0.0f, sy = 0.0f;
+    int cnt = 0;
+#pragma unroll
+    for (int pnt = 0; pnt < 25; ++pnt) {
+        const int dy = pnt / 5, dx = pnt % 5;
+        if (col[dx] >= 0 && row[dy] >= 0) {
+            const float4 q = __ldg(feat + col[dx] + row[dy]);
+            sx += q.y;
+            sy += q.z;
+            ++cnt;
+        }
+    }
+    const float mx = sx / (float)cnt, my = sy / (float)cnt;  // the cell itself is always inside
+    float op[kCols];
+#pragma unroll
+    for (int pnt = 0; pnt < 25; ++pnt) {
+        const int dy = pnt / 5, dx = pnt % 5;
+        float a0 = -1.0f, a1 = 0.0f, a2 = 0.0f;
+        if (col[dx] >= 0 && row[dy] >= 0) {
+            const float4 q = __ldg(feat + col[dx] + row[dy]);
+            a0 = q.x;
+            a1 = q.y - mx;
+            a2 = q.z - my;
+        }
+        op[3 * pnt] = a0;
+        op[3 * pnt + 1] = a1;
+        op[3 * pnt + 2] = a2;
+    }
+#pragma unroll
+    for (int k = 75; k < kCols; ++k) op[k] = k == 75 ? 1.0f : 0.0f;
+#pragma unroll
+    for (int j = 0; j < kCols / 2; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(op[2 * j], op[2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+}
+
 // channel ch (0 N, 1 Ux, 2 Uy) of stencil point pnt (5 dy + dx)
 __device__ __forceinline__ float stencil_value(const Stencil& S, const float4* __restrict__ feat, int pnt, int ch) {
     const int dy = pnt / 5, dx = pnt - 5 * dy;
@@ -399,17 +453,14 @@ __global__ void __launch_bounds__(kTcThreads, 4)
     for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const int r = tile * kTcRows + t;
         const bool live = r < total;
-        Stencil S{};
-        // 1. layer-1 operands of row t
-        {
-            if (!kRows && live) S = stencil_of(P, feat, r);
-            // operand column k: stencil point k / 3, channel k % 3
+        // 1. layer-1 operands of row t (operand column k: stencil point k / 3, channel k % 3)
+        bool inside = true;  // the stencil stays inside the walls
+        if (kRows) {
             auto operand = [&](int k) -> float {
                 if (k >= kFeat) return k == kFeat ? 1.0f : 0.0f;
                 if (!live) return 0.0f;
                 const int pnt = k / 3, ch = k - 3 * pnt;
-                if (kRows) return X[(size_t)r * kFeat + ch * 25 + pnt];
-                return stencil_value(S, feat, pnt, ch);
+                return X[(size_t)r * kFeat + ch * 25 + pnt];
             };
 #pragma unroll
             for (int j = 0; j < kTcK1 / 8; ++j) {
@@ -418,6 +469,23 @@ __global__ void __launch_bounds__(kTcThreads, 4)
                 for (int q = 0; q < 4; ++q) w[q] = pack_bf16(operand(8 * j + 2 * q), operand(8 * j + 2 * q + 1));
                 *reinterpret_cast<uint4*>(sm + kTcOffA + kmajor_offset(t, 8 * j, kTcK1)) = make_uint4(w[0], w[1], w[2], w[3]);
             }
+        } else {
+            uint32_t w[kTcK1 / 2];
+            if (live) {
+                stencil_operands<kTcK1>(P, feat, r, w);
+                if (bulkOnly) {
+                    const int ix = r / P.Ny, iy = r - ix * P.Ny;
+                    inside = (P.perx || (ix >= 2 && ix < P.Nx - 2)) && (P.pery || (iy >= 2 && iy < P.Ny - 2));
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < kTcK1 / 2; ++j)
+                    w[j] = pack_bf16(2 * j == kFeat ? 1.0f : 0.0f, 2 * j + 1 == kFeat ? 1.0f : 0.0f);
+            }
+#pragma unroll
+            for (int j = 0; j < kTcK1 / 8; ++j)
+                *reinterpret_cast<uint4*>(sm + kTcOffA + kmajor_offset(t, 8 * j, kTcK1)) =
+                    make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
         }
         tc_fence_smem_async();
         tc_fence_before();
@@ -488,9 +556,6 @@ __global__ void __launch_bounds__(kTcThreads, 4)
         }
         tc_fence_before();  // the next tile's MMAs overwrite these columns after the barrier
         if (!kRows && bulkOnly) {  // no learned kick where the stencil crosses a wall
-            bool inside = true;
-#pragma unroll
-            for (int d = 0; d < 5; ++d) inside = inside && S.col[d] >= 0 && S.row[d] >= 0;
             // bulkOnly 2: a NaN marks the cell, whose kick the caller computes itself
             if (!inside) o0 = o1 = (bulkOnly == 2) ? __int_as_float(0x7fc00000) : 0.0f;
         }

@@ -1109,10 +1109,15 @@ __device__ __forceinline__ void serial_finish(ZoneState<I, kF32>& S, const ZoneA
 }
 
 // ------------------------------------------------------------------ the zone body
-// Returns false if the zone must be re-run on the overflow path.
-template <bool kSerial, typename I, bool kF32 = false>
-__device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap, int nsmCap) {
-    ZoneState<I, kF32> S;
+// The zone body in four phases: set-up (the pass-input counts around the zone, the cells'
+// segments and ownership, the draw stream), one dense pass, the sparse phase, and the output
+// (momentum correction and the zone's stats). zone_body runs them back to back; the
+// phase-synchronous kernel runs the zones of a block in step, a barrier between phases.
+
+// Set-up; false if the zone must be re-run on the overflow path.
+template <bool kSerial, typename I, bool kF32>
+__device__ __forceinline__ bool zone_setup(ZoneState<I, kF32>& S, const ZoneArgs& A, int z, char* mem, int maxCells,
+                                           int winCap, int arenaCap, int nsmCap) {
     S.A = &A;
     S.lane = threadIdx.x & 31;
     S.zone = z;
@@ -1203,29 +1208,48 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     }
     __syncwarp();
     S.rng.init(M.mt, M.carry, A.seeds + (size_t)z * kMtN, lane);
+    return true;
+}
 
-    // dense passes (src/zone_pass.cpp:708-781)
-    int nHighAll = 0, nLowAll = 0;  // dense cells over the passes, sparse cells (stats[0], stats[1])
-    for (int pass = 0; pass < p.maxPasses && !S.failed && !S.fatal; ++pass) {
-        if (p.useLFF) S.compute_nsm();
-        S.mark_bulk();
-        const int nd = S.collect([&](int l) { return (double)M.len[l] > S.map_high(l); });
-        nHighAll += nd;
-        zone_shuffle_fast(M.list, nd, S.rng, lane);
-        for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
-    }
-    // sparse phase (src/zone_pass.cpp:783-854)
-    if (!S.failed && !S.fatal) {
-        // the smoothed occupancy feeds the maps only with local fluid-fraction thresholds;
-        // otherwise it is needed only if some cell is sparse (inward gradient, donor scores)
-        if (p.useLFF) S.compute_nsm();
-        S.mark_bulk();
-        const int nlow = S.collect([&](int l) { return M.len[l] > 0 && (double)M.len[l] < S.map_low(l); });
-        nLowAll = nlow;
-        if (!p.useLFF && nlow > 0) S.compute_nsm();
-        zone_shuffle_fast(M.list, nlow, S.rng, lane);
-        for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
-    }
+// One dense pass (src/zone_pass.cpp:708-781): the cells above their high map, in shuffled
+// order. Returns how many.
+template <typename I, bool kF32>
+__device__ __forceinline__ int zone_dense_pass(ZoneState<I, kF32>& S) {
+    const int lane = S.lane;
+    const DevParams& p = S.A->P;
+    ZoneMem<I>& M = S.M;
+    if (p.useLFF) S.compute_nsm();
+    S.mark_bulk();
+    const int nd = S.collect([&](int l) { return (double)M.len[l] > S.map_high(l); });
+    zone_shuffle_fast(M.list, nd, S.rng, lane);
+    for (int q = 0; q < nd && !S.failed && !S.fatal; ++q) S.dense_cell((int)M.list[q]);
+    return nd;
+}
+
+// The sparse phase (src/zone_pass.cpp:783-854). Returns the sparse cells.
+template <typename I, bool kF32>
+__device__ __forceinline__ int zone_sparse(ZoneState<I, kF32>& S) {
+    const int lane = S.lane;
+    const DevParams& p = S.A->P;
+    ZoneMem<I>& M = S.M;
+    // the smoothed occupancy feeds the maps only with local fluid-fraction thresholds;
+    // otherwise it is needed only if some cell is sparse (inward gradient, donor scores)
+    if (p.useLFF) S.compute_nsm();
+    S.mark_bulk();
+    const int nlow = S.collect([&](int l) { return M.len[l] > 0 && (double)M.len[l] < S.map_low(l); });
+    if (!p.useLFF && nlow > 0) S.compute_nsm();
+    zone_shuffle_fast(M.list, nlow, S.rng, lane);
+    for (int q = 0; q < nlow && !S.failed && !S.fatal; ++q) S.sparse_cell((int)M.list[q]);
+    return nlow;
+}
+
+// Output: the momentum correction and the zone's stats; false if the zone must be re-run on the
+// overflow path.
+template <bool kSerial, typename I, bool kF32>
+__device__ __forceinline__ bool zone_finish(ZoneState<I, kF32>& S, const ZoneArgs& A, int z, int nHighAll, int nLowAll) {
+    const int lane = S.lane;
+    const DevParams& p = A.P;
+    ZoneMem<I>& M = S.M;
     if (S.fatal) return true;
     if (S.failed) return false;
 
@@ -1363,6 +1387,17 @@ __device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int
     return true;
 }
 
+// Returns false if the zone must be re-run on the overflow path.
+template <bool kSerial, typename I, bool kF32 = false>
+__device__ bool zone_body(const ZoneArgs& A, int z, char* mem, int maxCells, int winCap, int arenaCap, int nsmCap) {
+    ZoneState<I, kF32> S;
+    if (!zone_setup<kSerial>(S, A, z, mem, maxCells, winCap, arenaCap, nsmCap)) return false;
+    int nHighAll = 0, nLowAll = 0;  // dense cells over the passes, sparse cells (stats[0], stats[1])
+    for (int pass = 0; pass < A.P.maxPasses && !S.failed && !S.fatal; ++pass) nHighAll += zone_dense_pass(S);
+    if (!S.failed && !S.fatal) nLowAll = zone_sparse(S);
+    return zone_finish<kSerial>(S, A, z, nHighAll, nLowAll);
+}
+
 // kF32: the FP32 precision form's state (A.in32, A.out32)
 template <bool kF32>
 __global__ void __launch_bounds__(32, 20) k_zone_pass(ZoneArgs A) {
@@ -1370,6 +1405,34 @@ __global__ void __launch_bounds__(32, 20) k_zone_pass(ZoneArgs A) {
     if ((int)blockIdx.x >= A.nZones) return;
     const int z = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
     if (!zone_body<false, uint16_t, kF32>(A, z, smem, A.maxCells, A.winCap, A.arenaCap, A.nsmCap) && (threadIdx.x & 31) == 0)
+        A.overflow[atomicAdd(A.nOverflow, 1)] = z;
+}
+
+// Phase-synchronous zone pass: kW zones per block, consecutive entries of the launch order
+// (heaviest first, so the zones of a block cost about the same), run in step with a block
+// barrier after the set-up, after each dense pass and after the sparse phase. The resident
+// warps of an SM then execute the same phase's code (the body is too large for the
+// instruction cache as a whole). Each warp carves its working set at perWarp bytes.
+template <bool kF32, int kW>
+__global__ void __launch_bounds__(32 * kW) k_zone_pass_sync(ZoneArgs A, int perWarp) {
+    extern __shared__ __align__(16) char smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = (int)blockIdx.x * kW + w;
+    const bool have = slot < A.nZones;
+    const int z = have ? (A.order ? A.order[slot] : slot) : 0;
+    ZoneState<uint16_t, kF32> S;
+    S.failed = S.fatal = false;
+    const bool ok = have && zone_setup<false>(S, A, z, smem + (size_t)perWarp * w, A.maxCells, A.winCap, A.arenaCap,
+                                               A.nsmCap);
+    int nHighAll = 0, nLowAll = 0;
+    __syncthreads();
+    for (int pass = 0; pass < A.P.maxPasses; ++pass) {
+        if (ok && !S.failed && !S.fatal) nHighAll += zone_dense_pass(S);
+        __syncthreads();
+    }
+    if (ok && !S.failed && !S.fatal) nLowAll = zone_sparse(S);
+    __syncthreads();
+    if (have && !(ok && zone_finish<false>(S, A, z, nHighAll, nLowAll)) && lane == 0)
         A.overflow[atomicAdd(A.nOverflow, 1)] = z;
 }
 
