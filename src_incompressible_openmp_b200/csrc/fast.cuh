@@ -957,6 +957,26 @@ struct FastZoneMem {
 
 constexpr uint8_t kZBulkD = 1, kZBulkS = 2, kZRecv = 4, kZBB = 8, kZSkip = 16;
 
+// A source cell's candidates, one per original slot j in lane j % 32: register j / 32 holds
+// slot lane + 32 (j / 32). Four named registers (an indexed array would live in local memory).
+struct Cands {
+    unsigned long long r0, r1, r2, r3;
+    __device__ __forceinline__ unsigned long long lowest() const {
+        const unsigned long long x = r0 < r1 ? r0 : r1, y = r2 < r3 ? r2 : r3;
+        return x < y ? x : y;
+    }
+    __device__ __forceinline__ void set(int r, unsigned long long v) {
+        r0 = r == 0 ? v : r0;
+        r1 = r == 1 ? v : r1;
+        r2 = r == 2 ? v : r2;
+        r3 = r == 3 ? v : r3;
+    }
+    // removes original slot j (its lane clears it)
+    __device__ __forceinline__ void take(int j, int lane) {
+        if ((j & 31) == lane) set(j >> 5, ~0ULL);
+    }
+};
+
 // A moved particle's position in its new cell: two 24-bit uniforms of one draw of the zone's
 // stream, keyed by the operation's salt and the move's index k in it (draw = salt << 8 | k)
 __device__ __forceinline__ float2 zone_draw_pos(uint64_t zseed, uint32_t draw) {
@@ -1004,16 +1024,17 @@ struct FastZone {
     // j % 32, register j / 32. A candidate is (key << 10) | (record flag << 9) | index: keys of at
     // most 54 bits whose low 31 bits are the particle id, original slots below 128 and records
     // below 512.
-    __device__ __forceinline__ void load_candidates(int l, bool dense, uint32_t salt, unsigned long long (&cand)[4]) const {
+    __device__ __forceinline__ void load_candidates(int l, bool dense, uint32_t salt, Cands& cand) const {
         const FastBins& B = A->b;
         const size_t ib = (size_t)gcell(l) * A->F.K;
         const int n0 = M.n0[l];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int j = lane + 32 * r;
-            cand[r] = ~0ULL;
+            unsigned long long v = ~0ULL;
             if (j < n0 && !(M.rm[4 * l + r] & (1u << lane)))
-                cand[r] = (member_key(dense, salt, (uint32_t)B.pid[ib + j], -1) << 10) | (unsigned long long)j;
+                v = (member_key(dense, salt, (uint32_t)B.pid[ib + j], -1) << 10) | (unsigned long long)j;
+            cand.set(r, v);
         }
     }
 
@@ -1022,14 +1043,12 @@ struct FastZone {
     // then the arrivals in order: src/zone_pass.cpp:541-583 takes the first ids), from the
     // candidates the caller loaded once for the cell; otherwise members chosen uniformly at
     // random (the sparse phase shuffles the donor's list) from candidates keyed afresh.
-    __device__ __forceinline__ void move_members(int l, int t, int nt, bool dense, unsigned long long (&cand)[4]) {
+    __device__ __forceinline__ void move_members(int l, int t, int nt, bool dense, Cands& cand) {
         const uint32_t salt = ++op;
         if (!dense) load_candidates(l, false, salt, cand);
         for (int k = 0; k < nt; ++k) {
             if (failed) return;
-            unsigned long long best = cand[0];
-#pragma unroll
-            for (int r = 1; r < 4; ++r) best = cand[r] < best ? cand[r] : best;
+            unsigned long long best = cand.lowest();
             if (M.nrecv[l] > 0) {
                 for (int r = lane; r < nrec; r += 32) {
                     if (M.recCur[r] != l) continue;
@@ -1048,9 +1067,7 @@ struct FastZone {
                     failed = true;
                     return;
                 }
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (r == (j >> 5) && (j & 31) == lane) cand[r] = ~0ULL;
+                cand.take(j, lane);
                 if (lane == 0) {
                     M.rm[4 * l + (j >> 5)] |= 1u << (j & 31);
                     M.recPid[nrec] = (int)((best >> 10) & 0x7fffffffULL);
@@ -1074,7 +1091,7 @@ struct FastZone {
     // spread_particles_from_dense_source_round_robin (src/zone_pass.cpp:527-589) over the
     // targets ranked as rank_dense_targets_unified does (:436-490); map: 0 low, 1 high.
     // Returns the particles moved; the receivers go to rcv[*nr ...].
-    __device__ int spread(int l, int needOut, int mapKind, int* rcv, int* nr, unsigned long long (&cand)[4]) {
+    __device__ __forceinline__ int spread(int l, int needOut, int mapKind, int* rcv, int* nr, Cands& cand) {
         // lane k < 24: the k-th neighbour of the bin-grouped offset table
         const int k = lane;
         int t = -1, ddx = 0, ddy = 0;
@@ -1135,14 +1152,9 @@ struct FastZone {
             nrec + needOut <= A->recCap) {
             unsigned long long mine = ~0ULL;
             for (int i = 0; i < needOut; ++i) {
-                unsigned long long best = cand[0];
-#pragma unroll
-                for (int r = 1; r < 4; ++r) best = cand[r] < best ? cand[r] : best;
-                best = warp_min_u64_r(best);
+                const unsigned long long best = warp_min_u64_r(cand.lowest());
                 const int j = (int)(best & 511ULL);
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (r == (j >> 5) && (j & 31) == lane) cand[r] = ~0ULL;
+                cand.take(j, lane);
                 if (lane == i) mine = best;
             }
             const int drank = __popc(defMask & lanemask_lt());
@@ -1233,7 +1245,7 @@ struct FastZone {
         const int needOut = max(0, (int)ceil((double)nc - hi));
         int nr = 0;
         int moved = 0;
-        unsigned long long cand[4];
+        Cands cand;
         load_candidates(l, true, 0, cand);
         // the low map first, then the high map for what is left (one call site: code size)
 #pragma unroll 1
@@ -1338,7 +1350,7 @@ struct FastZone {
             if (avail <= 0) continue;
             const int nt = min(need, min(avail, cnt(dn)));
             if (nt <= 0) continue;
-            unsigned long long cand[4];
+            Cands cand;
             move_members(dn, l, nt, false, cand);
             if (failed) break;
             if (lane == 0) {
