@@ -366,6 +366,14 @@ def run_ours(args):
             if st2 is not None:
                 chosen["profile"]["steps_learned"] = st2[1]
                 chosen["profile"]["steps_plain_fallback"] = st2[0]
+            if net is not None:
+                # what the network replaces: the same run with a zero network (no EOS kick in
+                # the bulk; the walls keep the plain one, the repair kick stays)
+                from src_incompressible_openmp_b200 import learned as L
+                pz, mz, _ = profile_run(native, p, 1, "fast", S, L.zero_network(), occ_limit, local)
+                chosen["profile"]["profile_l2_err_no_eos_kick"] = float(np.linalg.norm(pz - pa)) / na
+                chosen["profile"]["occStd_no_eos_kick"] = mz["occStd"]
+                chosen["profile"]["meanKinetic_no_eos_kick"] = mz["meanKinetic"]
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()

@@ -132,3 +132,35 @@ def test_channel_statistics_match_plain_form():
     ke_noise = abs(m2["meanKinetic"] - m1["meanKinetic"])
     assert abs(mf["meanKinetic"] - m1["meanKinetic"]) <= max(3 * ke_noise, 0.01 * m1["meanKinetic"])
     assert mf["occStd"] <= 2.0 * max(m1["occStd"], m2["occStd"])
+
+
+def test_learned_eos_kick_network_gain():
+    """The fast form's network (the EOS kick from the collided state's stencil) trained on 12
+    channels of the ensemble family explains most of the plain EOS kick on 2 held-out channels
+    (no kick explains none); deployed, it takes every step itself and keeps the plain closure's
+    kinetic energy and occupancy spread."""
+    native = _native()
+    from src_incompressible_openmp_b200 import learned as L
+    X, Y = L.collect(runs=12, seed=21, warmup=40, steps=10, stride=3, form="fast")
+    net, losses = L.train(X, Y, epochs=4, form="fast")
+    assert losses[-1] < 0.1 * losses[0], losses
+    Xh, Yh = L.collect(runs=2, seed=99, warmup=40, steps=5, stride=3, form="fast")
+    fvu = L.unexplained(net, Xh, Yh)
+    assert fvu < 0.2, fvu
+    assert L.unexplained(L.zero_network(), Xh, Yh) == pytest.approx(1.0)
+    p = poiseuille_params(512, 128, 20)
+    x, v = uniform_state(p, 1)
+    rows = {}
+    for name, params in (("plain", None), ("learned", net)):
+        with native.Context(p, form="fast") as ctx:
+            ctx.set_state(x, v)
+            if params is not None:
+                ctx.learned_set(params, 10.0)
+            ctx.step(0, 300)
+            rows[name] = ctx.step(300, 300, metrics=True)
+            if params is not None:
+                plain_steps, learned_steps, _ = ctx.learned_stats()
+                assert plain_steps == 0 and learned_steps == 600
+    assert abs(rows["learned"]["meanKinetic"] / rows["plain"]["meanKinetic"] - 1) < 0.02
+    assert abs(rows["learned"]["occStd"] / rows["plain"]["occStd"] - 1) < 0.05
+
