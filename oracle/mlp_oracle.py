@@ -19,7 +19,8 @@ this file restates the library's own definition of it, in float64:
             and bias rounded to BF16 (bf: round to nearest even); the operands of the two
             64-wide layers (x, a1) are BF16 too, a2 is not
   loss      mean over rows and both outputs of (output - target / scale)^2; gradients pass
-            straight through the roundings
+            straight through the roundings (loss_grad); the tensor-core training kernel
+            also rounds its backward operands dz2, dz1 to BF16 (loss_grad_tc)
   Adam      m = b1 m + (1 - b1) g; v = b2 v + (1 - b2) g^2;
             p -= lr * (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps)
 
@@ -102,6 +103,29 @@ def loss_grad(X, Y, params):
     g[OFF_W2:OFF_B2] = (d2.T @ a1).ravel()
     g[OFF_B2:OFF_W3] = d2.sum(0)
     d1 = (d2 @ W2) * gelu_d(z1)
+    g[OFF_W1:OFF_B1] = (d1.T @ X).ravel()
+    g[OFF_B1:OFF_W2] = d1.sum(0)
+    return loss, g
+
+
+def loss_grad_tc(X, Y, params):
+    """loss_grad as the tensor-core training kernel takes it: the backward products run on BF16
+    operands, so dz2 and dz1 are rounded to BF16 (through FP32) before they multiply; the
+    output layer's gradient stays in FP32 (here float64). Biases are the weights of a constant
+    input column, so their gradients are the sums of the same rounded dz."""
+    W1, b1, W2, b2, W3, b3, scale = unpack(params)
+    out, (X, z1, a1, z2, a2) = forward(X, params)
+    e = out - np.asarray(Y, np.float64) / scale
+    m = e.size
+    loss = float(np.sum(e * e) / m)
+    d3 = 2.0 * e / m
+    g = np.zeros(N_PARAMS)
+    g[OFF_W3:OFF_B3] = (d3.T @ a2).ravel()
+    g[OFF_B3:OFF_SCALE] = d3.sum(0)
+    d2 = bf16(((d3 @ W3) * gelu_d(z2)).astype(np.float32))
+    g[OFF_W2:OFF_B2] = (d2.T @ a1).ravel()
+    g[OFF_B2:OFF_W3] = d2.sum(0)
+    d1 = bf16(((d2 @ W2) * gelu_d(z1)).astype(np.float32))
     g[OFF_W1:OFF_B1] = (d1.T @ X).ravel()
     g[OFF_B1:OFF_W2] = d1.sum(0)
     return loss, g

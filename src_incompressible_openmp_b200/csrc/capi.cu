@@ -3175,6 +3175,14 @@ static int tc_setup(int device, int rows, int* grid) {
     return MPCD_OK;
 }
 
+// the tensor-core training kernel: its shared memory, and the SMs (one CTA each at most)
+static int tg_setup(int device, int* sms) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTgSmem));
+    CUDA_TRY(cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device));
+    return MPCD_OK;
+}
+static unsigned tg_grid(int rows, int sms) { return (unsigned)std::max(1, std::min((rows + 127) / 128, sms)); }
+
 static int ensure_learned_buffers(mpcd_ctx* c) {
     if (c->lparams) return MPCD_OK;
     int rc = tc_setup(c->device, c->Nc, &c->tcGrid);
@@ -3217,6 +3225,15 @@ struct LearnedDev {
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+// synchronises the learned-closure stream and reports its device status
+static int learned_status(LearnedDev& D, DevStatus* dS) {
+    DevStatus hs{};
+    CUDA_TRY(cudaMemcpyAsync(&hs, dS, sizeof hs, cudaMemcpyDeviceToHost, D.stream));
+    CUDA_TRY(cudaStreamSynchronize(D.stream));
+    if (hs.code) return set_err(MPCD_ERR_DEVICE, std::string(dev_error_text(hs.code)) + " (detail " + std::to_string(hs.detail) + ")");
+    return MPCD_OK;
+}
 
 static int learned_rows_ok(const float* X, const float* Y, int64_t rows, const float* params) {
     if (!X || !params || rows < 1 || rows > (int64_t)INT32_MAX / kFeat)
@@ -3391,9 +3408,11 @@ int mpcd_learned_grad(const float* features, const float* targets, int64_t rows,
     LearnedDev D;
     float *dX, *dY, *dP, *dG, *dL;
     int* dI;
+    DevStatus* dS;
+    int sms = 0;
     if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dY, (size_t)rows * kOut)) ||
         (rc = D.alloc(&dP, kParams)) || (rc = D.alloc(&dG, kParams)) || (rc = D.alloc(&dL, 1)) ||
-        (rc = D.alloc(&dI, (size_t)rows)))
+        (rc = D.alloc(&dI, (size_t)rows)) || (rc = D.alloc(&dS, 1)) || (rc = tg_setup(device, &sms)))
         return rc;
     std::vector<int> idx((size_t)rows);
     for (int64_t i = 0; i < rows; ++i) idx[(size_t)i] = (int)i;
@@ -3403,13 +3422,13 @@ int mpcd_learned_grad(const float* features, const float* targets, int64_t rows,
     CUDA_TRY(cudaMemcpyAsync(dI, idx.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, D.stream));
     CUDA_TRY(cudaMemsetAsync(dG, 0, sizeof(float) * kParams, D.stream));
     CUDA_TRY(cudaMemsetAsync(dL, 0, sizeof(float), D.stream));
-    k_mlp_grad<<<(unsigned)((rows + kMlpTile - 1) / kMlpTile), kMlpThreads, 0, D.stream>>>(
-        dX, dY, dI, (int)rows, (int)rows, 1.0f / params[kOffScale], dP, dG, dL);
+    CUDA_TRY(cudaMemsetAsync(dS, 0, sizeof(DevStatus), D.stream));
+    k_mlp_grad_tc<<<tg_grid((int)rows, sms), 128, kTgSmem, D.stream>>>(dX, dY, dI, (int)rows, (int)rows,
+                                                                       1.0f / params[kOffScale], dP, dG, dL, dS);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(grad, dG, sizeof(float) * kParams, cudaMemcpyDeviceToHost, D.stream));
     CUDA_TRY(cudaMemcpyAsync(loss, dL, sizeof(float), cudaMemcpyDeviceToHost, D.stream));
-    CUDA_TRY(cudaStreamSynchronize(D.stream));
-    return MPCD_OK;
+    return learned_status(D, dS);
 }
 
 int mpcd_learned_train(const float* features, const float* targets, int64_t rows, float* params, int32_t epochs,
@@ -3427,11 +3446,15 @@ int mpcd_learned_train(const float* features, const float* targets, int64_t rows
     LearnedDev D;
     float *dX, *dY, *dP, *dG, *dM, *dV, *dL;
     int* dI;
+    DevStatus* dS;
+    int sms = 0;
     const int64_t nb = (rows + batch - 1) / batch;
     if ((rc = D.open(device)) || (rc = D.alloc(&dX, (size_t)rows * kFeat)) || (rc = D.alloc(&dY, (size_t)rows * kOut)) ||
         (rc = D.alloc(&dP, kParams)) || (rc = D.alloc(&dG, kParams)) || (rc = D.alloc(&dM, kParams)) ||
-        (rc = D.alloc(&dV, kParams)) || (rc = D.alloc(&dL, (size_t)nb)) || (rc = D.alloc(&dI, (size_t)rows)))
+        (rc = D.alloc(&dV, kParams)) || (rc = D.alloc(&dL, (size_t)nb)) || (rc = D.alloc(&dI, (size_t)rows)) ||
+        (rc = D.alloc(&dS, 1)) || (rc = tg_setup(device, &sms)))
         return rc;
+    CUDA_TRY(cudaMemsetAsync(dS, 0, sizeof(DevStatus), D.stream));
     CUDA_TRY(cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * rows, cudaMemcpyHostToDevice, D.stream));
     CUDA_TRY(cudaMemcpyAsync(dY, targets, sizeof(float) * kOut * rows, cudaMemcpyHostToDevice, D.stream));
     CUDA_TRY(cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, D.stream));
@@ -3452,15 +3475,14 @@ int mpcd_learned_train(const float* features, const float* targets, int64_t rows
             const int64_t r0 = b * batch;
             const int n = (int)std::min<int64_t>(batch, rows - r0);
             ++t;
-            k_mlp_grad<<<(unsigned)((n + kMlpTile - 1) / kMlpTile), kMlpThreads, 0, D.stream>>>(dX, dY, dI + r0, n, n, yinv,
-                                                                                               dP, dG, dL + b);
+            k_mlp_grad_tc<<<tg_grid(n, sms), 128, kTgSmem, D.stream>>>(dX, dY, dI + r0, n, n, yinv, dP, dG, dL + b, dS);
             k_adam<<<(kTrained + 255) / 256, 256, 0, D.stream>>>(dP, dG, dM, dV, kTrained, lr, b1, b2, eps,
                                                                  1.0f - (float)std::pow((double)b1, (double)t),
                                                                  1.0f - (float)std::pow((double)b2, (double)t));
         }
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemcpyAsync(lossB.data(), dL, sizeof(float) * nb, cudaMemcpyDeviceToHost, D.stream));
-        CUDA_TRY(cudaStreamSynchronize(D.stream));
+        if ((rc = learned_status(D, dS))) return rc;
         if (epoch_loss) {
             double sum = 0.0;
             for (int64_t b = 0; b < nb; ++b) sum += (double)lossB[(size_t)b] * (double)std::min<int64_t>(batch, rows - b * batch);

@@ -17,7 +17,7 @@
 //                  run on the tensor cores), the 64 -> 2 output layer takes a2 in FP32
 //
 // Parameters live in one float array: W1[64][75], b1[64], W2[64][64], b2[64], W3[2][64], b3[2],
-// scale. Training (k_mlp_grad + k_adam) keeps FP32 master weights and fits output = target /
+// scale. Training (k_mlp_grad_tc on the tensor cores + k_adam) keeps FP32 master weights and fits output = target /
 // scale (gradients pass straight through the BF16 roundings). The scale is not trained (the
 // trainer sets it to the targets' RMS).
 #pragma once
@@ -168,10 +168,6 @@ __global__ void k_fast_learned_samples(DevParams P, const float4* __restrict__ f
     Y[2 * (size_t)s + 1] = (float)eosY[c];
 }
 
-__device__ __forceinline__ void stage_weights(const float* __restrict__ params, __nv_bfloat16* sw) {
-    for (int i = threadIdx.x; i < kTrained; i += blockDim.x) sw[i] = __float2bfloat16_rn(params[i]);
-}
-
 // features and targets of every stride-th cell from offset (dataset collection)
 __global__ void k_learned_samples(DevParams P, const float4* __restrict__ feat, const double* __restrict__ duRX,
                                   const double* __restrict__ duRY, const double* __restrict__ eosX,
@@ -185,110 +181,6 @@ __global__ void k_learned_samples(DevParams P, const float4* __restrict__ feat, 
     const double beta = beta_applied(P, red[0], red[1]);
     Y[2 * (size_t)s] = (float)__dadd_rn(__dmul_rn(beta, duRX[c]), eosX[c]);
     Y[2 * (size_t)s + 1] = (float)__dadd_rn(__dmul_rn(beta, duRY[c]), eosY[c]);
-}
-
-// One block: forward and backward of kMlpTile samples (rows idx[blockIdx.x * kMlpTile ..] of
-// X and Y), accumulating the gradient of the mean squared error of output - Y * yinv over the
-// batch (batch rows, 2 outputs each) into grad (atomics) and the loss into loss[0].
-constexpr int kMlpTile = 16, kMlpThreads = 256;
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restrict__ X, const float* __restrict__ Y,
-                                                          const int* __restrict__ idx, int rows, int batch, float yinv,
-                                                          const float* __restrict__ params, float* __restrict__ grad,
-                                                          float* __restrict__ loss) {
-    __shared__ __nv_bfloat16 sw[kTrained];
-    __shared__ float x[kMlpTile][kFeat + 1];
-    __shared__ float z1[kMlpTile][kHid], a1[kMlpTile][kHid], z2[kMlpTile][kHid], a2[kMlpTile][kHid];
-    __shared__ float dout[kMlpTile][kOut];
-    const int t = threadIdx.x;
-    const int r0 = blockIdx.x * kMlpTile;
-    const int nr = min(kMlpTile, rows - r0);
-    stage_weights(params, sw);
-    for (int i = t; i < kMlpTile * kFeat; i += blockDim.x) {
-        const int r = i / kFeat, k = i - r * kFeat;
-        x[r][k] = (r < nr) ? bf16r(X[(size_t)idx[r0 + r] * kFeat + k]) : 0.0f;
-    }
-    __syncthreads();
-    for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
-        const int r = i / kHid, j = i - r * kHid;
-        float z = __bfloat162float(sw[kOffB1 + j]);
-        for (int k = 0; k < kFeat; ++k) z = fmaf(__bfloat162float(sw[kOffW1 + j * kFeat + k]), x[r][k], z);
-        z1[r][j] = z;
-        a1[r][j] = bf16r(gelu(z));
-    }
-    __syncthreads();
-    for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
-        const int r = i / kHid, j = i - r * kHid;
-        float z = __bfloat162float(sw[kOffB2 + j]);
-        for (int k = 0; k < kHid; ++k) z = fmaf(__bfloat162float(sw[kOffW2 + j * kHid + k]), a1[r][k], z);
-        z2[r][j] = z;
-        a2[r][j] = gelu(z);
-    }
-    __syncthreads();
-    if (t < kMlpTile * kOut) {
-        const int r = t / kOut, o = t - r * kOut;
-        float z = __bfloat162float(sw[kOffB3 + o]);
-        for (int k = 0; k < kHid; ++k) z = fmaf(__bfloat162float(sw[kOffW3 + o * kHid + k]), a2[r][k], z);
-        float d = 0.0f;
-        if (r < nr) {
-            const float e = z - Y[(size_t)idx[r0 + r] * kOut + o] * yinv;
-            d = 2.0f * e / (float)(batch * kOut);  // d(mean squared error)/d(output)
-            atomicAdd(loss, e * e / (float)(batch * kOut));
-        }
-        dout[r][o] = d;
-    }
-    __syncthreads();
-    // layer 3: dW3, db3; da2 -> dz2 (kept in z2)
-    for (int i = t; i < kOut * kHid; i += blockDim.x) {
-        const int o = i / kHid, k = i - o * kHid;
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g = fmaf(dout[r][o], a2[r][k], g);
-        atomicAdd(grad + kOffW3 + i, g);
-    }
-    if (t < kOut) {
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g += dout[r][t];
-        atomicAdd(grad + kOffB3 + t, g);
-    }
-    __syncthreads();
-    for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
-        const int r = i / kHid, k = i - r * kHid;
-        float d = 0.0f;
-        for (int o = 0; o < kOut; ++o) d = fmaf(dout[r][o], __bfloat162float(sw[kOffW3 + o * kHid + k]), d);
-        z2[r][k] = d * gelu_d(z2[r][k]);
-    }
-    __syncthreads();
-    // layer 2: dW2, db2; da1 -> dz1 (kept in z1)
-    for (int i = t; i < kHid * kHid; i += blockDim.x) {
-        const int j = i / kHid, k = i - j * kHid;
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g = fmaf(z2[r][j], a1[r][k], g);
-        atomicAdd(grad + kOffW2 + i, g);
-    }
-    if (t < kHid) {
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g += z2[r][t];
-        atomicAdd(grad + kOffB2 + t, g);
-    }
-    __syncthreads();
-    for (int i = t; i < kMlpTile * kHid; i += blockDim.x) {
-        const int r = i / kHid, k = i - r * kHid;
-        float d = 0.0f;
-        for (int j = 0; j < kHid; ++j) d = fmaf(z2[r][j], __bfloat162float(sw[kOffW2 + j * kHid + k]), d);
-        z1[r][k] = d * gelu_d(z1[r][k]);
-    }
-    __syncthreads();
-    // layer 1: dW1, db1
-    for (int i = t; i < kHid * kFeat; i += blockDim.x) {
-        const int j = i / kFeat, k = i - j * kFeat;
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g = fmaf(z1[r][j], x[r][k], g);
-        atomicAdd(grad + kOffW1 + i, g);
-    }
-    if (t < kHid) {
-        float g = 0.0f;
-        for (int r = 0; r < kMlpTile; ++r) g += z1[r][t];
-        atomicAdd(grad + kOffB1 + t, g);
-    }
 }
 
 // Adam (Kingma & Ba) on the FP32 master weights; clears the gradient for the next batch.
@@ -621,6 +513,265 @@ __global__ void k_learned_decide(const double* __restrict__ sums, int Nc, double
     if (var < 0.0) var = 0.0;
     const double occStd = sqrt(var) / (gamma > 1e-12 ? gamma : 1e-12);
     *mode = (limit <= 0.0 || occStd <= limit) ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ training on the tensor cores
+// Forward and backward of 128-row tiles with tcgen05: one persistent CTA of 128 threads per SM,
+// row t of a tile in thread t (TMEM lane t).
+//   forward:  Z1 = X W1^T (b1 in operand column 75), a1 = bf16(gelu(Z1));
+//             Z2 = A1 W2^T (b2 in operand column 64 of A1), a2 = gelu(Z2); out = W3 a2 + b3 (FP32)
+//   backward: dout = 2 (out - y / scale) / (batch * 2); dW3, db3 in FP32 on the CUDA cores;
+//             dz2 = bf16(dout W3 * gelu'(Z2)); dA1 = dz2 W2;  dz1 = bf16(dA1 * gelu'(Z1));
+//             dW2^T += A1^T dz2 and dW1^T += X^T dz1, accumulated in TMEM over the CTA's tiles
+//             (their rows 64 and 75, the constant columns, are db2 and db1)
+// The transposed operands are written to shared memory beside the row-major ones, in the
+// canonical no-swizzle K-major layout with K = 128 rows. Five MMAs (M = 128, N = 64) per tile.
+// TMEM columns: Z1 [0, 64), Z2 [64, 128), dA1 [128, 192), dW2^T [192, 256), dW1^T [256, 320).
+constexpr int kTgK1 = 80, kTgK2 = 80, kTgKR = 128;
+constexpr uint32_t kTgOffX = 0;                                   // [128][80] bf16
+constexpr uint32_t kTgOffXT = kTgOffX + 128 * kTgK1 * 2;          // [128][128] bf16 (rows: operand column)
+constexpr uint32_t kTgOffA1 = kTgOffXT + 128 * kTgKR * 2;         // [128][80] bf16
+constexpr uint32_t kTgOffA1T = kTgOffA1 + 128 * kTgK2 * 2;        // [128][128] bf16
+constexpr uint32_t kTgOffD2 = kTgOffA1T + 128 * kTgKR * 2;        // [128][64] bf16
+constexpr uint32_t kTgOffD2T = kTgOffD2 + 128 * kHid * 2;         // [64][128] bf16
+constexpr uint32_t kTgOffD1T = kTgOffD2T + kHid * kTgKR * 2;      // [64][128] bf16
+constexpr uint32_t kTgOffW1 = kTgOffD1T + kHid * kTgKR * 2;       // [64][80] bf16 (b1 in column 75)
+constexpr uint32_t kTgOffW2 = kTgOffW1 + kHid * kTgK1 * 2;        // [64][80] bf16 (b2 in column 64)
+constexpr uint32_t kTgOffW2T = kTgOffW2 + kHid * kTgK2 * 2;       // [64][64] bf16: W2^T
+constexpr uint32_t kTgOffA2 = kTgOffW2T + kHid * kHid * 2;        // [128][64] f32
+constexpr uint32_t kTgOffDO = kTgOffA2 + 128 * kHid * 4;          // [128][2] f32
+constexpr uint32_t kTgOffW3 = kTgOffDO + 128 * kOut * 4;          // [2][64] f32, b3[2], pad
+constexpr uint32_t kTgOffBar = kTgOffW3 + kOut * kHid * 4 + 16;   // mbarrier
+constexpr uint32_t kTgOffTmem = kTgOffBar + 8;
+constexpr uint32_t kTgSmem = kTgOffTmem + 8;
+constexpr uint32_t kTgTmemCols = 512;
+static_assert(kTgSmem <= 227 * 1024, "training tile exceeds shared memory");
+static_assert(2 * (kTgSmem + 1024) > 228 * 1024, "one training CTA per SM (its TMEM takes all 512 columns)");
+constexpr uint32_t kTgIdesc = kTcIdesc;  // D F32, A and B BF16 K-major, N = 64, M = 128
+
+// the MMA of a K-major A [128 x K] and B [64 x K] at shared addresses a, b into TMEM column d
+__device__ __forceinline__ void tg_mma(uint32_t d, uint32_t a, uint32_t b, int K, bool accumulate) {
+    for (int ks = 0; ks < K / 16; ++ks)
+        tc_mma(d, tc_desc(a + ks * 256, 128, K * 16), tc_desc(b + ks * 256, 128, K * 16),
+               (accumulate || ks > 0) ? 1u : 0u);
+}
+
+__device__ __forceinline__ void tg_put(unsigned char* sm, uint32_t off, int r, int k, int K, float v) {
+    *reinterpret_cast<__nv_bfloat16*>(sm + off + kmajor_offset(r, k, K)) = __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(128, 1)
+    k_mlp_grad_tc(const float* __restrict__ X, const float* __restrict__ Y, const int* __restrict__ idx, int rows,
+                  int batch, float yinv, const float* __restrict__ params, float* __restrict__ grad,
+                  float* __restrict__ loss, DevStatus* st) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t bar = sbase + kTgOffBar;
+    float* sA2 = reinterpret_cast<float*>(sm + kTgOffA2);
+    float* sDO = reinterpret_cast<float*>(sm + kTgOffDO);
+    float* sW3 = reinterpret_cast<float*>(sm + kTgOffW3);
+    // weights (W1 in the point-major operand order of the features), zero padding of the
+    // transposed operands' unused rows
+    for (int i = t; i < kHid * kTgK1; i += 128) {
+        const int n = i / kTgK1, k = i - n * kTgK1;
+        const int pk = (k % 3) * 25 + k / 3;
+        const float w = k < kFeat ? params[kOffW1 + n * kFeat + pk] : (k == kFeat ? params[kOffB1 + n] : 0.0f);
+        tg_put(sm, kTgOffW1, n, k, kTgK1, w);
+    }
+    for (int i = t; i < kHid * kTgK2; i += 128) {
+        const int n = i / kTgK2, k = i - n * kTgK2;
+        const float w = k < kHid ? params[kOffW2 + n * kHid + k] : (k == kHid ? params[kOffB2 + n] : 0.0f);
+        tg_put(sm, kTgOffW2, n, k, kTgK2, w);
+    }
+    for (int i = t; i < kHid * kHid; i += 128) {
+        const int n = i / kHid, k = i - n * kHid;  // W2^T[n][k] = W2[k][n]
+        tg_put(sm, kTgOffW2T, n, k, kHid, params[kOffW2 + k * kHid + n]);
+    }
+    for (int i = t; i < kOut * kHid; i += 128) sW3[i] = bf16r(params[kOffW3 + i]);
+    if (t < kOut) sW3[kOut * kHid + t] = bf16r(params[kOffB3 + t]);
+    for (int i = t; i < 128 * kTgKR; i += 128) {
+        const int r = i / kTgKR, k = i - r * kTgKR;
+        if (r >= kTgK1 - 4) tg_put(sm, kTgOffXT, r, k, kTgKR, 0.0f);   // operand columns 76..127
+        if (r > kHid) tg_put(sm, kTgOffA1T, r, k, kTgKR, 0.0f);       // columns 65..127
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kTgOffTmem),
+                     "r"(kTgTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_smem_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTgOffTmem);
+    const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 TMEM lanes
+    const float b3a = sW3[kOut * kHid], b3b = sW3[kOut * kHid + 1];
+    const float dscale = 2.0f / (float)(batch * kOut);
+    const int tiles = (rows + 127) / 128;
+    uint32_t phase = 0;
+    bool ok = true, first = true;
+    float accW3 = 0.0f, accB3 = 0.0f, lossAcc = 0.0f;
+    auto sync_mma = [&](auto issue) {  // shared stores visible, one thread issues, all wait
+        tc_fence_smem_async();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+            issue();
+            tc_commit(bar);
+        }
+        ok = tc_wait(bar, phase);
+        phase ^= 1;
+        if (__syncthreads_and(ok) == 0) {
+            if (t == 0) raise_error(st, kErrTensorWait, blockIdx.x);
+            ok = false;
+        }
+        tc_fence_after();
+        return ok;
+    };
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int r = tile * 128 + t;
+        const bool live = r < rows;
+        const int src = live ? idx[r] : 0;
+        // 1. the row's operands, row-major and transposed (point-major feature order)
+        float y0 = 0.0f, y1 = 0.0f;
+        if (live) {
+            y0 = Y[(size_t)src * kOut] * yinv;
+            y1 = Y[(size_t)src * kOut + 1] * yinv;
+        }
+        for (int k = 0; k < kTgK1; ++k) {
+            float v = 0.0f;
+            if (k < kFeat) v = live ? X[(size_t)src * kFeat + (k % 3) * 25 + k / 3] : 0.0f;
+            else if (k == kFeat) v = 1.0f;
+            tg_put(sm, kTgOffX, t, k, kTgK1, v);
+            if (k <= kFeat) tg_put(sm, kTgOffXT, k, t, kTgKR, v);
+        }
+        // 2. Z1 = X W1^T
+        if (!sync_mma([&] { tg_mma(tmem, sbase + kTgOffX, sbase + kTgOffW1, kTgK1, false); })) break;
+        // 3. a1 = bf16(gelu(Z1)), row-major (column 64: the constant of b2) and transposed
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16];
+            tc_ld16(lb + 16 * h, z);
+            tc_ld_wait16(z);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float a = gelu(__uint_as_float(z[q]));
+                tg_put(sm, kTgOffA1, t, 16 * h + q, kTgK2, a);
+                tg_put(sm, kTgOffA1T, 16 * h + q, t, kTgKR, a);
+            }
+        }
+        for (int k = kHid; k < kTgK2; ++k) tg_put(sm, kTgOffA1, t, k, kTgK2, k == kHid ? 1.0f : 0.0f);
+        tg_put(sm, kTgOffA1T, kHid, t, kTgKR, 1.0f);
+        // 4. Z2 = A1 W2^T
+        if (!sync_mma([&] { tg_mma(tmem + kHid, sbase + kTgOffA1, sbase + kTgOffW2, kTgK2, false); })) break;
+        // 5. a2, the output layer, dout; dz2 = bf16(dout W3 * gelu'(Z2)), row-major and transposed
+        float o0 = b3a, o1 = b3b;
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16];
+            tc_ld16(lb + kHid + 16 * h, z);
+            tc_ld_wait16(z);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int j = 16 * h + q;
+                const float a = gelu(__uint_as_float(z[q]));
+                sA2[t * kHid + j] = a;
+                o0 = fmaf(sW3[j], a, o0);
+                o1 = fmaf(sW3[kHid + j], a, o1);
+            }
+        }
+        const float e0 = o0 - y0, e1 = o1 - y1;
+        const float d0 = live ? dscale * e0 : 0.0f, d1 = live ? dscale * e1 : 0.0f;
+        if (live) lossAcc += (e0 * e0 + e1 * e1) / (float)(batch * kOut);
+        sDO[2 * t] = d0;
+        sDO[2 * t + 1] = d1;
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16];
+            tc_ld16(lb + kHid + 16 * h, z);
+            tc_ld_wait16(z);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int j = 16 * h + q;
+                const float dz = (d0 * sW3[j] + d1 * sW3[kHid + j]) * gelu_d(__uint_as_float(z[q]));
+                tg_put(sm, kTgOffD2, t, j, kHid, dz);
+                tg_put(sm, kTgOffD2T, j, t, kTgKR, dz);
+            }
+        }
+        // 6. dA1 = dz2 W2; dW2^T += A1^T dz2
+        if (!sync_mma([&] {
+                tg_mma(tmem + 2 * kHid, sbase + kTgOffD2, sbase + kTgOffW2T, kHid, false);
+                tg_mma(tmem + 3 * kHid, sbase + kTgOffA1T, sbase + kTgOffD2T, kTgKR, !first);
+            }))
+            break;
+        // dW3, db3 over the tile's rows (thread i: entry i of W3)
+        {
+            const int o = t / kHid, k = t - o * kHid;
+            float g = 0.0f, gb = 0.0f;
+            for (int rr = 0; rr < 128; ++rr) {
+                const float d = sDO[2 * rr + o];
+                g = fmaf(d, sA2[rr * kHid + k], g);
+                gb += d;
+            }
+            accW3 += g;
+            if (k == 0) accB3 += gb;
+        }
+        // 7. dz1 = bf16(dA1 * gelu'(Z1)), transposed
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t z[16], d[16];
+            tc_ld16(lb + 16 * h, z);
+            tc_ld16(lb + 2 * kHid + 16 * h, d);
+            tc_ld_wait16(z);
+            tc_ld_wait16(d);
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                tg_put(sm, kTgOffD1T, 16 * h + q, t, kTgKR, __uint_as_float(d[q]) * gelu_d(__uint_as_float(z[q])));
+        }
+        // 8. dW1^T += X^T dz1 (the wait also frees the operands for the next tile)
+        if (!sync_mma([&] { tg_mma(tmem + 4 * kHid, sbase + kTgOffXT, sbase + kTgOffD1T, kTgKR, !first); })) break;
+        first = false;
+    }
+    // the accumulated gradients: lane t of dW1^T is operand column t (feature, or b1 at 75),
+    // lane t of dW2^T is A1 column t (or b2 at 64)
+    if (ok && !first) {
+        const int pk = t < kFeat ? (t % 3) * 25 + t / 3 : -1;
+#pragma unroll
+        for (int h = 0; h < kHid / 16; ++h) {
+            uint32_t a[16], b[16];
+            tc_ld16(lb + 4 * kHid + 16 * h, a);
+            tc_ld16(lb + 3 * kHid + 16 * h, b);
+            tc_ld_wait16(a);
+            tc_ld_wait16(b);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int j = 16 * h + q;
+                if (t < kFeat) atomicAdd(grad + kOffW1 + j * kFeat + pk, __uint_as_float(a[q]));
+                else if (t == kFeat) atomicAdd(grad + kOffB1 + j, __uint_as_float(a[q]));
+                if (t < kHid) atomicAdd(grad + kOffW2 + j * kHid + t, __uint_as_float(b[q]));
+                else if (t == kHid) atomicAdd(grad + kOffB2 + j, __uint_as_float(b[q]));
+            }
+        }
+        atomicAdd(grad + kOffW3 + t, accW3);
+        if (t % kHid == 0) atomicAdd(grad + kOffB3 + t / kHid, accB3);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lossAcc += __shfl_xor_sync(0xffffffffu, lossAcc, o);
+    if (lane == 0 && lossAcc != 0.0f) atomicAdd(loss, lossAcc);
+    if (!ok) tc_wait(bar, phase ^ 1);  // an MMA did not complete in time: one more bounded wait
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTgTmemCols) : "memory");
+    }
 }
 
 }  // namespace mpcd_dev

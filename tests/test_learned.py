@@ -149,7 +149,7 @@ def test_gradient_matches_oracle(rows):
     native = _native()
     X, Y, p = _rand_case(rows, 20 + rows)
     g, loss = native.learned_grad(X, Y, p)
-    loss_o, g_o = MO.loss_grad(X, Y, p)
+    loss_o, g_o = MO.loss_grad_tc(X, Y, p)  # the tensor-core kernel's BF16 backward operands
     assert abs(loss - loss_o) <= 1e-5 * loss_o
     assert g[MO.OFF_SCALE] == 0.0
     scale = np.max(np.abs(g_o))
@@ -165,7 +165,7 @@ def test_adam_step_matches_oracle():
     X, Y, p = _rand_case(64, 31)
     lr = 1e-3
     q, losses = native.learned_train(X, Y, p, epochs=1, batch=64, lr=lr, seed=1)
-    loss_o, g_o = MO.loss_grad(X, Y, p)
+    loss_o, g_o = MO.loss_grad_tc(X, Y, p)
     assert abs(losses[0] - loss_o) <= 1e-5 * loss_o
     want, _, _ = MO.adam_step(p, g_o, np.zeros_like(g_o), np.zeros_like(g_o), 1, lr)
     big = np.abs(g_o) > 1e-3 * np.max(np.abs(g_o))  # g / (|g| + eps) is ill-conditioned near 0
