@@ -197,6 +197,11 @@ struct mpcd_ctx {
     int* fzRecPid = nullptr;
     float2* fzRecOff = nullptr;
     int2* fzRecQ = nullptr;
+    // launch order of the decision kernel (zones of similar cost together, heaviest first in
+    // each window): per zone its cost, the order
+    bool fzOrderOn = true;
+    int* fzCost = nullptr;
+    int* fzOrder = nullptr;
     // velocity profile accumulation (mpcd_profile_*): per row, momentum (int64 at 2^-32) and count
     bool profOn = false;
     unsigned long long* profP = nullptr;

@@ -863,6 +863,9 @@ struct FastZoneArgs {
     int* recPidG;
     float2* recOffG;
     int2* recQG;
+    // nullable: the zone each slot of the decision kernel runs (slot = block * zones per block +
+    // warp), heaviest zones first, so that the zones of one block finish their phases together
+    const int* order;
 };
 
 // The 24 range-2 neighbour offsets grouped by the angular bin of atan2(dy, dx)
@@ -1618,7 +1621,8 @@ template <int kW>
 __global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int wib = threadIdx.x >> 5;
-    const int z = blockIdx.x * kW + wib;
+    const int slot = blockIdx.x * kW + wib;
+    const int z = A.order && slot < A.nZones ? A.order[slot] : slot;
     FastZone Z;
     Z.A = &A;
     Z.lane = threadIdx.x & 31;
@@ -1715,6 +1719,73 @@ __global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) 
         }
         if (Z.failed) atomicAdd(A.recOverflow, 1);
     }
+}
+
+// Launch order of the decision kernel. The work of a zone is its particles above the high map
+// plus its cells below the low map (its dense and sparse phases), from the pass-input counts;
+// one warp per zone. A zone's decisions do not depend on when it runs, so the order changes
+// only how evenly the zones of a block (which run their phases together) are loaded.
+constexpr int kFastCostBuckets = 256;
+constexpr int kFastOrderWindow = 1024;  // zones sorted together (one block of k_fast_zone_rank)
+__global__ void k_fast_zone_cost(FastZoneArgs A, int* __restrict__ cost) {
+    const int z = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (z >= A.nZones) return;
+    const DevParams& P = A.P;
+    const int4 R = A.rects[z];
+    const int TY = R.w - R.z, nl = (R.y - R.x) * TY;
+    int w = 0;
+    for (int l = lane; l < nl; l += 32) {
+        int gx = R.x + l / TY, gy = R.z + l % TY;
+        if (P.perx) gx = wrap_index(gx, P.Nx);
+        if (P.pery) gy = wrap_index(gy, P.Ny);
+        if (gx < 0 || gx >= P.Nx || gy < 0 || gy >= P.Ny) continue;
+        const int n = min(A.cntIn[gy + P.Ny * gx], A.F.K);
+        if (n > 0 && (double)n > P.highThr) w += (int)ceil((double)n - P.highThr);
+        else if (n > 0 && (double)n < P.lowThrBulk) ++w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if (lane == 0) cost[z] = min(kFastCostBuckets - 1, w);
+}
+
+// The zones of each window of kFastOrderWindow slots in descending cost: a counting sort in
+// shared memory (places within a bucket come from shared atomics, in no fixed order).
+__global__ void __launch_bounds__(kFastOrderWindow) k_fast_zone_rank(const int* __restrict__ cost, int nZones,
+                                                                     int* __restrict__ order) {
+    __shared__ int hist[kFastCostBuckets];
+    const int t = threadIdx.x;
+    const int z = blockIdx.x * kFastOrderWindow + t;
+    const bool live = z < nZones;
+    if (t < kFastCostBuckets) hist[t] = 0;
+    __syncthreads();
+    const int b = live ? cost[z] : 0;
+    const int r = live ? atomicAdd(hist + b, 1) : 0;
+    __syncthreads();
+    if (t < 32) {  // exclusive offsets, buckets in descending cost: 8 buckets per lane
+        int v[kFastCostBuckets / 32], acc = 0;
+#pragma unroll
+        for (int k = 0; k < kFastCostBuckets / 32; ++k) {
+            v[k] = hist[kFastCostBuckets - 1 - (8 * t + k)];
+            acc += v[k];
+        }
+        int incl = acc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (t >= o) incl += u;
+        }
+        int run = incl - acc;
+#pragma unroll
+        for (int k = 0; k < kFastCostBuckets / 32; ++k) {
+            const int bucket = kFastCostBuckets - 1 - (8 * t + k);
+            const int cnt = v[k];
+            hist[bucket] = run;
+            run += cnt;
+        }
+    }
+    __syncthreads();
+    if (live) order[blockIdx.x * kFastOrderWindow + hist[b] + r] = z;
 }
 
 // ------------------------------------------------------------------ closure

@@ -142,9 +142,9 @@ def profile_error(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def time_case(Nx, Ny, ppc, steps, params=None):
-    """Device ms per step of the plain and the learned closure on one channel (an untrained
-    Glorot network when params is None: the cost does not depend on the weights)."""
+def time_case(Nx, Ny, ppc, steps, params=None, form="f64"):
+    """Device ms per step of the plain and the learned closure on one channel, in one form
+    (an untrained Glorot network when params is None: the cost does not depend on the weights)."""
     from .cases import poiseuille_params
     p = poiseuille_params(Nx, Ny, ppc)
     x, v = uniform_state(p, 1)
@@ -152,7 +152,7 @@ def time_case(Nx, Ny, ppc, steps, params=None):
         params = native.learned_init(1)
         params[-1] = 0.07
     out = {}
-    with native.Context(p) as ctx:
+    with native.Context(p, form=form) as ctx:
         ctx.set_state(x, v)
         ctx.step(0, 3)
         out["plain_ms"] = 1e3 * ctx.step_timed(3, steps) / steps
@@ -172,9 +172,10 @@ def main():
     ap.add_argument("--out", default="net.npy")
     ap.add_argument("--time-case", type=int, nargs=4, metavar=("NX", "NY", "PPC", "STEPS"),
                     help="only time plain and learned steps on one channel")
+    ap.add_argument("--form", choices=["f64", "f32", "fast"], default="f64", help="state form of --time-case")
     a = ap.parse_args()
     if a.time_case:
-        print(time_case(*a.time_case))
+        print(time_case(*a.time_case, form=a.form))
         return
     t0 = time.time()
     X, Y = collect(a.runs, stride=a.stride, capacity=a.samples, log=print)
