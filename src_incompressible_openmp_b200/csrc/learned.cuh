@@ -48,6 +48,49 @@ __device__ __forceinline__ float gelu_d(float z) {
     return fmaf(z * s * (1.0f - s), kGeluC2 * fmaf(3.0f * kGeluA, z * z, 1.0f), s);
 }
 
+// Pairs of FP32 values in one 64-bit register, for the packed f32x2 arithmetic of sm_100a
+// (per element the IEEE rounding of the scalar instruction, two elements per issue).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// GELU of a pair, the tanh form as z * sigmoid(2u) = z / (1 + 2^(-2u log2 e)): the power by
+// ex2.approx, the quotient by rcp.approx (the special-function unit, one value per issue),
+// the rest packed
+constexpr float kGeluE = (float)(-1.5957691216057308 * 1.4426950408889634);  // -2 sqrt(2/pi) log2(e)
+__device__ __forceinline__ f32x2 gelu2(f32x2 z) {
+    const f32x2 t = f2_fma(f2_mul(z, f2_pack(kGeluA, kGeluA)), f2_mul(z, z), z);  // z + a z^3
+    float e0, e1;
+    f2_unpack(f2_mul(t, f2_pack(kGeluE, kGeluE)), e0, e1);
+    asm("ex2.approx.ftz.f32 %0, %0;" : "+f"(e0));
+    asm("ex2.approx.ftz.f32 %0, %0;" : "+f"(e1));
+    float d0, d1;
+    f2_unpack(f2_add(f2_pack(e0, e1), f2_pack(1.0f, 1.0f)), d0, d1);
+    asm("rcp.approx.ftz.f32 %0, %0;" : "+f"(d0));
+    asm("rcp.approx.ftz.f32 %0, %0;" : "+f"(d1));
+    return f2_mul(z, f2_pack(d0, d1));
+}
+
 // Stencil of cell c: start of each column jx (-1 beyond a wall) and each row jy (-1), and the
 // mean velocity over the points inside the walls.
 struct Stencil {
@@ -407,7 +450,11 @@ __global__ void __launch_bounds__(kTcThreads, 4)
             tc_ld_wait16(z);
             uint32_t w[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) w[q] = pack_bf16(gelu(__uint_as_float(z[2 * q])), gelu(__uint_as_float(z[2 * q + 1])));
+            for (int q = 0; q < 8; ++q) {
+                float g0, g1;
+                f2_unpack(gelu2(f2_pack(__uint_as_float(z[2 * q]), __uint_as_float(z[2 * q + 1]))), g0, g1);
+                w[q] = pack_bf16(g0, g1);
+            }
             *reinterpret_cast<uint4*>(sm + kTcOffH + kmajor_offset(t, 16 * h, kHid)) = make_uint4(w[0], w[1], w[2], w[3]);
             *reinterpret_cast<uint4*>(sm + kTcOffH + kmajor_offset(t, 16 * h + 8, kHid)) = make_uint4(w[4], w[5], w[6], w[7]);
         }
@@ -431,21 +478,26 @@ __global__ void __launch_bounds__(kTcThreads, 4)
             break;
         }
         tc_fence_after();
-        // 5. output layer in FP32
-        float o0 = sB3[0], o1 = sB3[1];
+        // 5. output layer in FP32, over pairs of hidden units (even and odd partial sums)
+        f32x2 p0 = f2_pack(0.0f, 0.0f), p1 = p0;
 #pragma unroll
         for (int h = 0; h < kHid / 16; ++h) {
             uint32_t z[16];
             tc_ld16(lane_base + kHid + 16 * h, z);
             tc_ld_wait16(z);
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int j = 16 * h + q;
-                const float a = gelu(__uint_as_float(z[q]) + sB2[j]);
-                o0 = fmaf(sW3[j], a, o0);
-                o1 = fmaf(sW3[kHid + j], a, o1);
+            for (int q = 0; q < 8; ++q) {
+                const int j = 16 * h + 2 * q;
+                const f32x2 a = gelu2(f2_add(f2_pack(__uint_as_float(z[2 * q]), __uint_as_float(z[2 * q + 1])),
+                                             *reinterpret_cast<const f32x2*>(sB2 + j)));
+                p0 = f2_fma(a, *reinterpret_cast<const f32x2*>(sW3 + j), p0);
+                p1 = f2_fma(a, *reinterpret_cast<const f32x2*>(sW3 + kHid + j), p1);
             }
         }
+        float e0, e1, f0, f1;
+        f2_unpack(p0, e0, e1);
+        f2_unpack(p1, f0, f1);
+        float o0 = sB3[0] + (e0 + e1), o1 = sB3[1] + (f0 + f1);
         tc_fence_before();  // the next tile's MMAs overwrite these columns after the barrier
         if (!kRows && bulkOnly) {  // no learned kick where the stencil crosses a wall
             // bulkOnly 2: a NaN marks the cell, whose kick the caller computes itself
