@@ -327,6 +327,12 @@ mpcd_ctx* mpcd_batch_member(mpcd_batch* batch, int index);
 /* steps step0+1 .. step0+nsteps for every replica; device_seconds (nullable): CUDA-event time
  * of the whole batch */
 int mpcd_batch_step(mpcd_batch* batch, int64_t step0, int64_t nsteps, double* device_seconds);
+/* A batch in a state form (mpcd_state_form): MPCD_FORM_F64 is mpcd_batch_create; with
+ * MPCD_FORM_FAST every phase of a step is one launch for all replicas, each replica's state
+ * bit-identical to that replica stepped alone (plain closure; no learned closure or profile
+ * accumulation on a batch). No counterpart in the reference, which runs one channel per
+ * process. */
+int mpcd_batch_create_form(const mpcd_params_c* params, int count, int device, int32_t form, mpcd_batch** out);
 
 /* ---------------------------------------------------------------- learned closure */
 /* A stencil MLP standing in for the liquid closure's per-cell velocity correction

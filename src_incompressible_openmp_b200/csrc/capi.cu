@@ -26,6 +26,7 @@
 #include "closure.cuh"
 #include "common.cuh"
 #include "fast.cuh"
+#include "fast_batch.cuh"
 #include "learned.cuh"
 #include "sort.cuh"
 #include "zone.cuh"
@@ -2774,8 +2775,10 @@ extern "C" int mpcd_cell_fields_static(const mpcd_params_c* params, const double
 // Batched replicas: independent contexts (own parameters, sizes, states and zone layouts) that
 // advance together. Each step is issued for every replica before the next step, each replica
 // on its own streams and from its own step graph, so their kernels run side by side on the GPU.
+struct FastBatch;
 struct mpcd_batch {
     int device = 0;
+    FastBatch* fast = nullptr;  // fast-form replicas: one launch per phase (fast_batch.inc)
     std::vector<mpcd_ctx*> members;
     cudaStream_t stream = nullptr;  // timing and the fork/join of the members' streams
     cudaEvent_t start = nullptr, stop = nullptr, fork = nullptr;
@@ -2805,6 +2808,8 @@ struct mpcd_batch {
     int* dOffsRank = nullptr;   // count + 1: blocks of the rank sort
     int histBlocks = 0, rankBlocks = 0;
 };
+
+#include "fast_batch.inc"
 
 __global__ void k_set_steps(long long** steps, int n, long long value) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2994,6 +2999,7 @@ int mpcd_batch_destroy(mpcd_batch* b) {
     if (!b) return MPCD_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    fast_batch_free(b->fast);
     for (auto& g : b->gexec)
         if (g) cudaGraphExecDestroy(g);
     if (b->hArgs) cudaFreeHost(b->hArgs);
@@ -3112,6 +3118,39 @@ int mpcd_batch_create(const mpcd_params_c* params, int count, int device, mpcd_b
     return MPCD_OK;
 }
 
+int mpcd_batch_create_form(const mpcd_params_c* params, int count, int device, int32_t form, mpcd_batch** out) {
+    if (form == MPCD_FORM_F64) return mpcd_batch_create(params, count, device, out);
+    if (form != MPCD_FORM_FAST) return set_err(MPCD_ERR_INVALID_ARG, "batched replicas: the F64 and fast forms");
+    if (!params || !out || count < 1) return set_err(MPCD_ERR_INVALID_ARG, "null argument or empty batch");
+    *out = nullptr;
+    mpcd_batch* b = new mpcd_batch();
+    b->device = device;
+    for (int i = 0; i < count; ++i) {
+        mpcd_ctx* c = nullptr;
+        const int rc = mpcd_ctx_create_form(params + i, device, MPCD_FORM_FAST, &c);
+        if (rc) {
+            const std::string msg = "replica " + std::to_string(i) + ": " + g_err;
+            mpcd_batch_destroy(b);
+            return set_err(rc, msg);
+        }
+        b->members.push_back(c);
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->start) != cudaSuccess || cudaEventCreate(&b->stop) != cudaSuccess) {
+        cudaGetLastError();
+        mpcd_batch_destroy(b);
+        return set_err(MPCD_ERR_CUDA, "batch stream");
+    }
+    const int rc = fast_batch_init(b);
+    if (rc) {
+        const std::string msg = g_err;
+        mpcd_batch_destroy(b);
+        return set_err(rc, msg);
+    }
+    *out = b;
+    return MPCD_OK;
+}
+
 int mpcd_batch_size(mpcd_batch* b) { return b ? (int)b->members.size() : 0; }
 
 mpcd_ctx* mpcd_batch_member(mpcd_batch* b, int i) {
@@ -3122,6 +3161,7 @@ mpcd_ctx* mpcd_batch_member(mpcd_batch* b, int i) {
 int mpcd_batch_step(mpcd_batch* b, int64_t step0, int64_t nsteps, double* device_seconds) {
     if (!b) return set_err(MPCD_ERR_INVALID_ARG, "null batch");
     if (nsteps < 0) return set_err(MPCD_ERR_INVALID_ARG, "nsteps must be >= 0");
+    if (b->fast) return fast_batch_step(b, step0, nsteps, device_seconds);
     for (mpcd_ctx* c : b->members)
         if (!c->pc.useIncompressibleRedistribution || !c->pc.useZoneRedistribution || !c->pc.useLiquidClosure)
             return set_err(MPCD_ERR_INVALID_ARG, "the benchmark step needs useIncompressibleRedistribution, useZoneRedistribution and useLiquidClosure");

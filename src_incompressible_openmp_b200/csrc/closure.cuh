@@ -41,10 +41,11 @@ __global__ void k_pdrive(DevParams P, const double* __restrict__ pkin, const dou
     raw[c] = __dadd_rn(pkin[c], pvir[c]);
 }
 
-__global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, const int* __restrict__ mask, int anyMask,
-                               double* __restrict__ pdrive, const int* skip) {
+__device__ __forceinline__ void pdrive_blend_block(int bx, const DevParams& P, const double* __restrict__ raw,
+                                                   const int* __restrict__ mask, int anyMask, double* __restrict__ pdrive,
+                                                   const int* skip) {
     if (skip && *skip) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = bx * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     double v = raw[c];
     if (anyMask && mask[c] != 0) {
@@ -53,6 +54,11 @@ __global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, cons
         v = __dadd_rn(__dmul_rn(__dsub_rn(1.0, P.smoothBlend), raw[c]), __dmul_rn(P.smoothBlend, ps));
     }
     pdrive[c] = v;
+}
+
+__global__ void k_pdrive_blend(DevParams P, const double* __restrict__ raw, const int* __restrict__ mask, int anyMask,
+                               double* __restrict__ pdrive, const int* skip) {
+    pdrive_blend_block((int)blockIdx.x, P, raw, mask, anyMask, pdrive, skip);
 }
 
 __global__ void k_eos(DevParams P, const double* __restrict__ pd, double* __restrict__ eosX, double* __restrict__ eosY,
@@ -124,12 +130,11 @@ __global__ void k_closure_cells(DevParams P, const uint64_t* __restrict__ start,
 // K interleaved columns over n rows; kind bit k set -> max instead of sum for column k.
 constexpr int kRedThreads = 256;
 constexpr int kRedMaxCols = 16;
-__global__ void __launch_bounds__(kRedThreads) k_reduce_partial(const double* __restrict__ in, int64_t n, int K,
-                                                                unsigned maxMask, int rowsPerBlock,
-                                                                double* __restrict__ partial) {
+__device__ __forceinline__ void reduce_partial_block(int bx, const double* __restrict__ in, int64_t n, int K,
+                                                     unsigned maxMask, int rowsPerBlock, double* __restrict__ partial) {
     __shared__ double sh[kRedMaxCols][kRedThreads];
     const int t = threadIdx.x;
-    const int64_t r0 = (int64_t)blockIdx.x * rowsPerBlock;
+    const int64_t r0 = (int64_t)bx * rowsPerBlock;
     const int64_t r1 = min((int64_t)n, r0 + rowsPerBlock);
     for (int k = 0; k < K; ++k) {
         double a = 0.0;
@@ -146,11 +151,17 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_partial(const double* __
                 sh[k][t] = ((maxMask >> k) & 1u) ? smax(sh[k][t], sh[k][t + o]) : __dadd_rn(sh[k][t], sh[k][t + o]);
         __syncthreads();
     }
-    if (t < K) partial[(size_t)blockIdx.x * K + t] = sh[t][0];
+    if (t < K) partial[(size_t)bx * K + t] = sh[t][0];
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_reduce_final(const double* __restrict__ partial, int nb, int K,
-                                                              unsigned maxMask, double* __restrict__ out) {
+__global__ void __launch_bounds__(kRedThreads) k_reduce_partial(const double* __restrict__ in, int64_t n, int K,
+                                                                unsigned maxMask, int rowsPerBlock,
+                                                                double* __restrict__ partial) {
+    reduce_partial_block((int)blockIdx.x, in, n, K, maxMask, rowsPerBlock, partial);
+}
+
+__device__ __forceinline__ void reduce_final_block(const double* __restrict__ partial, int nb, int K, unsigned maxMask,
+                                                   double* __restrict__ out) {
     __shared__ double sh[kRedMaxCols][kRedThreads];
     const int t = threadIdx.x;
     for (int k = 0; k < K; ++k) {
@@ -169,6 +180,11 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_final(const double* __re
         __syncthreads();
     }
     if (t < K) out[t] = sh[t][0];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_reduce_final(const double* __restrict__ partial, int nb, int K,
+                                                              unsigned maxMask, double* __restrict__ out) {
+    reduce_final_block(partial, nb, K, maxMask, out);
 }
 
 // beta_applied from num/den (src/liquid_closure.cpp:364-377)

@@ -143,8 +143,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64_r(unsigned long long 
 }
 
 // ------------------------------------------------------------------ step begin
-__global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W, int* nSpill) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void fast_step_begin(const FastParams& F, FastStep* S, FastWall* W, int* nSpill) {
     *nSpill = 0;
     const long long s = S->step + 1;
     S->step = s;
@@ -157,6 +156,11 @@ __global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W, int* n
     S->seed = fhash(F.seed, (uint64_t)s, 0x5354ULL);
     for (int k = 0; k < 4; ++k) W->n[k] = 0;
     W->dE2 = 0;
+}
+
+__global__ void k_fast_step_begin(FastParams F, FastStep* S, FastWall* W, int* nSpill) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    fast_step_begin(F, S, W, nSpill);
 }
 
 // ------------------------------------------------------------------ stream + walls + binning
@@ -201,10 +205,11 @@ __device__ __forceinline__ void reflect_high(int& c, float& r, int L) {
 // (src/boundary_conditions.cpp:37-202: up to four sweeps of left, right, bottom, top, then the
 // final wrap or clamp), and files each particle into the bin of its new cell (warp-aggregated
 // slot claims).
-__global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams F, const FastStep* __restrict__ S,
-                                                     FastBins in, FastBins out, const int2* __restrict__ kick,
-                                                     FastWall* __restrict__ W, DevStatus* st) {
-    const int c0 = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5) * kStreamCells;
+__device__ __forceinline__ void fast_stream_block(int bx, const DevParams& P, const FastParams& F,
+                                                  const FastStep* __restrict__ S, const FastBins& in,
+                                                  const FastBins& out, const int2* __restrict__ kick,
+                                                  FastWall* __restrict__ W, DevStatus* st) {
+    const int c0 = (int)((bx * (size_t)blockDim.x + threadIdx.x) >> 5) * kStreamCells;
     const int lane = threadIdx.x & 31;
     if (c0 >= P.Nc) return;
     // lanes below kStreamCells: their cell's count and the exclusive prefix of the counts
@@ -421,6 +426,12 @@ __global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams 
     }
 }
 
+__global__ void __launch_bounds__(256, 4) k_fast_stream(DevParams P, FastParams F, const FastStep* __restrict__ S,
+                                                     FastBins in, FastBins out, const int2* __restrict__ kick,
+                                                     FastWall* __restrict__ W, DevStatus* st) {
+    fast_stream_block((int)blockIdx.x, P, F, S, in, out, kick, W, st);
+}
+
 // ------------------------------------------------------------------ SRD collision
 // The SRD cell along one axis of a particle at standard cell g with offset r: the grid shifted
 // by ss in [-1/2, 1/2) cells (srd_cell_id_with_random_shift, src/srd_collision.cpp:9-45:
@@ -571,14 +582,13 @@ __device__ void block_scan(const int* v, int* out, int n, int* wsum) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kCollThreads) k_fast_collide_tile(CollideArgs A) {
-    extern __shared__ __align__(16) char smem[];
+__device__ __forceinline__ void fast_collide_tile_block(int bx, const CollideArgs& A, char* smem) {
     const DevParams& P = A.P;
     const int K = A.F.K;
     const int tid = threadIdx.x;
     CollideMem M;
     M.carve(smem, A.pcap);
-    const int tile = blockIdx.x;
+    const int tile = bx;
     const int X0 = (tile / A.tilesY) * kCollTX, Y0 = (tile % A.tilesY) * A.TY;
     const int TXc = min(kCollTX, P.Nx - X0), TYc = min(A.TY, P.Ny - Y0);
     const float ssx = (float)A.S->sx, ssy = (float)A.S->sy;
@@ -714,10 +724,15 @@ __global__ void __launch_bounds__(kCollThreads) k_fast_collide_tile(CollideArgs 
     }
 }
 
+__global__ void __launch_bounds__(kCollThreads) k_fast_collide_tile(CollideArgs A) {
+    extern __shared__ __align__(16) char smem[];
+    fast_collide_tile_block((int)blockIdx.x, A, smem);
+}
+
 // The tiles the tile kernel left (more particles than its shared memory holds): one warp per
 // SRD cell, its members found among the particles of the two-by-two standard cells under it
 // and read twice from global memory. The same arithmetic as the tile kernel.
-__global__ void __launch_bounds__(256) k_fast_collide_spill(CollideArgs A) {
+__device__ __forceinline__ void fast_collide_spill_block(int bx, int gx, const CollideArgs& A) {
     const DevParams& P = A.P;
     const int K = A.F.K;
     const int lane = threadIdx.x & 31;
@@ -727,8 +742,8 @@ __global__ void __launch_bounds__(256) k_fast_collide_spill(CollideArgs A) {
     const int ex = ssx < 0.0f ? 1 : 0, ey = ssy < 0.0f ? 1 : 0;
     const int cellsPerTile = kCollTX * A.TY;
     const long long items = (long long)nsp * cellsPerTile;
-    const long long wstep = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long it = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; it < items; it += wstep) {
+    const long long wstep = (long long)gx * (blockDim.x >> 5);
+    for (long long it = (bx * (long long)blockDim.x + threadIdx.x) >> 5; it < items; it += wstep) {
         const int tile = A.spill[it / cellsPerTile];
         const int kk = (int)(it % cellsPerTile);
         const int X0 = (tile / A.tilesY) * kCollTX, Y0 = (tile % A.tilesY) * A.TY;
@@ -828,6 +843,10 @@ __global__ void __launch_bounds__(256) k_fast_collide_spill(CollideArgs A) {
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_fast_collide_spill(CollideArgs A) {
+    fast_collide_spill_block((int)blockIdx.x, (int)gridDim.x, A);
 }
 
 // ------------------------------------------------------------------ zone redistribution
@@ -1462,8 +1481,8 @@ __device__ __forceinline__ long long floor_div_small(long long a, int b) {
 // share per member, the remainder to the member of smallest id. A cell is read four slots at a
 // time (32-byte loads: bins start on 128-byte boundaries, K being a multiple of 16) before it is
 // written; no thread reads another cell's slots (the arrivals come from the exported records).
-__global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
-    const int c = (int)(blockIdx.x * (size_t)blockDim.x + threadIdx.x);
+__device__ __forceinline__ void fast_zone_apply_block(int blk, const FastZoneArgs& A) {
+    const int c = (int)(blk * (size_t)blockDim.x + threadIdx.x);
     if (c >= A.P.Nc) return;
     const int K = A.F.K;
     const FastBins& B = A.b;
@@ -1615,13 +1634,16 @@ __global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_fast_zone_apply(FastZoneArgs A) {
+    fast_zone_apply_block((int)blockIdx.x, A);
+}
+
 // kW zones per block, in step: a block barrier after the set-up, after each dense pass and
 // after the sparse phase, so that the resident warps of an SM execute the same phase's code
 template <int kW>
-__global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) {
-    extern __shared__ __align__(16) char smem[];
+__device__ __forceinline__ void fast_zone_block(int bx, const FastZoneArgs& A, char* smem) {
     const int wib = threadIdx.x >> 5;
-    const int slot = blockIdx.x * kW + wib;
+    const int slot = bx * kW + wib;
     const int z = A.order && slot < A.nZones ? A.order[slot] : slot;
     FastZone Z;
     Z.A = &A;
@@ -1721,14 +1743,20 @@ __global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) 
     }
 }
 
+template <int kW>
+__global__ void __launch_bounds__(32 * kW, 24 / kW) k_fast_zone(FastZoneArgs A) {
+    extern __shared__ __align__(16) char smem[];
+    fast_zone_block<kW>((int)blockIdx.x, A, smem);
+}
+
 // Launch order of the decision kernel. The work of a zone is its particles above the high map
 // plus its cells below the low map (its dense and sparse phases), from the pass-input counts;
 // one warp per zone. A zone's decisions do not depend on when it runs, so the order changes
 // only how evenly the zones of a block (which run their phases together) are loaded.
 constexpr int kFastCostBuckets = 256;
 constexpr int kFastOrderWindow = 1024;  // zones sorted together (one block of k_fast_zone_rank)
-__global__ void k_fast_zone_cost(FastZoneArgs A, int* __restrict__ cost) {
-    const int z = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+__device__ __forceinline__ void fast_zone_cost_block(int bx, const FastZoneArgs& A, int* __restrict__ cost) {
+    const int z = (int)((bx * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (z >= A.nZones) return;
     const DevParams& P = A.P;
@@ -1749,13 +1777,15 @@ __global__ void k_fast_zone_cost(FastZoneArgs A, int* __restrict__ cost) {
     if (lane == 0) cost[z] = min(kFastCostBuckets - 1, w);
 }
 
+__global__ void k_fast_zone_cost(FastZoneArgs A, int* __restrict__ cost) { fast_zone_cost_block((int)blockIdx.x, A, cost); }
+
 // The zones of each window of kFastOrderWindow slots in descending cost: a counting sort in
 // shared memory (places within a bucket come from shared atomics, in no fixed order).
-__global__ void __launch_bounds__(kFastOrderWindow) k_fast_zone_rank(const int* __restrict__ cost, int nZones,
-                                                                     int* __restrict__ order) {
+__device__ __forceinline__ void fast_zone_rank_block(int bx, const int* __restrict__ cost, int nZones,
+                                                     int* __restrict__ order) {
     __shared__ int hist[kFastCostBuckets];
     const int t = threadIdx.x;
-    const int z = blockIdx.x * kFastOrderWindow + t;
+    const int z = bx * kFastOrderWindow + t;
     const bool live = z < nZones;
     if (t < kFastCostBuckets) hist[t] = 0;
     __syncthreads();
@@ -1785,7 +1815,12 @@ __global__ void __launch_bounds__(kFastOrderWindow) k_fast_zone_rank(const int* 
         }
     }
     __syncthreads();
-    if (live) order[blockIdx.x * kFastOrderWindow + hist[b] + r] = z;
+    if (live) order[bx * kFastOrderWindow + hist[b] + r] = z;
+}
+
+__global__ void __launch_bounds__(kFastOrderWindow) k_fast_zone_rank(const int* __restrict__ cost, int nZones,
+                                                                     int* __restrict__ order) {
+    fast_zone_rank_block((int)blockIdx.x, cost, nZones, order);
 }
 
 // ------------------------------------------------------------------ closure
@@ -1793,10 +1828,12 @@ __global__ void __launch_bounds__(kFastOrderWindow) k_fast_zone_rank(const int* 
 // pass read (N, Ux, Uy, T, rho, Pkin, Pvir: src/common_grid.cpp:32-100), and pdriveRaw = Pkin + Pvir
 // (src/liquid_closure.cpp:401-405); the red momenta, duRepair = (P_ref - P_red) / gamma and the
 // beta_opt terms (:343-360) into cols (num term, den term).
-__global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ ref, const longlong2* __restrict__ red,
-                                     const int* __restrict__ redN, double* __restrict__ pdRaw, double* __restrict__ duRX,
-                                     double* __restrict__ duRY, double* __restrict__ cols, float4* __restrict__ feat) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void fast_closure_cells_block(int bx, const DevParams& P, const longlong4* __restrict__ ref,
+                                                         const longlong2* __restrict__ red, const int* __restrict__ redN,
+                                                         double* __restrict__ pdRaw, double* __restrict__ duRX,
+                                                         double* __restrict__ duRY, double* __restrict__ cols,
+                                                         float4* __restrict__ feat) {
+    const int c = bx * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const longlong4 r = ref[c];
     const int n = (int)r.w;
@@ -1836,6 +1873,12 @@ __global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ 
     }
 }
 
+__global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ ref, const longlong2* __restrict__ red,
+                                     const int* __restrict__ redN, double* __restrict__ pdRaw, double* __restrict__ duRX,
+                                     double* __restrict__ duRY, double* __restrict__ cols, float4* __restrict__ feat) {
+    fast_closure_cells_block((int)blockIdx.x, P, ref, red, redN, pdRaw, duRX, duRY, cols, feat);
+}
+
 // EOS kick from the blended pressure drive (src/liquid_closure.cpp:243-295, :424-430) plus
 // beta_applied * duRepair, rounded per cell to the grid (the pending kick of the next step).
 // learned (nullable): per cell (duX, duY) of the learned closure replacing the EOS kick where
@@ -1845,12 +1888,15 @@ __global__ void k_fast_closure_cells(DevParams P, const longlong4* __restrict__ 
 // of a field and moves the mean flow by a negligible amount, while a network's residual bias,
 // though small against the kick, is of the size of the body force per step.
 // eosX, eosY (nullable): the plain EOS kick per cell (training samples).
-__global__ void k_fast_kick_cells(DevParams P, const double* __restrict__ pd, const double* __restrict__ duRX,
-                                  const double* __restrict__ duRY, const double* __restrict__ numDen,
-                                  const double* __restrict__ learnedX, const double* __restrict__ learnedY,
-                                  const long long* __restrict__ learnedSum, const int* __restrict__ mode,
-                                  int2* __restrict__ kick, double* __restrict__ eosX, double* __restrict__ eosY) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void fast_kick_cells_block(int bx, const DevParams& P, const double* __restrict__ pd,
+                                                      const double* __restrict__ duRX, const double* __restrict__ duRY,
+                                                      const double* __restrict__ numDen,
+                                                      const double* __restrict__ learnedX,
+                                                      const double* __restrict__ learnedY,
+                                                      const long long* __restrict__ learnedSum,
+                                                      const int* __restrict__ mode, int2* __restrict__ kick,
+                                                      double* __restrict__ eosX, double* __restrict__ eosY) {
+    const int c = bx * blockDim.x + threadIdx.x;
     if (c >= P.Nc) return;
     const double beta = beta_applied(P, numDen[0], numDen[1]);
     double ex, ey;
@@ -1881,6 +1927,15 @@ __global__ void k_fast_kick_cells(DevParams P, const double* __restrict__ pd, co
     }
     const double dx = beta * duRX[c] + ex, dy = beta * duRY[c] + ey;
     kick[c] = make_int2((int)llrint(dx * kFastQ), (int)llrint(dy * kFastQ));
+}
+
+__global__ void k_fast_kick_cells(DevParams P, const double* __restrict__ pd, const double* __restrict__ duRX,
+                                  const double* __restrict__ duRY, const double* __restrict__ numDen,
+                                  const double* __restrict__ learnedX, const double* __restrict__ learnedY,
+                                  const long long* __restrict__ learnedSum, const int* __restrict__ mode,
+                                  int2* __restrict__ kick, double* __restrict__ eosX, double* __restrict__ eosY) {
+    fast_kick_cells_block((int)blockIdx.x, P, pd, duRX, duRY, numDen, learnedX, learnedY, learnedSum, mode, kick, eosX,
+                          eosY);
 }
 
 // per cell of the bins: count and count^2 (the learned closure's occupancy-variance check)

@@ -81,6 +81,7 @@ def lib():
         "mpcd_ctx_set_graphs": ([C.c_void_p, C.c_int], C.c_int),
         "mpcd_ctx_collide_shape": ([C.c_void_p, C.c_int32, P(C.c_int32)], C.c_int),
         "mpcd_batch_create": ([P(_abi.ParamsC), C.c_int, C.c_int, P(C.c_void_p)], C.c_int),
+        "mpcd_batch_create_form": ([P(_abi.ParamsC), C.c_int, C.c_int, C.c_int32, P(C.c_void_p)], C.c_int),
         "mpcd_batch_destroy": ([C.c_void_p], C.c_int),
         "mpcd_batch_size": ([C.c_void_p], C.c_int),
         "mpcd_batch_member": ([C.c_void_p, C.c_int], C.c_void_p),
@@ -463,13 +464,15 @@ class _Member(Context):
 
 class Batch:
     """Independent replicas advanced together (mpcd_batch_*): each keeps its own parameters,
-    size, state and zone layout; member(i) is the i-th replica's context."""
+    size, state and zone layout; member(i) is the i-th replica's context. form "f64" (the plain
+    form) or "fast" (every phase of a step one launch for all replicas)."""
 
-    def __init__(self, params_list, device=0):
+    def __init__(self, params_list, device=0, form="f64"):
         self.params = [dict(p) for p in params_list]
+        self.form = form
         arr = (_abi.ParamsC * len(self.params))(*[to_c(p) for p in self.params])
         h = C.c_void_p()
-        _check(lib().mpcd_batch_create(arr, len(self.params), device, C.byref(h)))
+        _check(lib().mpcd_batch_create_form(arr, len(self.params), device, FORMS[form], C.byref(h)))
         self.h = h
         self.members = [_Member(p, lib().mpcd_batch_member(self.h, i)) for i, p in enumerate(self.params)]
 
