@@ -429,42 +429,108 @@ def ensemble_params(W):
     return ensemble_family(W["replicas"], W["seed"])
 
 
-def run_ensemble(args):
-    """Aggregate particle-steps/s of the batched ensemble (one GPU; rank 0 only)."""
-    from src_incompressible_openmp_b200 import native
+def _ensemble_batch(native, reps, form, seed_shift=0):
+    """A batch of the ensemble's replicas with their initial states (seed + seed_shift)."""
     from src_incompressible_openmp_b200.cases import uniform_state
+
+    B = native.Batch([p for p, _ in reps], form=form)
+    for i, (p, seed) in enumerate(reps):
+        x, v = uniform_state(p, seed + seed_shift)
+        B.member(i).set_state(x, v)
+    return B
+
+
+def _ensemble_flux(B, reps, step0, rounds, every):
+    """Per replica the flux Qx = meanUx * Ly (src/main_benchmark_poiseuille_openmp_profiled_
+    shifted_profiled.cpp:124-126: meanUx the mean over cells of the cell mean vx), averaged over
+    `rounds` states taken every `every` steps after step0."""
+    import numpy as np
+
+    q = np.zeros(len(reps))
+    for k in range(rounds):
+        B.step(step0 + k * every, every)
+        for i, (p, _) in enumerate(reps):
+            x, v = B.member(i).get_state()
+            ax, ay = p["Lx"] / p["Nx"], p["Ly"] / p["Ny"]
+            ix = np.clip(np.floor(x[0::2] / ax).astype(np.int64), 0, p["Nx"] - 1)
+            iy = np.clip(np.floor(x[1::2] / ay).astype(np.int64), 0, p["Ny"] - 1)
+            c = iy + p["Ny"] * ix
+            n = np.bincount(c, minlength=p["Nc"])
+            sx = np.bincount(c, weights=v[0::2], minlength=p["Nc"])
+            ux = np.where(n > 0, sx / np.maximum(n, 1), 0.0)
+            q[i] += ux.mean() * p["Ly"] / rounds
+    return q
+
+
+def run_ensemble(args):
+    """Aggregate particle-steps/s of the batched ensemble (one GPU; rank 0 only): the FP64 plain
+    batch as the line's value, the fast-form batch beside it, and each replica's flux error of
+    the fast form against FP64."""
+    import numpy as np
+    from src_incompressible_openmp_b200 import native
 
     if env_int("RANK", 0) != 0:
         return
     reps = ensemble_params(WORKLOAD)
-    B = native.Batch([p for p, _ in reps])
-    for i, (p, seed) in enumerate(reps):
-        x, v = uniform_state(p, seed)
-        B.member(i).set_state(x, v)
     W, K = args.warmup, args.steps
-    B.step(0, W)
-    sampler = ClockSampler(0)
-    sampler.start()
-    time.sleep(0.3)
-    l0 = sum(B.member(i).launch_count() for i in range(len(reps)))
-    t_wall0 = time.time()
-    t_dev = B.step(W, K)
-    t_wall1 = time.time()
-    l1 = sum(B.member(i).launch_count() for i in range(len(reps)))
-    clocks = sampler.stop(t_wall0, t_wall1)
     n_tot = sum(p["n"] for p, _ in reps)
     nc_tot = sum(p["Nc"] for p, _ in reps)
+    rounds, every = 5, 10
+    arms = {}
+    for form in ("f64", "fast"):
+        B = _ensemble_batch(native, reps, form)
+        B.step(0, W)
+        sampler = ClockSampler(0)
+        sampler.start()
+        time.sleep(0.3)
+        l0 = sum(B.member(i).launch_count() for i in range(len(reps)))
+        t_wall0 = time.time()
+        t_dev = B.step(W, K)
+        t_wall1 = time.time()
+        l1 = sum(B.member(i).launch_count() for i in range(len(reps)))
+        clocks = sampler.stop(t_wall0, t_wall1)
+        flux = _ensemble_flux(B, reps, W + K, rounds, every)
+        B.close()
+        arms[form] = dict(t=t_dev, launches=int(l1 - l0), clocks=clocks, flux=flux)
+    # the noise floor: the FP64 batch from other initial states, against the first
+    B = _ensemble_batch(native, reps, "f64", seed_shift=5000)
+    B.step(0, W + K)
+    flux_other = _ensemble_flux(B, reps, W + K, rounds, every)
     B.close()
+    q64, qf = arms["f64"]["flux"], arms["fast"]["flux"]
+    scale = np.maximum(np.abs(q64), 1e-12)
+    err = np.abs(qf - q64) / scale
+    floor = np.abs(flux_other - q64) / scale
+    g = np.array([p["bodyForceX"] for p, _ in reps])
+    strong = g >= np.median(g)
+    t64, tf = arms["f64"]["t"], arms["fast"]["t"]
     line = {
-        "metric": METRIC, "value": n_tot * K / t_dev, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "value": n_tot * K / t64, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * t64 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic: per replica seeded uniform positions, Maxwellian velocities",
         "config": {"workload": WORKLOAD["name"], "replicas": len(reps), "n_particles": n_tot, "n_cells": nc_tot,
                    "form": "plain_f64, one context and stream per replica, steps replayed from CUDA graphs",
                    "parallelism": "single GPU"},
         "step_hbm": {"algorithmic_bytes_per_step": 256 * n_tot + 128 * nc_tot,
-                     "achieved_GBps": (256 * n_tot + 128 * nc_tot) * K / t_dev / 1e9},
-        "e2e": None, "gpu_launches": int(l1 - l0), "clocks": clocks,
+                     "achieved_GBps": (256 * n_tot + 128 * nc_tot) * K / t64 / 1e9},
+        "e2e": None, "gpu_launches": arms["f64"]["launches"], "clocks": arms["f64"]["clocks"],
+        "fast_batch": {
+            "form": "fast form (FP32 state, int64 cell sums), every phase one launch for all replicas",
+            "value": n_tot * K / tf, "unit": UNIT, "ms_per_step": 1e3 * tf / K, "ratio_vs_f64_batch": t64 / tf,
+            "gpu_launches": arms["fast"]["launches"], "launches_per_step": arms["fast"]["launches"] / K,
+            "clocks": arms["fast"]["clocks"],
+            "flux_error": {
+                "definition": "per replica |Qx_fast - Qx_f64| / |Qx_f64|, Qx = meanUx * Ly averaged over "
+                              f"{rounds} states every {every} steps after step {W + K}, both forms from the same "
+                              "initial state; noise floor: the FP64 batch from other initial states",
+                "median": float(np.median(err)), "p90": float(np.percentile(err, 90)),
+                "median_noise_floor": float(np.median(floor)), "p90_noise_floor": float(np.percentile(floor, 90)),
+                "median_upper_half_forcing": float(np.median(err[strong])),
+                "median_noise_floor_upper_half_forcing": float(np.median(floor[strong])),
+                "aggregate_signed": float(np.sum(qf - q64) / np.sum(np.abs(q64))),
+                "aggregate_signed_noise_floor": float(np.sum(flux_other - q64) / np.sum(np.abs(q64))),
+            },
+        },
     }
     print(json.dumps(line))
 
