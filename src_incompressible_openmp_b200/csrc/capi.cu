@@ -179,6 +179,7 @@ struct mpcd_ctx {
     int* fspill = nullptr;   // collision tiles left to the spill kernel, and their count
     int* fnSpill = nullptr;
     int fcTY = 16, fcTilesY = 0, fcTiles = 0, fcPcap = 0;  // collision tiles: rows, tile rows, tiles, capacity
+    bool fcTuned = false;  // the collision's tile rows chosen by timing (fast_tune_collide)
     size_t fcSmem = 0;
     FastStep* fstep = nullptr;
     FastWall* fwall = nullptr;

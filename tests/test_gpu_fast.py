@@ -105,6 +105,24 @@ def test_collision_spill_path_matches_tiles():
     assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
 
 
+def test_collision_autotuner_leaves_state_unchanged(monkeypatch):
+    """The collision's autotuner times every tile height on the live state (first step) and
+    restores it: the run equals one without tuning, bit for bit."""
+    native = _native()
+    p = poiseuille_params(64, 40, 20)
+    x, v = uniform_state(p, 9)
+    out = []
+    for tune in ("1", "0"):
+        monkeypatch.setenv("MPCD_FAST_COLLIDE_TUNE", tune)
+        with native.Context(p, form="fast") as ctx:
+            ctx.set_state(x, v)
+            ctx.step(0, 4)
+            out.append(ctx.get_state())
+    (x1, v1), (x2, v2) = out
+    assert not np.isnan(v1).any()
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+
+
 def _profile(native, p, seed, form, steps, avg_from):
     x, v = uniform_state(p, seed)
     with native.Context(p, form=form) as ctx:
