@@ -78,6 +78,16 @@ def test_fast_batch_equals_replicas_alone():
     _compare(_batched(native, cases), _alone(native, cases))
 
 
+def test_fast_batch_graph_replay_equals_eager(monkeypatch):
+    # batched steps replayed from CUDA graphs (the default) against the same steps launched
+    # one kernel at a time
+    native = _native()
+    cases = [_case(*r) for r in REPLICAS]
+    replayed = _batched(native, cases)
+    monkeypatch.setenv("MPCD_FAST_BATCH_GRAPHS", "0")
+    _compare(_batched(native, cases), replayed)
+
+
 def test_fast_batch_spill_path(monkeypatch):
     # a small staging capacity sends fuller collision tiles to the spill kernel, in the batch
     # as in the replicas alone
