@@ -192,6 +192,7 @@ struct mpcd_ctx {
     int fnz[2] = {0, 0};
     int zSyncWarps = 0;  // zones per block of the phase-synchronous zone pass (0: one per block)
     int fzMaxCells = 0, fzWinCap = 0, fzNsmCap = 0, fzRecCap = 0, fzWarps = 8;
+    bool fzTuned = false;  // zones per block of the decision kernel chosen by timing (fast_tune_zone)
     size_t fzSmem = 0;
     // zone decisions handed to the apply kernel: per cell summary and removal masks, per zone records
     unsigned long long* fzMeta = nullptr;

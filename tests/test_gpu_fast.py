@@ -105,22 +105,30 @@ def test_collision_spill_path_matches_tiles():
     assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
 
 
-def test_collision_autotuner_leaves_state_unchanged(monkeypatch):
-    """The collision's autotuner times every tile height on the live state (first step) and
-    restores it: the run equals one without tuning, bit for bit."""
+def test_autotuners_leave_state_unchanged(monkeypatch):
+    """The collision's autotuner times every tile height on the live state and restores it, and
+    the zone autotuner runs the first base pass's decisions with 8 and 4 zones per block (both
+    at the first step): the run, and the first step's move counters, equal a run without
+    tuning, bit for bit."""
     native = _native()
     p = poiseuille_params(64, 40, 20)
     x, v = uniform_state(p, 9)
     out = []
-    for tune in ("1", "0"):
-        monkeypatch.setenv("MPCD_FAST_COLLIDE_TUNE", tune)
+    for tune in (True, False):
+        monkeypatch.setenv("MPCD_FAST_COLLIDE_TUNE", "1" if tune else "0")
+        if tune:
+            monkeypatch.delenv("MPCD_FAST_ZONE_WARPS", raising=False)
+        else:
+            monkeypatch.setenv("MPCD_FAST_ZONE_WARPS", "8")
         with native.Context(p, form="fast") as ctx:
             ctx.set_state(x, v)
-            ctx.step(0, 4)
-            out.append(ctx.get_state())
-    (x1, v1), (x2, v2) = out
+            m1 = ctx.step(0, 1, metrics=True)
+            ctx.step(1, 3)
+            out.append((ctx.get_state(), m1))
+    ((x1, v1), m1), ((x2, v2), m2) = out
     assert not np.isnan(v1).any()
     assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+    assert m1["base"] == m2["base"] and m1["shifted"] == m2["shifted"]
 
 
 def _profile(native, p, seed, form, steps, avg_from):
