@@ -166,7 +166,7 @@ enum mpcd_state_form { MPCD_FORM_F64 = 0, MPCD_FORM_F32 = 1, MPCD_FORM_FAST = 2 
  * the plain form (stream, walls, shifted-grid SRD rotation with thermostat, base and shifted
  * zone passes, liquid closure), but every random draw comes from a hash of (step, what the
  * draw is for), so zones, cells and particles proceed independently; results are therefore
- * not the reference's trajectories but the same physics, judged statistically against the
+ * not the reference's trajectories but the same physics, compared statistically with the
  * plain form. State: per cell a bin of FP32 offsets inside the cell, FP32 velocities on the
  * 2^-20 grid and particle ids; cell sums are exact int64 sums, so the collision keeps every
  * SRD cell's momentum and each redistribution keeps the momentum of every cell it corrects,
